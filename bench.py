@@ -1,0 +1,328 @@
+"""Benchmark: SOCS-24 aerial images/s at 1024x1024 (configuration 3), one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+A step is one batch of 64 binary Manhattan clips (1024x1024, 2 nm/pixel) imaged with the 24 SOCS kernels of
+the vector TCC of an annular 0.7/0.95 source (PntNum 41).  Kernels are built once per optics key (TCC + FP64
+eigendecomposition, reported as `setup_s`) and stay resident, as they do in serving.
+
+  value  images/s with the masks already in HBM (256 MB of float32 masks per step: larger than L2)
+  e2e    images/s through the public batched API from pinned host uint8 masks to host float32 images,
+         host<->device copies inside the timed region
+The path shards by clip with no exchange, so N GPUs run N independent replicas ("scaling": "weak").
+--impl reference times the reference's SOCS algorithm (full-grid FFTs, complex64) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "aerial images/s + p99 ms (1024², SOCS-24), served vs plain, err≤1e-4 vs FP64"
+UNIT = "images/s"
+BATCH, N_PIX, PERIOD, ORDER = 64, 1024, 2048.0, 24
+WORKLOAD = ("config 3: SOCS-24 from the vector TCC of an annular 0.7/0.95 source (PntNum 41, 2048 nm period, "
+            "immersion-mapped optics), batches of 64 binary Manhattan clips 1024x1024 at 2 nm/pixel (~35% fill)")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as fh:
+            p = json.load(fh)
+        return float(p['hbm_gbs']), float(p['bf16_tflops']), 'measured'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, 'fallback'
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples (200 ms) while the timed region runs."""
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index, self.proc, self.lines = index, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.FIELDS}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == 'active':
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device('cuda', local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        torch.distributed.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def build_kernels():
+    from opticalimaging_b200 import imaging, workloads as W
+    sr, po, nm = W.config3_optics(order=ORDER)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    T, fg = imaging.CalculateTCCMatrix(sr, [PERIOD, PERIOD], po, 0.0, nm)
+    sk = imaging.socs_kernels_from_tcc(T, fg, [N_PIX, N_PIX], nm)
+    torch.cuda.synchronize()
+    return sk, time.perf_counter() - t0, (sr, po, nm, T, fg)
+
+
+def stage_times(sk, masks, reps=3):
+    """Average device time of each native stage over `reps` batches (CUDA events on the launching stream)."""
+    acc = {}
+    for _ in range(reps):
+        marks = []
+        sk.image(masks, marks=marks)
+        torch.cuda.synchronize()
+        for (_, a), (name, b) in zip(marks[:-1], marks[1:]):
+            acc[name] = acc.get(name, 0.0) + a.elapsed_time(b) / reps
+    return acc
+
+
+def cpu_reference_sample(sk_info, masks_np, budget_s, threads):
+    """Time the reference's algorithm (oracle/cpu_reference.py) on host cores for a bounded sample of clips."""
+    from oracle import cpu_reference as R
+    from opticalimaging_b200 import imaging
+    sr, po, nm, T, fg = sk_info
+    kern = imaging.DecomposeTCC_SOCS(T, fg, [N_PIX, N_PIX], nm).cpu().numpy()
+    npx = PERIOD / (sr.Wavelength / po.NA)
+    times, n = [], 0
+    t_start = time.perf_counter()
+    while n < len(masks_np) and (time.perf_counter() - t_start) < budget_s:
+        field = np.zeros((N_PIX, N_PIX, 3), np.complex64)
+        field[:, :, 0] = masks_np[n]
+        t0 = time.perf_counter()
+        R.socs_clip(field, kern, npx, npx, threads)
+        times.append(time.perf_counter() - t0)
+        n += 1
+    med = statistics.median(times[1:] if len(times) > 2 else times)
+    return 1.0 / med, n
+
+
+def accuracy_vs_fp64(sk, masks_np, sk_info, engine_images):
+    """Max and RMS error of the engine image vs the FP64 oracle SOCS image with the same K (one clip)."""
+    from oracle import optics64 as O
+    from opticalimaging_b200 import imaging, workloads as W
+    from opticalimaging_b200.params import Scatter
+    sr, po, nm, T, fg = sk_info
+    kern = imaging.DecomposeTCC_SOCS(T, fg, [N_PIX, N_PIX], nm).cpu().numpy().astype(np.complex128)
+    sc = Scatter()
+    sc.Period_X = sc.Period_Y = PERIOD
+    sc.ScatterField = W.thin_field(masks_np[0])
+    ref = O.socs(sc, kern, sr, po)
+    d = engine_images[0].astype(np.float64) - ref
+    peak = float(np.max(np.abs(ref)))
+    return {"max": float(np.max(np.abs(d)) / peak), "rms": float(np.sqrt(np.mean(d ** 2)) / peak),
+            "relative_to": "peak of the FP64 SOCS-24 image (same kernels)"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from opticalimaging_b200 import workloads as W
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    masks = W.config3_masks(count=args.steps + args.warmup, n=N_PIX, seed=3)
+    from oracle import cpu_reference as R
+    sr, po, nm = W.config3_optics(order=ORDER)
+    t0 = time.perf_counter()
+    kern = R.socs_kernels(sr, po, nm, [PERIOD, PERIOD], [N_PIX, N_PIX])
+    setup_s = time.perf_counter() - t0
+    npx = PERIOD / (sr.Wavelength / po.NA)
+    fields = []
+    for m in masks:
+        f = np.zeros((N_PIX, N_PIX, 3), np.complex64)
+        f[:, :, 0] = m
+        fields.append(f)
+    for i in range(args.warmup):
+        R.socs_clip(fields[i], kern, npx, npx, threads)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        R.socs_clip(fields[args.warmup + i], kern, npx, npx, threads)
+    dt = time.perf_counter() - t0
+    v = args.steps / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "step": "one clip per step on the host cores"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} clips of 1024x1024, 72 full-grid complex64 FFTs each "
+                                       "(torch CPU FFT, all host threads)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "setup_s": setup_s}
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args, world, rank, local):
+    from opticalimaging_b200 import workloads as W
+    dev = torch.device('cuda', local)
+    sk, setup_s, info = build_kernels()
+    masks_np = W.config3_masks(count=BATCH, n=N_PIX, seed=3 + 1000 * rank)
+    masks = torch.from_numpy(masks_np).to(dev)
+    out = torch.empty((BATCH, N_PIX, N_PIX), dtype=torch.float32, device=dev)
+    for _ in range(max(args.warmup, 3)):
+        sk.image(masks, out=out)
+    torch.cuda.synchronize()
+    # ---- device-resident throughput
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            sk.image(masks, out=out)
+        end.record()
+        torch.cuda.synchronize()
+        barrier(world)
+    ms = max_over_ranks(start.elapsed_time(end), world)
+    value = world * BATCH * args.steps / (ms / 1000.0)
+    # ---- end to end through the public API: pinned uint8 masks in, float32 images out
+    host_in = torch.from_numpy(masks_np.astype(np.uint8)).pin_memory()
+    host_out = torch.empty((BATCH, N_PIX, N_PIX), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        d_in = host_in.to(dev, non_blocking=True)
+        img = sk.image(d_in, out=out)
+        host_out.copy_(img, non_blocking=True)
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e2.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_e2e = max_over_ranks(s2.elapsed_time(e2), world)
+    e2e_value = world * BATCH * args.steps / (ms_e2e / 1000.0)
+    # ---- per-stage device times (outside the timed region) and the roofline of the dominant stage
+    st = stage_times(sk, masks)
+    hbm, bf16, src = peaks()
+    dominant = max(st, key=st.get)
+    px = BATCH * N_PIX * N_PIX
+    alg_bytes = {'band_spectrum': 4 * px, 'coarse_to_image': 4 * px}
+    if dominant in alg_bytes:
+        ach = alg_bytes[dominant] / (st[dominant] / 1e3) / 1e9
+        roof = {"kernel": dominant, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "traffic": None, "peak_source": src}
+    else:
+        b = sk.band
+        flops = 8.0 * BATCH * sk.count * (sk.plan.mr * b.br * b.bc + sk.plan.mr * b.bc * sk.plan.mc)
+        ach = flops / (st[dominant] / 1e3) / 1e12
+        roof = {"kernel": dominant, "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
+                "frac": ach / bf16, "traffic": None, "peak_source": src}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "batch_per_gpu": BATCH, "kernels": sk.count, "band": [sk.band.br,
+                       sk.band.bc], "coarse": [sk.plan.mr, sk.plan.mc], "l2": "inputs larger than L2 "
+                       "(256 MB float32 masks + 256 MB images per step)", "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_in.numel()),
+                    "d2h_bytes_per_step": int(host_out.numel() * 4)},
+            "gpu_launches": 5 * args.steps, "setup_s": setup_s,
+            "stage_ms": {k: round(v, 4) for k, v in st.items()}, "roofline": roof, "clocks": clk.summary()}
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        torch.set_num_threads(threads)
+        imgs = out[:1].cpu().numpy()
+        line["accuracy_vs_fp64"] = accuracy_vs_fp64(sk, masks_np, info, imgs)
+        v, n = cpu_reference_sample(info, masks_np, args.cpu_budget, threads)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{n} clips of 1024x1024 through the reference's SOCS algorithm "
+                                          "(72 full-grid complex64 FFTs per clip, torch CPU FFT)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='engine', choices=['engine', 'reference'])
+    ap.add_argument('--cpu-budget', type=float, default=15.0)
+    ap.add_argument('--no-cpu', action='store_true')
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == 'reference':
+            run_reference(args, world, rank)
+        else:
+            run_engine(args, world, rank, local)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

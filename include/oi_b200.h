@@ -1,0 +1,134 @@
+/*
+ * oi_b200.h -- C ABI of the B200 aerial-image engine (liboi_b200.so).
+ *
+ * The reference exposes its imaging path as Python functions over torch tensors; it has no native ABI.
+ * Each entry point below replaces the numerical core of one of those functions, so a binding (ctypes,
+ * cffi, pybind) can call it with plain device pointers:
+ *
+ *   oi_band_spectrum      <- Scatter.CalculateSpectrum                    (Scatter.py:10-35)
+ *   oi_abbe_pupils        <- the per-source-point pupil of CalculateAbbeImage (CalculateAerialImage.py:46-75)
+ *   oi_coherent_coarse    <- the |fft2(.)|^2 accumulation of CalculateAbbeImage (CalculateAerialImage.py:76-92)
+ *                            and of CalculateAerialImage_SOCS               (CalculateAerialImage_SOCS.py:5-10)
+ *   oi_coarse_to_image    <- the final fftshift + normalisation of both     (CalculateAerialImage.py:89-92,
+ *                                                                             CalculateAerialImage_SOCS.py:10)
+ *   oi_tcc_pupils64       <- the shifted-pupil matrix of CalculateTCCMatrix  (CalculateTCCMatrix.py:17-51)
+ *   oi_tcc_assemble64     <- GetTCCMatrix                                    (CalculateTCCMatrix.py:58-75)
+ *   oi_twiddle            <- (no counterpart: fills the phase tables the transforms read)
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative OI_E* status; oi_last_error() describes the last
+ *     failure on the calling thread.  Nothing aborts the process.
+ *   - All pointers are device pointers owned by the caller; nothing here allocates device memory.
+ *   - `stream` is a cudaStream_t passed as void*; all work is enqueued on it and nothing synchronises.
+ *   - float2 / double2 are interleaved (re, im) pairs, the layout of torch complex64 / complex128.
+ *   - Frequencies are centred integers: band row i means frequency m0r + i (cycles per period).
+ *   - Image convention: out[y][x] = sum_fields w * |sum_m P(m) c(m) exp(-2 pi i (m_r y/Ny + m_c x/Nx))|^2
+ *     with c(m) = 1/(Ny Nx) sum_{y,x} h[y][x] exp(+2 pi i (m_r y/Ny + m_c x/Nx)).  This equals the
+ *     reference's fftshift(sum |fft2(...)|^2) * dfdg^2 output index for index, for even and odd sizes.
+ */
+#ifndef OI_B200_H
+#define OI_B200_H
+
+#if defined(__GNUC__)
+#define OI_API __attribute__((visibility("default")))
+#else
+#define OI_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  OI_OK = 0,
+  OI_EINVAL = -1,      /* invalid argument (sizes, null pointers, unsupported kind) */
+  OI_ECUDA = -2,       /* a CUDA launch or runtime call failed */
+  OI_ERANGE = -3,      /* a size is above a compiled limit */
+};
+
+/* Field kinds for oi_band_spectrum. */
+enum {
+  OI_FIELD_REAL_F32 = 0,     /* float  [batch][ny][nx]            (thin real transmission)          */
+  OI_FIELD_COMPLEX_C64 = 1,  /* float2 [batch][ny][nx][nch]       (the reference's ScatterField)    */
+  OI_FIELD_U8 = 2,           /* uint8  [batch][ny][nx], raw value (fold any grey scaling into `scale`) */
+};
+
+OI_API const char* oi_last_error(void);
+OI_API int oi_version(void);
+
+/*
+ * Phase table  out[a][b] = scale * exp(sign * 2 pi i * ((a + a0) * (b + b0) mod n) / n)
+ * for a < rows, b < cols.  The phase index is reduced exactly in 64-bit integers, the value computed in
+ * double precision and stored as float2.
+ */
+OI_API int oi_twiddle(void* out, int rows, int cols, long long a0, long long b0, long long n, int sign, double scale,
+               void* stream);
+
+/*
+ * Band-limited forward spectrum (Scatter.py:10-35 restricted to a band):
+ *   band[b][c][ir][ic] = scale * sum_{y,x} h[b][y][x][c] * wy[y][ir] * wx[x][ic]
+ * with wx[x][ic] = exp(+2 pi i (m0c+ic) x / nx) and wy[y][ir] = exp(+2 pi i (m0r+ir) y / ny) (oi_twiddle).
+ * scratch: float2 [batch * nch * ny * bc].
+ */
+OI_API int oi_band_spectrum(const void* field, int kind, int batch, int ny, int nx, int nch, int br, int bc,
+                     const void* wx, const void* wy, float scale, void* scratch, void* band, void* stream);
+
+/*
+ * Abbe pupils (CalculateAerialImage.py:46-75), one per (plane z, source point j, field component e):
+ *   pupil[z][j*ne+e][ir][ic] = valid * obliquity * exp(2 pi i W) * defocus_z * transfer_e     (complex64)
+ *   weight[z][j*ne+e]        = index_image * v[j] / weight_sum
+ * fr[ir] / fc[ic]: the reference's float32 row (Y, g) and column (X, f) frequency values of the band.
+ * sx/sy/sv: float32 source points; focus: double [nz] (all device pointers).
+ * zern (37 Fringe coefficients, may be NULL) and jones (Px.re, Px.im, Py.re, Py.im) are HOST pointers.
+ * Membership `valid` repeats the reference's float32 test (CalculateAerialImage.py:43-57) bit for bit.
+ */
+OI_API int oi_abbe_pupils(const float* fr, const float* fc, int br, int bc, const float* sx, const float* sy,
+                   const float* sv, int nsrc, double weight_sum, const double* focus, int nz, const double* zern,
+                   int vector,
+                   const double* jones, double na, double mag, double index_image, double wavelength,
+                   void* pupil, float* weight, void* stream);
+
+/*
+ * Coherent sum on the coarse grid (the |.|^2 accumulation of both imaging paths):
+ *   coarse[b][z][sr][sc] = sum_{k<nk, c<nch} w[z][k] |sum_{ir,ic} fr[sr][ir] (P[z][k] .* band[b][c])[ir][ic] fcs[ic][sc]|^2
+ * fr  = oi_twiddle(mr x br, sign -1) row phases, fcs = oi_twiddle(bc x mc, sign -1) column phases.
+ * mc must be a multiple of 64 and at most 256; br, bc at most 256.
+ * `pupil_batch_stride` = 0 shares the pupils across the batch (SOCS kernels), else it is the element stride
+ * between images' pupil sets.
+ */
+OI_API int oi_coherent_coarse(const void* band, int batch, int nch, int br, int bc, const void* pupil,
+                       long long pupil_batch_stride, const float* weight, int nz, int nk, int mr, int mc,
+                       const void* frow, const void* fcol, float* coarse, void* stream);
+
+/*
+ * Exact band-limited resampling of the coarse intensity to the output grid:
+ *   out[i][y][x] = sum_{|qr|<br, |qc|<bc} Ihat_i(q) exp(-2 pi i (qr y/ny + qc x/nx)),
+ *   Ihat_i(q)    = 1/(mr mc) sum_s coarse[i][s] exp(+2 pi i (qr sr/mr + qc sc/mc)).
+ * Tables (oi_twiddle): gc [mc][bc] (+, b0=0), gr [mr][2br-1] (+, b0=-(br-1)), sy [ny][2br-1] (-, b0=-(br-1)),
+ * sx [bc][nx] (-, a0=0).  scratch: float2 [count * (2br-1) * bc].
+ */
+OI_API int oi_coarse_to_image(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc,
+                       const void* gr, const void* sy, const void* sx, int ny, int nx, void* scratch,
+                       float* out, void* stream);
+
+/*
+ * Shifted pupil matrix of the TCC (CalculateTCCMatrix.py:17-51), FP64, scaled for a Gram product:
+ *   h[e][p][j] = sqrt(index_image * v[j] / weight_sum) * valid * obliquity * exp(2 pi i W) * defocus * transfer_e
+ * p = i_f * lg + i_g over the TCC grid (ff = f32 row frequencies, gg = f32 column frequencies); ne = 1 or 3.
+ * Membership repeats the reference's float32 test sqrt(f^2+g^2) <= 1 (CalculateTCCMatrix.py:27-29).
+ * zern and jones are HOST pointers, as for oi_abbe_pupils.
+ */
+OI_API int oi_tcc_pupils64(const float* ff, int lf, const float* gg, int lg, const float* sx, const float* sy,
+                    const float* sv, int nsrc, double weight_sum, double focus, const double* zern, int vector,
+                    const double* jones, double na, double mag, double index_image, double wavelength,
+                    void* h, void* stream);
+
+/*
+ * TCC = sum_e h_e h_e^H (GetTCCMatrix, CalculateTCCMatrix.py:58-75), complex128 [fg][fg], full Hermitian.
+ */
+OI_API int oi_tcc_assemble64(const void* h, int ne, int fg, int nsrc, void* tcc, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OI_B200_H */

@@ -1,0 +1,154 @@
+// Exact band-limited resampling of the coarse intensity to the output grid: the last step of both imaging
+// paths (the fftshift + normalisation of CalculateAerialImage.py:89-92 and CalculateAerialImage_SOCS.py:10).
+//
+// The intensity of fields band-limited to Br x Bc has a spectrum supported on |qr| < Br, |qc| < Bc.  Its
+// samples on the coarse Mr x Mc grid (Mr >= 2Br-1, Mc >= 2Bc-1) determine that spectrum exactly:
+//   Ihat(q) = 1/(Mr Mc) sum_s coarse[s] exp(+2 pi i (qr sr/Mr + qc sc/Mc))             (spec kernel)
+// and the output is its trigonometric polynomial evaluated on the Ny x Nx grid.  The intensity is real, so
+// only qc >= 0 is kept (qc > 0 doubled) and the x synthesis is a real dot product:
+//   V[y][qc]   = sum_qr Ihat(qr, qc) exp(-2 pi i qr y/Ny)
+//   out[y][x]  = sum_qc Re(V[y][qc] exp(-2 pi i qc x/Nx))                                 (synth kernel)
+#include "oi_common.cuh"
+
+namespace oi {
+
+constexpr int SP_QT = 16;  // qc per spec block
+
+// grid (ceil(bc/16), count).  ihat[i][jr][qc], jr = qr + br - 1.
+__global__ void __launch_bounds__(256) coarse_spec_kernel(const float* __restrict__ coarse, int mr, int mc, int br,
+                                                          int bc, const float2* __restrict__ gc,
+                                                          const float2* __restrict__ gr, float2* __restrict__ ihat) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* us = (float2*)smem_raw;  // [mr][SP_QT]
+  const int tid = threadIdx.x, ql = tid % SP_QT, rg = tid / SP_QT;  // rg 0..15
+  const int qc0 = blockIdx.x * SP_QT;
+  const long long img = blockIdx.y;
+  const float* cimg = coarse + img * (long long)mr * mc;
+  const int qc = qc0 + ql;
+  const int nq = 2 * br - 1;
+  // U[sr][qc] = sum_sc coarse[sr][sc] gc[sc][qc]
+  for (int sr = rg; sr < mr; sr += 16) {
+    float2 u = make_float2(0.f, 0.f);
+    if (qc < bc) {
+      const float* row = cimg + (long long)sr * mc;
+      for (int sc = 0; sc < mc; ++sc) {
+        float v = __ldg(row + sc);
+        float2 t = __ldg(gc + (long long)sc * bc + qc);
+        u.x = fmaf(v, t.x, u.x);
+        u.y = fmaf(v, t.y, u.y);
+      }
+    }
+    us[sr * SP_QT + ql] = u;
+  }
+  __syncthreads();
+  const float norm = (qc == 0 ? 1.0f : 2.0f) / ((float)mr * (float)mc);
+  for (int jr = rg; jr < nq; jr += 16) {
+    if (qc >= bc) continue;
+    float2 acc = make_float2(0.f, 0.f);
+    for (int sr = 0; sr < mr; ++sr) cfma(acc, __ldg(gr + (long long)sr * nq + jr), us[sr * SP_QT + ql]);
+    ihat[(img * nq + jr) * (long long)bc + qc] = make_float2(acc.x * norm, acc.y * norm);
+  }
+}
+
+constexpr int SY_TY = 8;  // output rows per synth block
+
+// grid (ceil(ny/8), count).
+template <int NV>
+__global__ void __launch_bounds__(256) synth_kernel(const float2* __restrict__ ihat, int br, int bc,
+                                                    const float2* __restrict__ sy, const float2* __restrict__ sx,
+                                                    int ny, int nx, float* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* vs = (float2*)smem_raw;  // [SY_TY][bc]
+  const int tid = threadIdx.x;
+  const int y0 = blockIdx.x * SY_TY;
+  const long long img = blockIdx.y;
+  const int nq = 2 * br - 1;
+  const float2* ih = ihat + img * (long long)nq * bc;
+  // V[r][qc] = sum_jr sy[y0+r][jr] ihat[jr][qc]
+  for (int e = tid; e < SY_TY * bc; e += 256) {
+    int r = e / bc, qc = e - r * bc, y = y0 + r;
+    float2 acc = make_float2(0.f, 0.f);
+    if (y < ny) {
+      const float2* srow = sy + (long long)y * nq;
+      for (int jr = 0; jr < nq; ++jr) cfma(acc, __ldg(srow + jr), __ldg(ih + (long long)jr * bc + qc));
+    }
+    vs[e] = acc;
+  }
+  __syncthreads();
+  // out[y][x] = sum_qc (V.re * sx.re - V.im * sx.im)
+  float acc[SY_TY][NV];
+#pragma unroll
+  for (int r = 0; r < SY_TY; ++r)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[r][v] = 0.f;
+  for (int qc = 0; qc < bc; ++qc) {
+    float2 t[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      int x = tid + 256 * v;
+      t[v] = x < nx ? __ldg(sx + (long long)qc * nx + x) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int r = 0; r < SY_TY; ++r) {
+      float2 vv = vs[r * bc + qc];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) acc[r][v] = fmaf(vv.x, t[v].x, fmaf(-vv.y, t[v].y, acc[r][v]));
+    }
+  }
+  float* o = out + img * (long long)ny * nx;
+#pragma unroll
+  for (int r = 0; r < SY_TY; ++r) {
+    int y = y0 + r;
+    if (y >= ny) continue;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      int x = tid + 256 * v;
+      if (x < nx) o[(long long)y * nx + x] = acc[r][v];
+    }
+  }
+}
+
+template <int NV>
+static void launch_synth(const float2* ihat, int count, int br, int bc, const float2* sy, const float2* sx, int ny,
+                         int nx, float* out, cudaStream_t s) {
+  dim3 grid((unsigned)ceil_div(ny, SY_TY), (unsigned)count);
+  synth_kernel<NV><<<grid, 256, sizeof(float2) * SY_TY * bc, s>>>(ihat, br, bc, sy, sx, ny, nx, out);
+}
+
+}  // namespace oi
+
+extern "C" int oi_coarse_to_image(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc,
+                                  const void* gr, const void* sy, const void* sx, int ny, int nx, void* scratch,
+                                  float* out, void* stream) {
+  using namespace oi;
+  if (!coarse || !gc || !gr || !sy || !sx || !scratch || !out || count <= 0 || mr <= 0 || mc <= 0 || br <= 0 ||
+      bc <= 0 || ny <= 0 || nx <= 0)
+    return fail(OI_EINVAL, "oi_coarse_to_image: bad arguments");
+  if (mr < 2 * br - 1 || mc < 2 * bc - 1)
+    return fail(OI_EINVAL, "oi_coarse_to_image: coarse grid %dx%d too small for band %dx%d", mr, mc, br, bc);
+  if (mr > 1024 || bc > 1024 || nx > 2048 || count > 65535)
+    return fail(OI_ERANGE, "oi_coarse_to_image: sizes out of range (mr=%d bc=%d nx=%d)", mr, bc, nx);
+  cudaStream_t s = (cudaStream_t)stream;
+  size_t smem = sizeof(float2) * (size_t)mr * SP_QT;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(coarse_spec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail(OI_ECUDA, "oi_coarse_to_image: smem attribute: %s", cudaGetErrorString(e));
+  }
+  dim3 g1((unsigned)ceil_div(bc, SP_QT), (unsigned)count);
+  coarse_spec_kernel<<<g1, 256, smem, s>>>(coarse, mr, mc, br, bc, (const float2*)gc, (const float2*)gr,
+                                           (float2*)scratch);
+  int rc = check_launch("oi_coarse_to_image/spec");
+  if (rc) return rc;
+  const float2* ih = (const float2*)scratch;
+  switch ((nx + 255) / 256) {
+    case 1: launch_synth<1>(ih, count, br, bc, (const float2*)sy, (const float2*)sx, ny, nx, out, s); break;
+    case 2: launch_synth<2>(ih, count, br, bc, (const float2*)sy, (const float2*)sx, ny, nx, out, s); break;
+    case 3: case 4:
+      launch_synth<4>(ih, count, br, bc, (const float2*)sy, (const float2*)sx, ny, nx, out, s); break;
+    case 5: case 6: case 7: case 8:
+      launch_synth<8>(ih, count, br, bc, (const float2*)sy, (const float2*)sx, ny, nx, out, s); break;
+    default:
+      return fail(OI_ERANGE, "oi_coarse_to_image: nx=%d above 2048 not supported", nx);
+  }
+  return check_launch("oi_coarse_to_image/synth");
+}

@@ -1,0 +1,239 @@
+"""Device-side orchestration of the imaging path: plans, band selection and the batched SOCS / Abbe calls.
+
+Every image the reference computes has the form
+    I[y, x] = sum_fields w * | sum_{m in band} P(m) c(m) exp(-2 pi i (m_r y/Ny + m_c x/Nx)) |^2
+with c(m) = 1/(Ny Nx) sum h[y, x] exp(+2 pi i (m_r y/Ny + m_c x/Nx)) the mask spectrum:
+  * Abbe (CalculateAerialImage.py:18-103): fields = (source point j, polarisation component e, channel),
+    P = shifted pupil of point j, w = n * v_j / sum(v);
+  * SOCS (CalculateAerialImage_SOCS.py:3-11): fields = (kernel k, channel), P = kernel k, w = 1.
+The engine computes it in three native stages (liboi_b200):
+  1. oi_band_spectrum   -- c(m) on the band only (Br x Bc frequencies), from the mask in one pass;
+  2. oi_coherent_coarse -- sum of |field|^2 on a coarse Mr x Mc grid (Mr >= 2Br-1), fields kept on chip;
+  3. oi_coarse_to_image -- exact band-limited resampling of that intensity to the Ny x Nx output.
+Stage 3 is exact because the intensity's spectrum lives on |q| < B; the result equals the reference's full
+grid FFT evaluation index for index.
+"""
+from __future__ import annotations
+
+import math
+import threading
+from dataclasses import dataclass
+
+import torch
+
+from . import _native as N
+
+COARSE_ALIGN = 64
+
+
+def coarse_size(b: int) -> int:
+    """Smallest multiple of 64 that holds the 2B-1 intensity frequencies of a B-wide band."""
+    return max(COARSE_ALIGN, ((2 * b - 1 + COARSE_ALIGN - 1) // COARSE_ALIGN) * COARSE_ALIGN)
+
+
+def require_cuda(device=None) -> torch.device:
+    if not torch.cuda.is_available():
+        raise N.NativeError('opticalimaging_b200 needs a CUDA device; there is no CPU path')
+    d = torch.device(device) if device is not None else torch.device('cuda', torch.cuda.current_device())
+    if d.type != 'cuda':
+        d = torch.device('cuda', torch.cuda.current_device())
+    N.load()
+    return d
+
+
+def twiddle(rows, cols, a0, b0, n, sign, device, scale=1.0):
+    """exp(sign 2 pi i (a+a0)(b+b0)/n) as a [rows, cols] complex64 device tensor."""
+    out = torch.empty((rows, cols), dtype=torch.complex64, device=device)
+    N.call('oi_twiddle', N.ptr(out), rows, cols, a0, b0, n, sign, float(scale), N.stream_handle(device))
+    return out
+
+
+@dataclass(frozen=True)
+class Band:
+    """Centred frequency band: rows m0r .. m0r+br-1, columns m0c .. m0c+bc-1."""
+    m0r: int
+    br: int
+    m0c: int
+    bc: int
+
+
+class Plan:
+    """Phase tables for one (output grid, band); cached and shared by every call with the same key."""
+
+    _cache: dict = {}
+    _lock = threading.Lock()
+
+    def __init__(self, ny, nx, band: Band, device):
+        self.ny, self.nx, self.band, self.device = ny, nx, band, device
+        b = band
+        self.mr, self.mc = coarse_size(b.br), coarse_size(b.bc)
+        nq = 2 * b.br - 1
+        t = lambda *a: twiddle(*a, device=device)  # noqa: E731
+        self.wx = t(nx, b.bc, 0, b.m0c, nx, +1)              # [nx][bc]   forward x
+        self.wy = t(ny, b.br, 0, b.m0r, ny, +1)              # [ny][br]   forward y
+        self.frow = t(self.mr, b.br, 0, b.m0r, self.mr, -1)  # [mr][br]   coarse rows
+        self.fcol = t(b.bc, self.mc, b.m0c, 0, self.mc, -1)  # [bc][mc]   coarse columns
+        self.gc = t(self.mc, b.bc, 0, 0, self.mc, +1)        # [mc][bc]   coarse -> spectrum (x)
+        self.gr = t(self.mr, nq, 0, -(b.br - 1), self.mr, +1)  # [mr][2br-1]
+        self.sy = t(ny, nq, 0, -(b.br - 1), ny, -1)          # [ny][2br-1] spectrum -> image (y)
+        self.sx = t(b.bc, nx, 0, 0, nx, -1)                  # [bc][nx]   spectrum -> image (x)
+
+    @classmethod
+    def get(cls, ny, nx, band: Band, device) -> 'Plan':
+        key = (ny, nx, band, str(device))
+        with cls._lock:
+            p = cls._cache.get(key)
+            if p is None:
+                p = cls._cache[key] = Plan(ny, nx, band, device)
+            return p
+
+
+# --------------------------------------------------------------------------------------------- stages
+def band_spectrum(field: torch.Tensor, kind: int, plan: Plan, nch: int = 1, scale: float = 1.0,
+                  scratch: torch.Tensor | None = None) -> torch.Tensor:
+    """c(m) on the plan's band: [batch, nch, br, bc] complex64.
+
+    field: float32 [B, ny, nx] (FIELD_REAL_F32), uint8 [B, ny, nx] (FIELD_U8) or complex64 [B, ny, nx, nch]
+    (FIELD_COMPLEX_C64), contiguous on the plan's device.  `scale` multiplies the 1/(ny nx) normalisation.
+    """
+    b = plan.band
+    batch = field.shape[0]
+    need = batch * nch * plan.ny * b.bc
+    if scratch is None or scratch.numel() < need:
+        scratch = torch.empty(need, dtype=torch.complex64, device=plan.device)
+    band = torch.empty((batch, nch, b.br, b.bc), dtype=torch.complex64, device=plan.device)
+    N.call('oi_band_spectrum', N.ptr(field), kind, batch, plan.ny, plan.nx, nch, b.br, b.bc, N.ptr(plan.wx),
+           N.ptr(plan.wy), float(scale / (plan.ny * plan.nx)), N.ptr(scratch), N.ptr(band),
+           N.stream_handle(plan.device))
+    return band
+
+
+def _mark(marks, name):
+    if marks is not None:
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record()
+        marks.append((name, ev))
+
+
+def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tensor, plan: Plan,
+                   pupil_batch_stride: int = 0, out: torch.Tensor | None = None, marks=None) -> torch.Tensor:
+    """sum_fields w |IDFT(P .* c)|^2 on the output grid: [batch, nz, ny, nx] float32.
+
+    band: [batch, nch, br, bc] complex64; pupils: [nz, nk, br, bc] complex64 (shared by the batch when
+    pupil_batch_stride == 0); weights: [nz, nk] float32.
+    """
+    b = plan.band
+    batch, nch = band.shape[0], band.shape[1]
+    nz, nk = pupils.shape[-4], pupils.shape[-3]
+    dev = plan.device
+    coarse = torch.empty((batch, nz, plan.mr, plan.mc), dtype=torch.float32, device=dev)
+    s = N.stream_handle(dev)
+    N.call('oi_coherent_coarse', N.ptr(band), batch, nch, b.br, b.bc, N.ptr(pupils), int(pupil_batch_stride),
+           N.ptr(weights), nz, nk, plan.mr, plan.mc, N.ptr(plan.frow), N.ptr(plan.fcol), N.ptr(coarse), s)
+    _mark(marks, 'coherent_coarse')
+    if out is None:
+        out = torch.empty((batch, nz, plan.ny, plan.nx), dtype=torch.float32, device=dev)
+    ihat = torch.empty(batch * nz * (2 * b.br - 1) * b.bc, dtype=torch.complex64, device=dev)
+    N.call('oi_coarse_to_image', N.ptr(coarse), batch * nz, plan.mr, plan.mc, b.br, b.bc, N.ptr(plan.gc),
+           N.ptr(plan.gr), N.ptr(plan.sy), N.ptr(plan.sx), plan.ny, plan.nx, N.ptr(ihat), N.ptr(out), s)
+    _mark(marks, 'coarse_to_image')
+    return out
+
+
+# --------------------------------------------------------------------------------------------- bands
+def clip_band(lo: int, hi: int, n: int):
+    """Intersect the centred frequency interval [lo, hi] with the grid's frequencies [-(n//2), (n+1)//2 - 1]."""
+    lo = max(lo, -(n // 2))
+    hi = min(hi, (n + 1) // 2 - 1)
+    return lo, hi
+
+
+def abbe_band(ny, nx, npy, npx, sx: torch.Tensor, sy: torch.Tensor) -> Band | None:
+    """Band covering every shifted pupil |m_r/npy + X|^2 + |m_c/npx + Y|^2 <= 1 (rows carry the source X,
+    CalculateAerialImage.py:31,55), widened by one frequency for float32 rounding; None if empty."""
+    xmax, xmin = float(sx.max()), float(sx.min())
+    ymax, ymin = float(sy.max()), float(sy.min())
+    r0, r1 = clip_band(math.floor(npy * (-1 - xmax)) - 1, math.ceil(npy * (1 - xmin)) + 1, ny)
+    c0, c1 = clip_band(math.floor(npx * (-1 - ymax)) - 1, math.ceil(npx * (1 - ymin)) + 1, nx)
+    if r1 < r0 or c1 < c0:
+        return None
+    return Band(r0, r1 - r0 + 1, c0, c1 - c0 + 1)
+
+
+def cyclic_support(nonzero: torch.Tensor):
+    """Smallest cyclic interval [start, start+length) of indices covering every True entry."""
+    n = nonzero.numel()
+    idx = torch.nonzero(nonzero).flatten().tolist()
+    if not idx:
+        return 0, 1
+    if len(idx) == 1:
+        return idx[0], 1
+    gaps = [(idx[(i + 1) % len(idx)] - idx[i]) % n for i in range(len(idx))]
+    i = max(range(len(idx)), key=lambda k: gaps[k])
+    if gaps[i] <= 1:
+        return 0, n
+    start = idx[(i + 1) % len(idx)]
+    return start, n - gaps[i] + 1
+
+
+def centred(start: int, n: int) -> int:
+    """Representative of index `start` (mod n) in the centred range [-(n//2), n - n//2)."""
+    s = start % n
+    return s - n if s >= n - n // 2 else s
+
+
+# ------------------------------------------------------------------------------------------ SOCS model
+class SocsKernels:
+    """SOCS kernels resident on the device in band form: [K, br, bc] complex64 on `band`, for a ny x nx grid.
+
+    This is the engine's form of the reference's full-grid kernel array (DecomposeTCC_SOCS.py:26-35): the same
+    values, with only the band that can be non-zero kept.
+    """
+
+    def __init__(self, kernels: torch.Tensor, band: Band, ny: int, nx: int):
+        if kernels.dim() != 3 or kernels.shape[1:] != (band.br, band.bc):
+            raise ValueError('kernels must be [K, br, bc] on the band')
+        if band.br > ny or band.bc > nx:
+            raise ValueError(f'kernel band {band.br}x{band.bc} does not fit the {ny}x{nx} grid')
+        self.device = require_cuda(kernels.device)
+        self.kernels = kernels.to(self.device, torch.complex64).contiguous()
+        self.band, self.ny, self.nx = band, ny, nx
+        self.weights = torch.ones((1, self.kernels.shape[0]), dtype=torch.float32, device=self.device)
+        self.plan = Plan.get(ny, nx, band, self.device)
+
+    @property
+    def count(self):
+        return self.kernels.shape[0]
+
+    @classmethod
+    def from_full_grid(cls, kernels: torch.Tensor) -> 'SocsKernels':
+        """Band form of a reference-layout kernel array [Ny, Nx, K] (frequency m at index m mod N)."""
+        ny, nx = kernels.shape[0], kernels.shape[1]
+        dev = require_cuda(kernels.device if kernels.is_cuda else None)
+        k = kernels.to(dev)
+        nzr = (k != 0).any(dim=2)
+        r0, br = cyclic_support(nzr.any(dim=1))
+        c0, bc = cyclic_support(nzr.any(dim=0))
+        band = Band(centred(r0, ny), br, centred(c0, nx), bc)
+        kb = torch.roll(k, shifts=(-band.m0r, -band.m0c), dims=(0, 1))[:br, :bc, :].permute(2, 0, 1)
+        return cls(kb.to(torch.complex64).contiguous(), band, ny, nx)
+
+    def image(self, masks: torch.Tensor, kind: int | None = None, nch: int = 1, scale: float = 1.0,
+              out: torch.Tensor | None = None, marks=None) -> torch.Tensor:
+        """SOCS aerial images of a batch of masks -> [B, ny, nx] float32.
+
+        masks: float32 [B, ny, nx] (real transmission), uint8 [B, ny, nx] or complex64 [B, ny, nx, nch].
+        `marks`, if a list, receives (stage name, CUDA event) pairs recorded after each native stage.
+        """
+        if kind is None:
+            kind = {torch.float32: N.FIELD_REAL_F32, torch.uint8: N.FIELD_U8,
+                    torch.complex64: N.FIELD_COMPLEX_C64}[masks.dtype]
+        if masks.shape[1] != self.ny or masks.shape[2] != self.nx:
+            raise ValueError(f'mask grid {tuple(masks.shape[1:3])} != kernel grid {(self.ny, self.nx)}')
+        _mark(marks, 'start')
+        band = band_spectrum(masks.contiguous(), kind, self.plan, nch=nch, scale=scale)
+        _mark(marks, 'band_spectrum')
+        img = coherent_image(band, self.kernels.unsqueeze(0), self.weights, self.plan,
+                             out=None if out is None else out.view(masks.shape[0], 1, self.ny, self.nx),
+                             marks=marks)
+        return img.view(masks.shape[0], self.ny, self.nx)

@@ -1,0 +1,403 @@
+"""Drop-in imaging entry points with the reference's names, arguments and return values.
+
+* ``CalculateAbbeImage``, ``CalculateHopkinsImage``, ``CalculateOptimized``  (CalculateAerialImage.py:18-152)
+* ``CalculateTCCMatrix``, ``GetTCCMatrix``                                   (CalculateTCCMatrix.py:9-75)
+* ``DecomposeTCC_SOCS``                                                       (DecomposeTCC_SOCS.py:3-37)
+* ``CalculateAerialImage_SOCS``, ``CalculateSOCS``                            (CalculateAerialImage_SOCS.py:3-32)
+* ``CalculateCharacteristicMatrix``                                           (CalculateCharacteristicMatrix.py:3-17)
+* ``calculate_spectrum`` behind ``Scatter.CalculateSpectrum``                 (Scatter.py:10-35)
+
+All numerical work runs in liboi_b200 on the current CUDA device.  Results come back on the device of the
+caller's ``ScatterField`` (CPU in, CPU out), with the reference's shapes.  Precision: FP32 transforms with FP64
+pupil synthesis; the TCC and its eigendecomposition are FP64 (so ``CalculateTCCMatrix`` returns complex128).
+
+Divergences from the reference, all deliberate and documented:
+* ``Hopkins_SettingType='threshold'`` works (the reference raises on a multi-element comparison): K is the
+  smallest count whose leading eigenvalues reach the threshold fraction of the trace.
+* An ``ImageCalculationMode`` other than 'scalar'/'vector' raises ValueError (the reference fails later with
+  UnboundLocalError or IndexError).
+* Out-of-domain optics (NA/Magnification > IndexImage, or NA >= 1, where the reference's obliquity and defocus
+  roots go negative) produce the reference's NaN image and a RuntimeWarning.
+"""
+from __future__ import annotations
+
+import warnings
+
+import torch
+
+from . import _native as N
+from .engine import Band, Plan, SocsKernels, abbe_band, band_spectrum, coherent_image, require_cuda
+from .params import ImageData, cartesian_to_polar  # noqa: F401
+
+__all__ = ['CalculateAbbeImage', 'CalculateHopkinsImage', 'CalculateOptimized', 'CalculateTCCMatrix',
+           'GetTCCMatrix', 'DecomposeTCC_SOCS', 'CalculateAerialImage_SOCS', 'CalculateSOCS',
+           'CalculateCharacteristicMatrix', 'calculate_spectrum', 'socs_kernels_from_tcc']
+
+
+# ------------------------------------------------------------------------------------------- helpers
+def _mode(numerics):
+    m = numerics.ImageCalculationMode
+    if m not in ('scalar', 'vector'):
+        raise ValueError(f"ImageCalculationMode must be 'scalar' or 'vector', got {m!r}")
+    return m == 'vector'
+
+
+def _check_domain(projector):
+    na, mag, n = float(projector.NA), float(projector.Magnification), float(projector.IndexImage)
+    if na / mag > n or na >= 1.0:
+        warnings.warn(f'optics outside the model domain (NA={na}, Magnification={mag}, IndexImage={n}): the '
+                      'obliquity or defocus root is negative inside the pupil and the image is NaN, as in the '
+                      'reference', RuntimeWarning, stacklevel=3)
+
+
+def _jones(source):
+    px, py = (complex(v) for v in source.PolarizationVector)
+    return N.host_doubles([px.real, px.imag, py.real, py.imag])
+
+
+def _zernike(projector):
+    z = torch.as_tensor(projector.Aberration_Zernike, dtype=torch.float64).flatten().tolist()
+    z = (z + [0.0] * 37)[:37]
+    return N.host_doubles(z)
+
+
+def _focus_list(projector):
+    return [float(v) for v in torch.as_tensor(projector.FocusRange).flatten().tolist()]
+
+
+def _axes(scatter, projector, source):
+    """The reference's float32 spectrum axes f (X, columns) and g (Y, rows) (Scatter.py:15-18)."""
+    ny, nx = scatter.ScatterField.shape[0], scatter.ScatterField.shape[1]
+    npx = scatter.Period_X / (source.Wavelength / projector.NA)
+    npy = scatter.Period_Y / (source.Wavelength / projector.NA)
+    f = (1 / npx) * torch.arange(-(nx // 2), (nx + 1) // 2)
+    g = (1 / npy) * torch.arange(-(ny // 2), (ny + 1) // 2)
+    return f, g, npx, npy
+
+
+def _field_on_device(scatter, dev):
+    """ScatterField [Ny, Nx, C] as complex64 on the device, with all-zero channels dropped."""
+    h = torch.as_tensor(scatter.ScatterField)
+    h = h.to(dev, non_blocking=True).to(torch.complex64)
+    live = [c for c in range(h.shape[2]) if bool((h[:, :, c] != 0).any())]
+    if not live:
+        live = [0]
+    if len(live) != h.shape[2]:
+        h = h[:, :, live]
+    return h.contiguous()
+
+
+def _result_device(scatter):
+    h = scatter.ScatterField
+    return h.device if isinstance(h, torch.Tensor) else torch.device('cpu')
+
+
+def _pupil_image(scatter, projector, source, h, dev):
+    """PupilImage of Scatter.CalculateSpectrum (Scatter.py:22-33): the cropped centred spectrum, NaN outside
+    the unit disc."""
+    ny, nx = h.shape[0], h.shape[1]
+    f, g, npx, npy = _axes(scatter, projector, source)
+    ox, oy = int(npx) + 3, int(npy) + 3
+    r0, c0 = ny // 2 - oy, nx // 2 - ox
+    if r0 >= 0 and c0 >= 0 and ny // 2 + oy <= ny and nx // 2 + ox <= nx:
+        band = Band(r0 - ny // 2, 2 * oy, c0 - nx // 2, 2 * ox)
+        hk = _spectrum_band(h, band, npx * npy, dev)
+        fm, gm = torch.meshgrid(g[r0:r0 + 2 * oy], f[c0:c0 + 2 * ox], indexing='ij')
+    else:   # crop window leaves the grid: Python slicing of the full spectrum, as the reference does
+        hk = _spectrum_band(h, Band(-(ny // 2), ny, -(nx // 2), nx), npx * npy, dev)
+        fm, gm = torch.meshgrid(g, f, indexing='ij')
+        sl = (slice(ny // 2 - oy, ny // 2 + oy), slice(nx // 2 - ox, nx // 2 + ox))
+        hk, fm, gm = hk[sl], fm[sl], gm[sl]
+    out = hk.clone()
+    out[(fm ** 2 + gm ** 2 > 1).to(out.device)] = float('nan')
+    return out
+
+
+def _spectrum_band(h, band: Band, scale, dev):
+    """Centred spectrum on `band` of a [Ny, Nx, C] complex64 device field -> [br, bc, C]."""
+    ny, nx, nch = h.shape
+    plan = Plan.get(ny, nx, band, dev)
+    c = band_spectrum(h.unsqueeze(0), N.FIELD_COMPLEX_C64, plan, nch=nch, scale=scale)
+    return c[0].permute(1, 2, 0)
+
+
+def calculate_spectrum(scatter, projector, source):
+    """Hk [Ny, Nx, 3], f, g and PupilImage (Scatter.py:10-35), computed on the device."""
+    dev = require_cuda()
+    h = torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
+    ny, nx = h.shape[0], h.shape[1]
+    f, g, npx, npy = _axes(scatter, projector, source)
+    hk = _spectrum_band(h, Band(-(ny // 2), ny, -(nx // 2), nx), npx * npy, dev)
+    pim = _pupil_image(scatter, projector, source, h, dev)
+    rd = _result_device(scatter)
+    return hk.to(rd), f, g, pim.to(rd)
+
+
+def _image_data(intensity, scatter, projector):
+    out = ImageData()
+    out.Intensity = intensity
+    out.ImageX = torch.linspace(-scatter.Period_X / 2, scatter.Period_X / 2, scatter.ScatterField.shape[1])
+    out.ImageY = torch.linspace(-scatter.Period_Y / 2, scatter.Period_Y / 2, scatter.ScatterField.shape[0])
+    out.ImageZ = projector.FocusRange
+    return out
+
+
+# ----------------------------------------------------------------------------------------------- Abbe
+def abbe_intensity(source, scatter, projector, numerics, h=None):
+    """Abbe image [nFocus, Ny, Nx] float32 on the device (CalculateAerialImage.py:18-92)."""
+    vector = _mode(numerics)
+    _check_domain(projector)
+    dev = require_cuda()
+    sd = source.Calc_SourceSimple()
+    X, Y, V = (t.reshape(-1).to(torch.float32) for t in (sd.X, sd.Y, sd.Value))
+    if h is None:
+        h = _field_on_device(scatter, dev)
+    ny, nx, nch = h.shape
+    zs = _focus_list(projector)
+    f, g, npx, npy = _axes(scatter, projector, source)
+    nsrc = X.numel()
+    if nsrc == 0:   # the reference divides 0 by a zero source weight
+        return torch.full((len(zs), ny, nx), float('nan'), device=dev)
+    band = abbe_band(ny, nx, npy, npx, X, Y)
+    if band is None:
+        return torch.zeros((len(zs), ny, nx), device=dev)
+    ne = 3 if vector else 1
+    fr = g[band.m0r + ny // 2: band.m0r + ny // 2 + band.br].to(dev)
+    fc = f[band.m0c + nx // 2: band.m0c + nx // 2 + band.bc].to(dev)
+    Xd, Yd, Vd = X.to(dev), Y.to(dev), V.to(dev)
+    focus = torch.tensor(zs, dtype=torch.float64, device=dev)
+    pupils = torch.empty((len(zs), nsrc * ne, band.br, band.bc), dtype=torch.complex64, device=dev)
+    weights = torch.empty((len(zs), nsrc * ne), dtype=torch.float32, device=dev)
+    wsum = float(torch.sum(V))
+    s = N.stream_handle(dev)
+    N.call('oi_abbe_pupils', N.ptr(fr), N.ptr(fc), band.br, band.bc, N.ptr(Xd), N.ptr(Yd), N.ptr(Vd), nsrc,
+           wsum, N.ptr(focus), len(zs), _zernike(projector), int(vector), _jones(source), float(projector.NA),
+           float(projector.Magnification), float(projector.IndexImage), float(source.Wavelength), N.ptr(pupils),
+           N.ptr(weights), s)
+    plan = Plan.get(ny, nx, band, dev)
+    c = band_spectrum(h.unsqueeze(0), N.FIELD_COMPLEX_C64, plan, nch=nch)
+    return coherent_image(c, pupils, weights, plan)[0]
+
+
+def CalculateAbbeImage(source, scatter, projector, numerics):
+    """Abbe aerial image -> (ImageData, pupilImage) (CalculateAerialImage.py:18-103)."""
+    dev = require_cuda()
+    h = _field_on_device(scatter, dev)
+    inten = abbe_intensity(source, scatter, projector, numerics, h=h)
+    hfull = torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
+    pim = _pupil_image(scatter, projector, source, hfull, dev)
+    rd = _result_device(scatter)
+    return _image_data(inten.to(rd), scatter, projector), pim.to(rd)
+
+
+# ------------------------------------------------------------------------------------------------ TCC
+def _tcc_axes(source, xypitch, projector):
+    """TCC grid axes exactly as CalculateTCCMatrix.py:17-22 (float32 tensors)."""
+    npf = torch.tensor(xypitch[0] / (source.Wavelength / projector.NA))
+    npg = torch.tensor(xypitch[1] / (source.Wavelength / projector.NA))
+    nf = int(torch.ceil(2 * npf).int())
+    ng = int(torch.ceil(2 * npg).int())
+    f = (1 / npf) * torch.arange(-nf, nf + 1)
+    g = (1 / npg) * torch.arange(-ng, ng + 1)
+    return f, g
+
+
+def tcc_pupil_matrix(source, xypitch, projector, focus, numerics):
+    """h [ne, FG, S] complex128 with TCC = sum_e h_e h_e^H, and FG_ValidSize [len g, len f]."""
+    vector = _mode(numerics)
+    _check_domain(projector)
+    dev = require_cuda()
+    sd = source.Calc_SourceSimple()
+    X, Y, V = (t.reshape(-1).to(torch.float32) for t in (sd.X, sd.Y, sd.Value))
+    f, g = _tcc_axes(source, xypitch, projector)
+    ne = 3 if vector else 1
+    nsrc = X.numel()
+    h = torch.empty((ne, f.numel() * g.numel(), max(nsrc, 1)), dtype=torch.complex128, device=dev)
+    if nsrc == 0:
+        h.fill_(float('nan'))
+        return h, [g.numel(), f.numel()]
+    fd, gd, Xd, Yd, Vd = (t.to(dev) for t in (f, g, X, Y, V))   # held until the launch is enqueued
+    N.call('oi_tcc_pupils64', N.ptr(fd), f.numel(), N.ptr(gd), g.numel(), N.ptr(Xd), N.ptr(Yd), N.ptr(Vd), nsrc,
+           float(torch.sum(V)), float(focus), _zernike(projector), int(vector), _jones(source),
+           float(projector.NA), float(projector.Magnification), float(projector.IndexImage),
+           float(source.Wavelength), N.ptr(h), N.stream_handle(dev))
+    return h, [g.numel(), f.numel()]
+
+
+def CalculateTCCMatrix(source, xypitch, projector, focus, numerics):
+    """TCC [FG, FG] complex128 on the device and FG_ValidSize [len g, len f] (CalculateTCCMatrix.py:9-56)."""
+    h, fg = tcc_pupil_matrix(source, xypitch, projector, focus, numerics)
+    n = h.shape[1]
+    tcc = torch.empty((n, n), dtype=torch.complex128, device=h.device)
+    N.call('oi_tcc_assemble64', N.ptr(h), h.shape[0], n, h.shape[2], N.ptr(tcc), N.stream_handle(h.device))
+    return tcc, fg
+
+
+def GetTCCMatrix(sourceData, shiftedPupil):
+    """P diag(w) P^H / sum(w) for a [FG, S] pupil matrix (CalculateTCCMatrix.py:58-75), FP64 on the device."""
+    dev = require_cuda()
+    w = sourceData.Value.reshape(-1).to(torch.float64)
+    p = torch.as_tensor(shiftedPupil).to(dev, torch.complex128)
+    h = (p * torch.sqrt(w.to(dev) / torch.sum(w).to(dev))).contiguous().unsqueeze(0)
+    n = h.shape[1]
+    tcc = torch.empty((n, n), dtype=torch.complex128, device=dev)
+    N.call('oi_tcc_assemble64', N.ptr(h), 1, n, h.shape[2], N.ptr(tcc), N.stream_handle(dev))
+    return tcc
+
+
+def _socs_count(numerics, evals, size):
+    kind = numerics.Hopkins_SettingType.lower()
+    if kind == 'order':
+        return min(numerics.Hopkins_Order, size - 1)
+    if kind == 'threshold':
+        c = torch.cumsum(evals, 0)
+        k = int(torch.searchsorted(c, numerics.Hopkins_Threshold * c[-1], right=True))
+        return min(k, size - 1)
+    raise ValueError('Error: Hopkins_SettingType should be order or threshold!')
+
+
+def _eig_desc(tcc):
+    """Eigenpairs of the Hermitian TCC, eigenvalues descending and clamped at zero (FP64, on the device)."""
+    lam, U = torch.linalg.eigh(tcc)
+    return torch.clamp(lam.flip(0), min=0), U.flip(1)
+
+
+def _placement(n, length):
+    """Frequency of the first kernel row/column as DecomposeTCC_SOCS places it: centred embedding at
+    (n - length + 1)//2 then fftshift (DecomposeTCC_SOCS.py:29-31).  For odd n this lands one frequency
+    below the centre, and the engine keeps that placement so its images match the reference's."""
+    return (n - length + 1) // 2 + n // 2 - n
+
+
+def socs_kernels_from_tcc(tcc, FG_ValidSize, Nfg, numerics) -> SocsKernels:
+    """Top-K SOCS kernels sqrt(lambda_k) u_k in band form, placed as the reference places them."""
+    nf, ng = Nfg
+    lg, lf = FG_ValidSize
+    if lf > ng or lg > nf:
+        raise ValueError(f'TCC grid {lf}x{lg} does not fit the {ng}x{nf} image grid')
+    lam, U = _eig_desc(tcc)
+    k = _socs_count(numerics, lam, U.shape[1])
+    kb = (U[:, :k] * torch.sqrt(lam[:k])).T.reshape(k, lf, lg)
+    band = Band(_placement(ng, lf), lf, _placement(nf, lg), lg)
+    return SocsKernels(kb.to(torch.complex64), band, ng, nf)
+
+
+def DecomposeTCC_SOCS(TCCMatrix_Stacked, FG_ValidSize, Nfg, numerics):
+    """Full-grid SOCS kernels [Ny, Nx, K] complex64 on the device (DecomposeTCC_SOCS.py:3-37)."""
+    dev = require_cuda()
+    tcc = torch.as_tensor(TCCMatrix_Stacked).to(dev, torch.complex128)
+    sk = socs_kernels_from_tcc(tcc, FG_ValidSize, Nfg, numerics)
+    nf, ng = Nfg
+    full = torch.zeros((ng, nf, sk.count), dtype=torch.complex64, device=dev)
+    b = sk.band
+    full[:b.br, :b.bc, :] = sk.kernels.permute(1, 2, 0)
+    return torch.roll(full, shifts=(b.m0r, b.m0c), dims=(0, 1))
+
+
+def CalculateAerialImage_SOCS(scatter, TCCMatrix_SOCS, source, projector):
+    """SOCS aerial image [Ny, Nx] and pupilImage (CalculateAerialImage_SOCS.py:3-11)."""
+    dev = require_cuda()
+    sk = TCCMatrix_SOCS if isinstance(TCCMatrix_SOCS, SocsKernels) else \
+        SocsKernels.from_full_grid(torch.as_tensor(TCCMatrix_SOCS).to(dev))
+    h = _field_on_device(scatter, dev)
+    img = sk.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
+    hfull = torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
+    pim = _pupil_image(scatter, projector, source, hfull, dev)
+    rd = _result_device(scatter)
+    return img.to(rd), pim.to(rd)
+
+
+def hopkins_intensity(source, scatter, projector, numerics, h=None):
+    """Hopkins image [nFocus, Ny, Nx] on the device: per plane TCC -> top-K kernels -> SOCS image."""
+    dev = require_cuda()
+    if h is None:
+        h = _field_on_device(scatter, dev)
+    ny, nx = h.shape[0], h.shape[1]
+    zs = _focus_list(projector)
+    out = torch.empty((len(zs), ny, nx), dtype=torch.float32, device=dev)
+    for i, z in enumerate(zs):
+        tcc, fg = CalculateTCCMatrix(source, [scatter.Period_Y, scatter.Period_X], projector, z, numerics)
+        sk = socs_kernels_from_tcc(tcc, fg, [nx, ny], numerics)
+        out[i] = sk.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
+    return out
+
+
+def CalculateHopkinsImage(source, scatter, projector, numerics):
+    """Hopkins aerial image -> (ImageData, pupilImage) (CalculateAerialImage.py:105-130)."""
+    dev = require_cuda()
+    h = _field_on_device(scatter, dev)
+    inten = hopkins_intensity(source, scatter, projector, numerics, h=h)
+    hfull = torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
+    pim = _pupil_image(scatter, projector, source, hfull, dev)
+    rd = _result_device(scatter)
+    return _image_data(inten.to(rd), scatter, projector), pim.to(rd)
+
+
+# ------------------------------------------------------------------------------ Floquet-mode ("optimized")
+def CalculateSOCS(FloquetMode, TCCMatrix_SOCS, numerics):
+    """Direct-DFT SOCS image [ScatterGrid_X, ScatterGrid_Y] from Floquet modes (CalculateAerialImage_SOCS.py:13-32).
+
+    I[x][y] = sum_{k,c} |sum_o exp(2 pi i (ox (x+1/2)/Gx + oy (y+1/2)/Gy)) FM[o, c] kern_k[o]|^2 over the
+    (2 ScatterOrder_X + 1) x (2 ScatterOrder_Y + 1) orders o, with kern_k = ifftshift(transpose(kernels)) paired
+    with FM by flat index exactly as the reference reshapes them.  The engine's coherent-sum stages evaluate it:
+    each (k, c) is one field on the order band; the half-pixel offset is a phase per order, and the positive
+    exponent is the engine's negative one applied to the order-reversed field.
+    """
+    dev = require_cuda()
+    fm = torch.as_tensor(FloquetMode).to(dev, torch.complex64)
+    ker = torch.as_tensor(TCCMatrix_SOCS).to(dev, torch.complex64)
+    gx, gy = numerics.ScatterGrid_X, numerics.ScatterGrid_Y
+    ox, oy = numerics.ScatterOrder_X, numerics.ScatterOrder_Y
+    nox, noy = 2 * ox + 1, 2 * oy + 1
+    kt = torch.fft.ifftshift(ker.transpose(0, 1), dim=(0, 1))
+    if tuple(fm.shape) != (nox, noy, 3) or tuple(kt.shape[:2]) != (nox, noy):
+        raise ValueError(f'FloquetMode {tuple(fm.shape)} / kernels {tuple(ker.shape)} do not match the '
+                         f'{nox}x{noy} scatter orders')
+    k = kt.shape[2]
+    qx = torch.arange(-ox, ox + 1, device=dev, dtype=torch.float64)
+    qy = torch.arange(-oy, oy + 1, device=dev, dtype=torch.float64)
+    half = torch.exp(1j * torch.pi * (qx[:, None] / gx + qy[None, :] / gy)).to(torch.complex64)
+    a = fm.permute(2, 0, 1)[None] * kt.permute(2, 0, 1)[:, None] * half    # [K, 3, nox, noy]
+    fields = torch.flip(a, dims=(2, 3)).reshape(1, k * 3, nox, noy).contiguous()
+    plan = Plan.get(gx, gy, Band(-ox, nox, -oy, noy), dev)
+    ones = torch.ones((1, 1, nox, noy), dtype=torch.complex64, device=dev)
+    w = torch.ones((1, 1), dtype=torch.float32, device=dev)
+    img = coherent_image(fields, ones, w, plan)[0, 0]
+    return img.to(_tensor_device(FloquetMode))
+
+
+def _tensor_device(t):
+    return t.device if isinstance(t, torch.Tensor) else torch.device('cpu')
+
+
+def CalculateOptimized(source, scatter, projector, numerics):
+    """Floquet-mode SOCS image -> (ImageData, empty tensor) (CalculateAerialImage.py:131-152)."""
+    pitchxy = [scatter.Period_Y, scatter.Period_X]
+    fm = scatter.FloquetMode
+    nfg = [fm.shape[0], fm.shape[1]]
+    zs = projector.FocusRange
+    out = torch.zeros(len(_focus_list(projector)), numerics.ScatterGrid_X, numerics.ScatterGrid_Y)
+    for i, z in enumerate(_focus_list(projector)):
+        tcc, fg = CalculateTCCMatrix(source, pitchxy, projector, z, numerics)
+        ker = DecomposeTCC_SOCS(tcc, fg, nfg, numerics)
+        out[i] = CalculateSOCS(fm, ker, numerics).cpu()
+    img = ImageData()
+    img.Intensity = out
+    img.ImageX = torch.linspace(-scatter.Period_X / 2, scatter.Period_X / 2, numerics.ScatterGrid_X)
+    img.ImageY = torch.linspace(-scatter.Period_Y / 2, scatter.Period_Y / 2, numerics.ScatterGrid_Y)
+    img.ImageZ = zs
+    return img, torch.tensor([])
+
+
+def CalculateCharacteristicMatrix(f_calc, g_calc, NA, indexImage):
+    """Polarisation transfer terms (CalculateCharacteristicMatrix.py:3-17), torch complex on the input's device.
+
+    The engine evaluates this inside its pupil kernels; this host form is the reference's public helper.
+    """
+    alpha = torch.complex((NA / indexImage) * f_calc, torch.zeros_like(f_calc))
+    beta = torch.complex((NA / indexImage) * g_calc, torch.zeros_like(g_calc))
+    gamma = torch.sqrt(1 - alpha ** 2 - beta ** 2)
+    mxx = 1 - alpha ** 2 / (1 + gamma)
+    myx = -alpha * beta / (1 + gamma)
+    myy = 1 - beta ** 2 / (1 + gamma)
+    return mxx, myx, myx, myy, -alpha, -beta

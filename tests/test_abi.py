@@ -1,0 +1,42 @@
+"""The C-ABI library builds, loads without a GPU, and exports every entry point include/oi_b200.h declares."""
+import os
+import re
+import subprocess
+
+from opticalimaging_b200 import _native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    src = open(os.path.join(ROOT, 'include', 'oi_b200.h')).read()
+    return sorted(set(re.findall(r'^OI_API\s+[\w\s\*]*?\b(oi_\w+)\s*\(', src, flags=re.M)))
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    assert 'oi_coherent_coarse' in names and 'oi_last_error' in names
+    assert len(names) >= 9
+
+
+def test_library_exports_declared_symbols():
+    lib = N.load()
+    for name in declared():
+        assert hasattr(lib, name), name
+    out = subprocess.run(['nm', '-D', '--defined-only', N.lib_path()], capture_output=True, text=True).stdout
+    exported = set(re.findall(r'\bT (oi_\w+)', out))
+    assert set(declared()) <= exported
+    # nothing but the ABI is exported
+    assert all(s.startswith('oi_') for s in exported)
+
+
+def test_binding_covers_header():
+    assert set(declared()) <= set(N.exported_symbols())
+
+
+def test_errors_are_reported_not_raised_in_c():
+    lib = N.load()
+    rc = lib.oi_twiddle(None, 0, 0, 0, 0, 0, 1, 1.0, None)
+    assert rc == -1
+    assert b'oi_twiddle' in lib.oi_last_error()
+    assert lib.oi_version() >= 1

@@ -1,0 +1,199 @@
+"""Parity of the CUDA engine with the FP64 oracle and with the reference's own outputs (golden fixtures).
+
+Tolerances are relative to the peak of the reference image: the FP32 engine form must agree with the FP64
+oracle to 1e-5 of peak, and with the complex64 reference to 2e-5 of peak (the reference's own rounding).
+"""
+import warnings
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import optics64 as O
+from tests.fixtures import build, load, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FP32_VS_FP64 = 1e-5
+FP32_VS_REF = 2e-5
+
+
+@pytest.fixture(scope='module')
+def oi():
+    import opticalimaging_b200.imaging as imaging
+    from opticalimaging_b200 import _native
+    _native.load()
+    return imaging
+
+
+def test_band_spectrum_matches_numpy(oi):
+    from opticalimaging_b200 import engine as E, _native as N
+    dev = torch.device('cuda')
+    rng = np.random.default_rng(0)
+    for ny, nx, band in ((64, 48, E.Band(-7, 15, -5, 11)), (45, 63, E.Band(-22, 45, -31, 63)),
+                         (17, 23, E.Band(-3, 4, 2, 5))):
+        h = (rng.standard_normal((2, ny, nx, 3)) + 1j * rng.standard_normal((2, ny, nx, 3))).astype(np.complex64)
+        plan = E.Plan.get(ny, nx, band, dev)
+        got = E.band_spectrum(torch.from_numpy(h).to(dev), N.FIELD_COMPLEX_C64, plan, nch=3).cpu().numpy()
+        full = np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(h.astype(np.complex128), axes=(1, 2)), axes=(1, 2)),
+                               axes=(1, 2))
+        rows = np.arange(band.m0r, band.m0r + band.br) + ny // 2
+        cols = np.arange(band.m0c, band.m0c + band.bc) + nx // 2
+        want = full[:, rows][:, :, cols].transpose(0, 3, 1, 2)
+        assert rel_err(got, want) < 2e-6
+        # real and uint8 kinds of the same data
+        r = (rng.random((3, ny, nx)) > 0.5)
+        want_r = np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(r.astype(np.float64), axes=(1, 2)), axes=(1, 2)),
+                                 axes=(1, 2))[:, rows][:, :, cols]
+        got_f = E.band_spectrum(torch.from_numpy(r.astype(np.float32)).to(dev), N.FIELD_REAL_F32, plan)
+        got_u = E.band_spectrum(torch.from_numpy(r.astype(np.uint8)).to(dev), N.FIELD_U8, plan)
+        assert rel_err(got_f[:, 0].cpu().numpy(), want_r) < 2e-6
+        assert rel_err(got_u[:, 0].cpu().numpy(), want_r) < 2e-6
+
+
+@pytest.mark.parametrize('name', ['cfg1', 'vec_small', 'odd_scalar'])
+def test_abbe_parity(oi, name):
+    meta, a = load(name)
+    sr, sc, po, nm = build(meta, a)
+    img, pim = oi.CalculateAbbeImage(sr, sc, po, nm)
+    got = img.Intensity.numpy()
+    assert got.shape == a['abbe'].shape
+    assert rel_err(got, O.abbe(sr, sc, po, nm)) < FP32_VS_FP64
+    assert rel_err(got, a['abbe']) < FP32_VS_REF
+    np.testing.assert_array_equal(np.isnan(pim.numpy()), np.isnan(a['abbe_pupil']))
+    ok = ~np.isnan(a['abbe_pupil'])
+    assert rel_err(pim.numpy()[ok], a['abbe_pupil'][ok]) < 1e-5
+
+
+def test_socs_with_reference_kernels(oi):
+    meta, a = load('vec_small')
+    sr, sc, po, nm = build(meta, a)
+    got, _ = oi.CalculateAerialImage_SOCS(sc, torch.from_numpy(a['kernels']), sr, po)
+    assert rel_err(got.numpy(), a['socs']) < FP32_VS_REF
+    assert rel_err(got.numpy(), O.socs(sc, a['kernels'].astype(np.complex128), sr, po)) < FP32_VS_FP64
+
+
+@pytest.mark.parametrize('name', ['vec_small', 'odd_scalar', 'cfg3_small'])
+def test_hopkins_parity(oi, name):
+    meta, a = load(name)
+    sr, sc, po, nm = build(meta, a)
+    img, _ = oi.CalculateHopkinsImage(sr, sc, po, nm)
+    assert rel_err(img.Intensity.numpy(), a['hopkins']) < FP32_VS_REF
+
+
+def test_tcc_fp64(oi):
+    meta, a = load('vec_small')
+    sr, sc, po, nm = build(meta, a)
+    T, fg = oi.CalculateTCCMatrix(sr, [meta['Period_Y'], meta['Period_X']], po, meta['focus'][0], nm)
+    assert T.dtype == torch.complex128 and list(fg) == list(a['fg'])
+    To, _ = O.tcc(sr, [meta['Period_Y'], meta['Period_X']], po, meta['focus'][0], nm)
+    assert rel_err(T.cpu().numpy(), To) < 1e-12
+    assert rel_err(T.cpu().numpy(), a['tcc']) < 2e-6
+    K = oi.DecomposeTCC_SOCS(T, fg, [sc.ScatterField.shape[1], sc.ScatterField.shape[0]], nm)
+    Ko = O.decompose(To, fg, [sc.ScatterField.shape[1], sc.ScatterField.shape[0]], nm)
+    assert K.shape == Ko.shape
+    # same subspace: the rank-K TCC sum_k K_k K_k^H agrees (kernel phases are arbitrary)
+    kg, ko = K.cpu().numpy().reshape(-1, K.shape[2]), Ko.reshape(-1, Ko.shape[2])
+    assert rel_err(kg @ kg.conj().T, ko @ ko.conj().T) < 1e-6
+
+
+def test_tcc_cfg3_spectrum(oi):
+    from opticalimaging_b200 import workloads as W
+    meta, a = load('cfg3_tcc')
+    sr, po, nm = W.config3_optics()
+    T, fg = oi.CalculateTCCMatrix(sr, [2048, 2048], po, 0.0, nm)
+    lam = torch.linalg.eigvalsh(T).flip(0)[:64].cpu().numpy()
+    np.testing.assert_allclose(lam, a['sv'], rtol=0, atol=1e-5 * lam[0])
+    assert abs(float(torch.real(torch.trace(T))) - meta['trace']) < 1e-5 * meta['trace']
+
+
+def test_floquet_optimized_form(oi):
+    meta, a = load('floquet')
+
+    class Nm:
+        pass
+    nm = Nm()
+    for k in ('ScatterOrder_X', 'ScatterOrder_Y', 'ScatterGrid_X', 'ScatterGrid_Y'):
+        setattr(nm, k, meta[k])
+    got = oi.CalculateSOCS(torch.from_numpy(a['floquet']), torch.from_numpy(a['kernels']), nm)
+    assert rel_err(got.numpy(), a['image']) < FP32_VS_REF
+
+
+def test_spectrum_api(oi):
+    from opticalimaging_b200.params import Projection, Scatter, Source
+    meta, a = load('spectrum')
+    sc, po, sr = Scatter(), Projection(), Source()
+    sc.Period_X, sc.Period_Y, sc.ScatterField = meta['Period_X'], meta['Period_Y'], torch.from_numpy(a['field'])
+    po.NA, sr.Wavelength = meta['NA'], meta['Wavelength']
+    hk, f, g, pim = sc.CalculateSpectrum(po, sr)
+    assert rel_err(hk.numpy(), a['hk']) < 2e-6
+    np.testing.assert_array_equal(f.numpy(), a['f'])
+    np.testing.assert_array_equal(np.isnan(pim.numpy()), np.isnan(a['pupil']))
+
+
+def test_raw_optics_nan_with_warning(oi):
+    meta, a = load('raw_nan')
+    sr, sc, po, nm = build(meta, a)
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter('always')
+        img, _ = oi.CalculateAbbeImage(sr, sc, po, nm)
+    assert np.isnan(img.Intensity.numpy()).all()
+    assert any(issubclass(x.category, RuntimeWarning) for x in w)
+
+
+def test_batched_socs_matches_single(oi):
+    """SocsKernels.image on a batch (float32 and uint8 masks) equals the per-clip drop-in call."""
+    from opticalimaging_b200 import workloads as W
+    from opticalimaging_b200.params import Scatter
+    sr, po, nm = W.config3_optics(order=8)
+    T, fg = oi.CalculateTCCMatrix(sr, [2048, 2048], po, 0.0, nm)
+    sk = oi.socs_kernels_from_tcc(T, fg, [256, 256], nm)
+    masks = W.manhattan_masks(5, 256, 2048.0, seed=9)
+    md = torch.from_numpy(masks).cuda()
+    batch = sk.image(md)
+    batch_u8 = sk.image(md.to(torch.uint8))
+    for i in range(5):
+        sc = Scatter()
+        sc.Period_X = sc.Period_Y = 2048
+        sc.ScatterField = W.thin_field(masks[i])
+        one, _ = oi.CalculateAerialImage_SOCS(sc, sk, sr, po)
+        assert rel_err(batch[i].cpu().numpy(), one.numpy()) < 1e-6
+        assert rel_err(batch_u8[i].cpu().numpy(), one.numpy()) < 1e-6
+        if i == 0:
+            ref = O.socs(sc, oi.DecomposeTCC_SOCS(T, fg, [256, 256], nm).cpu().numpy().astype(np.complex128), sr, po)
+            assert rel_err(one.numpy(), ref) < FP32_VS_FP64
+
+
+@pytest.mark.parametrize('ny,nx', [(17, 23), (64, 64), (33, 40)])
+def test_small_and_odd_grids_single_point(oi, ny, nx):
+    """Edge cases: tiny odd grids, a single source point on axis (ideal low-pass), K=1."""
+    from opticalimaging_b200.params import Numerics, Projection, Scatter, Source
+    sr, po, nm, sc = Source(), Projection(), Numerics(), Scatter()
+    sr.Shape, sr.PntNum = 'pixel', 3
+    c = torch.linspace(-1, 1, 3)
+    sr.SPointX, sr.SPointY = torch.meshgrid(c, c, indexing='ij')
+    v = torch.zeros(3, 3)
+    v[0, 1] = 1.0   # one off-centre point (the centre is always zeroed)
+    sr.SPointValue = v
+    po.NA, po.IndexImage, po.Magnification = 0.8, 1.0, 1.0
+    sr.Wavelength = 200.0
+    nm.ImageCalculationMode = 'scalar'
+    sc.Period_X, sc.Period_Y = 10.0 * nx, 10.0 * ny
+    rng = np.random.default_rng(ny * nx)
+    f = np.zeros((ny, nx, 3), np.complex64)
+    f[:, :, 0] = rng.random((ny, nx)) > 0.5
+    sc.ScatterField = torch.from_numpy(f)
+    img, _ = oi.CalculateAbbeImage(sr, sc, po, nm)
+    assert rel_err(img.Intensity.numpy(), O.abbe(sr, sc, po, nm)) < FP32_VS_FP64
+    nm.Hopkins_SettingType, nm.Hopkins_Order = 'order', 1
+    h, _ = oi.CalculateHopkinsImage(sr, sc, po, nm)
+    assert rel_err(h.Intensity.numpy(), O.hopkins(sr, sc, po, nm)) < FP32_VS_FP64
+
+
+def test_clear_field_is_uniform(oi):
+    """Known answer: a clear mask (h = 1) gives the uniform intensity n * sum_j w_j |P_j(0)|^2 / sum w = n."""
+    from opticalimaging_b200 import workloads as W
+    sr, sc, po, nm = W.config1()
+    sc.ScatterField = W.thin_field(np.ones((256, 256), np.float32))
+    img, _ = oi.CalculateAbbeImage(sr, sc, po, nm)
+    np.testing.assert_allclose(img.Intensity.numpy(), 1.0, rtol=0, atol=2e-6)
