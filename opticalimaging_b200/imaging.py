@@ -114,11 +114,19 @@ def _pupil_image(scatter, projector, source, h, dev):
 
 
 def _spectrum_band(h, band: Band, scale, dev):
-    """Centred spectrum on `band` of a [Ny, Nx, C] complex64 device field -> [br, bc, C]."""
+    """Centred spectrum Hk on `band` of a [Ny, Nx, C] complex64 device field -> [br, bc, C].
+
+    The engine's band spectrum has its origin at pixel 0; the reference's centred spectrum has it at pixel
+    N//2 (ifftshift before the transform, Scatter.py:20), i.e. an extra phase exp(-2 pi i m (N//2)/N) per axis.
+    The phase cancels in every intensity, so only the spectrum outputs apply it.
+    """
     ny, nx, nch = h.shape
     plan = Plan.get(ny, nx, band, dev)
     c = band_spectrum(h.unsqueeze(0), N.FIELD_COMPLEX_C64, plan, nch=nch, scale=scale)
-    return c[0].permute(1, 2, 0)
+    mr = torch.arange(band.m0r, band.m0r + band.br, dtype=torch.float64)
+    mc = torch.arange(band.m0c, band.m0c + band.bc, dtype=torch.float64)
+    ph = torch.exp(-2j * torch.pi * ((mr * (ny // 2) % ny / ny)[:, None] + (mc * (nx // 2) % nx / nx)[None, :]))
+    return c[0].permute(1, 2, 0) * ph.to(dev, torch.complex64)[:, :, None]
 
 
 def calculate_spectrum(scatter, projector, source):

@@ -46,6 +46,7 @@ def build(meta, arrays):
 
 def rel_err(a, b):
     """max |a - b| / max |b|: error relative to the peak of the reference image."""
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
+    a, b = np.asarray(a), np.asarray(b)
+    dt = np.complex128 if (np.iscomplexobj(a) or np.iscomplexobj(b)) else np.float64
+    a, b = a.astype(dt), b.astype(dt)
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))

@@ -35,16 +35,15 @@ def test_band_spectrum_matches_numpy(oi):
         h = (rng.standard_normal((2, ny, nx, 3)) + 1j * rng.standard_normal((2, ny, nx, 3))).astype(np.complex64)
         plan = E.Plan.get(ny, nx, band, dev)
         got = E.band_spectrum(torch.from_numpy(h).to(dev), N.FIELD_COMPLEX_C64, plan, nch=3).cpu().numpy()
-        full = np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(h.astype(np.complex128), axes=(1, 2)), axes=(1, 2)),
-                               axes=(1, 2))
-        rows = np.arange(band.m0r, band.m0r + band.br) + ny // 2
-        cols = np.arange(band.m0c, band.m0c + band.bc) + nx // 2
+        # header definition: c(m) = 1/(ny nx) sum h exp(+2 pi i m.y/N), origin at pixel 0 (= ifft2 at m mod N)
+        full = np.fft.ifft2(h.astype(np.complex128), axes=(1, 2))
+        rows = np.arange(band.m0r, band.m0r + band.br) % ny
+        cols = np.arange(band.m0c, band.m0c + band.bc) % nx
         want = full[:, rows][:, :, cols].transpose(0, 3, 1, 2)
         assert rel_err(got, want) < 2e-6
         # real and uint8 kinds of the same data
         r = (rng.random((3, ny, nx)) > 0.5)
-        want_r = np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(r.astype(np.float64), axes=(1, 2)), axes=(1, 2)),
-                                 axes=(1, 2))[:, rows][:, :, cols]
+        want_r = np.fft.ifft2(r.astype(np.float64), axes=(1, 2))[:, rows][:, :, cols]
         got_f = E.band_spectrum(torch.from_numpy(r.astype(np.float32)).to(dev), N.FIELD_REAL_F32, plan)
         got_u = E.band_spectrum(torch.from_numpy(r.astype(np.uint8)).to(dev), N.FIELD_U8, plan)
         assert rel_err(got_f[:, 0].cpu().numpy(), want_r) < 2e-6
@@ -196,4 +195,4 @@ def test_clear_field_is_uniform(oi):
     sr, sc, po, nm = W.config1()
     sc.ScatterField = W.thin_field(np.ones((256, 256), np.float32))
     img, _ = oi.CalculateAbbeImage(sr, sc, po, nm)
-    np.testing.assert_allclose(img.Intensity.numpy(), 1.0, rtol=0, atol=2e-6)
+    np.testing.assert_allclose(img.Intensity.numpy(), 1.0, rtol=0, atol=5e-6)
