@@ -31,7 +31,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "aerial images/s + p99 ms (1024², SOCS-24), served vs plain, err≤1e-4 vs FP64"
 UNIT = "images/s"
-BATCH, N_PIX, PERIOD, ORDER = 64, 1024, 2048.0, 24
+N_PIX, PERIOD, ORDER = 1024, 2048.0, 24
+BATCH = 64
 WORKLOAD = ("config 3: SOCS-24 from the vector TCC of an annular 0.7/0.95 source (PntNum 41, 2048 nm period, "
             "immersion-mapped optics), batches of 64 binary Manhattan clips 1024x1024 at 2 nm/pixel (~35% fill)")
 
@@ -312,7 +313,10 @@ def main():
     ap.add_argument('--impl', default='engine', choices=['engine', 'reference'])
     ap.add_argument('--cpu-budget', type=float, default=15.0)
     ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--batch', type=int, default=64, help='clips per step (64 in the benchmark configuration)')
     args = ap.parse_args()
+    global BATCH
+    BATCH = args.batch
     world, rank, local = dist_setup()
     try:
         if args.impl == 'reference':
