@@ -13,6 +13,8 @@
  *                                                                             CalculateAerialImage_SOCS.py:10)
  *   oi_tcc_pupils64       <- the shifted-pupil matrix of CalculateTCCMatrix  (CalculateTCCMatrix.py:17-51)
  *   oi_tcc_assemble64     <- GetTCCMatrix                                    (CalculateTCCMatrix.py:58-75)
+ *   oi_band_spectrum_fft / oi_coarse_to_image_fft
+ *                         <- the same two stages in FFT form (power-of-two grids 256..2048)
  *   oi_twiddle            <- (no counterpart: fills the phase tables the transforms read)
  *
  * Conventions
@@ -110,6 +112,24 @@ OI_API int oi_coherent_coarse(const void* band, int batch, int nch, int br, int 
 OI_API int oi_coarse_to_image(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc,
                        const void* gr, const void* sy, const void* sx, int ny, int nx, void* scratch,
                        float* out, void* stream);
+
+/*
+ * FFT form of the two N-point transforms (grids of 256, 512, 1024 or 2048 per axis).  oi_fft_supported(ny, nx)
+ * returns 1 when both axes qualify.
+ *
+ * oi_band_spectrum_fft: as oi_band_spectrum for real float32 / uint8 masks [batch][ny][nx], band rows
+ *   m0r .. m0r+br-1 and columns m0c .. m0c+bc-1 (2 max|m_c| < nx, br <= ny).  wn_x / wn_y: oi_twiddle(1, n, 1,
+ *   0, n, +1) for n = nx / ny.  scratch: float2 [batch * bc * ny].  band: float2 [batch][br][bc].
+ * oi_coarse_to_image_fft: as oi_coarse_to_image (same gc, gr tables), with the y and x syntheses done as
+ *   pruned inverse FFTs.  scratch_ihat: float2 [count * (2br-1) * bc]; scratch_v: float2 [count * bc * ny].
+ */
+OI_API int oi_fft_supported(int ny, int nx);
+OI_API int oi_band_spectrum_fft(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c,
+                                int bc, const void* wn_x, const void* wn_y, float scale, void* scratch, void* band,
+                                void* stream);
+OI_API int oi_coarse_to_image_fft(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc,
+                                  const void* gr, const void* wn_y, const void* wn_x, int ny, int nx,
+                                  void* scratch_ihat, void* scratch_v, float* out, void* stream);
 
 /*
  * Shifted pupil matrix of the TCC (CalculateTCCMatrix.py:17-51), FP64, scaled for a Gram product:

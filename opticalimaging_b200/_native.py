@@ -23,6 +23,9 @@ _SIGS = {
     'oi_coarse_to_image': [_vp, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp],
     'oi_tcc_pupils64': [_vp, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _d, _vp, _i, _vp, _d, _d, _d, _d, _vp, _vp],
     'oi_tcc_assemble64': [_vp, _i, _i, _i, _vp, _vp],
+    'oi_fft_supported': [_i, _i],
+    'oi_band_spectrum_fft': [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],
+    'oi_coarse_to_image_fft': [_vp, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp],
 }
 
 FIELD_REAL_F32, FIELD_COMPLEX_C64, FIELD_U8 = 0, 1, 2
@@ -69,7 +72,7 @@ def call(name, *args):
     """Call entry point `name`; raise NativeError with the library's message on a non-zero status."""
     lib = load()
     rc = getattr(lib, name)(*args)
-    if rc != 0:
+    if rc < 0:
         msg = lib.oi_last_error().decode(errors='replace')
         raise NativeError(f'{name} failed ({rc}): {msg}')
 

@@ -1,0 +1,444 @@
+// FFT form of the two N-point transforms of the imaging path, FP32 on the CUDA cores:
+//   forward  mask -> band spectrum      (Scatter.CalculateSpectrum, Scatter.py:10-35, on the band only)
+//   inverse  intensity spectrum -> image (the final synthesis of CalculateAerialImage_SOCS.py:7-10)
+//
+// Four-step decomposition N = 32 * N1 (N1 = 8, 16, 32, 64 for N = 256 .. 2048), x = n1 + N1 n2, k = k2 + 32 k1:
+//   X[k2 + 32 k1] = sum_n1 W_N1^{k1 n1} W_N^{k2 n1} [ sum_n2 x[n1 + N1 n2] W_32^{k2 n2} ]
+// Each of the N1 threads of a group owns one n1 and runs the 32-point transform in registers; the groups
+// exchange through shared memory.  Only the band is wanted, so:
+//   forward: the outer N1-term sum is evaluated for the band bins only (59 of 1024 at configuration 3);
+//   inverse: the input is zero outside the band, so the first N1-term stage sums the few non-zero k1 only.
+// Real rows travel in pairs as one complex row (x = a + i b); the forward pass separates the two spectra,
+// the inverse pass builds one Hermitian spectrum per row so that the real and imaginary parts of one complex
+// transform are the two output rows.
+//
+// Memory: the forward row pass reads each mask row once (coalesced: thread n1 reads x[n1 + N1 n2]) and writes
+// the band columns transposed, [b][ic][y], so the column pass reads contiguous columns; the inverse passes
+// write [b][qc][y] then rows [b][y][x], again coalesced.
+#include "oi_common.cuh"
+#include <cstdint>
+
+namespace oi {
+
+// cos / sin of 2 pi t / 32 for t = 0..15 (exact decimal expansions of the standard values)
+__host__ __device__ constexpr float c32(int t) {
+  return t == 0 ? 1.0f : t == 1 ? 0.980785280403230449f : t == 2 ? 0.923879532511286756f
+       : t == 3 ? 0.831469612302545237f : t == 4 ? 0.707106781186547524f : t == 5 ? 0.555570233019602225f
+       : t == 6 ? 0.382683432365089772f : t == 7 ? 0.195090322016128268f : t == 8 ? 0.0f
+       : t == 9 ? -0.195090322016128268f : t == 10 ? -0.382683432365089772f : t == 11 ? -0.555570233019602225f
+       : t == 12 ? -0.707106781186547524f : t == 13 ? -0.831469612302545237f : t == 14 ? -0.923879532511286756f
+       : -0.980785280403230449f;
+}
+__host__ __device__ constexpr float s32(int t) { return t <= 8 ? c32(8 - t) : c32(t - 8); }
+__host__ __device__ constexpr int bitrev5(int i) {
+  return ((i & 1) << 4) | ((i & 2) << 2) | (i & 4) | ((i & 8) >> 2) | ((i & 16) >> 4);
+}
+
+// d * exp(SIGN 2 pi i t / 32), t a compile-time constant after unrolling
+template <int SIGN>
+__device__ __forceinline__ float2 rot32(float2 d, int t) {
+  if (t == 0) return d;
+  if (t == 8) return SIGN > 0 ? make_float2(-d.y, d.x) : make_float2(d.y, -d.x);
+  const float c = c32(t), s = SIGN * s32(t);
+  return make_float2(d.x * c - d.y * s, d.x * s + d.y * c);
+}
+
+// In-register 32-point DFT, X[k] = sum_n v[n] exp(SIGN 2 pi i k n / 32), decimation in frequency.
+// Natural-order input; on return v[i] = X[bitrev5(i)].
+template <int SIGN>
+__device__ __forceinline__ void fft32(float2 (&v)[32]) {
+#pragma unroll
+  for (int len = 32; len >= 2; len >>= 1) {
+    const int half = len >> 1, step = 32 / len;
+#pragma unroll
+    for (int blk = 0; blk < 32; blk += len) {
+#pragma unroll
+      for (int j = 0; j < half; ++j) {
+        float2 u = v[blk + j], w = v[blk + j + half];
+        v[blk + j] = make_float2(u.x + w.x, u.y + w.y);
+        v[blk + j + half] = rot32<SIGN>(make_float2(u.x - w.x, u.y - w.y), j * step);
+      }
+    }
+  }
+}
+
+// exp(SIGN 2 pi i j / N) from the +1 table wn[j] = exp(+2 pi i j / N)
+template <int SIGN>
+__device__ __forceinline__ float2 wn_get(const float2* wn, int j) {
+  float2 w = wn[j];
+  return SIGN > 0 ? w : make_float2(w.x, -w.y);
+}
+
+template <int KIND> __device__ __forceinline__ float load_real(const void* f, long long i);
+template <> __device__ __forceinline__ float load_real<OI_FIELD_REAL_F32>(const void* f, long long i) {
+  return __ldg((const float*)f + i);
+}
+template <> __device__ __forceinline__ float load_real<OI_FIELD_U8>(const void* f, long long i) {
+  return (float)__ldg((const uint8_t*)f + i);
+}
+
+// Shared by the four kernels: stage 2 + transpose.  z holds the bit-reversed 32-point result of thread n1;
+// multiply by W_N^{n1 k2} and store to ys[k2][n1] (row stride N1 + 1).
+template <int SIGN, int N1>
+__device__ __forceinline__ void twiddle_store(const float2 (&z)[32], const float2* wn, int n1, float2* ys) {
+  constexpr int N = 32 * N1;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const int k2 = bitrev5(i);
+    ys[k2 * (N1 + 1) + n1] = cmul(z[i], wn_get<SIGN>(wn, (n1 * k2) & (N - 1)));
+  }
+}
+
+// Z[k] = sum_n1 W_N1^{k1 n1} ys[k2][n1]  (forward outer stage for one bin k = k2 + 32 k1)
+template <int SIGN, int N1>
+__device__ __forceinline__ float2 outer_bin(const float2* ys, const float2* wn, int k) {
+  constexpr int N = 32 * N1;
+  const int k2 = k & 31, k1 = k >> 5;
+  const float2* row = ys + k2 * (N1 + 1);
+  float2 acc = make_float2(0.f, 0.f);
+#pragma unroll 8
+  for (int n1 = 0; n1 < N1; ++n1) cfma(acc, row[n1], wn_get<SIGN>(wn, (32 * k1 * n1) & (N - 1)));
+  return acc;
+}
+
+// --------------------------------------------------------------------------------- forward, rows
+// field rows [nrows = batch*ny][N] (real or u8) -> t[b][ic][y], ic over the band m0c .. m0c+bc-1.
+// Z is evaluated on the contiguous frequency range u0 .. u0+nu-1 that holds the band and its mirror.
+template <int N1, int KIND>
+__global__ void __launch_bounds__(256) fft_rows_fwd_kernel(const void* __restrict__ field, long long nrows, int ny,
+                                                           const float2* __restrict__ wn_g, int m0c, int bc, int u0,
+                                                           int nu, float2* __restrict__ t) {
+  constexpr int N = 32 * N1, G = 256 / N1;  // G row pairs per block
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* wn = (float2*)smem_raw;             // [N]
+  float2* ys = wn + N;                        // [G][32][N1+1]
+  float2* zs = ys + G * 32 * (N1 + 1);        // [G][nu]
+  const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
+  for (int j = tid; j < N; j += 256) wn[j] = wn_g[j];
+  const long long r0 = (long long)blockIdx.x * (2 * G) + 2 * g;
+  float2 z[32];
+  if (r0 + 1 < nrows) {
+    const long long o0 = r0 * N, o1 = o0 + N;
+#pragma unroll
+    for (int n2 = 0; n2 < 32; ++n2)
+      z[n2] = make_float2(load_real<KIND>(field, o0 + n1 + N1 * n2), load_real<KIND>(field, o1 + n1 + N1 * n2));
+  } else {
+#pragma unroll
+    for (int n2 = 0; n2 < 32; ++n2) z[n2] = make_float2(0.f, 0.f);
+  }
+  fft32<+1>(z);
+  __syncthreads();  // wn ready
+  float2* yg = ys + g * 32 * (N1 + 1);
+  twiddle_store<+1, N1>(z, wn, n1, yg);
+  __syncthreads();
+  float2* zg = zs + g * nu;
+  for (int q = n1; q < nu; q += N1) zg[q] = outer_bin<+1, N1>(yg, wn, (u0 + q) & (N - 1));
+  __syncthreads();
+  // separate the two real rows and write t[b][ic][y] with y fastest (2G consecutive rows of one image)
+  const long long rblk = (long long)blockIdx.x * (2 * G);
+  for (int e = tid; e < bc * 2 * G; e += 256) {
+    const int ic = e / (2 * G), rr = e % (2 * G), gg = rr >> 1;
+    const long long r = rblk + rr;
+    if (r >= nrows) continue;
+    const int m = m0c + ic;
+    const float2 zp = zs[gg * nu + (m - u0)], zm = zs[gg * nu + (-m - u0)];
+    float2 v;
+    if ((rr & 1) == 0) v = make_float2(0.5f * (zp.x + zm.x), 0.5f * (zp.y - zm.y));   // (Z(m) + conj Z(-m)) / 2
+    else v = make_float2(0.5f * (zp.y + zm.y), -0.5f * (zp.x - zm.x));               // (Z(m) - conj Z(-m)) / 2i
+    const long long b = r / ny;
+    const int y = (int)(r - b * ny);
+    t[(b * bc + ic) * (long long)ny + y] = v;
+  }
+}
+
+// ------------------------------------------------------------------------------ forward, columns
+// t[b][ic][y] (N = ny) -> band[b][ir][ic] = scale * sum_y t exp(+2 pi i (m0r+ir) y / ny)
+template <int N1>
+__global__ void __launch_bounds__(256) fft_cols_fwd_kernel(const float2* __restrict__ t, long long ncols, int bc,
+                                                           const float2* __restrict__ wn_g, int m0r, int br,
+                                                           float scale, float2* __restrict__ band) {
+  constexpr int N = 32 * N1, G = 256 / N1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* wn = (float2*)smem_raw;
+  float2* ys = wn + N;
+  const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
+  for (int j = tid; j < N; j += 256) wn[j] = wn_g[j];
+  const long long col = (long long)blockIdx.x * G + g;
+  float2 z[32];
+  if (col < ncols) {
+    const float2* src = t + col * N;
+#pragma unroll
+    for (int n2 = 0; n2 < 32; ++n2) z[n2] = src[n1 + N1 * n2];
+  } else {
+#pragma unroll
+    for (int n2 = 0; n2 < 32; ++n2) z[n2] = make_float2(0.f, 0.f);
+  }
+  fft32<+1>(z);
+  __syncthreads();
+  float2* yg = ys + g * 32 * (N1 + 1);
+  twiddle_store<+1, N1>(z, wn, n1, yg);
+  __syncthreads();
+  if (col >= ncols) return;
+  const long long b = col / bc;
+  const int ic = (int)(col - b * bc);
+  for (int ir = n1; ir < br; ir += N1) {
+    float2 v = outer_bin<+1, N1>(yg, wn, (m0r + ir) & (N - 1));
+    band[(b * br + ir) * (long long)bc + ic] = make_float2(v.x * scale, v.y * scale);
+  }
+}
+
+// --------------------------------------------------------------------------- inverse, shared part
+// Thread n1 of a group: z[k2] = W_N^{-k2 n1} sum_{k1} coef(k2 + 32 k1) W_N1^{-k1 n1} over the non-zero
+// coefficients, which sit at frequencies q in [-qmax, qmax] (index q mod N); coef(q) = cq[q + qmax].
+template <int N1>
+__device__ __forceinline__ void inverse_gather(float2 (&z)[32], const float2* cq, int qmax, const float2* wn,
+                                               int n1) {
+  constexpr int N = 32 * N1;
+#pragma unroll
+  for (int k2 = 0; k2 < 32; ++k2) {
+    float2 acc = make_float2(0.f, 0.f);
+    for (int k1 = 0; k2 + 32 * k1 <= qmax; ++k1)  // q = k2 + 32 k1 >= 0
+      cfma(acc, cq[k2 + 32 * k1 + qmax], wn_get<-1>(wn, (32 * k1 * n1) & (N - 1)));
+    for (int k1 = N1 - 1; k1 > 0 && k2 + 32 * k1 >= N - qmax; --k1)  // q = k2 + 32 k1 - N < 0
+      cfma(acc, cq[k2 + 32 * k1 - N + qmax], wn_get<-1>(wn, (32 * k1 * n1) & (N - 1)));
+    z[k2] = cmul(acc, wn_get<-1>(wn, (k2 * n1) & (N - 1)));
+  }
+  fft32<-1>(z);
+}
+
+// ------------------------------------------------------------------------------ inverse, columns
+// ihat[i][jr][qc] (qr = jr - (br-1)) -> v[i][qc][y] = sum_qr ihat exp(-2 pi i qr y / ny)
+template <int N1>
+__global__ void __launch_bounds__(256) fft_cols_inv_kernel(const float2* __restrict__ ihat, long long ncols, int br,
+                                                           int bc, const float2* __restrict__ wn_g,
+                                                           float2* __restrict__ v) {
+  constexpr int N = 32 * N1, G = 256 / N1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* wn = (float2*)smem_raw;
+  const int nq = 2 * br - 1;
+  float2* cs = wn + N;  // [G][nq]
+  const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
+  for (int j = tid; j < N; j += 256) wn[j] = wn_g[j];
+  const long long col0 = (long long)blockIdx.x * G;
+  for (int e = tid; e < G * nq; e += 256) {
+    const int jr = e / G, gg = e % G;
+    const long long col = col0 + gg;
+    float2 c = make_float2(0.f, 0.f);
+    if (col < ncols) {
+      const long long i = col / bc;
+      const int qc = (int)(col - i * bc);
+      c = ihat[(i * nq + jr) * (long long)bc + qc];
+    }
+    cs[gg * nq + jr] = c;
+  }
+  __syncthreads();
+  const long long col = col0 + g;
+  float2 z[32];
+  inverse_gather<N1>(z, cs + g * nq, br - 1, wn, n1);
+  if (col >= ncols) return;
+  float2* dst = v + col * N;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) dst[n1 + N1 * bitrev5(i)] = z[i];
+}
+
+// --------------------------------------------------------------------------------- inverse, rows
+// v[i][qc][y] (qc = 0..bc-1, qc > 0 doubled) -> out[i][y][x] = sum_qc Re(v exp(-2 pi i qc x / nx))
+template <int N1>
+__global__ void __launch_bounds__(256) fft_rows_inv_kernel(const float2* __restrict__ v, long long nrows, int ny,
+                                                           int bc, const float2* __restrict__ wn_g,
+                                                           float* __restrict__ out) {
+  constexpr int N = 32 * N1, G = 256 / N1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* wn = (float2*)smem_raw;
+  const int nq = 2 * bc - 1;
+  float2* vs = wn + N;           // [bc][2G]
+  float2* cs = vs + bc * 2 * G;  // [G][nq]
+  const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
+  for (int j = tid; j < N; j += 256) wn[j] = wn_g[j];
+  const long long rblk = (long long)blockIdx.x * (2 * G);
+  for (int e = tid; e < bc * 2 * G; e += 256) {
+    const int qc = e / (2 * G), rr = e % (2 * G);
+    const long long r = rblk + rr;
+    float2 c = make_float2(0.f, 0.f);
+    if (r < nrows) {
+      const long long i = r / ny;
+      const int y = (int)(r - i * ny);
+      c = v[(i * bc + qc) * (long long)ny + y];
+    }
+    vs[e] = c;
+  }
+  __syncthreads();
+  // Hermitian spectra of the row pair packed as F_a + i F_b, q in [-(bc-1), bc-1]
+  for (int e = tid; e < G * nq; e += 256) {
+    const int gg = e / nq, j = e % nq, q = j - (bc - 1), aq = q < 0 ? -q : q;
+    float2 a = vs[aq * 2 * G + 2 * gg], b = vs[aq * 2 * G + 2 * gg + 1];
+    const float h = aq == 0 ? 1.0f : 0.5f;
+    if (q < 0) {
+      a.y = -a.y;
+      b.y = -b.y;
+    }
+    cs[e] = make_float2(h * (a.x - b.y), h * (a.y + b.x));  // h (a + i b)
+  }
+  __syncthreads();
+  const long long r0 = rblk + 2 * g;
+  float2 z[32];
+  inverse_gather<N1>(z, cs + g * nq, bc - 1, wn, n1);
+  if (r0 >= nrows) return;
+  float* o0 = out + r0 * N;
+  float* o1 = o0 + N;
+  const bool second = r0 + 1 < nrows;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const int x = n1 + N1 * bitrev5(i);
+    o0[x] = z[i].x;
+    if (second) o1[x] = z[i].y;
+  }
+}
+
+template <int N1>
+static size_t smem_rows_fwd(int nu) { return sizeof(float2) * (32 * N1 + (256 / N1) * 32 * (N1 + 1) + (256 / N1) * nu); }
+template <int N1>
+static size_t smem_cols_fwd() { return sizeof(float2) * (32 * N1 + (256 / N1) * 32 * (N1 + 1)); }
+
+template <typename K>
+static int set_smem(K kern, size_t bytes, const char* what) {
+  if (bytes > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return fail(OI_ECUDA, "%s: smem attribute: %s", what, cudaGetErrorString(e));
+  }
+  return OI_OK;
+}
+
+template <int N1>
+static int band_fft(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c, int bc,
+                    const float2* wn_x, const float2* wn_y, float scale, float2* t, float2* band, cudaStream_t s) {
+  // row transforms have length nx = 32 * N1; the column kernel picks its own N1 for ny
+  const int u0 = min(m0c, -(m0c + bc - 1)), u1 = max(m0c + bc - 1, -m0c), nu = u1 - u0 + 1;
+  constexpr int G = 256 / N1;
+  const long long nrows = (long long)batch * ny;
+  size_t smem = smem_rows_fwd<N1>(nu);
+  int rc;
+  if (kind == OI_FIELD_U8) {
+    rc = set_smem(fft_rows_fwd_kernel<N1, OI_FIELD_U8>, smem, "oi_band_spectrum_fft/rows");
+    if (rc) return rc;
+    fft_rows_fwd_kernel<N1, OI_FIELD_U8><<<(unsigned)ceil_div(nrows, 2 * G), 256, smem, s>>>(
+        field, nrows, ny, wn_x, m0c, bc, u0, nu, t);
+  } else {
+    rc = set_smem(fft_rows_fwd_kernel<N1, OI_FIELD_REAL_F32>, smem, "oi_band_spectrum_fft/rows");
+    if (rc) return rc;
+    fft_rows_fwd_kernel<N1, OI_FIELD_REAL_F32><<<(unsigned)ceil_div(nrows, 2 * G), 256, smem, s>>>(
+        field, nrows, ny, wn_x, m0c, bc, u0, nu, t);
+  }
+  return check_launch("oi_band_spectrum_fft/rows");
+}
+
+template <int N1>
+static int cols_fwd(const float2* t, int batch, int bc, const float2* wn_y, int m0r, int br, float scale,
+                    float2* band, cudaStream_t s) {
+  constexpr int G = 256 / N1;
+  size_t smem = smem_cols_fwd<N1>();
+  int rc = set_smem(fft_cols_fwd_kernel<N1>, smem, "oi_band_spectrum_fft/cols");
+  if (rc) return rc;
+  const long long ncols = (long long)batch * bc;
+  fft_cols_fwd_kernel<N1><<<(unsigned)ceil_div(ncols, G), 256, smem, s>>>(t, ncols, bc, wn_y, m0r, br, scale, band);
+  return check_launch("oi_band_spectrum_fft/cols");
+}
+
+template <int N1>
+static int cols_inv(const float2* ihat, int count, int br, int bc, const float2* wn_y, float2* v, cudaStream_t s) {
+  constexpr int G = 256 / N1;
+  size_t smem = sizeof(float2) * (32 * N1 + G * (2 * br - 1));
+  int rc = set_smem(fft_cols_inv_kernel<N1>, smem, "oi_coarse_to_image_fft/cols");
+  if (rc) return rc;
+  const long long ncols = (long long)count * bc;
+  fft_cols_inv_kernel<N1><<<(unsigned)ceil_div(ncols, G), 256, smem, s>>>(ihat, ncols, br, bc, wn_y, v);
+  return check_launch("oi_coarse_to_image_fft/cols");
+}
+
+template <int N1>
+static int rows_inv(const float2* v, int count, int ny, int bc, const float2* wn_x, float* out, cudaStream_t s) {
+  constexpr int G = 256 / N1;
+  size_t smem = sizeof(float2) * (32 * N1 + bc * 2 * G + G * (2 * bc - 1));
+  int rc = set_smem(fft_rows_inv_kernel<N1>, smem, "oi_coarse_to_image_fft/rows");
+  if (rc) return rc;
+  const long long nrows = (long long)count * ny;
+  fft_rows_inv_kernel<N1><<<(unsigned)ceil_div(nrows, 2 * G), 256, smem, s>>>(v, nrows, ny, bc, wn_x, out);
+  return check_launch("oi_coarse_to_image_fft/rows");
+}
+
+static int n1_of(int n) {
+  switch (n) {
+    case 256: return 8;
+    case 512: return 16;
+    case 1024: return 32;
+    case 2048: return 64;
+  }
+  return 0;
+}
+
+}  // namespace oi
+
+extern "C" int oi_fft_supported(int ny, int nx) {
+  return oi::n1_of(ny) != 0 && oi::n1_of(nx) != 0 ? 1 : 0;
+}
+
+extern "C" int oi_band_spectrum_fft(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c,
+                                    int bc, const void* wn_x, const void* wn_y, float scale, void* scratch,
+                                    void* band, void* stream) {
+  using namespace oi;
+  if (!field || !wn_x || !wn_y || !scratch || !band || batch <= 0 || br <= 0 || bc <= 0)
+    return fail(OI_EINVAL, "oi_band_spectrum_fft: bad arguments");
+  if (kind != OI_FIELD_REAL_F32 && kind != OI_FIELD_U8)
+    return fail(OI_EINVAL, "oi_band_spectrum_fft: real float32 or uint8 masks only (kind=%d)", kind);
+  const int nx1 = n1_of(nx), ny1 = n1_of(ny);
+  if (!nx1 || !ny1) return fail(OI_ERANGE, "oi_band_spectrum_fft: grid %dx%d is not 256..2048, power of 2", ny, nx);
+  const int maxc = max(abs(m0c), abs(m0c + bc - 1));
+  if (2 * maxc >= nx || br > ny)
+    return fail(OI_ERANGE, "oi_band_spectrum_fft: band (%d+%d, %d+%d) too wide for %dx%d", m0r, br, m0c, bc, ny, nx);
+  cudaStream_t s = (cudaStream_t)stream;
+  float2* t = (float2*)scratch;
+  int rc;
+  switch (nx1) {
+    case 8: rc = band_fft<8>(field, kind, batch, ny, nx, m0r, br, m0c, bc, (const float2*)wn_x, (const float2*)wn_y, scale, t, (float2*)band, s); break;
+    case 16: rc = band_fft<16>(field, kind, batch, ny, nx, m0r, br, m0c, bc, (const float2*)wn_x, (const float2*)wn_y, scale, t, (float2*)band, s); break;
+    case 32: rc = band_fft<32>(field, kind, batch, ny, nx, m0r, br, m0c, bc, (const float2*)wn_x, (const float2*)wn_y, scale, t, (float2*)band, s); break;
+    default: rc = band_fft<64>(field, kind, batch, ny, nx, m0r, br, m0c, bc, (const float2*)wn_x, (const float2*)wn_y, scale, t, (float2*)band, s); break;
+  }
+  if (rc) return rc;
+  switch (ny1) {
+    case 8: return cols_fwd<8>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+    case 16: return cols_fwd<16>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+    case 32: return cols_fwd<32>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+    default: return cols_fwd<64>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+  }
+}
+
+
+extern "C" int oi_coarse_to_image_fft(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc,
+                                      const void* gr, const void* wn_y, const void* wn_x, int ny, int nx,
+                                      void* scratch_ihat, void* scratch_v, float* out, void* stream) {
+  using namespace oi;
+  if (!coarse || !gc || !gr || !wn_y || !wn_x || !scratch_ihat || !scratch_v || !out || count <= 0)
+    return fail(OI_EINVAL, "oi_coarse_to_image_fft: bad arguments");
+  const int nx1 = n1_of(nx), ny1 = n1_of(ny);
+  if (!nx1 || !ny1) return fail(OI_ERANGE, "oi_coarse_to_image_fft: grid %dx%d is not 256..2048, power of 2", ny, nx);
+  if (2 * br - 1 > ny || 2 * bc - 1 > nx) return fail(OI_ERANGE, "oi_coarse_to_image_fft: band too wide for grid");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = coarse_spectrum(coarse, count, mr, mc, br, bc, gc, gr, scratch_ihat, s);
+  if (rc) return rc;
+  const float2* ih = (const float2*)scratch_ihat;
+  float2* v = (float2*)scratch_v;
+  switch (ny1) {
+    case 8: rc = cols_inv<8>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+    case 16: rc = cols_inv<16>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+    case 32: rc = cols_inv<32>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+    default: rc = cols_inv<64>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+  }
+  if (rc) return rc;
+  switch (nx1) {
+    case 8: return rows_inv<8>(v, count, ny, bc, (const float2*)wn_x, out, s);
+    case 16: return rows_inv<16>(v, count, ny, bc, (const float2*)wn_x, out, s);
+    case 32: return rows_inv<32>(v, count, ny, bc, (const float2*)wn_x, out, s);
+    default: return rows_inv<64>(v, count, ny, bc, (const float2*)wn_x, out, s);
+  }
+}

@@ -108,6 +108,22 @@ __global__ void __launch_bounds__(256) synth_kernel(const float2* __restrict__ i
   }
 }
 
+int coarse_spectrum(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc, const void* gr,
+                    void* ihat, cudaStream_t s) {
+  if (mr < 2 * br - 1 || mc < 2 * bc - 1)
+    return fail(OI_EINVAL, "coarse grid %dx%d too small for band %dx%d", mr, mc, br, bc);
+  if (mr > 1024 || count > 65535) return fail(OI_ERANGE, "coarse grid mr=%d or count=%d out of range", mr, count);
+  size_t smem = sizeof(float2) * (size_t)mr * SP_QT;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(coarse_spec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail(OI_ECUDA, "coarse spectrum: smem attribute: %s", cudaGetErrorString(e));
+  }
+  dim3 g1((unsigned)ceil_div(bc, SP_QT), (unsigned)count);
+  coarse_spec_kernel<<<g1, 256, smem, s>>>(coarse, mr, mc, br, bc, (const float2*)gc, (const float2*)gr,
+                                           (float2*)ihat);
+  return check_launch("coarse spectrum");
+}
+
 template <int NV>
 static void launch_synth(const float2* ihat, int count, int br, int bc, const float2* sy, const float2* sx, int ny,
                          int nx, float* out, cudaStream_t s) {
@@ -126,18 +142,10 @@ extern "C" int oi_coarse_to_image(const float* coarse, int count, int mr, int mc
     return fail(OI_EINVAL, "oi_coarse_to_image: bad arguments");
   if (mr < 2 * br - 1 || mc < 2 * bc - 1)
     return fail(OI_EINVAL, "oi_coarse_to_image: coarse grid %dx%d too small for band %dx%d", mr, mc, br, bc);
-  if (mr > 1024 || bc > 1024 || nx > 2048 || count > 65535)
+  if (mr > 1024 || bc > 512 || nx > 2048 || count > 65535)
     return fail(OI_ERANGE, "oi_coarse_to_image: sizes out of range (mr=%d bc=%d nx=%d)", mr, bc, nx);
   cudaStream_t s = (cudaStream_t)stream;
-  size_t smem = sizeof(float2) * (size_t)mr * SP_QT;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(coarse_spec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return fail(OI_ECUDA, "oi_coarse_to_image: smem attribute: %s", cudaGetErrorString(e));
-  }
-  dim3 g1((unsigned)ceil_div(bc, SP_QT), (unsigned)count);
-  coarse_spec_kernel<<<g1, 256, smem, s>>>(coarse, mr, mc, br, bc, (const float2*)gc, (const float2*)gr,
-                                           (float2*)scratch);
-  int rc = check_launch("oi_coarse_to_image/spec");
+  int rc = coarse_spectrum(coarse, count, mr, mc, br, bc, gc, gr, scratch, s);
   if (rc) return rc;
   const float2* ih = (const float2*)scratch;
   switch ((nx + 255) / 256) {

@@ -57,6 +57,18 @@ class Band:
     bc: int
 
 
+FORMS = ('fft', 'dft')
+
+
+def fft_supported(ny: int, nx: int, band: Band) -> bool:
+    """The FFT form covers power-of-two grids of 256..2048 per axis with the band inside Nyquist."""
+    lib = N.load()
+    if not lib.oi_fft_supported(ny, nx):
+        return False
+    maxc = max(abs(band.m0c), abs(band.m0c + band.bc - 1))
+    return 2 * maxc < nx and band.br <= ny and 2 * band.br - 1 <= ny and 2 * band.bc - 1 <= nx
+
+
 class Plan:
     """Phase tables for one (output grid, band); cached and shared by every call with the same key."""
 
@@ -77,6 +89,15 @@ class Plan:
         self.gr = t(self.mr, nq, 0, -(b.br - 1), self.mr, +1)  # [mr][2br-1]
         self.sy = t(ny, nq, 0, -(b.br - 1), ny, -1)          # [ny][2br-1] spectrum -> image (y)
         self.sx = t(b.bc, nx, 0, 0, nx, -1)                  # [bc][nx]   spectrum -> image (x)
+        self.fft = fft_supported(ny, nx, band)
+        if self.fft:                                          # exp(+2 pi i j/n), j < n, for the FFT form
+            self.wn_x = t(1, nx, 1, 0, nx, +1)
+            self.wn_y = t(1, ny, 1, 0, ny, +1)
+
+    def use_fft(self, form):
+        if form not in (None,) + FORMS:
+            raise ValueError(f'form must be one of {FORMS}')
+        return self.fft and form != 'dft'
 
     @classmethod
     def get(cls, ny, nx, band: Band, device) -> 'Plan':
@@ -90,11 +111,12 @@ class Plan:
 
 # --------------------------------------------------------------------------------------------- stages
 def band_spectrum(field: torch.Tensor, kind: int, plan: Plan, nch: int = 1, scale: float = 1.0,
-                  scratch: torch.Tensor | None = None) -> torch.Tensor:
+                  scratch: torch.Tensor | None = None, form: str | None = None) -> torch.Tensor:
     """c(m) on the plan's band: [batch, nch, br, bc] complex64.
 
     field: float32 [B, ny, nx] (FIELD_REAL_F32), uint8 [B, ny, nx] (FIELD_U8) or complex64 [B, ny, nx, nch]
     (FIELD_COMPLEX_C64), contiguous on the plan's device.  `scale` multiplies the 1/(ny nx) normalisation.
+    form: 'fft' (default where the grid allows: real or uint8 masks on 256..2048 power-of-two grids) or 'dft'.
     """
     b = plan.band
     batch = field.shape[0]
@@ -102,9 +124,14 @@ def band_spectrum(field: torch.Tensor, kind: int, plan: Plan, nch: int = 1, scal
     if scratch is None or scratch.numel() < need:
         scratch = torch.empty(need, dtype=torch.complex64, device=plan.device)
     band = torch.empty((batch, nch, b.br, b.bc), dtype=torch.complex64, device=plan.device)
-    N.call('oi_band_spectrum', N.ptr(field), kind, batch, plan.ny, plan.nx, nch, b.br, b.bc, N.ptr(plan.wx),
-           N.ptr(plan.wy), float(scale / (plan.ny * plan.nx)), N.ptr(scratch), N.ptr(band),
-           N.stream_handle(plan.device))
+    s = N.stream_handle(plan.device)
+    sc = float(scale / (plan.ny * plan.nx))
+    if plan.use_fft(form) and kind != N.FIELD_COMPLEX_C64 and nch == 1:
+        N.call('oi_band_spectrum_fft', N.ptr(field), kind, batch, plan.ny, plan.nx, b.m0r, b.br, b.m0c, b.bc,
+               N.ptr(plan.wn_x), N.ptr(plan.wn_y), sc, N.ptr(scratch), N.ptr(band), s)
+    else:
+        N.call('oi_band_spectrum', N.ptr(field), kind, batch, plan.ny, plan.nx, nch, b.br, b.bc, N.ptr(plan.wx),
+               N.ptr(plan.wy), sc, N.ptr(scratch), N.ptr(band), s)
     return band
 
 
@@ -116,7 +143,8 @@ def _mark(marks, name):
 
 
 def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tensor, plan: Plan,
-                   pupil_batch_stride: int = 0, out: torch.Tensor | None = None, marks=None) -> torch.Tensor:
+                   pupil_batch_stride: int = 0, out: torch.Tensor | None = None, marks=None,
+                   form: str | None = None) -> torch.Tensor:
     """sum_fields w |IDFT(P .* c)|^2 on the output grid: [batch, nz, ny, nx] float32.
 
     band: [batch, nch, br, bc] complex64; pupils: [nz, nk, br, bc] complex64 (shared by the batch when
@@ -134,8 +162,14 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
     if out is None:
         out = torch.empty((batch, nz, plan.ny, plan.nx), dtype=torch.float32, device=dev)
     ihat = torch.empty(batch * nz * (2 * b.br - 1) * b.bc, dtype=torch.complex64, device=dev)
-    N.call('oi_coarse_to_image', N.ptr(coarse), batch * nz, plan.mr, plan.mc, b.br, b.bc, N.ptr(plan.gc),
-           N.ptr(plan.gr), N.ptr(plan.sy), N.ptr(plan.sx), plan.ny, plan.nx, N.ptr(ihat), N.ptr(out), s)
+    if plan.use_fft(form):
+        v = torch.empty(batch * nz * b.bc * plan.ny, dtype=torch.complex64, device=dev)
+        N.call('oi_coarse_to_image_fft', N.ptr(coarse), batch * nz, plan.mr, plan.mc, b.br, b.bc, N.ptr(plan.gc),
+               N.ptr(plan.gr), N.ptr(plan.wn_y), N.ptr(plan.wn_x), plan.ny, plan.nx, N.ptr(ihat), N.ptr(v),
+               N.ptr(out), s)
+    else:
+        N.call('oi_coarse_to_image', N.ptr(coarse), batch * nz, plan.mr, plan.mc, b.br, b.bc, N.ptr(plan.gc),
+               N.ptr(plan.gr), N.ptr(plan.sy), N.ptr(plan.sx), plan.ny, plan.nx, N.ptr(ihat), N.ptr(out), s)
     _mark(marks, 'coarse_to_image')
     return out
 
@@ -219,11 +253,12 @@ class SocsKernels:
         return cls(kb.to(torch.complex64).contiguous(), band, ny, nx)
 
     def image(self, masks: torch.Tensor, kind: int | None = None, nch: int = 1, scale: float = 1.0,
-              out: torch.Tensor | None = None, marks=None) -> torch.Tensor:
+              out: torch.Tensor | None = None, marks=None, form: str | None = None) -> torch.Tensor:
         """SOCS aerial images of a batch of masks -> [B, ny, nx] float32.
 
         masks: float32 [B, ny, nx] (real transmission), uint8 [B, ny, nx] or complex64 [B, ny, nx, nch].
         `marks`, if a list, receives (stage name, CUDA event) pairs recorded after each native stage.
+        `form` picks the transform form of the two N-point stages: 'fft' (default where supported) or 'dft'.
         """
         if kind is None:
             kind = {torch.float32: N.FIELD_REAL_F32, torch.uint8: N.FIELD_U8,
@@ -231,9 +266,9 @@ class SocsKernels:
         if masks.shape[1] != self.ny or masks.shape[2] != self.nx:
             raise ValueError(f'mask grid {tuple(masks.shape[1:3])} != kernel grid {(self.ny, self.nx)}')
         _mark(marks, 'start')
-        band = band_spectrum(masks.contiguous(), kind, self.plan, nch=nch, scale=scale)
+        band = band_spectrum(masks.contiguous(), kind, self.plan, nch=nch, scale=scale, form=form)
         _mark(marks, 'band_spectrum')
         img = coherent_image(band, self.kernels.unsqueeze(0), self.weights, self.plan,
                              out=None if out is None else out.view(masks.shape[0], 1, self.ny, self.nx),
-                             marks=marks)
+                             marks=marks, form=form)
         return img.view(masks.shape[0], self.ny, self.nx)

@@ -1,0 +1,77 @@
+"""FFT form of the two N-point stages vs numpy and vs the DFT form, on every supported grid size."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import optics64 as O
+from tests.fixtures import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def eng():
+    from opticalimaging_b200 import engine
+    return engine
+
+
+@pytest.mark.parametrize('ny,nx,band', [
+    (256, 256, (-15, 31, -15, 31)),
+    (512, 256, (-20, 29, -7, 30)),      # asymmetric column band: the mirror range is wider than the band
+    (1024, 1024, (-29, 59, -29, 59)),
+    (256, 2048, (-3, 7, -100, 201)),
+    (2048, 512, (-60, 121, -1, 3)),
+])
+def test_band_spectrum_fft(eng, ny, nx, band):
+    from opticalimaging_b200 import _native as N
+    dev = torch.device('cuda')
+    b = eng.Band(*band)
+    plan = eng.Plan.get(ny, nx, b, dev)
+    assert plan.fft
+    rng = np.random.default_rng(ny + nx)
+    m = (rng.random((3, ny, nx)) > 0.6).astype(np.float32)
+    m[1] *= rng.random((ny, nx)).astype(np.float32)          # a grey mask too
+    want = np.fft.ifft2(m.astype(np.float64), axes=(1, 2))
+    rows = np.arange(b.m0r, b.m0r + b.br) % ny
+    cols = np.arange(b.m0c, b.m0c + b.bc) % nx
+    want = want[:, rows][:, :, cols]
+    md = torch.from_numpy(m).to(dev)
+    got = eng.band_spectrum(md, N.FIELD_REAL_F32, plan, form='fft')[:, 0].cpu().numpy()
+    dft = eng.band_spectrum(md, N.FIELD_REAL_F32, plan, form='dft')[:, 0].cpu().numpy()
+    assert rel_err(got, want) < 3e-6
+    assert rel_err(dft, want) < 3e-6
+    u8 = torch.from_numpy((m[[0, 2]] > 0).astype(np.uint8)).to(dev)
+    got8 = eng.band_spectrum(u8, N.FIELD_U8, plan, form='fft')[:, 0].cpu().numpy()
+    assert rel_err(got8, want[[0, 2]]) < 3e-6
+
+
+@pytest.mark.parametrize('ny,nx,order', [(256, 256, 8), (512, 1024, 12), (1024, 1024, 24), (2048, 256, 6)])
+def test_socs_fft_matches_dft_and_oracle(eng, ny, nx, order):
+    from opticalimaging_b200 import imaging, workloads as W
+    from opticalimaging_b200.params import Scatter
+    sr, po, nm = W.config3_optics(order=order)
+    T, fg = imaging.CalculateTCCMatrix(sr, [2048.0 * ny / 1024, 2048.0 * nx / 1024], po, 0.0, nm)
+    sk = imaging.socs_kernels_from_tcc(T, fg, [nx, ny], nm)
+    assert sk.plan.fft
+    rng = np.random.default_rng(order)
+    masks = np.stack([W.rect_mask(ny, nx, 2.0 * ny, 2.0 * nx, 40, 30, 400, rng) for _ in range(2)])
+    md = torch.from_numpy(masks).cuda()
+    fft = sk.image(md, form='fft').cpu().numpy()
+    dft = sk.image(md, form='dft').cpu().numpy()
+    assert rel_err(fft, dft) < 5e-6
+    if ny * nx <= 512 * 1024:
+        sc = Scatter()
+        sc.Period_X, sc.Period_Y = 2.0 * nx, 2.0 * ny
+        sc.ScatterField = W.thin_field(masks[0])
+        K = imaging.DecomposeTCC_SOCS(T, fg, [nx, ny], nm).cpu().numpy().astype(np.complex128)
+        assert rel_err(fft[0], O.socs(sc, K, sr, po)) < 1e-5
+
+
+def test_fft_rejects_unsupported_grid(eng):
+    from opticalimaging_b200 import _native as N
+    lib = N.load()
+    assert lib.oi_fft_supported(1024, 1024) == 1
+    assert lib.oi_fft_supported(1000, 1024) == 0
+    assert lib.oi_fft_supported(128, 1024) == 0
+    plan = eng.Plan.get(45, 63, eng.Band(-5, 11, -5, 11), torch.device('cuda'))
+    assert not plan.fft   # odd grids take the DFT form
