@@ -156,8 +156,8 @@ def test_batched_socs_matches_single(oi):
         sc.Period_X = sc.Period_Y = 2048
         sc.ScatterField = W.thin_field(masks[i])
         one, _ = oi.CalculateAerialImage_SOCS(sc, sk, sr, po)
-        assert rel_err(batch[i].cpu().numpy(), one.numpy()) < 1e-6
-        assert rel_err(batch_u8[i].cpu().numpy(), one.numpy()) < 1e-6
+        assert rel_err(batch[i].cpu().numpy(), one.numpy()) < 5e-6   # FFT form vs the drop-in DFT form
+        assert rel_err(batch_u8[i].cpu().numpy(), one.numpy()) < 5e-6
         if i == 0:
             ref = O.socs(sc, oi.DecomposeTCC_SOCS(T, fg, [256, 256], nm).cpu().numpy().astype(np.complex128), sr, po)
             assert rel_err(one.numpy(), ref) < FP32_VS_FP64
