@@ -13,8 +13,8 @@
  *                                                                             CalculateAerialImage_SOCS.py:10)
  *   oi_tcc_pupils64       <- the shifted-pupil matrix of CalculateTCCMatrix  (CalculateTCCMatrix.py:17-51)
  *   oi_tcc_assemble64     <- GetTCCMatrix                                    (CalculateTCCMatrix.py:58-75)
- *   oi_band_spectrum_fft / oi_coarse_to_image_fft
- *                         <- the same two stages in FFT form (power-of-two grids 256..2048)
+ *   oi_band_spectrum_fft / oi_coherent_coarse_fft / oi_coarse_to_image_fft
+ *                         <- the same three stages in FFT form (power-of-two grids)
  *   oi_twiddle            <- (no counterpart: fills the phase tables the transforms read)
  *
  * Conventions
@@ -64,7 +64,7 @@ OI_API int oi_version(void);
  * double precision and stored as float2.
  */
 OI_API int oi_twiddle(void* out, int rows, int cols, long long a0, long long b0, long long n, int sign, double scale,
-               void* stream);
+                      void* stream);
 
 /*
  * Band-limited forward spectrum (Scatter.py:10-35 restricted to a band):
@@ -73,7 +73,7 @@ OI_API int oi_twiddle(void* out, int rows, int cols, long long a0, long long b0,
  * scratch: float2 [batch * nch * ny * bc].
  */
 OI_API int oi_band_spectrum(const void* field, int kind, int batch, int ny, int nx, int nch, int br, int bc,
-                     const void* wx, const void* wy, float scale, void* scratch, void* band, void* stream);
+                            const void* wx, const void* wy, float scale, void* scratch, void* band, void* stream);
 
 /*
  * Abbe pupils (CalculateAerialImage.py:46-75), one per (plane z, source point j, field component e):
@@ -85,10 +85,10 @@ OI_API int oi_band_spectrum(const void* field, int kind, int batch, int ny, int 
  * Membership `valid` repeats the reference's float32 test (CalculateAerialImage.py:43-57) bit for bit.
  */
 OI_API int oi_abbe_pupils(const float* fr, const float* fc, int br, int bc, const float* sx, const float* sy,
-                   const float* sv, int nsrc, double weight_sum, const double* focus, int nz, const double* zern,
-                   int vector,
-                   const double* jones, double na, double mag, double index_image, double wavelength,
-                   void* pupil, float* weight, void* stream);
+                          const float* sv, int nsrc, double weight_sum, const double* focus, int nz, const double* zern,
+                          int vector,
+                          const double* jones, double na, double mag, double index_image, double wavelength,
+                          void* pupil, float* weight, void* stream);
 
 /*
  * Coherent sum on the coarse grid (the |.|^2 accumulation of both imaging paths):
@@ -99,19 +99,20 @@ OI_API int oi_abbe_pupils(const float* fr, const float* fc, int br, int bc, cons
  * between images' pupil sets.
  */
 OI_API int oi_coherent_coarse(const void* band, int batch, int nch, int br, int bc, const void* pupil,
-                       long long pupil_batch_stride, const float* weight, int nz, int nk, int mr, int mc,
-                       const void* frow, const void* fcol, float* coarse, void* stream);
+                              long long pupil_batch_stride, const float* weight, int nz, int nk, int mr, int mc,
+                              const void* frow, const void* fcol, float* coarse, void* stream);
 
 /*
  * Exact band-limited resampling of the coarse intensity to the output grid:
  *   out[i][y][x] = sum_{|qr|<br, |qc|<bc} Ihat_i(q) exp(-2 pi i (qr y/ny + qc x/nx)),
- *   Ihat_i(q)    = 1/(mr mc) sum_s coarse[i][s] exp(+2 pi i (qr sr/mr + qc sc/mc)).
+ *   Ihat_i(q)    = 1/(mr mc) sum_s coarse[i][s] exp(+2 pi i (qr sr/mr + qc sc/mc)),
+ * where coarse holds `nparts` partial sums one after another (count*mr*mc floats each; 1 for oi_coherent_coarse).
  * Tables (oi_twiddle): gc [mc][bc] (+, b0=0), gr [mr][2br-1] (+, b0=-(br-1)), sy [ny][2br-1] (-, b0=-(br-1)),
  * sx [bc][nx] (-, a0=0).  scratch: float2 [count * (2br-1) * bc].
  */
-OI_API int oi_coarse_to_image(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc,
-                       const void* gr, const void* sy, const void* sx, int ny, int nx, void* scratch,
-                       float* out, void* stream);
+OI_API int oi_coarse_to_image(const float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
+                              const void* gc, const void* gr, const void* sy, const void* sx, int ny, int nx,
+                              void* scratch, float* out, void* stream);
 
 /*
  * FFT form of the two N-point transforms (grids of 256, 512, 1024 or 2048 per axis).  oi_fft_supported(ny, nx)
@@ -121,15 +122,27 @@ OI_API int oi_coarse_to_image(const float* coarse, int count, int mr, int mc, in
  *   m0r .. m0r+br-1 and columns m0c .. m0c+bc-1 (2 max|m_c| < nx, br <= ny).  wn_x / wn_y: oi_twiddle(1, n, 1,
  *   0, n, +1) for n = nx / ny.  scratch: float2 [batch * bc * ny].  band: float2 [batch][br][bc].
  * oi_coarse_to_image_fft: as oi_coarse_to_image (same gc, gr tables), with the y and x syntheses done as
- *   pruned inverse FFTs.  scratch_ihat: float2 [count * (2br-1) * bc]; scratch_v: float2 [count * bc * ny].
+ *   pruned inverse FFTs; the coarse input holds `nparts` partial sums one after another (count*mr*mc floats
+ *   each).  scratch_ihat: float2 [count * (2br-1) * bc]; scratch_v: float2 [count * bc * ny].
  */
 OI_API int oi_fft_supported(int ny, int nx);
 OI_API int oi_band_spectrum_fft(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c,
                                 int bc, const void* wn_x, const void* wn_y, float scale, void* scratch, void* band,
                                 void* stream);
-OI_API int oi_coarse_to_image_fft(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc,
-                                  const void* gr, const void* wn_y, const void* wn_x, int ny, int nx,
+OI_API int oi_coarse_to_image_fft(const float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
+                                  const void* gc, const void* gr, const void* wn_y, const void* wn_x, int ny, int nx,
                                   void* scratch_ihat, void* scratch_v, float* out, void* stream);
+
+/*
+ * FFT form of oi_coherent_coarse for coarse grids of 64 or 128 per axis: the fields of each (image, plane) are
+ * split over `nsplit` blocks that write partial sums coarse[s][b][z][mr][mc] (s < nsplit), which
+ * oi_coarse_to_image_fft adds (nparts = nsplit).  wr / wc: oi_twiddle(1, m, 1, 0, m, +1) for m = mr / mc.
+ * The band starts at frequency (m0r, m0c).
+ */
+OI_API int oi_coherent_coarse_fft(const void* band, int batch, int nch, int m0r, int br, int m0c, int bc,
+                                  const void* pupil, long long pupil_batch_stride, const float* weight, int nz,
+                                  int nk, int mr, int mc, const void* wr, const void* wc, int nsplit, float* coarse,
+                                  void* stream);
 
 /*
  * Shifted pupil matrix of the TCC (CalculateTCCMatrix.py:17-51), FP64, scaled for a Gram product:
@@ -139,9 +152,9 @@ OI_API int oi_coarse_to_image_fft(const float* coarse, int count, int mr, int mc
  * zern and jones are HOST pointers, as for oi_abbe_pupils.
  */
 OI_API int oi_tcc_pupils64(const float* ff, int lf, const float* gg, int lg, const float* sx, const float* sy,
-                    const float* sv, int nsrc, double weight_sum, double focus, const double* zern, int vector,
-                    const double* jones, double na, double mag, double index_image, double wavelength,
-                    void* h, void* stream);
+                           const float* sv, int nsrc, double weight_sum, double focus, const double* zern, int vector,
+                           const double* jones, double na, double mag, double index_image, double wavelength,
+                           void* h, void* stream);
 
 /*
  * TCC = sum_e h_e h_e^H (GetTCCMatrix, CalculateTCCMatrix.py:58-75), complex128 [fg][fg], full Hermitian.

@@ -20,12 +20,13 @@ _SIGS = {
     'oi_abbe_pupils': [_vp, _vp, _i, _i, _vp, _vp, _vp, _i, _d, _vp, _i, _vp, _i, _vp, _d, _d, _d, _d, _vp, _vp,
                        _vp],
     'oi_coherent_coarse': [_vp, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp],
-    'oi_coarse_to_image': [_vp, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp],
+    'oi_coarse_to_image': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp],
     'oi_tcc_pupils64': [_vp, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _d, _vp, _i, _vp, _d, _d, _d, _d, _vp, _vp],
     'oi_tcc_assemble64': [_vp, _i, _i, _i, _vp, _vp],
     'oi_fft_supported': [_i, _i],
     'oi_band_spectrum_fft': [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],
-    'oi_coarse_to_image_fft': [_vp, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp],
+    'oi_coarse_to_image_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp],
+    'oi_coherent_coarse_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _i, _i, _vp, _vp, _i, _vp, _vp],
 }
 
 FIELD_REAL_F32, FIELD_COMPLEX_C64, FIELD_U8 = 0, 1, 2

@@ -414,17 +414,17 @@ extern "C" int oi_band_spectrum_fft(const void* field, int kind, int batch, int 
 }
 
 
-extern "C" int oi_coarse_to_image_fft(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc,
-                                      const void* gr, const void* wn_y, const void* wn_x, int ny, int nx,
-                                      void* scratch_ihat, void* scratch_v, float* out, void* stream) {
+extern "C" int oi_coarse_to_image_fft(const float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
+                                      const void* gc, const void* gr, const void* wn_y, const void* wn_x, int ny,
+                                      int nx, void* scratch_ihat, void* scratch_v, float* out, void* stream) {
   using namespace oi;
-  if (!coarse || !gc || !gr || !wn_y || !wn_x || !scratch_ihat || !scratch_v || !out || count <= 0)
+  if (!coarse || !gc || !gr || !wn_y || !wn_x || !scratch_ihat || !scratch_v || !out || count <= 0 || nparts <= 0)
     return fail(OI_EINVAL, "oi_coarse_to_image_fft: bad arguments");
   const int nx1 = n1_of(nx), ny1 = n1_of(ny);
   if (!nx1 || !ny1) return fail(OI_ERANGE, "oi_coarse_to_image_fft: grid %dx%d is not 256..2048, power of 2", ny, nx);
   if (2 * br - 1 > ny || 2 * bc - 1 > nx) return fail(OI_ERANGE, "oi_coarse_to_image_fft: band too wide for grid");
   cudaStream_t s = (cudaStream_t)stream;
-  int rc = coarse_spectrum(coarse, count, mr, mc, br, bc, gc, gr, scratch_ihat, s);
+  int rc = coarse_spectrum(coarse, count, mr, mc, br, bc, gc, gr, scratch_ihat, s, nparts);
   if (rc) return rc;
   const float2* ih = (const float2*)scratch_ihat;
   float2* v = (float2*)scratch_v;

@@ -4,6 +4,7 @@
 // The intensity of fields band-limited to Br x Bc has a spectrum supported on |qr| < Br, |qc| < Bc.  Its
 // samples on the coarse Mr x Mc grid (Mr >= 2Br-1, Mc >= 2Bc-1) determine that spectrum exactly:
 //   Ihat(q) = 1/(Mr Mc) sum_s coarse[s] exp(+2 pi i (qr sr/Mr + qc sc/Mc))             (spec kernel)
+// (the coarse intensity may arrive as `nparts` partial sums laid out one after another; they are added here)
 // and the output is its trigonometric polynomial evaluated on the Ny x Nx grid.  The intensity is real, so
 // only qc >= 0 is kept (qc > 0 doubled) and the x synthesis is a real dot product:
 //   V[y][qc]   = sum_qr Ihat(qr, qc) exp(-2 pi i qr y/Ny)
@@ -15,7 +16,8 @@ namespace oi {
 constexpr int SP_QT = 16;  // qc per spec block
 
 // grid (ceil(bc/16), count).  ihat[i][jr][qc], jr = qr + br - 1.
-__global__ void __launch_bounds__(256) coarse_spec_kernel(const float* __restrict__ coarse, int mr, int mc, int br,
+__global__ void __launch_bounds__(256) coarse_spec_kernel(const float* __restrict__ coarse, int nparts,
+                                                          long long part_stride, int mr, int mc, int br,
                                                           int bc, const float2* __restrict__ gc,
                                                           const float2* __restrict__ gr, float2* __restrict__ ihat) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -33,6 +35,7 @@ __global__ void __launch_bounds__(256) coarse_spec_kernel(const float* __restric
       const float* row = cimg + (long long)sr * mc;
       for (int sc = 0; sc < mc; ++sc) {
         float v = __ldg(row + sc);
+        for (int p = 1; p < nparts; ++p) v += __ldg(row + p * part_stride + sc);
         float2 t = __ldg(gc + (long long)sc * bc + qc);
         u.x = fmaf(v, t.x, u.x);
         u.y = fmaf(v, t.y, u.y);
@@ -109,7 +112,7 @@ __global__ void __launch_bounds__(256) synth_kernel(const float2* __restrict__ i
 }
 
 int coarse_spectrum(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc, const void* gr,
-                    void* ihat, cudaStream_t s) {
+                    void* ihat, cudaStream_t s, int nparts) {
   if (mr < 2 * br - 1 || mc < 2 * bc - 1)
     return fail(OI_EINVAL, "coarse grid %dx%d too small for band %dx%d", mr, mc, br, bc);
   if (mr > 1024 || count > 65535) return fail(OI_ERANGE, "coarse grid mr=%d or count=%d out of range", mr, count);
@@ -119,8 +122,8 @@ int coarse_spectrum(const float* coarse, int count, int mr, int mc, int br, int 
     if (e != cudaSuccess) return fail(OI_ECUDA, "coarse spectrum: smem attribute: %s", cudaGetErrorString(e));
   }
   dim3 g1((unsigned)ceil_div(bc, SP_QT), (unsigned)count);
-  coarse_spec_kernel<<<g1, 256, smem, s>>>(coarse, mr, mc, br, bc, (const float2*)gc, (const float2*)gr,
-                                           (float2*)ihat);
+  coarse_spec_kernel<<<g1, 256, smem, s>>>(coarse, nparts, (long long)count * mr * mc, mr, mc, br, bc,
+                                           (const float2*)gc, (const float2*)gr, (float2*)ihat);
   return check_launch("coarse spectrum");
 }
 
@@ -133,19 +136,19 @@ static void launch_synth(const float2* ihat, int count, int br, int bc, const fl
 
 }  // namespace oi
 
-extern "C" int oi_coarse_to_image(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc,
-                                  const void* gr, const void* sy, const void* sx, int ny, int nx, void* scratch,
-                                  float* out, void* stream) {
+extern "C" int oi_coarse_to_image(const float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
+                                  const void* gc, const void* gr, const void* sy, const void* sx, int ny, int nx,
+                                  void* scratch, float* out, void* stream) {
   using namespace oi;
-  if (!coarse || !gc || !gr || !sy || !sx || !scratch || !out || count <= 0 || mr <= 0 || mc <= 0 || br <= 0 ||
-      bc <= 0 || ny <= 0 || nx <= 0)
+  if (!coarse || !gc || !gr || !sy || !sx || !scratch || !out || nparts <= 0 || count <= 0 || mr <= 0 || mc <= 0 ||
+      br <= 0 || bc <= 0 || ny <= 0 || nx <= 0)
     return fail(OI_EINVAL, "oi_coarse_to_image: bad arguments");
   if (mr < 2 * br - 1 || mc < 2 * bc - 1)
     return fail(OI_EINVAL, "oi_coarse_to_image: coarse grid %dx%d too small for band %dx%d", mr, mc, br, bc);
   if (mr > 1024 || bc > 512 || nx > 2048 || count > 65535)
     return fail(OI_ERANGE, "oi_coarse_to_image: sizes out of range (mr=%d bc=%d nx=%d)", mr, bc, nx);
   cudaStream_t s = (cudaStream_t)stream;
-  int rc = coarse_spectrum(coarse, count, mr, mc, br, bc, gc, gr, scratch, s);
+  int rc = coarse_spectrum(coarse, count, mr, mc, br, bc, gc, gr, scratch, s, nparts);
   if (rc) return rc;
   const float2* ih = (const float2*)scratch;
   switch ((nx + 255) / 256) {

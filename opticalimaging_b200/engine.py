@@ -93,11 +93,30 @@ class Plan:
         if self.fft:                                          # exp(+2 pi i j/n), j < n, for the FFT form
             self.wn_x = t(1, nx, 1, 0, nx, +1)
             self.wn_y = t(1, ny, 1, 0, ny, +1)
+        self.coarse_fft = self.mr in (64, 128) and self.mc in (64, 128)
+        if self.coarse_fft:                                   # the coarse-grid FFT tables
+            self.wm_r = t(1, self.mr, 1, 0, self.mr, +1)
+            self.wm_c = t(1, self.mc, 1, 0, self.mc, +1)
 
     def use_fft(self, form):
         if form not in (None,) + FORMS:
             raise ValueError(f'form must be one of {FORMS}')
         return self.fft and form != 'dft'
+
+    def use_coarse_fft(self, form):
+        return self.coarse_fft and form != 'dft'
+
+
+SM_COUNT = 148
+
+
+def field_split(nfields: int, blocks: int) -> int:
+    """Smallest divisor d of nfields with blocks * d >= 3 waves of one block per SM (nfields if none)."""
+    target = 3 * SM_COUNT
+    for d in range(1, nfields + 1):
+        if nfields % d == 0 and blocks * d >= target:
+            return d
+    return nfields
 
     @classmethod
     def get(cls, ny, nx, band: Band, device) -> 'Plan':
@@ -154,21 +173,31 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
     batch, nch = band.shape[0], band.shape[1]
     nz, nk = pupils.shape[-4], pupils.shape[-3]
     dev = plan.device
-    coarse = torch.empty((batch, nz, plan.mr, plan.mc), dtype=torch.float32, device=dev)
     s = N.stream_handle(dev)
-    N.call('oi_coherent_coarse', N.ptr(band), batch, nch, b.br, b.bc, N.ptr(pupils), int(pupil_batch_stride),
-           N.ptr(weights), nz, nk, plan.mr, plan.mc, N.ptr(plan.frow), N.ptr(plan.fcol), N.ptr(coarse), s)
+    if plan.use_coarse_fft(form):
+        nsplit = field_split(nk * nch, batch * nz)
+        coarse = torch.empty((nsplit, batch, nz, plan.mr, plan.mc), dtype=torch.float32, device=dev)
+        N.call('oi_coherent_coarse_fft', N.ptr(band), batch, nch, b.m0r, b.br, b.m0c, b.bc, N.ptr(pupils),
+               int(pupil_batch_stride), N.ptr(weights), nz, nk, plan.mr, plan.mc, N.ptr(plan.wm_r),
+               N.ptr(plan.wm_c), nsplit, N.ptr(coarse), s)
+    else:
+        nsplit = 1
+        coarse = torch.empty((batch, nz, plan.mr, plan.mc), dtype=torch.float32, device=dev)
+        N.call('oi_coherent_coarse', N.ptr(band), batch, nch, b.br, b.bc, N.ptr(pupils), int(pupil_batch_stride),
+               N.ptr(weights), nz, nk, plan.mr, plan.mc, N.ptr(plan.frow), N.ptr(plan.fcol), N.ptr(coarse), s)
     _mark(marks, 'coherent_coarse')
     if out is None:
         out = torch.empty((batch, nz, plan.ny, plan.nx), dtype=torch.float32, device=dev)
     ihat = torch.empty(batch * nz * (2 * b.br - 1) * b.bc, dtype=torch.complex64, device=dev)
     if plan.use_fft(form):
         v = torch.empty(batch * nz * b.bc * plan.ny, dtype=torch.complex64, device=dev)
-        N.call('oi_coarse_to_image_fft', N.ptr(coarse), batch * nz, plan.mr, plan.mc, b.br, b.bc, N.ptr(plan.gc),
+        N.call('oi_coarse_to_image_fft', N.ptr(coarse), nsplit, batch * nz, plan.mr, plan.mc, b.br, b.bc,
+               N.ptr(plan.gc),
                N.ptr(plan.gr), N.ptr(plan.wn_y), N.ptr(plan.wn_x), plan.ny, plan.nx, N.ptr(ihat), N.ptr(v),
                N.ptr(out), s)
     else:
-        N.call('oi_coarse_to_image', N.ptr(coarse), batch * nz, plan.mr, plan.mc, b.br, b.bc, N.ptr(plan.gc),
+        N.call('oi_coarse_to_image', N.ptr(coarse), nsplit, batch * nz, plan.mr, plan.mc, b.br, b.bc,
+               N.ptr(plan.gc),
                N.ptr(plan.gr), N.ptr(plan.sy), N.ptr(plan.sx), plan.ny, plan.nx, N.ptr(ihat), N.ptr(out), s)
     _mark(marks, 'coarse_to_image')
     return out
