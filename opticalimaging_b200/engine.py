@@ -107,6 +107,16 @@ class Plan:
         return self.coarse_fft and form != 'dft'
 
 
+    @classmethod
+    def get(cls, ny, nx, band: Band, device) -> 'Plan':
+        key = (ny, nx, band, str(device))
+        with cls._lock:
+            p = cls._cache.get(key)
+            if p is None:
+                p = cls._cache[key] = Plan(ny, nx, band, device)
+            return p
+
+
 SM_COUNT = 148
 
 
@@ -117,15 +127,6 @@ def field_split(nfields: int, blocks: int) -> int:
         if nfields % d == 0 and blocks * d >= target:
             return d
     return nfields
-
-    @classmethod
-    def get(cls, ny, nx, band: Band, device) -> 'Plan':
-        key = (ny, nx, band, str(device))
-        with cls._lock:
-            p = cls._cache.get(key)
-            if p is None:
-                p = cls._cache[key] = Plan(ny, nx, band, device)
-            return p
 
 
 # --------------------------------------------------------------------------------------------- stages
