@@ -107,10 +107,11 @@ OI_API int oi_coherent_coarse(const void* band, int batch, int nch, int br, int 
  *   out[i][y][x] = sum_{|qr|<br, |qc|<bc} Ihat_i(q) exp(-2 pi i (qr y/ny + qc x/nx)),
  *   Ihat_i(q)    = 1/(mr mc) sum_s coarse[i][s] exp(+2 pi i (qr sr/mr + qc sc/mc)),
  * where coarse holds `nparts` partial sums one after another (count*mr*mc floats each; 1 for oi_coherent_coarse).
+ * With nparts > 1 the partials are added into the first one in place (the buffer is scratch afterwards).
  * Tables (oi_twiddle): gc [mc][bc] (+, b0=0), gr [mr][2br-1] (+, b0=-(br-1)), sy [ny][2br-1] (-, b0=-(br-1)),
  * sx [bc][nx] (-, a0=0).  scratch: float2 [count * (2br-1) * bc].
  */
-OI_API int oi_coarse_to_image(const float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
+OI_API int oi_coarse_to_image(float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
                               const void* gc, const void* gr, const void* sy, const void* sx, int ny, int nx,
                               void* scratch, float* out, void* stream);
 
@@ -129,7 +130,7 @@ OI_API int oi_fft_supported(int ny, int nx);
 OI_API int oi_band_spectrum_fft(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c,
                                 int bc, const void* wn_x, const void* wn_y, float scale, void* scratch, void* band,
                                 void* stream);
-OI_API int oi_coarse_to_image_fft(const float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
+OI_API int oi_coarse_to_image_fft(float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
                                   const void* gc, const void* gr, const void* wn_y, const void* wn_x, int ny, int nx,
                                   void* scratch_ihat, void* scratch_v, float* out, void* stream);
 

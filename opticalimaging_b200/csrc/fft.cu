@@ -414,7 +414,7 @@ extern "C" int oi_band_spectrum_fft(const void* field, int kind, int batch, int 
 }
 
 
-extern "C" int oi_coarse_to_image_fft(const float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
+extern "C" int oi_coarse_to_image_fft(float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
                                       const void* gc, const void* gr, const void* wn_y, const void* wn_x, int ny,
                                       int nx, void* scratch_ihat, void* scratch_v, float* out, void* stream) {
   using namespace oi;

@@ -111,11 +111,33 @@ __global__ void __launch_bounds__(256) synth_kernel(const float2* __restrict__ i
   }
 }
 
-int coarse_spectrum(const float* coarse, int count, int mr, int mc, int br, int bc, const void* gc, const void* gr,
+// part[0][i] += part[1][i] + ... + part[nparts-1][i], in place (float4 lanes; n is a multiple of 4).
+__global__ void sum_parts_kernel(float* __restrict__ coarse, int nparts, long long n) {
+  long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (i >= n) return;
+  float4 acc = *(const float4*)(coarse + i);
+  for (int p = 1; p < nparts; ++p) {
+    const float4 v = __ldg((const float4*)(coarse + p * n + i));
+    acc.x += v.x;
+    acc.y += v.y;
+    acc.z += v.z;
+    acc.w += v.w;
+  }
+  *(float4*)(coarse + i) = acc;
+}
+
+int coarse_spectrum(float* coarse, int count, int mr, int mc, int br, int bc, const void* gc, const void* gr,
                     void* ihat, cudaStream_t s, int nparts) {
   if (mr < 2 * br - 1 || mc < 2 * bc - 1)
     return fail(OI_EINVAL, "coarse grid %dx%d too small for band %dx%d", mr, mc, br, bc);
   if (mr > 1024 || count > 65535) return fail(OI_ERANGE, "coarse grid mr=%d or count=%d out of range", mr, count);
+  if (nparts > 1) {  // fold the partial sums into the first one, once, before the transform reads them
+    const long long n = (long long)count * mr * mc;  // mc is a multiple of 64
+    sum_parts_kernel<<<(unsigned)ceil_div(n / 4, 256), 256, 0, s>>>(coarse, nparts, n);
+    int rc = check_launch("coarse spectrum/sum parts");
+    if (rc) return rc;
+    nparts = 1;
+  }
   size_t smem = sizeof(float2) * (size_t)mr * SP_QT;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(coarse_spec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -136,7 +158,7 @@ static void launch_synth(const float2* ihat, int count, int br, int bc, const fl
 
 }  // namespace oi
 
-extern "C" int oi_coarse_to_image(const float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
+extern "C" int oi_coarse_to_image(float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
                                   const void* gc, const void* gr, const void* sy, const void* sx, int ny, int nx,
                                   void* scratch, float* out, void* stream) {
   using namespace oi;
