@@ -124,15 +124,18 @@ OI_API int oi_coarse_to_image(float* coarse, int nparts, int count, int mr, int 
  *   0, n, +1) for n = nx / ny.  scratch: float2 [batch * bc * ny].  band: float2 [batch][br][bc].
  * oi_coarse_to_image_fft: as oi_coarse_to_image (same gc, gr tables), with the y and x syntheses done as
  *   pruned inverse FFTs; the coarse input holds `nparts` partial sums one after another (count*mr*mc floats
- *   each).  scratch_ihat: float2 [count * (2br-1) * bc]; scratch_v: float2 [count * bc * ny].
+ *   each).  When wm_r / wm_c (oi_twiddle(1, m, 1, 0, m, +1) for m = mr / mc) are given and mr, mc are 64 or
+ *   128, the coarse spectrum is an FFT too (one block per image); else it is the DFT of oi_coarse_to_image.
+ *   scratch_ihat: float2 [count * (2br-1) * bc]; scratch_v: float2 [count * bc * ny].
  */
 OI_API int oi_fft_supported(int ny, int nx);
 OI_API int oi_band_spectrum_fft(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c,
                                 int bc, const void* wn_x, const void* wn_y, float scale, void* scratch, void* band,
                                 void* stream);
 OI_API int oi_coarse_to_image_fft(float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
-                                  const void* gc, const void* gr, const void* wn_y, const void* wn_x, int ny, int nx,
-                                  void* scratch_ihat, void* scratch_v, float* out, void* stream);
+                                  const void* gc, const void* gr, const void* wm_r, const void* wm_c,
+                                  const void* wn_y, const void* wn_x, int ny, int nx, void* scratch_ihat,
+                                  void* scratch_v, float* out, void* stream);
 
 /*
  * FFT form of oi_coherent_coarse for coarse grids of 64 or 128 per axis: the fields of each (image, plane) are

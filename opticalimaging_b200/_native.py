@@ -25,7 +25,8 @@ _SIGS = {
     'oi_tcc_assemble64': [_vp, _i, _i, _i, _vp, _vp],
     'oi_fft_supported': [_i, _i],
     'oi_band_spectrum_fft': [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],
-    'oi_coarse_to_image_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp],
+    'oi_coarse_to_image_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp,
+                               _vp],
     'oi_coherent_coarse_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _i, _i, _vp, _vp, _i, _vp, _vp],
 }
 

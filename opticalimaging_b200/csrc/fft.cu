@@ -69,6 +69,15 @@ __device__ __forceinline__ float2 wn_get(const float2* wn, int j) {
   return SIGN > 0 ? w : make_float2(w.x, -w.y);
 }
 
+template <typename K>
+static int set_smem(K kern, size_t bytes, const char* what) {
+  if (bytes > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return fail(OI_ECUDA, "%s: smem attribute: %s", what, cudaGetErrorString(e));
+  }
+  return OI_OK;
+}
+
 template <int KIND> __device__ __forceinline__ float load_real(const void* f, long long i);
 template <> __device__ __forceinline__ float load_real<OI_FIELD_REAL_F32>(const void* f, long long i) {
   return __ldg((const float*)f + i);
@@ -295,19 +304,92 @@ __global__ void __launch_bounds__(256) fft_rows_inv_kernel(const float2* __restr
   }
 }
 
+// --------------------------------------------------------------- coarse intensity -> its spectrum
+// One block per coarse image (mr = 32 N1R, mc = 32 N1C, each 64 or 128):
+//   ihat[i][jr][qc] = (qc ? 2 : 1) / (mr mc) * sum_{sr,sc} coarse[i][sr][sc] exp(+2 pi i (qr sr/mr + qc sc/mc))
+// for qr = jr - (br-1) in [-(br-1), br-1] and qc in [0, bc).  Row FFTs of the real image in pairs (two rows per
+// complex transform), the band bins of each separated into U[sr][qc]; then column FFTs of U at the qr bins.
+template <int N1R, int N1C>
+__global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __restrict__ coarse, int br, int bc,
+                                                              const float2* __restrict__ wr_g,
+                                                              const float2* __restrict__ wc_g, int area_f2,
+                                                              float2* __restrict__ ihat) {
+  constexpr int MR = 32 * N1R, MC = 32 * N1C, T = 512;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* wr = (float2*)smem_raw;      // [MR]
+  float2* wc = wr + MR;                // [MC]
+  float2* area = wc + MC;              // [area_f2] union: coarse image / row transposes / column transposes
+  float2* u = area + area_f2;          // [MR][bc]
+  const int tid = threadIdx.x;
+  const long long img = blockIdx.x;
+  for (int j = tid; j < MR; j += T) wr[j] = wr_g[j];
+  for (int j = tid; j < MC; j += T) wc[j] = wc_g[j];
+  float* cimg = (float*)area;
+  const float4* src = (const float4*)(coarse + img * (long long)MR * MC);
+  for (int j = tid; j < MR * MC / 4; j += T) ((float4*)cimg)[j] = __ldg(src + j);
+  __syncthreads();
+  // row pass: pair p = rows (2p, 2p+1), thread n1
+  const int p = tid / N1C, n1 = tid % N1C;
+  const bool row_task = p < MR / 2;
+  float2 z[32];
+  if (row_task) {
+#pragma unroll
+    for (int n2 = 0; n2 < 32; ++n2)
+      z[n2] = make_float2(cimg[(2 * p) * MC + n1 + N1C * n2], cimg[(2 * p + 1) * MC + n1 + N1C * n2]);
+    fft32<+1>(z);
+  }
+  __syncthreads();  // the image is consumed; the area now holds row transposes
+  if (row_task) twiddle_store<+1, N1C>(z, wc, n1, area + p * 32 * (N1C + 1));
+  __syncthreads();
+  for (int e = tid; e < (MR / 2) * bc; e += T) {
+    const int pp = e / bc, qc = e % bc;
+    const float2* ys = area + pp * 32 * (N1C + 1);
+    const float2 zp = outer_bin<+1, N1C>(ys, wc, qc & (MC - 1));
+    const float2 zm = outer_bin<+1, N1C>(ys, wc, (-qc) & (MC - 1));
+    u[(2 * pp) * bc + qc] = make_float2(0.5f * (zp.x + zm.x), 0.5f * (zp.y - zm.y));
+    u[(2 * pp + 1) * bc + qc] = make_float2(0.5f * (zp.y + zm.y), -0.5f * (zp.x - zm.x));
+  }
+  __syncthreads();
+  // column pass: column qc of U, thread n1r
+  const int qc = tid / N1R, n1r = tid % N1R;
+  const bool col_task = qc < bc;
+  if (col_task) {
+#pragma unroll
+    for (int n2 = 0; n2 < 32; ++n2) z[n2] = u[(n1r + N1R * n2) * bc + qc];
+    fft32<+1>(z);
+  }
+  __syncthreads();  // row transposes are consumed; the area now holds column transposes
+  if (col_task) twiddle_store<+1, N1R>(z, wr, n1r, area + qc * 32 * (N1R + 1));
+  __syncthreads();
+  const int nq = 2 * br - 1;
+  const float norm = 1.0f / ((float)MR * (float)MC);
+  for (int e = tid; e < nq * bc; e += T) {
+    const int jr = e / bc, c = e % bc;
+    const float2 v = outer_bin<+1, N1R>(area + c * 32 * (N1R + 1), wr, (jr - (br - 1)) & (MR - 1));
+    const float s = (c == 0 ? 1.0f : 2.0f) * norm;
+    ihat[(img * nq + jr) * (long long)bc + c] = make_float2(v.x * s, v.y * s);
+  }
+}
+
+template <int N1R, int N1C>
+static int launch_coarse_spec_fft(float* coarse, int count, int br, int bc, const float2* wr, const float2* wc,
+                                  float2* ihat, cudaStream_t s) {
+  constexpr int MR = 32 * N1R, MC = 32 * N1C;
+  const int rows_ys = (MR / 2) * 32 * (N1C + 1), c_f2 = MR * MC / 2, cols_ys = bc * 32 * (N1R + 1);
+  const int area_f2 = max(rows_ys, max(c_f2, cols_ys));
+  const size_t smem = sizeof(float2) * ((size_t)MR + MC + area_f2 + (size_t)MR * bc);
+  auto kern = coarse_spec_fft_kernel<N1R, N1C>;
+  int rc = set_smem(kern, smem, "coarse spectrum fft");
+  if (rc) return rc;
+  kern<<<count, 512, smem, s>>>(coarse, br, bc, wr, wc, area_f2, ihat);
+  return check_launch("coarse spectrum fft");
+}
+
 template <int N1>
 static size_t smem_rows_fwd(int nu) { return sizeof(float2) * (32 * N1 + (256 / N1) * 32 * (N1 + 1) + (256 / N1) * nu); }
 template <int N1>
 static size_t smem_cols_fwd() { return sizeof(float2) * (32 * N1 + (256 / N1) * 32 * (N1 + 1)); }
 
-template <typename K>
-static int set_smem(K kern, size_t bytes, const char* what) {
-  if (bytes > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return fail(OI_ECUDA, "%s: smem attribute: %s", what, cudaGetErrorString(e));
-  }
-  return OI_OK;
-}
 
 template <int N1>
 static int band_fft(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c, int bc,
@@ -415,8 +497,9 @@ extern "C" int oi_band_spectrum_fft(const void* field, int kind, int batch, int 
 
 
 extern "C" int oi_coarse_to_image_fft(float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
-                                      const void* gc, const void* gr, const void* wn_y, const void* wn_x, int ny,
-                                      int nx, void* scratch_ihat, void* scratch_v, float* out, void* stream) {
+                                      const void* gc, const void* gr, const void* wm_r, const void* wm_c,
+                                      const void* wn_y, const void* wn_x, int ny, int nx, void* scratch_ihat,
+                                      void* scratch_v, float* out, void* stream) {
   using namespace oi;
   if (!coarse || !gc || !gr || !wn_y || !wn_x || !scratch_ihat || !scratch_v || !out || count <= 0 || nparts <= 0)
     return fail(OI_EINVAL, "oi_coarse_to_image_fft: bad arguments");
@@ -424,7 +507,19 @@ extern "C" int oi_coarse_to_image_fft(float* coarse, int nparts, int count, int 
   if (!nx1 || !ny1) return fail(OI_ERANGE, "oi_coarse_to_image_fft: grid %dx%d is not 256..2048, power of 2", ny, nx);
   if (2 * br - 1 > ny || 2 * bc - 1 > nx) return fail(OI_ERANGE, "oi_coarse_to_image_fft: band too wide for grid");
   cudaStream_t s = (cudaStream_t)stream;
-  int rc = coarse_spectrum(coarse, count, mr, mc, br, bc, gc, gr, scratch_ihat, s, nparts);
+  int rc;
+  if (wm_r && wm_c && (mr == 64 || mr == 128) && (mc == 64 || mc == 128) && bc <= 64) {
+    rc = fold_parts(coarse, nparts, (long long)count * mr * mc, s);
+    if (rc) return rc;
+    float2* ih = (float2*)scratch_ihat;
+    const float2 *tr = (const float2*)wm_r, *tc = (const float2*)wm_c;
+    if (mr == 128 && mc == 128) rc = launch_coarse_spec_fft<4, 4>(coarse, count, br, bc, tr, tc, ih, s);
+    else if (mr == 64 && mc == 64) rc = launch_coarse_spec_fft<2, 2>(coarse, count, br, bc, tr, tc, ih, s);
+    else if (mr == 128) rc = launch_coarse_spec_fft<4, 2>(coarse, count, br, bc, tr, tc, ih, s);
+    else rc = launch_coarse_spec_fft<2, 4>(coarse, count, br, bc, tr, tc, ih, s);
+  } else {
+    rc = coarse_spectrum(coarse, count, mr, mc, br, bc, gc, gr, scratch_ihat, s, nparts);
+  }
   if (rc) return rc;
   const float2* ih = (const float2*)scratch_ihat;
   float2* v = (float2*)scratch_v;

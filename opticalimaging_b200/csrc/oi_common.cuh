@@ -44,6 +44,9 @@ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 // The coarse-intensity spectrum stage shared by oi_coarse_to_image and oi_coarse_to_image_fft (synth.cu):
 // ihat[i][jr][qc] = (qc ? 2 : 1) / (mr mc) * sum_s coarse[i][s] exp(+2 pi i (qr sr/mr + qc sc/mc)).
+// Adds partial sums 1..nparts-1 (each n floats, one after another) into the first, in place.
+int fold_parts(float* coarse, int nparts, long long n, cudaStream_t s);
+
 // The coarse intensity may be split in `nparts` partial sums, each count*mr*mc floats, added in order.
 int coarse_spectrum(float* coarse, int count, int mr, int mc, int br, int bc, const void* gc, const void* gr,
                     void* ihat, cudaStream_t s, int nparts);

@@ -126,18 +126,21 @@ __global__ void sum_parts_kernel(float* __restrict__ coarse, int nparts, long lo
   *(float4*)(coarse + i) = acc;
 }
 
+int fold_parts(float* coarse, int nparts, long long n, cudaStream_t s) {
+  if (nparts <= 1) return OI_OK;
+  if (n % 4 != 0) return fail(OI_EINVAL, "partial sums of %lld floats are not float4 aligned", n);
+  sum_parts_kernel<<<(unsigned)ceil_div(n / 4, 256), 256, 0, s>>>(coarse, nparts, n);
+  return check_launch("coarse spectrum/sum parts");
+}
+
 int coarse_spectrum(float* coarse, int count, int mr, int mc, int br, int bc, const void* gc, const void* gr,
                     void* ihat, cudaStream_t s, int nparts) {
   if (mr < 2 * br - 1 || mc < 2 * bc - 1)
     return fail(OI_EINVAL, "coarse grid %dx%d too small for band %dx%d", mr, mc, br, bc);
   if (mr > 1024 || count > 65535) return fail(OI_ERANGE, "coarse grid mr=%d or count=%d out of range", mr, count);
-  if (nparts > 1) {  // fold the partial sums into the first one, once, before the transform reads them
-    const long long n = (long long)count * mr * mc;  // mc is a multiple of 64
-    sum_parts_kernel<<<(unsigned)ceil_div(n / 4, 256), 256, 0, s>>>(coarse, nparts, n);
-    int rc = check_launch("coarse spectrum/sum parts");
-    if (rc) return rc;
-    nparts = 1;
-  }
+  int rc = fold_parts(coarse, nparts, (long long)count * mr * mc, s);
+  if (rc) return rc;
+  nparts = 1;
   size_t smem = sizeof(float2) * (size_t)mr * SP_QT;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(coarse_spec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

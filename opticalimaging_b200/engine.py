@@ -192,14 +192,14 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
     ihat = torch.empty(batch * nz * (2 * b.br - 1) * b.bc, dtype=torch.complex64, device=dev)
     if plan.use_fft(form):
         v = torch.empty(batch * nz * b.bc * plan.ny, dtype=torch.complex64, device=dev)
+        wm_r, wm_c = (plan.wm_r, plan.wm_c) if plan.coarse_fft else (None, None)
         N.call('oi_coarse_to_image_fft', N.ptr(coarse), nsplit, batch * nz, plan.mr, plan.mc, b.br, b.bc,
-               N.ptr(plan.gc),
-               N.ptr(plan.gr), N.ptr(plan.wn_y), N.ptr(plan.wn_x), plan.ny, plan.nx, N.ptr(ihat), N.ptr(v),
-               N.ptr(out), s)
+               N.ptr(plan.gc), N.ptr(plan.gr), N.ptr(wm_r), N.ptr(wm_c), N.ptr(plan.wn_y), N.ptr(plan.wn_x),
+               plan.ny, plan.nx, N.ptr(ihat), N.ptr(v), N.ptr(out), s)
     else:
         N.call('oi_coarse_to_image', N.ptr(coarse), nsplit, batch * nz, plan.mr, plan.mc, b.br, b.bc,
-               N.ptr(plan.gc),
-               N.ptr(plan.gr), N.ptr(plan.sy), N.ptr(plan.sx), plan.ny, plan.nx, N.ptr(ihat), N.ptr(out), s)
+               N.ptr(plan.gc), N.ptr(plan.gr), N.ptr(plan.sy), N.ptr(plan.sx), plan.ny, plan.nx, N.ptr(ihat),
+               N.ptr(out), s)
     _mark(marks, 'coarse_to_image')
     return out
 
