@@ -62,13 +62,6 @@ __device__ __forceinline__ void fft32(float2 (&v)[32]) {
   }
 }
 
-// exp(SIGN 2 pi i j / N) from the +1 table wn[j] = exp(+2 pi i j / N)
-template <int SIGN>
-__device__ __forceinline__ float2 wn_get(const float2* wn, int j) {
-  float2 w = wn[j];
-  return SIGN > 0 ? w : make_float2(w.x, -w.y);
-}
-
 template <typename K>
 static int set_smem(K kern, size_t bytes, const char* what) {
   if (bytes > 48 * 1024) {
@@ -86,27 +79,49 @@ template <> __device__ __forceinline__ float load_real<OI_FIELD_U8>(const void* 
   return (float)__ldg((const uint8_t*)f + i);
 }
 
-// Shared by the four kernels: stage 2 + transpose.  z holds the bit-reversed 32-point result of thread n1;
-// multiply by W_N^{n1 k2} and store to ys[k2][n1] (row stride N1 + 1).
-template <int SIGN, int N1>
-__device__ __forceinline__ void twiddle_store(const float2 (&z)[32], const float2* wn, int n1, float2* ys) {
+// Per-block twiddle tables, laid out so that a warp reading one k for all n1 touches consecutive entries:
+//   t2[k2][n1] = W_N^{k2 n1}  (32 x N1)      t1[k1][n1] = W_N1^{k1 n1} = W_N^{32 k1 n1}  (N1 x N1)
+// with W_N = exp(+2 pi i / N), built from the 1-D table wn_g[j] = W_N^j.  (Reading the 1-D table at index
+// k n1 mod N across a warp is a stride-k access, up to 32-way bank conflicts.)
+template <int N1>
+__device__ __forceinline__ void build_tables(const float2* __restrict__ wn_g, float2* t2, float2* t1, int tid,
+                                             int nthreads) {
   constexpr int N = 32 * N1;
+  for (int e = tid; e < 32 * N1; e += nthreads) {
+    const int k2 = e / N1, n1 = e % N1;
+    t2[e] = __ldg(wn_g + ((k2 * n1) & (N - 1)));
+  }
+  for (int e = tid; e < N1 * N1; e += nthreads) {
+    const int k1 = e / N1, n1 = e % N1;
+    t1[e] = __ldg(wn_g + ((32 * k1 * n1) & (N - 1)));
+  }
+}
+template <int N1>
+constexpr int table_f2() { return 32 * N1 + N1 * N1; }
+
+template <int SIGN>
+__device__ __forceinline__ float2 sgn(float2 w) { return SIGN > 0 ? w : make_float2(w.x, -w.y); }
+
+// Stage 2 + transpose: z holds the bit-reversed 32-point result of thread n1; multiply by W_N^{n1 k2} and
+// store to ys[k2][n1] (row stride N1 + 1).
+template <int SIGN, int N1>
+__device__ __forceinline__ void twiddle_store(const float2 (&z)[32], const float2* t2, int n1, float2* ys) {
 #pragma unroll
   for (int i = 0; i < 32; ++i) {
     const int k2 = bitrev5(i);
-    ys[k2 * (N1 + 1) + n1] = cmul(z[i], wn_get<SIGN>(wn, (n1 * k2) & (N - 1)));
+    ys[k2 * (N1 + 1) + n1] = cmul(z[i], sgn<SIGN>(t2[k2 * N1 + n1]));
   }
 }
 
 // Z[k] = sum_n1 W_N1^{k1 n1} ys[k2][n1]  (forward outer stage for one bin k = k2 + 32 k1)
 template <int SIGN, int N1>
-__device__ __forceinline__ float2 outer_bin(const float2* ys, const float2* wn, int k) {
-  constexpr int N = 32 * N1;
+__device__ __forceinline__ float2 outer_bin(const float2* ys, const float2* t1, int k) {
   const int k2 = k & 31, k1 = k >> 5;
   const float2* row = ys + k2 * (N1 + 1);
+  const float2* tw = t1 + k1 * N1;
   float2 acc = make_float2(0.f, 0.f);
 #pragma unroll 8
-  for (int n1 = 0; n1 < N1; ++n1) cfma(acc, row[n1], wn_get<SIGN>(wn, (32 * k1 * n1) & (N - 1)));
+  for (int n1 = 0; n1 < N1; ++n1) cfma(acc, row[n1], sgn<SIGN>(tw[n1]));
   return acc;
 }
 
@@ -119,11 +134,12 @@ __global__ void __launch_bounds__(256) fft_rows_fwd_kernel(const void* __restric
                                                            int nu, float2* __restrict__ t) {
   constexpr int N = 32 * N1, G = 256 / N1;  // G row pairs per block
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* wn = (float2*)smem_raw;             // [N]
-  float2* ys = wn + N;                        // [G][32][N1+1]
+  float2* t2 = (float2*)smem_raw;             // [32][N1]
+  float2* t1 = t2 + 32 * N1;                  // [N1][N1]
+  float2* ys = t1 + N1 * N1;                  // [G][32][N1+1]
   float2* zs = ys + G * 32 * (N1 + 1);        // [G][nu]
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
-  for (int j = tid; j < N; j += 256) wn[j] = wn_g[j];
+  build_tables<N1>(wn_g, t2, t1, tid, 256);
   const long long r0 = (long long)blockIdx.x * (2 * G) + 2 * g;
   float2 z[32];
   if (r0 + 1 < nrows) {
@@ -136,12 +152,12 @@ __global__ void __launch_bounds__(256) fft_rows_fwd_kernel(const void* __restric
     for (int n2 = 0; n2 < 32; ++n2) z[n2] = make_float2(0.f, 0.f);
   }
   fft32<+1>(z);
-  __syncthreads();  // wn ready
+  __syncthreads();  // tables ready
   float2* yg = ys + g * 32 * (N1 + 1);
-  twiddle_store<+1, N1>(z, wn, n1, yg);
+  twiddle_store<+1, N1>(z, t2, n1, yg);
   __syncthreads();
   float2* zg = zs + g * nu;
-  for (int q = n1; q < nu; q += N1) zg[q] = outer_bin<+1, N1>(yg, wn, (u0 + q) & (N - 1));
+  for (int q = n1; q < nu; q += N1) zg[q] = outer_bin<+1, N1>(yg, t1, (u0 + q) & (N - 1));
   __syncthreads();
   // separate the two real rows and write t[b][ic][y] with y fastest (2G consecutive rows of one image)
   const long long rblk = (long long)blockIdx.x * (2 * G);
@@ -168,10 +184,11 @@ __global__ void __launch_bounds__(256) fft_cols_fwd_kernel(const float2* __restr
                                                            float scale, float2* __restrict__ band) {
   constexpr int N = 32 * N1, G = 256 / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* wn = (float2*)smem_raw;
-  float2* ys = wn + N;
+  float2* t2 = (float2*)smem_raw;
+  float2* t1 = t2 + 32 * N1;
+  float2* ys = t1 + N1 * N1;
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
-  for (int j = tid; j < N; j += 256) wn[j] = wn_g[j];
+  build_tables<N1>(wn_g, t2, t1, tid, 256);
   const long long col = (long long)blockIdx.x * G + g;
   float2 z[32];
   if (col < ncols) {
@@ -185,13 +202,13 @@ __global__ void __launch_bounds__(256) fft_cols_fwd_kernel(const float2* __restr
   fft32<+1>(z);
   __syncthreads();
   float2* yg = ys + g * 32 * (N1 + 1);
-  twiddle_store<+1, N1>(z, wn, n1, yg);
+  twiddle_store<+1, N1>(z, t2, n1, yg);
   __syncthreads();
   if (col >= ncols) return;
   const long long b = col / bc;
   const int ic = (int)(col - b * bc);
   for (int ir = n1; ir < br; ir += N1) {
-    float2 v = outer_bin<+1, N1>(yg, wn, (m0r + ir) & (N - 1));
+    float2 v = outer_bin<+1, N1>(yg, t1, (m0r + ir) & (N - 1));
     band[(b * br + ir) * (long long)bc + ic] = make_float2(v.x * scale, v.y * scale);
   }
 }
@@ -200,17 +217,17 @@ __global__ void __launch_bounds__(256) fft_cols_fwd_kernel(const float2* __restr
 // Thread n1 of a group: z[k2] = W_N^{-k2 n1} sum_{k1} coef(k2 + 32 k1) W_N1^{-k1 n1} over the non-zero
 // coefficients, which sit at frequencies q in [-qmax, qmax] (index q mod N); coef(q) = cq[q + qmax].
 template <int N1>
-__device__ __forceinline__ void inverse_gather(float2 (&z)[32], const float2* cq, int qmax, const float2* wn,
-                                               int n1) {
+__device__ __forceinline__ void inverse_gather(float2 (&z)[32], const float2* cq, int qmax, const float2* t2,
+                                               const float2* t1, int n1) {
   constexpr int N = 32 * N1;
 #pragma unroll
   for (int k2 = 0; k2 < 32; ++k2) {
     float2 acc = make_float2(0.f, 0.f);
     for (int k1 = 0; k2 + 32 * k1 <= qmax; ++k1)  // q = k2 + 32 k1 >= 0
-      cfma(acc, cq[k2 + 32 * k1 + qmax], wn_get<-1>(wn, (32 * k1 * n1) & (N - 1)));
+      cfma(acc, cq[k2 + 32 * k1 + qmax], sgn<-1>(t1[k1 * N1 + n1]));
     for (int k1 = N1 - 1; k1 > 0 && k2 + 32 * k1 >= N - qmax; --k1)  // q = k2 + 32 k1 - N < 0
-      cfma(acc, cq[k2 + 32 * k1 - N + qmax], wn_get<-1>(wn, (32 * k1 * n1) & (N - 1)));
-    z[k2] = cmul(acc, wn_get<-1>(wn, (k2 * n1) & (N - 1)));
+      cfma(acc, cq[k2 + 32 * k1 - N + qmax], sgn<-1>(t1[k1 * N1 + n1]));
+    z[k2] = cmul(acc, sgn<-1>(t2[k2 * N1 + n1]));
   }
   fft32<-1>(z);
 }
@@ -223,11 +240,12 @@ __global__ void __launch_bounds__(256) fft_cols_inv_kernel(const float2* __restr
                                                            float2* __restrict__ v) {
   constexpr int N = 32 * N1, G = 256 / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* wn = (float2*)smem_raw;
+  float2* t2 = (float2*)smem_raw;
+  float2* t1 = t2 + 32 * N1;
   const int nq = 2 * br - 1;
-  float2* cs = wn + N;  // [G][nq]
+  float2* cs = t1 + N1 * N1;  // [G][nq]
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
-  for (int j = tid; j < N; j += 256) wn[j] = wn_g[j];
+  build_tables<N1>(wn_g, t2, t1, tid, 256);
   const long long col0 = (long long)blockIdx.x * G;
   for (int e = tid; e < G * nq; e += 256) {
     const int jr = e / G, gg = e % G;
@@ -243,7 +261,7 @@ __global__ void __launch_bounds__(256) fft_cols_inv_kernel(const float2* __restr
   __syncthreads();
   const long long col = col0 + g;
   float2 z[32];
-  inverse_gather<N1>(z, cs + g * nq, br - 1, wn, n1);
+  inverse_gather<N1>(z, cs + g * nq, br - 1, t2, t1, n1);
   if (col >= ncols) return;
   float2* dst = v + col * N;
 #pragma unroll
@@ -258,12 +276,13 @@ __global__ void __launch_bounds__(256) fft_rows_inv_kernel(const float2* __restr
                                                            float* __restrict__ out) {
   constexpr int N = 32 * N1, G = 256 / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* wn = (float2*)smem_raw;
+  float2* t2 = (float2*)smem_raw;
+  float2* t1 = t2 + 32 * N1;
   const int nq = 2 * bc - 1;
-  float2* vs = wn + N;           // [bc][2G]
+  float2* vs = t1 + N1 * N1;     // [bc][2G]
   float2* cs = vs + bc * 2 * G;  // [G][nq]
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
-  for (int j = tid; j < N; j += 256) wn[j] = wn_g[j];
+  build_tables<N1>(wn_g, t2, t1, tid, 256);
   const long long rblk = (long long)blockIdx.x * (2 * G);
   for (int e = tid; e < bc * 2 * G; e += 256) {
     const int qc = e / (2 * G), rr = e % (2 * G);
@@ -291,7 +310,7 @@ __global__ void __launch_bounds__(256) fft_rows_inv_kernel(const float2* __restr
   __syncthreads();
   const long long r0 = rblk + 2 * g;
   float2 z[32];
-  inverse_gather<N1>(z, cs + g * nq, bc - 1, wn, n1);
+  inverse_gather<N1>(z, cs + g * nq, bc - 1, t2, t1, n1);
   if (r0 >= nrows) return;
   float* o0 = out + r0 * N;
   float* o1 = o0 + N;
@@ -316,14 +335,16 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
                                                               float2* __restrict__ ihat) {
   constexpr int MR = 32 * N1R, MC = 32 * N1C, T = 512;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* wr = (float2*)smem_raw;      // [MR]
-  float2* wc = wr + MR;                // [MC]
-  float2* area = wc + MC;              // [area_f2] union: coarse image / row transposes / column transposes
+  float2* r2 = (float2*)smem_raw;      // row-axis (MR) tables: [32][N1R], [N1R][N1R]
+  float2* r1 = r2 + 32 * N1R;
+  float2* c2 = r1 + N1R * N1R;         // column-axis (MC) tables: [32][N1C], [N1C][N1C]
+  float2* c1 = c2 + 32 * N1C;
+  float2* area = c1 + N1C * N1C;       // [area_f2] union: coarse image / row transposes / column transposes
   float2* u = area + area_f2;          // [MR][bc]
   const int tid = threadIdx.x;
   const long long img = blockIdx.x;
-  for (int j = tid; j < MR; j += T) wr[j] = wr_g[j];
-  for (int j = tid; j < MC; j += T) wc[j] = wc_g[j];
+  build_tables<N1R>(wr_g, r2, r1, tid, T);
+  build_tables<N1C>(wc_g, c2, c1, tid, T);
   float* cimg = (float*)area;
   const float4* src = (const float4*)(coarse + img * (long long)MR * MC);
   for (int j = tid; j < MR * MC / 4; j += T) ((float4*)cimg)[j] = __ldg(src + j);
@@ -339,13 +360,13 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
     fft32<+1>(z);
   }
   __syncthreads();  // the image is consumed; the area now holds row transposes
-  if (row_task) twiddle_store<+1, N1C>(z, wc, n1, area + p * 32 * (N1C + 1));
+  if (row_task) twiddle_store<+1, N1C>(z, c2, n1, area + p * 32 * (N1C + 1));
   __syncthreads();
   for (int e = tid; e < (MR / 2) * bc; e += T) {
     const int pp = e / bc, qc = e % bc;
     const float2* ys = area + pp * 32 * (N1C + 1);
-    const float2 zp = outer_bin<+1, N1C>(ys, wc, qc & (MC - 1));
-    const float2 zm = outer_bin<+1, N1C>(ys, wc, (-qc) & (MC - 1));
+    const float2 zp = outer_bin<+1, N1C>(ys, c1, qc & (MC - 1));
+    const float2 zm = outer_bin<+1, N1C>(ys, c1, (-qc) & (MC - 1));
     u[(2 * pp) * bc + qc] = make_float2(0.5f * (zp.x + zm.x), 0.5f * (zp.y - zm.y));
     u[(2 * pp + 1) * bc + qc] = make_float2(0.5f * (zp.y + zm.y), -0.5f * (zp.x - zm.x));
   }
@@ -359,13 +380,13 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
     fft32<+1>(z);
   }
   __syncthreads();  // row transposes are consumed; the area now holds column transposes
-  if (col_task) twiddle_store<+1, N1R>(z, wr, n1r, area + qc * 32 * (N1R + 1));
+  if (col_task) twiddle_store<+1, N1R>(z, r2, n1r, area + qc * 32 * (N1R + 1));
   __syncthreads();
   const int nq = 2 * br - 1;
   const float norm = 1.0f / ((float)MR * (float)MC);
   for (int e = tid; e < nq * bc; e += T) {
     const int jr = e / bc, c = e % bc;
-    const float2 v = outer_bin<+1, N1R>(area + c * 32 * (N1R + 1), wr, (jr - (br - 1)) & (MR - 1));
+    const float2 v = outer_bin<+1, N1R>(area + c * 32 * (N1R + 1), r1, (jr - (br - 1)) & (MR - 1));
     const float s = (c == 0 ? 1.0f : 2.0f) * norm;
     ihat[(img * nq + jr) * (long long)bc + c] = make_float2(v.x * s, v.y * s);
   }
@@ -377,7 +398,7 @@ static int launch_coarse_spec_fft(float* coarse, int count, int br, int bc, cons
   constexpr int MR = 32 * N1R, MC = 32 * N1C;
   const int rows_ys = (MR / 2) * 32 * (N1C + 1), c_f2 = MR * MC / 2, cols_ys = bc * 32 * (N1R + 1);
   const int area_f2 = max(rows_ys, max(c_f2, cols_ys));
-  const size_t smem = sizeof(float2) * ((size_t)MR + MC + area_f2 + (size_t)MR * bc);
+  const size_t smem = sizeof(float2) * ((size_t)table_f2<N1R>() + table_f2<N1C>() + area_f2 + (size_t)MR * bc);
   auto kern = coarse_spec_fft_kernel<N1R, N1C>;
   int rc = set_smem(kern, smem, "coarse spectrum fft");
   if (rc) return rc;
@@ -386,9 +407,11 @@ static int launch_coarse_spec_fft(float* coarse, int count, int br, int bc, cons
 }
 
 template <int N1>
-static size_t smem_rows_fwd(int nu) { return sizeof(float2) * (32 * N1 + (256 / N1) * 32 * (N1 + 1) + (256 / N1) * nu); }
+static size_t smem_rows_fwd(int nu) {
+  return sizeof(float2) * (table_f2<N1>() + (256 / N1) * 32 * (N1 + 1) + (256 / N1) * nu);
+}
 template <int N1>
-static size_t smem_cols_fwd() { return sizeof(float2) * (32 * N1 + (256 / N1) * 32 * (N1 + 1)); }
+static size_t smem_cols_fwd() { return sizeof(float2) * (table_f2<N1>() + (256 / N1) * 32 * (N1 + 1)); }
 
 
 template <int N1>
@@ -429,7 +452,7 @@ static int cols_fwd(const float2* t, int batch, int bc, const float2* wn_y, int 
 template <int N1>
 static int cols_inv(const float2* ihat, int count, int br, int bc, const float2* wn_y, float2* v, cudaStream_t s) {
   constexpr int G = 256 / N1;
-  size_t smem = sizeof(float2) * (32 * N1 + G * (2 * br - 1));
+  size_t smem = sizeof(float2) * (table_f2<N1>() + G * (2 * br - 1));
   int rc = set_smem(fft_cols_inv_kernel<N1>, smem, "oi_coarse_to_image_fft/cols");
   if (rc) return rc;
   const long long ncols = (long long)count * bc;
@@ -440,7 +463,7 @@ static int cols_inv(const float2* ihat, int count, int br, int bc, const float2*
 template <int N1>
 static int rows_inv(const float2* v, int count, int ny, int bc, const float2* wn_x, float* out, cudaStream_t s) {
   constexpr int G = 256 / N1;
-  size_t smem = sizeof(float2) * (32 * N1 + bc * 2 * G + G * (2 * bc - 1));
+  size_t smem = sizeof(float2) * (table_f2<N1>() + bc * 2 * G + G * (2 * bc - 1));
   int rc = set_smem(fft_rows_inv_kernel<N1>, smem, "oi_coarse_to_image_fft/rows");
   if (rc) return rc;
   const long long nrows = (long long)count * ny;
