@@ -76,6 +76,22 @@ OI_API int oi_band_spectrum(const void* field, int kind, int batch, int ny, int 
                             const void* wx, const void* wy, float scale, void* scratch, void* band, void* stream);
 
 /*
+ * oi_band_spectrum without a scratch argument, for callers that cannot allocate device memory -- code handed
+ * only the pointers of a host application that owns every allocation, or running inside a memory budget that
+ * is already fully given out.  No counterpart in the reference (which allocates freely through torch).
+ *   - Same inputs, output and result as oi_band_spectrum; the row-transform scratch is an array built into the
+ *     library, OI_NOALLOC_SCRATCH_COMPLEX complex values (16 MiB) on every GPU that loads it, held until the
+ *     process exits.  batch * nch * ny * bc above that capacity is rejected with OI_ERANGE.
+ *   - Calls no cudaMalloc / cudaFree.  The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls on a device share the one array: calls that can overlap on the GPU (different streams without
+ *     ordering between them) race.  Nothing in the array needs clearing between calls.
+ */
+#define OI_NOALLOC_SCRATCH_COMPLEX (1LL << 21) /* built-in scratch of oi_band_spectrum_noalloc, complex values */
+OI_API int oi_band_spectrum_noalloc(const void* field, int kind, int batch, int ny, int nx, int nch, int br, int bc,
+                                    const void* wx, const void* wy, float scale, void* band, void* stream);
+
+/*
  * Abbe pupils (CalculateAerialImage.py:46-75), one per (plane z, source point j, field component e):
  *   pupil[z][j*ne+e][ir][ic] = valid * obliquity * exp(2 pi i W) * defocus_z * transfer_e     (complex64)
  *   weight[z][j*ne+e]        = index_image * v[j] / weight_sum

@@ -27,10 +27,12 @@ _SIGS = {
     'oi_band_spectrum_fft': [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],
     'oi_coarse_to_image_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp,
                                _vp],
+    'oi_band_spectrum_noalloc': [_vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp],
     'oi_coherent_coarse_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _i, _i, _vp, _vp, _i, _vp, _vp],
 }
 
 FIELD_REAL_F32, FIELD_COMPLEX_C64, FIELD_U8 = 0, 1, 2
+NOALLOC_SCRATCH_COMPLEX = 1 << 21   # OI_NOALLOC_SCRATCH_COMPLEX of include/oi_b200.h
 
 
 class NativeError(RuntimeError):

@@ -7,6 +7,7 @@
 // The x pass streams the whole mask once; it is the HBM-facing part.  The y pass reads the small t.
 #include "oi_common.cuh"
 #include <cstdint>
+#include <mutex>
 
 namespace oi {
 
@@ -202,4 +203,62 @@ extern "C" int oi_band_spectrum(const void* field, int kind, int batch, int ny, 
   dim3 gy((unsigned)ceil_div(bc, YB_N), (unsigned)ceil_div(br, YB_M), (unsigned)(batch * nch));
   band_y_kernel<<<gy, 256, 0, s>>>((const float2*)scratch, ny, br, bc, (const float2*)wy, scale, (float2*)band);
   return check_launch("oi_band_spectrum/y");
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Band spectrum for callers that cannot allocate device memory.
+//
+// oi_band_spectrum needs a caller-provided scratch buffer for the intermediate row transform.  Some callers
+// cannot provide one: code that only ever receives device pointers from a host application that owns every
+// allocation (and forbids its plug-ins from calling cudaMalloc), or code running where an allocation would
+// stall or fail (inside a fixed memory budget that is already fully handed out).  This entry point serves
+// them: its scratch is a fixed-size array compiled into the library, one copy on each GPU that loads it,
+// kept until the process exits.  Only the inputs and the output come from the caller.
+namespace oi {
+
+constexpr long long kStaticScratchF2 = OI_NOALLOC_SCRATCH_COMPLEX;  // complex values: 16 MiB per device
+static __device__ __align__(256) float2 g_static_scratch[kStaticScratchF2];
+
+// Device address of g_static_scratch on each device, looked up once per device.  In host code the symbol
+// itself is only a host-side handle, so the address must come from cudaGetSymbolAddress.
+static float2* g_static_scratch_ptr[64] = {nullptr};
+static std::mutex g_static_scratch_mu;
+
+static int static_scratch(float2** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(OI_ECUDA, "oi_band_spectrum_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return fail(OI_ERANGE, "oi_band_spectrum_noalloc: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_static_scratch_mu);
+  if (!g_static_scratch_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(OI_ECUDA, "oi_band_spectrum_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    g_static_scratch_ptr[dev] = (float2*)p;
+  }
+  *out = g_static_scratch_ptr[dev];
+  return OI_OK;
+}
+
+}  // namespace oi
+
+extern "C" int oi_band_spectrum_noalloc(const void* field, int kind, int batch, int ny, int nx, int nch, int br,
+                                        int bc, const void* wx, const void* wy, float scale, void* band,
+                                        void* stream) {
+  using namespace oi;
+  if (!field || !wx || !wy || !band || batch <= 0 || ny <= 0 || nx <= 0 || nch <= 0 || br <= 0 || bc <= 0)
+    return fail(OI_EINVAL, "oi_band_spectrum_noalloc: bad arguments (batch=%d ny=%d nx=%d nch=%d br=%d bc=%d)",
+                batch, ny, nx, nch, br, bc);
+  const long long need = (long long)batch * nch * ny * bc;
+  if (need > kStaticScratchF2)
+    return fail(OI_ERANGE,
+                "oi_band_spectrum_noalloc: needs %lld complex scratch values (batch*nch*ny*bc) but the built-in "
+                "scratch holds %lld; use oi_band_spectrum with a caller buffer or split the batch",
+                need, kStaticScratchF2);
+  float2* scratch = nullptr;
+  int rc = static_scratch(&scratch);
+  if (rc) return rc;
+  // every scratch entry the y pass reads is written by the x pass first: nothing needs clearing
+  return oi_band_spectrum(field, kind, batch, ny, nx, nch, br, bc, wx, wy, scale, scratch, band, stream);
 }
