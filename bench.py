@@ -156,6 +156,44 @@ def stage_times(sk, masks, out, reps=5):
     return acc
 
 
+def serve_measure(sk, info, masks_np, dev, args):
+    """Served throughput and latency of config-3 requests, against the plain path on the same requests."""
+    from opticalimaging_b200 import serve
+    sr, po, nm, T, fg = info
+    spec = serve.ModelSpec(('socs24', N_PIX, PERIOD), N_PIX, N_PIX, 1,
+                           build=lambda: serve_model_from(sk))
+    pinned = [torch.from_numpy(m.astype(np.uint8)).pin_memory() for m in masks_np]
+    nreq = max(4 * BATCH, args.serve_requests)
+    reqs = [pinned[i % len(pinned)] for i in range(nreq)]
+    ex = serve.CudaExecutor(device=dev, nslots=3)
+    srv = serve.Server(ex, hbm_budget=150e9, max_batch=BATCH)
+    for f in [srv.submit(spec, r) for r in reqs[:2 * BATCH]]:       # warm-up: model, buffers, graphs
+        f.result()
+    srv.completed.clear()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    futs = [srv.submit(spec, r) for r in reqs]
+    for f in futs:
+        f.result()
+    dt = time.perf_counter() - t0
+    lat = srv.latency_ms()
+    srv.close()
+    nplain = min(32, nreq)
+    _, tp = serve.plain_run([(spec, reqs[i]) for i in range(nplain)], device=dev)
+    served = nreq / dt
+    plain = nplain / tp
+    return {"images_per_s": served, "p50_ms": lat.get("p50_ms"), "p99_ms": lat.get("p99_ms"),
+            "requests": nreq, "arrival": "all submitted at once (saturated)", "batches": srv.batches,
+            "plain_images_per_s": plain, "served_over_plain": served / plain,
+            "plain": "one request at a time: H2D, image (batch 1, FP32 FFT form, no graph), D2H, synchronise",
+            "h2d_bytes_per_image": N_PIX * N_PIX, "d2h_bytes_per_image": 4 * N_PIX * N_PIX}
+
+
+def serve_model_from(sk):
+    from opticalimaging_b200.engine import CoherentModel
+    return CoherentModel(sk.pupils, sk.weights, sk.band, sk.ny, sk.nx)
+
+
 def cpu_reference_sample(sk_info, masks_np, budget_s, threads):
     """Time the reference's algorithm (oracle/cpu_reference.py) on host cores for a bounded sample of clips."""
     from oracle import cpu_reference as R
@@ -277,6 +315,9 @@ def run_engine(args, world, rank, local):
     barrier(world)
     ms_e2e = max_over_ranks(s2.elapsed_time(e2), world)
     e2e_value = world * BATCH * args.steps / (ms_e2e / 1000.0)
+    # ---- served: the same clips as requests through the continuous-batching server (pinned uint8 in,
+    # host float32 images out), saturated arrival; and the plain one-request-at-a-time path
+    serving = serve_measure(sk, info, masks_np, dev, args)
     # ---- per-stage device times (outside the timed region) and the roofline of the dominant stage
     st = stage_times(sk, masks, out)
     hbm, bf16, src = peaks()
@@ -301,7 +342,7 @@ def run_engine(args, world, rank, local):
                        "(256 MB float32 masks + 256 MB images per step)", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_in.numel()),
                     "d2h_bytes_per_step": int(host_out.numel() * 4)},
-            "gpu_launches": 5 * args.steps, "setup_s": setup_s,
+            "gpu_launches": 5 * args.steps, "setup_s": setup_s, "serving": serving,
             "stage_ms": {k: round(v, 4) for k, v in st.items()}, "roofline": roof, "clocks": clk.summary()}
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -325,6 +366,7 @@ def main():
     ap.add_argument('--cpu-budget', type=float, default=15.0)
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--batch', type=int, default=64, help='clips per step (64 in the benchmark configuration)')
+    ap.add_argument('--serve-requests', type=int, default=512, help='requests in the served measurement')
     args = ap.parse_args()
     global BATCH
     BATCH = args.batch

@@ -145,9 +145,9 @@ static int launch_coherent(const CoherentArgs& a, int batch, cudaStream_t s) {
   size_t smem = sizeof(float2) * ((size_t)CO_RC * NU * 64 + CO_TR * CO_RC + (size_t)CO_TR * NU * 64 +
                                   (size_t)CO_CC * a.mc);
   auto kern = coherent_coarse_kernel<NU, NJ>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return fail(OI_ECUDA, "oi_coherent_coarse: smem attribute: %s", cudaGetErrorString(e));
+  {
+    int rc_smem = ensure_smem((const void*)kern, smem, "oi_coherent_coarse");
+    if (rc_smem) return rc_smem;
   }
   dim3 grid((unsigned)ceil_div(a.mr, CO_TR), (unsigned)a.nz, (unsigned)batch);
   kern<<<grid, 256, smem, s>>>(a);

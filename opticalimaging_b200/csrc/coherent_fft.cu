@@ -147,9 +147,9 @@ static int launch_cfft(const CoherentFftArgs& a, int batch, cudaStream_t s) {
   constexpr int MR = 32 * N1R, MC = 32 * N1C, T = MC * N1R;
   size_t smem = sizeof(float2) * ((size_t)MR + MC + (size_t)a.br * a.bc + (size_t)a.br * (MC + 1));
   auto kern = coherent_fft_kernel<N1R, N1C>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return fail(OI_ECUDA, "oi_coherent_coarse_fft: smem attribute: %s", cudaGetErrorString(e));
+  {
+    int rc_smem = ensure_smem((const void*)kern, smem, "oi_coherent_coarse_fft");
+    if (rc_smem) return rc_smem;
   }
   dim3 grid((unsigned)a.nsplit, (unsigned)a.nz, (unsigned)batch);
   kern<<<grid, T, smem, s>>>(a);

@@ -64,11 +64,7 @@ __device__ __forceinline__ void fft32(float2 (&v)[32]) {
 
 template <typename K>
 static int set_smem(K kern, size_t bytes, const char* what) {
-  if (bytes > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return fail(OI_ECUDA, "%s: smem attribute: %s", what, cudaGetErrorString(e));
-  }
-  return OI_OK;
+  return ensure_smem((const void*)kern, bytes, what);
 }
 
 template <int KIND> __device__ __forceinline__ float load_real(const void* f, long long i);

@@ -13,6 +13,11 @@ int fail(int code, const char* fmt, ...);
 // Checks the launch just enqueued; returns OI_OK or OI_ECUDA with the CUDA error text recorded.
 int check_launch(const char* what);
 
+// Lets `kern` use `bytes` of dynamic shared memory.  Above the 48 KB default the kernel's limit is raised to
+// the device's opt-in maximum, once per (kernel, device) -- so later launches, including ones inside CUDA-graph
+// capture, make no attribute call.
+int ensure_smem(const void* kern, size_t bytes, const char* what);
+
 __host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }

@@ -142,9 +142,9 @@ int coarse_spectrum(float* coarse, int count, int mr, int mc, int br, int bc, co
   if (rc) return rc;
   nparts = 1;
   size_t smem = sizeof(float2) * (size_t)mr * SP_QT;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(coarse_spec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return fail(OI_ECUDA, "coarse spectrum: smem attribute: %s", cudaGetErrorString(e));
+  {
+    int rc_smem = ensure_smem((const void*)coarse_spec_kernel, smem, "coarse spectrum");
+    if (rc_smem) return rc_smem;
   }
   dim3 g1((unsigned)ceil_div(bc, SP_QT), (unsigned)count);
   coarse_spec_kernel<<<g1, 256, smem, s>>>(coarse, nparts, (long long)count * mr * mc, mr, mc, br, bc,

@@ -1,6 +1,9 @@
 // Phase tables, status reporting and version of liboi_b200.
 #include "oi_common.cuh"
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <utility>
 
 namespace oi {
 
@@ -12,6 +15,26 @@ int fail(int code, const char* fmt, ...) {
   vsnprintf(g_err, sizeof(g_err), fmt, ap);
   va_end(ap);
   return code;
+}
+
+int ensure_smem(const void* kern, size_t bytes, const char* what) {
+  if (bytes <= 48 * 1024) return OI_OK;
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(OI_ECUDA, "%s: cudaGetDevice: %s", what, cudaGetErrorString(e));
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;  // (kernel, device) pairs raised to the opt-in maximum
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({kern, dev})) return OI_OK;
+  int optin = 0;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return fail(OI_ECUDA, "%s: shared memory limit: %s", what, cudaGetErrorString(e));
+  if (bytes > (size_t)optin)
+    return fail(OI_ERANGE, "%s: needs %zu bytes of shared memory, the device allows %d", what, bytes, optin);
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  if (e != cudaSuccess) return fail(OI_ECUDA, "%s: smem attribute: %s", what, cudaGetErrorString(e));
+  done.insert({kern, dev});
+  return OI_OK;
 }
 
 int check_launch(const char* what) {

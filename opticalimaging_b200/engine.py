@@ -246,28 +246,83 @@ def centred(start: int, n: int) -> int:
     return s - n if s >= n - n // 2 else s
 
 
-# ------------------------------------------------------------------------------------------ SOCS model
-class SocsKernels:
-    """SOCS kernels resident on the device in band form: [K, br, bc] complex64 on `band`, for a ny x nx grid.
+# ------------------------------------------------------------------------------------- resident models
+class CoherentModel:
+    """Fields resident on the device for one optics key and grid: pupils [Z, K, br, bc] complex64 with weights
+    [Z, K] on `band`, for a ny x nx grid.  image() of a batch of masks is
+        out[b, z] = sum_k w[z, k] |IDFT(P[z, k] .* c_b)|^2        (summed over the masks' channels too)
+    -- SOCS kernels of Z focus planes (w = 1, CalculateAerialImage_SOCS.py:3-11) or the Abbe pupils of every
+    (source point, field component) (w = n v_j / sum v, CalculateAerialImage.py:46-92).
+    """
+
+    def __init__(self, pupils: torch.Tensor, weights: torch.Tensor, band: Band, ny: int, nx: int, kind: str = 'socs'):
+        if pupils.dim() != 4 or pupils.shape[2:] != (band.br, band.bc):
+            raise ValueError('pupils must be [Z, K, br, bc] on the band')
+        if weights.shape != pupils.shape[:2]:
+            raise ValueError('weights must be [Z, K]')
+        if band.br > ny or band.bc > nx:
+            raise ValueError(f'band {band.br}x{band.bc} does not fit the {ny}x{nx} grid')
+        self.device = require_cuda(pupils.device)
+        self.pupils = pupils.to(self.device, torch.complex64).contiguous()
+        self.weights = weights.to(self.device, torch.float32).contiguous()
+        self.band, self.ny, self.nx, self.kind = band, ny, nx, kind
+        self.plan = Plan.get(ny, nx, band, self.device)
+
+    @property
+    def planes(self):
+        return self.pupils.shape[0]
+
+    @property
+    def count(self):
+        return self.pupils.shape[1]
+
+    @property
+    def nbytes(self):
+        return self.pupils.numel() * 8 + self.weights.numel() * 4
+
+    def workspace_bytes(self, batch: int, nch: int = 1) -> int:
+        """Device bytes one image() call of `batch` masks allocates besides its input and output."""
+        b, p = self.band, self.plan
+        nz = self.planes
+        split = field_split(self.count * nch, batch * nz) if p.use_coarse_fft(None) else 1
+        return 8 * (batch * nch * p.ny * b.bc + batch * nch * b.br * b.bc + batch * nz * (2 * b.br - 1) * b.bc
+                    + batch * nz * b.bc * p.ny) + 4 * split * batch * nz * p.mr * p.mc
+
+    def _kind(self, masks):
+        return {torch.float32: N.FIELD_REAL_F32, torch.uint8: N.FIELD_U8,
+                torch.complex64: N.FIELD_COMPLEX_C64}[masks.dtype]
+
+    def image(self, masks: torch.Tensor, kind: int | None = None, nch: int = 1, scale: float = 1.0,
+              out: torch.Tensor | None = None, marks=None, form: str | None = None) -> torch.Tensor:
+        """Aerial images of a batch of masks -> [B, Z, ny, nx] float32.
+
+        masks: float32 [B, ny, nx] (real transmission), uint8 [B, ny, nx] or complex64 [B, ny, nx, nch].
+        `marks`, if a list, receives (stage name, CUDA event) pairs recorded after each native stage.
+        `form` picks the transform form of the two N-point stages: 'fft' (default where supported) or 'dft'.
+        """
+        if kind is None:
+            kind = self._kind(masks)
+        if masks.shape[1] != self.ny or masks.shape[2] != self.nx:
+            raise ValueError(f'mask grid {tuple(masks.shape[1:3])} != model grid {(self.ny, self.nx)}')
+        _mark(marks, 'start')
+        band = band_spectrum(masks.contiguous(), kind, self.plan, nch=nch, scale=scale, form=form)
+        _mark(marks, 'band_spectrum')
+        return coherent_image(band, self.pupils, self.weights, self.plan, out=out, marks=marks, form=form)
+
+
+class SocsKernels(CoherentModel):
+    """SOCS kernels of one focus plane resident on the device in band form: [K, br, bc] complex64.
 
     This is the engine's form of the reference's full-grid kernel array (DecomposeTCC_SOCS.py:26-35): the same
-    values, with only the band that can be non-zero kept.
+    values, with only the band that can be non-zero kept.  image() returns [B, ny, nx].
     """
 
     def __init__(self, kernels: torch.Tensor, band: Band, ny: int, nx: int):
         if kernels.dim() != 3 or kernels.shape[1:] != (band.br, band.bc):
             raise ValueError('kernels must be [K, br, bc] on the band')
-        if band.br > ny or band.bc > nx:
-            raise ValueError(f'kernel band {band.br}x{band.bc} does not fit the {ny}x{nx} grid')
-        self.device = require_cuda(kernels.device)
-        self.kernels = kernels.to(self.device, torch.complex64).contiguous()
-        self.band, self.ny, self.nx = band, ny, nx
-        self.weights = torch.ones((1, self.kernels.shape[0]), dtype=torch.float32, device=self.device)
-        self.plan = Plan.get(ny, nx, band, self.device)
-
-    @property
-    def count(self):
-        return self.kernels.shape[0]
+        k = kernels.shape[0]
+        super().__init__(kernels.unsqueeze(0), torch.ones((1, k), device=kernels.device), band, ny, nx, 'socs')
+        self.kernels = self.pupils[0]
 
     @classmethod
     def from_full_grid(cls, kernels: torch.Tensor) -> 'SocsKernels':
@@ -284,21 +339,7 @@ class SocsKernels:
 
     def image(self, masks: torch.Tensor, kind: int | None = None, nch: int = 1, scale: float = 1.0,
               out: torch.Tensor | None = None, marks=None, form: str | None = None) -> torch.Tensor:
-        """SOCS aerial images of a batch of masks -> [B, ny, nx] float32.
-
-        masks: float32 [B, ny, nx] (real transmission), uint8 [B, ny, nx] or complex64 [B, ny, nx, nch].
-        `marks`, if a list, receives (stage name, CUDA event) pairs recorded after each native stage.
-        `form` picks the transform form of the two N-point stages: 'fft' (default where supported) or 'dft'.
-        """
-        if kind is None:
-            kind = {torch.float32: N.FIELD_REAL_F32, torch.uint8: N.FIELD_U8,
-                    torch.complex64: N.FIELD_COMPLEX_C64}[masks.dtype]
-        if masks.shape[1] != self.ny or masks.shape[2] != self.nx:
-            raise ValueError(f'mask grid {tuple(masks.shape[1:3])} != kernel grid {(self.ny, self.nx)}')
-        _mark(marks, 'start')
-        band = band_spectrum(masks.contiguous(), kind, self.plan, nch=nch, scale=scale, form=form)
-        _mark(marks, 'band_spectrum')
-        img = coherent_image(band, self.kernels.unsqueeze(0), self.weights, self.plan,
-                             out=None if out is None else out.view(masks.shape[0], 1, self.ny, self.nx),
-                             marks=marks, form=form)
+        """SOCS aerial images of a batch of masks -> [B, ny, nx] float32 (see CoherentModel.image)."""
+        o = None if out is None else out.view(masks.shape[0], 1, self.ny, self.nx)
+        img = super().image(masks, kind=kind, nch=nch, scale=scale, out=o, marks=marks, form=form)
         return img.view(masks.shape[0], self.ny, self.nx)

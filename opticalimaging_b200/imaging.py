@@ -26,12 +26,14 @@ import warnings
 import torch
 
 from . import _native as N
-from .engine import Band, Plan, SocsKernels, abbe_band, band_spectrum, coherent_image, require_cuda
+from .engine import (Band, CoherentModel, Plan, SocsKernels, abbe_band, band_spectrum, coherent_image,
+                     require_cuda)
 from .params import ImageData, cartesian_to_polar  # noqa: F401
 
 __all__ = ['CalculateAbbeImage', 'CalculateHopkinsImage', 'CalculateOptimized', 'CalculateTCCMatrix',
            'GetTCCMatrix', 'DecomposeTCC_SOCS', 'CalculateAerialImage_SOCS', 'CalculateSOCS',
-           'CalculateCharacteristicMatrix', 'calculate_spectrum', 'socs_kernels_from_tcc']
+           'CalculateCharacteristicMatrix', 'calculate_spectrum', 'socs_kernels_from_tcc', 'socs_model',
+           'abbe_model']
 
 
 # ------------------------------------------------------------------------------------------- helpers
@@ -151,40 +153,54 @@ def _image_data(intensity, scatter, projector):
 
 
 # ----------------------------------------------------------------------------------------------- Abbe
-def abbe_intensity(source, scatter, projector, numerics, h=None):
-    """Abbe image [nFocus, Ny, Nx] float32 on the device (CalculateAerialImage.py:18-92)."""
+def abbe_model(source, projector, numerics, period_y, period_x, ny, nx, focus=None) -> CoherentModel:
+    """Abbe pupils of every (focus plane, source point, field component) resident on the device
+    (CalculateAerialImage.py:30-75): a CoherentModel whose image() is the Abbe image of a batch of masks."""
     vector = _mode(numerics)
     _check_domain(projector)
     dev = require_cuda()
     sd = source.Calc_SourceSimple()
     X, Y, V = (t.reshape(-1).to(torch.float32) for t in (sd.X, sd.Y, sd.Value))
-    if h is None:
-        h = _field_on_device(scatter, dev)
-    ny, nx, nch = h.shape
-    zs = _focus_list(projector)
-    f, g, npx, npy = _axes(scatter, projector, source)
+    zs = _focus_list(projector) if focus is None else [float(z) for z in focus]
+    npx = period_x / (source.Wavelength / projector.NA)
+    npy = period_y / (source.Wavelength / projector.NA)
+    f = (1 / npx) * torch.arange(-(nx // 2), (nx + 1) // 2)
+    g = (1 / npy) * torch.arange(-(ny // 2), (ny + 1) // 2)
     nsrc = X.numel()
-    if nsrc == 0:   # the reference divides 0 by a zero source weight
-        return torch.full((len(zs), ny, nx), float('nan'), device=dev)
+    if nsrc == 0:
+        raise ValueError('the source has no points above the weight threshold')
     band = abbe_band(ny, nx, npy, npx, X, Y)
     if band is None:
-        return torch.zeros((len(zs), ny, nx), device=dev)
+        return None
     ne = 3 if vector else 1
     fr = g[band.m0r + ny // 2: band.m0r + ny // 2 + band.br].to(dev)
     fc = f[band.m0c + nx // 2: band.m0c + nx // 2 + band.bc].to(dev)
     Xd, Yd, Vd = X.to(dev), Y.to(dev), V.to(dev)
-    focus = torch.tensor(zs, dtype=torch.float64, device=dev)
+    fz = torch.tensor(zs, dtype=torch.float64, device=dev)
     pupils = torch.empty((len(zs), nsrc * ne, band.br, band.bc), dtype=torch.complex64, device=dev)
     weights = torch.empty((len(zs), nsrc * ne), dtype=torch.float32, device=dev)
-    wsum = float(torch.sum(V))
-    s = N.stream_handle(dev)
     N.call('oi_abbe_pupils', N.ptr(fr), N.ptr(fc), band.br, band.bc, N.ptr(Xd), N.ptr(Yd), N.ptr(Vd), nsrc,
-           wsum, N.ptr(focus), len(zs), _zernike(projector), int(vector), _jones(source), float(projector.NA),
-           float(projector.Magnification), float(projector.IndexImage), float(source.Wavelength), N.ptr(pupils),
-           N.ptr(weights), s)
-    plan = Plan.get(ny, nx, band, dev)
-    c = band_spectrum(h.unsqueeze(0), N.FIELD_COMPLEX_C64, plan, nch=nch)
-    return coherent_image(c, pupils, weights, plan)[0]
+           float(torch.sum(V)), N.ptr(fz), len(zs), _zernike(projector), int(vector), _jones(source),
+           float(projector.NA), float(projector.Magnification), float(projector.IndexImage),
+           float(source.Wavelength), N.ptr(pupils), N.ptr(weights), N.stream_handle(dev))
+    return CoherentModel(pupils, weights, band, ny, nx, kind='abbe')
+
+
+def abbe_intensity(source, scatter, projector, numerics, h=None):
+    """Abbe image [nFocus, Ny, Nx] float32 on the device (CalculateAerialImage.py:18-92)."""
+    dev = require_cuda()
+    if h is None:
+        h = _field_on_device(scatter, dev)
+    ny, nx, nch = h.shape
+    zs = _focus_list(projector)
+    sd = source.Calc_SourceSimple()
+    if sd.Value.numel() == 0:   # the reference divides 0 by a zero source weight
+        _mode(numerics)
+        return torch.full((len(zs), ny, nx), float('nan'), device=dev)
+    model = abbe_model(source, projector, numerics, scatter.Period_Y, scatter.Period_X, ny, nx)
+    if model is None:
+        return torch.zeros((len(zs), ny, nx), device=dev)
+    return model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=nch)[0]
 
 
 def CalculateAbbeImage(source, scatter, projector, numerics):
@@ -315,19 +331,31 @@ def CalculateAerialImage_SOCS(scatter, TCCMatrix_SOCS, source, projector):
     return img.to(rd), pim.to(rd)
 
 
+def socs_model(source, projector, numerics, period_y, period_x, ny, nx, focus=None) -> CoherentModel:
+    """SOCS kernels of every focus plane resident on the device: per plane TCC -> FP64 top-K eigenpairs ->
+    kernels placed as the reference places them (CalculateAerialImage.py:112-119).  image() gives the Hopkins
+    image of a batch of masks, all planes in one pass."""
+    zs = _focus_list(projector) if focus is None else [float(z) for z in focus]
+    sets = []
+    for z in zs:
+        tcc, fg = CalculateTCCMatrix(source, [period_y, period_x], projector, z, numerics)
+        sets.append(socs_kernels_from_tcc(tcc, fg, [nx, ny], numerics))
+    k = max(s.count for s in sets)   # 'threshold' may keep a different count per plane: pad with zero kernels
+    pupils = torch.zeros((len(zs), k, sets[0].band.br, sets[0].band.bc), dtype=torch.complex64,
+                         device=sets[0].kernels.device)
+    for i, s in enumerate(sets):
+        pupils[i, :s.count] = s.kernels
+    return CoherentModel(pupils, torch.ones((len(zs), k), device=pupils.device), sets[0].band, ny, nx, 'socs')
+
+
 def hopkins_intensity(source, scatter, projector, numerics, h=None):
     """Hopkins image [nFocus, Ny, Nx] on the device: per plane TCC -> top-K kernels -> SOCS image."""
     dev = require_cuda()
     if h is None:
         h = _field_on_device(scatter, dev)
     ny, nx = h.shape[0], h.shape[1]
-    zs = _focus_list(projector)
-    out = torch.empty((len(zs), ny, nx), dtype=torch.float32, device=dev)
-    for i, z in enumerate(zs):
-        tcc, fg = CalculateTCCMatrix(source, [scatter.Period_Y, scatter.Period_X], projector, z, numerics)
-        sk = socs_kernels_from_tcc(tcc, fg, [nx, ny], numerics)
-        out[i] = sk.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
-    return out
+    model = socs_model(source, projector, numerics, scatter.Period_Y, scatter.Period_X, ny, nx)
+    return model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
 
 
 def CalculateHopkinsImage(source, scatter, projector, numerics):

@@ -1,0 +1,423 @@
+"""Continuous-batching aerial-image server.
+
+Requests -- one mask each, for any optics key and grid -- arrive from any thread through ``Server.submit`` and
+get a ``concurrent.futures.Future``.  A scheduler thread groups waiting requests that share a resident model
+(same optics key, grid and mask dtype), and whenever an execution slot is free it admits the oldest group's
+next batch, provided the device memory it needs fits the HBM budget (idle models and buffers are evicted,
+least recently used first, to make room).  The executor runs the batch on the slot's own CUDA stream: one
+host->device copy per mask, the replay of the CUDA graph captured for that (model, batch size, slot), one
+device->host copy of the images.  Batches on different slots overlap on the device, so copies of one batch run
+under the kernels of another, and requests that arrive while batches are in flight join the next batch formed
+-- continuous batching rather than a queue.
+
+The scheduler only talks to an executor interface (``launch`` / ``poll`` / ``collect`` / memory accounting), so
+its batching, admission and failure handling are exercised on the CPU with a fake executor in the tests; the
+device executor is ``CudaExecutor``.
+
+Failure behaviour: a malformed request (wrong shape or dtype) fails at submit; a request whose batch can never
+fit the budget fails with MemoryError; a cancelled future is dropped before launch; an executor error fails
+the futures of its batch and the server keeps serving.
+"""
+from __future__ import annotations
+
+import collections
+import concurrent.futures as cf
+import math
+import threading
+import time
+from dataclasses import dataclass, field
+
+import torch
+
+
+# ------------------------------------------------------------------------------------------- requests
+@dataclass(frozen=True)
+class ModelSpec:
+    """A resident imaging model: `key` identifies it, `build()` creates it on the device (CoherentModel)."""
+    key: tuple
+    ny: int
+    nx: int
+    planes: int
+    build: object = field(compare=False, hash=False, repr=False)
+
+    @property
+    def pixels(self):
+        return self.ny * self.nx
+
+
+@dataclass
+class Request:
+    spec: ModelSpec
+    mask: torch.Tensor
+    future: cf.Future
+    t_submit: float
+    t_done: float = 0.0
+    rid: int = 0
+
+
+def bucket(n: int) -> int:
+    """Batch sizes are rounded up to powers of two, so one captured graph serves a range of batch sizes."""
+    return 1 << max(0, math.ceil(math.log2(max(1, n))))
+
+
+# ------------------------------------------------------------------------------------------ scheduler
+class Server:
+    """Continuous-batching scheduler over an executor (see module docstring)."""
+
+    def __init__(self, executor, hbm_budget: float = 150e9, max_batch_pixels: int = 64 * 1024 * 1024,
+                 max_batch: int = 256, idle_wait: float = 0.0002):
+        self.ex = executor
+        self.budget = float(hbm_budget)
+        self.max_batch_pixels = max_batch_pixels
+        self.max_batch = max_batch
+        self.idle_wait = idle_wait
+        self._inbox = collections.deque()
+        self._cv = threading.Condition()
+        self._pending: dict = collections.OrderedDict()   # group key -> deque of requests
+        self._slots = [None] * executor.nslots            # slot -> (spec, [requests])
+        self._last_used: dict = {}
+        self._closed = False
+        self._rid = 0
+        self.completed = []          # finished requests (for latency statistics)
+        self.batches = 0
+        self.rejected = 0
+        self._thread = threading.Thread(target=self._run, name='oi-serve', daemon=True)
+        self._thread.start()
+
+    # ---- public
+    def submit(self, spec: ModelSpec, mask: torch.Tensor) -> cf.Future:
+        """Queue one mask [ny, nx] (uint8 or float32, host or device) for imaging with `spec`'s model.
+        The future's result is the image [planes, ny, nx] float32 on the executor's result device."""
+        fut = cf.Future()
+        if not isinstance(mask, torch.Tensor) or mask.dim() != 2 or tuple(mask.shape) != (spec.ny, spec.nx):
+            fut.set_exception(ValueError(f'mask must be a [{spec.ny}, {spec.nx}] tensor, got '
+                                         f'{tuple(mask.shape) if isinstance(mask, torch.Tensor) else type(mask)}'))
+            return fut
+        if mask.dtype not in (torch.uint8, torch.float32):
+            fut.set_exception(ValueError(f'mask dtype must be uint8 or float32, got {mask.dtype}'))
+            return fut
+        with self._cv:
+            if self._closed:
+                fut.set_exception(RuntimeError('server is closed'))
+                return fut
+            self._rid += 1
+            self._inbox.append(Request(spec, mask, fut, time.perf_counter(), rid=self._rid))
+            self._cv.notify()
+        return fut
+
+    def close(self, wait: bool = True):
+        with self._cv:
+            self._closed = True
+            self._cv.notify()
+        if wait:
+            self._thread.join()
+
+    def drain(self, timeout: float = 600.0):
+        """Block until every submitted request has completed."""
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < timeout:
+            with self._cv:
+                busy = self._inbox or any(self._pending.values()) or any(s is not None for s in self._slots)
+            if not busy:
+                return
+            time.sleep(0.0005)
+        raise TimeoutError('requests still pending')
+
+    def latency_ms(self):
+        lat = sorted((r.t_done - r.t_submit) * 1e3 for r in self.completed)
+        if not lat:
+            return {}
+        pick = lambda q: lat[min(len(lat) - 1, int(math.ceil(q * len(lat))) - 1)]  # noqa: E731
+        return {"p50_ms": pick(0.50), "p99_ms": pick(0.99), "max_ms": lat[-1], "count": len(lat)}
+
+    # ---- scheduler thread
+    def _group_key(self, r: Request):
+        return (r.spec.key, r.mask.dtype)
+
+    def _max_batch(self, spec: ModelSpec) -> int:
+        return max(1, min(self.max_batch, self.max_batch_pixels // spec.pixels, self.ex.max_batch(spec)))
+
+    def _run(self):
+        init = getattr(self.ex, 'thread_init', None)
+        if init is not None:
+            init()
+        while True:
+            with self._cv:
+                while self._inbox:
+                    r = self._inbox.popleft()
+                    self._pending.setdefault(self._group_key(r), collections.deque()).append(r)
+                closing = self._closed
+            progressed = self._complete() | self._launch()
+            with self._cv:
+                idle = not self._inbox and not any(self._pending.values()) and all(s is None for s in self._slots)
+                if closing and idle:
+                    self.ex.shutdown()
+                    return
+                if not progressed and not self._inbox:
+                    self._cv.wait(self.idle_wait)
+
+    def _complete(self) -> bool:
+        done = False
+        for i, s in enumerate(self._slots):
+            if s is None or not self.ex.poll(i):
+                continue
+            spec, reqs = s
+            try:
+                results = self.ex.collect(i)
+                err = None
+            except Exception as e:  # noqa: BLE001 -- an executor failure fails this batch only
+                results, err = None, e
+            now = time.perf_counter()
+            for j, r in enumerate(reqs):
+                r.t_done = now
+                if err is not None:
+                    r.future.set_exception(err)
+                else:
+                    r.future.set_result(results[j])
+                    self.completed.append(r)
+            self._slots[i] = None
+            done = True
+        return done
+
+    def _take(self, key, spec):
+        q = self._pending[key]
+        batch = []
+        limit = self._max_batch(spec)
+        while q and len(batch) < limit:
+            r = q.popleft()
+            if r.future.set_running_or_notify_cancel():
+                batch.append(r)
+        if not q:
+            del self._pending[key]
+        return batch
+
+    def _fits(self, spec, n) -> bool:
+        need = self.ex.bytes_needed(spec, n)
+        if self.ex.resident_bytes() + need <= self.budget:
+            return True
+        busy = {s[0].key for s in self._slots if s is not None}
+        for key in sorted(self._last_used, key=self._last_used.get):   # least recently used first
+            if key in busy or key == spec.key:
+                continue
+            self.ex.evict(key)
+            self._last_used.pop(key, None)
+            if self.ex.resident_bytes() + need <= self.budget:
+                return True
+        return False
+
+    def _launch(self) -> bool:
+        launched = False
+        while self._pending:
+            free = [i for i, s in enumerate(self._slots) if s is None]
+            if not free:
+                break
+            # the group whose oldest request has waited longest
+            key = min(self._pending, key=lambda k: self._pending[k][0].t_submit if self._pending[k] else math.inf)
+            if not self._pending[key]:
+                del self._pending[key]
+                continue
+            spec = self._pending[key][0].spec
+            n = min(len(self._pending[key]), self._max_batch(spec))
+            if not self._fits(spec, n):
+                if all(s is None for s in self._slots):     # nothing will free memory: refuse the group
+                    err = MemoryError(f'model {spec.key!r} with a batch of {n} needs '
+                                      f'{self.ex.bytes_needed(spec, n) / 1e9:.2f} GB, over the '
+                                      f'{self.budget / 1e9:.2f} GB budget')
+                    for r in self._pending.pop(key):
+                        if r.future.set_running_or_notify_cancel():
+                            r.future.set_exception(err)
+                            self.rejected += 1
+                    continue
+                break                                          # wait for an in-flight batch to free memory
+            batch = self._take(key, spec)
+            if not batch:
+                continue
+            slot = free[0]
+            try:
+                self.ex.launch(slot, spec, batch)
+            except Exception as e:  # noqa: BLE001
+                for r in batch:
+                    r.future.set_exception(e)
+                continue
+            self._slots[slot] = (spec, batch)
+            self._last_used[spec.key] = time.perf_counter()
+            self.batches += 1
+            launched = True
+        return launched
+
+
+# ------------------------------------------------------------------------------------------- executor
+class CudaExecutor:
+    """Runs batches on `nslots` CUDA streams of one device, with CUDA graphs per (model, batch bucket, slot).
+
+    Device memory it holds (and reports to the scheduler): resident models, and per (model, slot) an input and
+    an output buffer for the largest batch plus the graph pools.  Results are host float32 tensors (views of a
+    pinned batch buffer) or, with result_device='cuda', device tensors.
+    """
+
+    def __init__(self, device=None, nslots: int = 3, use_graphs: bool = True, result_device: str = 'cpu',
+                 max_batch: int = 256):
+        from .engine import require_cuda
+        self.device = require_cuda(device)
+        self.nslots = nslots
+        self.use_graphs = use_graphs
+        self.result_device = result_device
+        self._max_batch = max_batch
+        self.streams = [torch.cuda.Stream(self.device) for _ in range(nslots)]
+        self.events = [None] * nslots
+        self.pending = [None] * nslots
+        self.models: dict = {}        # key -> CoherentModel
+        self.buffers: dict = {}       # (key, slot, dtype) -> (d_in, d_out)
+        self.graphs: dict = {}        # (key, slot, dtype, bucket) -> (graph, bytes)
+        self._bytes: dict = {}        # key -> device bytes attributed to it
+
+    def thread_init(self):
+        torch.cuda.set_device(self.device)
+
+    def max_batch(self, spec):
+        return self._max_batch
+
+    def resident_bytes(self):
+        return sum(self._bytes.values())
+
+    def bytes_needed(self, spec, n):
+        """Device bytes a batch of n would add: the model if absent, plus one slot's buffers and graph pool
+        for the batch bucket (an upper bound: buffers already allocated are counted again)."""
+        b = bucket(n)
+        model = self.models.get(spec.key)
+        need = 0 if model is not None else self._model_bytes(spec)
+        per = spec.pixels * (4 + 4 * spec.planes)
+        ws = model.workspace_bytes(b) if model is not None else 16 * b * spec.pixels // 4
+        return need + b * per + ws
+
+    def _model_bytes(self, spec):
+        return 64 << 20
+
+    def _model(self, spec):
+        m = self.models.get(spec.key)
+        if m is None:
+            with torch.cuda.device(self.device):
+                m = spec.build()
+            torch.cuda.synchronize(self.device)   # built on the default stream; the slot streams read it
+            self.models[spec.key] = m
+            self._bytes[spec.key] = self._bytes.get(spec.key, 0) + m.nbytes
+        return m
+
+    def _buffers(self, spec, slot, dtype, n):
+        key = (spec.key, slot, dtype)
+        buf = self.buffers.get(key)
+        if buf is None or buf[0].shape[0] < n:
+            cap = bucket(max(n, 1))
+            if buf is not None:
+                self._bytes[spec.key] -= buf[0].numel() * buf[0].element_size() + buf[1].numel() * 4
+                for gk in [g for g in self.graphs if g[:3] == key]:
+                    self._bytes[spec.key] -= self.graphs.pop(gk)[1]
+            d_in = torch.empty((cap, spec.ny, spec.nx), dtype=dtype, device=self.device)
+            d_out = torch.empty((cap, spec.planes, spec.ny, spec.nx), dtype=torch.float32, device=self.device)
+            buf = self.buffers[key] = (d_in, d_out)
+            self._bytes[spec.key] = self._bytes.get(spec.key, 0) + d_in.numel() * d_in.element_size() + \
+                d_out.numel() * 4
+        return buf
+
+    def _graph(self, spec, model, slot, dtype, b, d_in, d_out):
+        gk = (spec.key, slot, dtype, b)
+        g = self.graphs.get(gk)
+        if g is None:
+            s = self.streams[slot]
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(s):
+                model.image(d_in[:b], out=d_out[:b])            # warm-up: plans, attributes, allocator
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            torch.cuda.synchronize(self.device)
+            free0 = torch.cuda.mem_get_info(self.device)[0]
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=s):
+                model.image(d_in[:b], out=d_out[:b])
+            used = max(0, free0 - torch.cuda.mem_get_info(self.device)[0])
+            g = self.graphs[gk] = (graph, used)
+            self._bytes[spec.key] = self._bytes.get(spec.key, 0) + used
+        return g[0]
+
+    def launch(self, slot, spec, reqs):
+        model = self._model(spec)
+        n = len(reqs)
+        b = bucket(n)
+        dtype = reqs[0].mask.dtype
+        d_in, d_out = self._buffers(spec, slot, dtype, b)
+        graph = self._graph(spec, model, slot, dtype, b, d_in, d_out) if self.use_graphs else None
+        s = self.streams[slot]
+        with torch.cuda.device(self.device), torch.cuda.stream(s):
+            for i, r in enumerate(reqs):
+                d_in[i].copy_(r.mask, non_blocking=True)
+            if graph is not None:
+                graph.replay()
+            else:
+                model.image(d_in[:n], out=d_out[:n])
+            if self.result_device == 'cpu':
+                host = torch.empty((n, spec.planes, spec.ny, spec.nx), dtype=torch.float32, pin_memory=True)
+                host.copy_(d_out[:n], non_blocking=True)
+                out = host
+            else:
+                out = d_out[:n].clone()
+            ev = torch.cuda.Event()
+            ev.record(s)
+        self.events[slot] = ev
+        self.pending[slot] = out
+
+    def poll(self, slot):
+        ev = self.events[slot]
+        return ev is not None and ev.query()
+
+    def collect(self, slot):
+        out = self.pending[slot]
+        self.events[slot] = None
+        self.pending[slot] = None
+        return [out[i] for i in range(out.shape[0])]
+
+    def evict(self, key):
+        self.models.pop(key, None)
+        for k in [k for k in self.buffers if k[0] == key]:
+            del self.buffers[k]
+        for k in [k for k in self.graphs if k[0] == key]:
+            del self.graphs[k]
+        self._bytes.pop(key, None)
+
+    def shutdown(self):
+        for s in self.streams:
+            s.synchronize()
+
+
+def plain_run(spec_masks, device=None):
+    """The plain path: one request at a time, no batching, no graphs, no overlap -- copy in, image, copy out,
+    synchronise.  Returns (results, seconds)."""
+    dev = torch.device('cuda', torch.cuda.current_device()) if device is None else torch.device(device)
+    models = {}
+    out = []
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for spec, mask in spec_masks:
+        m = models.get(spec.key)
+        if m is None:
+            m = models[spec.key] = spec.build()
+        d = mask.to(dev).unsqueeze(0)
+        img = m.image(d)
+        out.append(img[0].cpu())
+    torch.cuda.synchronize(dev)
+    return out, time.perf_counter() - t0
+
+
+# ------------------------------------------------------------------------------------------- specs
+def socs_spec(source, projector, numerics, period, n, focus=(0.0,), name='socs'):
+    """SOCS model of an n x n clip of `period` nm with the kernels of every focus plane."""
+    from .imaging import socs_model
+    key = (name, n, float(period), tuple(float(z) for z in focus))
+    return ModelSpec(key, n, n, len(focus),
+                     lambda: socs_model(source, projector, numerics, period, period, n, n, focus=list(focus)))
+
+
+def abbe_spec(source, projector, numerics, period, n, focus=(0.0,), name='abbe'):
+    """Abbe model (resident pupils of every source point) of an n x n clip of `period` nm."""
+    from .imaging import abbe_model
+    key = (name, n, float(period), tuple(float(z) for z in focus))
+    return ModelSpec(key, n, n, len(focus),
+                     lambda: abbe_model(source, projector, numerics, period, period, n, n, focus=list(focus)))

@@ -1,0 +1,67 @@
+"""Continuous batching on the device: every result of a mixed stream equals the same request imaged alone."""
+import numpy as np
+import pytest
+import torch
+
+from tests.fixtures import rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 2e-6   # same kernels; only the batch composition (and so the summation split) differs
+
+
+def _specs():
+    import math
+    from opticalimaging_b200 import serve, workloads as W
+    from opticalimaging_b200.params import Numerics, Projection, Source
+    sr, po, nm = W.config3_optics(order=8)
+    q, qp, qn = Source(), Projection(), Numerics()
+    q.Shape, q.PntNum, q.SigmaIn, q.SigmaOut, q.OpenAngle = 'quasar', 15, 0.5, 0.85, math.pi / 6
+    W.mapped_optics(qp, q)
+    qn.ImageCalculationMode = 'vector'
+    return [serve.socs_spec(sr, po, nm, 512.0, 256),
+            serve.socs_spec(sr, po, nm, 1024.0, 512),
+            serve.socs_spec(sr, po, nm, 512.0, 256, focus=(-40.0, 0.0, 40.0), name='socs3'),
+            serve.abbe_spec(q, qp, qn, 512.0, 256)]
+
+
+@pytest.mark.parametrize('graphs', [True, False])
+def test_mixed_stream_matches_alone(graphs):
+    from opticalimaging_b200 import serve, workloads as W
+    specs = _specs()
+    rng = np.random.default_rng(7)
+    reqs = []
+    for i in range(40):
+        sp = specs[i % len(specs)]
+        m = W.rect_mask(sp.ny, sp.nx, 2.0 * sp.ny, 2.0 * sp.nx, 20, 30, 300, rng)
+        t = torch.from_numpy(m if i % 2 else (m > 0).astype(np.uint8)).pin_memory()
+        reqs.append((sp, t))
+    ex = serve.CudaExecutor(nslots=3, use_graphs=graphs)
+    srv = serve.Server(ex, hbm_budget=40e9, max_batch=8)
+    futs = [srv.submit(sp, t) for sp, t in reqs]
+    out = [f.result(timeout=300) for f in futs]
+    srv.close()
+    assert srv.batches < len(reqs)
+    models = {}
+    for (sp, t), got in zip(reqs, out):
+        m = models.setdefault(sp.key, ex.models[sp.key])
+        alone = m.image(t.cuda().unsqueeze(0))[0].cpu()
+        assert got.shape == (sp.planes, sp.ny, sp.nx)
+        assert rel_err(got.numpy(), alone.numpy()) < TOL
+    lat = srv.latency_ms()
+    assert lat['count'] == len(reqs)
+
+
+def test_plain_path_matches_served():
+    from opticalimaging_b200 import serve, workloads as W
+    specs = _specs()[:2]
+    rng = np.random.default_rng(3)
+    reqs = [(sp, torch.from_numpy(W.rect_mask(sp.ny, sp.nx, 2.0 * sp.ny, 2.0 * sp.nx, 20, 30, 300, rng)))
+            for sp in specs for _ in range(3)]
+    plain, seconds = serve.plain_run(reqs)
+    srv = serve.Server(serve.CudaExecutor(nslots=2), hbm_budget=40e9)
+    served = [f.result(timeout=300) for f in [srv.submit(sp, t) for sp, t in reqs]]
+    srv.close()
+    assert seconds > 0
+    for a, b in zip(plain, served):
+        assert rel_err(b.numpy(), a.numpy()) < TOL

@@ -1,0 +1,136 @@
+"""Scheduler of the continuous-batching server on the CPU, with a fake executor: batching, admission by the
+memory budget, eviction, cancellation, malformed requests and executor failures.  No GPU involved."""
+import threading
+import time
+
+import pytest
+import torch
+
+from opticalimaging_b200.serve import ModelSpec, Server, bucket
+
+
+class FakeExecutor:
+    """Completes a batch `delay` seconds after launch; the 'image' of a mask is 2 * mask as one plane."""
+
+    def __init__(self, nslots=2, delay=0.002, model_bytes=100, per_image=10, fail_keys=()):
+        self.nslots, self.delay = nslots, delay
+        self.model_bytes, self.per_image = model_bytes, per_image
+        self.fail_keys = set(fail_keys)
+        self.models, self.evicted, self.launched = {}, [], []
+        self.slot = [None] * nslots
+        self.lock = threading.Lock()
+
+    def max_batch(self, spec):
+        return 8
+
+    def resident_bytes(self):
+        return sum(self.models.values())
+
+    def bytes_needed(self, spec, n):
+        return (0 if spec.key in self.models else self.model_bytes) + self.per_image * bucket(n)
+
+    def launch(self, slot, spec, reqs):
+        if spec.key in self.fail_keys:
+            raise RuntimeError('device failure injected on the host')
+        self.models[spec.key] = self.model_bytes + self.per_image * bucket(len(reqs))
+        self.launched.append((spec.key, len(reqs)))
+        self.slot[slot] = (time.perf_counter() + self.delay, [2 * r.mask.float().unsqueeze(0) for r in reqs])
+
+    def poll(self, slot):
+        return self.slot[slot] is not None and time.perf_counter() >= self.slot[slot][0]
+
+    def collect(self, slot):
+        out = self.slot[slot][1]
+        self.slot[slot] = None
+        return out
+
+    def evict(self, key):
+        self.evicted.append(key)
+        self.models.pop(key, None)
+
+    def shutdown(self):
+        pass
+
+
+def spec(name, n=4):
+    return ModelSpec((name, n), n, n, 1, build=None)
+
+
+def test_every_request_completes_and_batches_form():
+    ex = FakeExecutor()
+    srv = Server(ex, hbm_budget=1e9)
+    a, b = spec('a'), spec('b')
+    futs = [(m, srv.submit(a if i % 3 else b, m)) for i, m in enumerate(torch.randint(0, 2, (50, 4, 4)).float())]
+    for m, f in futs:
+        torch.testing.assert_close(f.result(timeout=10), 2 * m.unsqueeze(0))
+    srv.drain()
+    srv.close()
+    assert srv.batches < 50                        # requests were batched
+    assert all(n <= 8 for _, n in ex.launched)
+    lat = srv.latency_ms()
+    assert lat['count'] == 50 and lat['p50_ms'] <= lat['p99_ms']
+
+
+def test_requests_arriving_during_flight_join_later_batches():
+    ex = FakeExecutor(nslots=1, delay=0.02)
+    srv = Server(ex, hbm_budget=1e9)
+    a = spec('a')
+    first = [srv.submit(a, torch.ones(4, 4)) for _ in range(3)]
+    time.sleep(0.005)                               # the first batch is in flight
+    later = [srv.submit(a, torch.zeros(4, 4)) for _ in range(5)]
+    for f in first + later:
+        f.result(timeout=10)
+    srv.close()
+    assert ex.launched[0][1] == 3 and sum(n for _, n in ex.launched) == 8 and len(ex.launched) >= 2
+
+
+def test_malformed_and_cancelled_requests():
+    ex = FakeExecutor(nslots=1, delay=0.05)
+    srv = Server(ex, hbm_budget=1e9)
+    a = spec('a')
+    with pytest.raises(ValueError):
+        srv.submit(a, torch.zeros(3, 4)).result(timeout=1)
+    with pytest.raises(ValueError):
+        srv.submit(a, torch.zeros(4, 4, dtype=torch.float64)).result(timeout=1)
+    busy = srv.submit(a, torch.ones(4, 4))          # occupies the only slot
+    time.sleep(0.01)
+    victim = srv.submit(a, torch.ones(4, 4))
+    assert victim.cancel()                          # cancelled while waiting: dropped before launch
+    ok = srv.submit(a, torch.ones(4, 4))
+    assert busy.result(timeout=10) is not None and ok.result(timeout=10) is not None
+    srv.close()
+    assert victim.cancelled()
+
+
+def test_budget_refusal_and_eviction():
+    ex = FakeExecutor(nslots=1, delay=0.001, model_bytes=100, per_image=10)
+    srv = Server(ex, hbm_budget=150)
+    a, b, huge = spec('a'), spec('b'), spec('huge', n=4)
+    assert srv.submit(a, torch.ones(4, 4)).result(timeout=10) is not None
+    # b does not fit next to a: a is idle, so it is evicted to make room
+    assert srv.submit(b, torch.ones(4, 4)).result(timeout=10) is not None
+    assert ('a', 4) in ex.evicted
+    # a batch that can never fit is refused with MemoryError
+    ex.model_bytes = 10 ** 6
+    with pytest.raises(MemoryError):
+        srv.submit(huge, torch.ones(4, 4)).result(timeout=10)
+    srv.close()
+    assert srv.rejected == 1
+
+
+def test_executor_failure_fails_only_its_batch():
+    ex = FakeExecutor(fail_keys={('bad', 4)})
+    srv = Server(ex, hbm_budget=1e9)
+    bad = srv.submit(spec('bad'), torch.ones(4, 4))
+    good = srv.submit(spec('good'), torch.ones(4, 4))
+    with pytest.raises(RuntimeError, match='injected'):
+        bad.result(timeout=10)
+    assert good.result(timeout=10) is not None
+    srv.close()
+
+
+def test_submit_after_close_is_refused():
+    srv = Server(FakeExecutor(), hbm_budget=1e9)
+    srv.close()
+    with pytest.raises(RuntimeError):
+        srv.submit(spec('a'), torch.ones(4, 4)).result(timeout=1)
