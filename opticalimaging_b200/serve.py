@@ -78,7 +78,7 @@ class Server:
         self._last_used: dict = {}
         self._closed = False
         self._rid = 0
-        self.completed = []          # finished requests (for latency statistics)
+        self.completed = []          # (submit, done) times of finished requests, for latency statistics
         self.batches = 0
         self.rejected = 0
         self._thread = threading.Thread(target=self._run, name='oi-serve', daemon=True)
@@ -124,7 +124,7 @@ class Server:
         raise TimeoutError('requests still pending')
 
     def latency_ms(self):
-        lat = sorted((r.t_done - r.t_submit) * 1e3 for r in self.completed)
+        lat = sorted((done - sub) * 1e3 for sub, done in self.completed)
         if not lat:
             return {}
         pick = lambda q: lat[min(len(lat) - 1, int(math.ceil(q * len(lat))) - 1)]  # noqa: E731
@@ -174,7 +174,7 @@ class Server:
                     r.future.set_exception(err)
                 else:
                     r.future.set_result(results[j])
-                    self.completed.append(r)
+                    self.completed.append((r.t_submit, now))   # not the request: it holds the result
             self._slots[i] = None
             done = True
         return done
