@@ -156,57 +156,62 @@ def stage_times(sk, masks, out, reps=5):
     return acc
 
 
-def _consume(futs):
-    """Wait for every result and release it at once, as a client that writes results out does (the pinned
-    result buffers then return to the host caching allocator for the next batches)."""
-    for i in range(len(futs)):
-        futs[i].result()
-        futs[i] = None
-
-
 def serve_measure(sk, info, masks_np, dev, args):
     """Served throughput and latency of config-3 requests, against the plain path on the same requests.
 
-    Saturated: every request submitted at once (throughput).  Poisson: arrivals at 70 % of the saturated
-    rate (latency under load).  Plain: one request at a time."""
+    The client keeps a ring of pinned result buffers and passes one with each request (the server copies the
+    image into it).  Saturated: a closed loop keeping `window` requests outstanding (throughput).  Poisson:
+    open-loop arrivals at 70 % of the saturated rate (latency under load).  Plain: one request at a time."""
+    import collections
     import random
     from opticalimaging_b200 import serve
     spec = serve.ModelSpec(('socs24', N_PIX, PERIOD), N_PIX, N_PIX, 1, build=lambda: serve_model_from(sk))
     pinned = [torch.from_numpy(m.astype(np.uint8)).pin_memory() for m in masks_np]
     nreq = max(4 * BATCH, args.serve_requests)
-    reqs = [pinned[i % len(pinned)] for i in range(nreq)]
+    window = 4 * BATCH
+    ring = [torch.empty((1, N_PIX, N_PIX), dtype=torch.float32).pin_memory() for _ in range(nreq)]
     ex = serve.CudaExecutor(device=dev, nslots=3)
     srv = serve.Server(ex, hbm_budget=150e9, max_batch=BATCH)
-    _consume([srv.submit(spec, r) for r in reqs[:4 * BATCH]])        # warm-up: model, buffers, graphs, pinned pool
+
+    def closed_loop(n):
+        q = collections.deque()
+        for i in range(n):
+            if len(q) >= window:
+                q.popleft().result()
+            q.append(srv.submit(spec, pinned[i % len(pinned)], out=ring[i % window]))
+        while q:
+            q.popleft().result()
+
+    closed_loop(2 * window)                                       # warm-up: model, buffers, graphs
     srv.completed.clear()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    _consume([srv.submit(spec, r) for r in reqs])
+    closed_loop(nreq)
     dt = time.perf_counter() - t0
     sat = srv.latency_ms()
     served = nreq / dt
-    # Poisson arrivals at 70 % of the saturated rate
     srv.completed.clear()
     rng = random.Random(5)
     rate = 0.7 * served
     futs = []
     t_next = time.perf_counter()
-    for r in reqs:
+    for i in range(nreq):
         t_next += rng.expovariate(rate)
         while time.perf_counter() < t_next:
             pass
-        futs.append(srv.submit(spec, r))
-    _consume(futs)
+        futs.append(srv.submit(spec, pinned[i % len(pinned)], out=ring[i]))
+    for f in futs:
+        f.result()
     poisson = srv.latency_ms()
     batches = srv.batches
     srv.close()
     nplain = min(32, nreq)
-    _, tp = serve.plain_run([(spec, reqs[i]) for i in range(nplain)], device=dev)
+    _, tp = serve.plain_run([(spec, pinned[i % len(pinned)]) for i in range(nplain)], device=dev)
     plain = nplain / tp
     return {"images_per_s": served, "p50_ms": poisson.get("p50_ms"), "p99_ms": poisson.get("p99_ms"),
             "latency_at": f"Poisson arrivals at {rate:.0f} requests/s (70 % of the saturated rate)",
             "saturated_p50_ms": sat.get("p50_ms"), "saturated_p99_ms": sat.get("p99_ms"),
-            "requests": nreq, "batches": batches, "plain_images_per_s": plain,
+            "requests": nreq, "window": window, "batches": batches, "plain_images_per_s": plain,
             "served_over_plain": served / plain,
             "plain": "one request at a time: H2D, image (batch 1, FP32 FFT form, no graph), D2H, synchronise",
             "h2d_bytes_per_image": N_PIX * N_PIX, "d2h_bytes_per_image": 4 * N_PIX * N_PIX}

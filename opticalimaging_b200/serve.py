@@ -53,6 +53,7 @@ class Request:
     t_submit: float
     t_done: float = 0.0
     rid: int = 0
+    out: torch.Tensor | None = None   # caller-provided result storage [planes, ny, nx] float32
 
 
 def bucket(n: int) -> int:
@@ -85,10 +86,16 @@ class Server:
         self._thread.start()
 
     # ---- public
-    def submit(self, spec: ModelSpec, mask: torch.Tensor) -> cf.Future:
+    def submit(self, spec: ModelSpec, mask: torch.Tensor, out: torch.Tensor | None = None) -> cf.Future:
         """Queue one mask [ny, nx] (uint8 or float32, host or device) for imaging with `spec`'s model.
-        The future's result is the image [planes, ny, nx] float32 on the executor's result device."""
+
+        The future's result is the image [planes, ny, nx] float32: written into `out` when given (pinned host
+        or device memory the caller owns and reuses -- the high-throughput form), else a new tensor on the
+        executor's result device."""
         fut = cf.Future()
+        if out is not None and (tuple(out.shape) != (spec.planes, spec.ny, spec.nx) or out.dtype != torch.float32):
+            fut.set_exception(ValueError(f'out must be a float32 [{spec.planes}, {spec.ny}, {spec.nx}] tensor'))
+            return fut
         if not isinstance(mask, torch.Tensor) or mask.dim() != 2 or tuple(mask.shape) != (spec.ny, spec.nx):
             fut.set_exception(ValueError(f'mask must be a [{spec.ny}, {spec.nx}] tensor, got '
                                          f'{tuple(mask.shape) if isinstance(mask, torch.Tensor) else type(mask)}'))
@@ -101,7 +108,7 @@ class Server:
                 fut.set_exception(RuntimeError('server is closed'))
                 return fut
             self._rid += 1
-            self._inbox.append(Request(spec, mask, fut, time.perf_counter(), rid=self._rid))
+            self._inbox.append(Request(spec, mask, fut, time.perf_counter(), rid=self._rid, out=out))
             self._cv.notify()
         return fut
 
@@ -266,6 +273,7 @@ class CudaExecutor:
         self.streams = [torch.cuda.Stream(self.device) for _ in range(nslots)]
         self.events = [None] * nslots
         self.pending = [None] * nslots
+        self.batch = [None] * nslots
         self.models: dict = {}        # key -> CoherentModel
         self.buffers: dict = {}       # (key, slot, dtype) -> (d_in, d_out)
         self.graphs: dict = {}        # (key, slot, dtype, bucket) -> (graph, bytes)
@@ -353,26 +361,38 @@ class CudaExecutor:
                 graph.replay()
             else:
                 model.image(d_in[:n], out=d_out[:n])
-            if self.result_device == 'cpu':
-                host = torch.empty((n, spec.planes, spec.ny, spec.nx), dtype=torch.float32, pin_memory=True)
-                host.copy_(d_out[:n], non_blocking=True)
+            if all(r.out is not None for r in reqs):      # caller-provided storage: copy each image there
+                for i, r in enumerate(reqs):
+                    r.out.copy_(d_out[i], non_blocking=True)
+                out = [r.out for r in reqs]
+            elif self.result_device == 'cpu':
+                # bucket-sized pinned buffer: sizes repeat, so the host caching allocator recycles them
+                host = torch.empty((b, spec.planes, spec.ny, spec.nx), dtype=torch.float32, pin_memory=True)
+                host[:n].copy_(d_out[:n], non_blocking=True)
                 out = host
             else:
                 out = d_out[:n].clone()
+            for i, r in enumerate(reqs):
+                if r.out is not None and not isinstance(out, list):
+                    r.out.copy_(d_out[i], non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(s)
         self.events[slot] = ev
         self.pending[slot] = out
+        self.batch[slot] = reqs
 
     def poll(self, slot):
         ev = self.events[slot]
         return ev is not None and ev.query()
 
     def collect(self, slot):
-        out = self.pending[slot]
+        out, reqs = self.pending[slot], self.batch[slot]
         self.events[slot] = None
         self.pending[slot] = None
-        return [out[i] for i in range(out.shape[0])]
+        self.batch[slot] = None
+        if isinstance(out, list):
+            return out
+        return [r.out if r.out is not None else out[i] for i, r in enumerate(reqs)]
 
     def evict(self, key):
         self.models.pop(key, None)
