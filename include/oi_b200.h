@@ -15,6 +15,8 @@
  *   oi_tcc_assemble64     <- GetTCCMatrix                                    (CalculateTCCMatrix.py:58-75)
  *   oi_band_spectrum_fft / oi_coherent_coarse_fft / oi_coarse_to_image_fft
  *                         <- the same three stages in FFT form (power-of-two grids)
+ *   oi_spectrum_to_image(_fft) <- the synthesis half of the two above
+ *   oi_coherent_adjoint   <- (no counterpart: the reference differentiates through torch autograd)
  *   oi_twiddle            <- (no counterpart: fills the phase tables the transforms read)
  *
  * Conventions
@@ -163,6 +165,33 @@ OI_API int oi_coherent_coarse_fft(const void* band, int batch, int nch, int m0r,
                                   const void* pupil, long long pupil_batch_stride, const float* weight, int nz,
                                   int nk, int mr, int mc, const void* wr, const void* wc, int nsplit, float* coarse,
                                   void* stream);
+
+/*
+ * The synthesis half of oi_coarse_to_image(_fft) on its own: a real image from the Hermitian half of its
+ * spectrum, out[i][y][x] = sum_{|qr|<br, 0<=qc<bc} Re(ihat[i][qr+br-1][qc] exp(-2 pi i (qr y/ny + qc x/nx))),
+ * with the qc > 0 terms already doubled by the caller.  DFT form: sy [ny][2br-1] (-, b0=-(br-1)) and
+ * sx [bc][nx] tables of oi_coarse_to_image.  FFT form: wn tables as oi_coarse_to_image_fft, power-of-two grids,
+ * scratch_v float2 [count * bc * ny].  Used by the adjoint (gradients) and for band-limited resampling.
+ */
+OI_API int oi_spectrum_to_image(const void* ihat, int count, int br, int bc, const void* sy, const void* sx, int ny,
+                                int nx, float* out, void* stream);
+OI_API int oi_spectrum_to_image_fft(const void* ihat, int count, int br, int bc, const void* wn_y, const void* wn_x,
+                                    int ny, int nx, void* scratch_v, float* out, void* stream);
+
+/*
+ * Adjoint of the coherent sum (inverse lithography; no counterpart in the reference, whose gradients come from
+ * torch autograd through its FFTs).  For fields A_f = P[z][k] .* band[b][c] and the band-limited coarse copy
+ * gcoarse[b][z] (mr x mc = 128 x 128) of dL/dI:
+ *   wout[s][b][z][c][ir][ic] = sum_{f in split s} w[z][k] conj(P[z][k][ir][ic]) F_f(ir, ic),
+ *   F_f(m) = sum_sr,sc gcoarse(s) E_f^c(s) exp(+2 pi i m.s/M)       (E_f^c: the field on the coarse grid),
+ *   field_dot[b][z][f] = sum_s gcoarse(s) |E_f^c(s)|^2              (optional, NULL to skip).
+ * The mask gradient is 2/(ny nx) Re sum_m W(m) exp(-2 pi i m.y/N) with W summed over s and z.  Band at most
+ * 64 x 64 (2br-1, 2bc-1 <= 128); wr / wc: oi_twiddle(1, 128, 1, 0, 128, +1).
+ */
+OI_API int oi_coherent_adjoint(const void* band, int batch, int nch, int m0r, int br, int m0c, int bc,
+                               const void* pupil, const float* weight, int nz, int nk, const float* gcoarse, int mr,
+                               int mc, const void* wr, const void* wc, int nsplit, void* wout, float* field_dot,
+                               void* stream);
 
 /*
  * Shifted pupil matrix of the TCC (CalculateTCCMatrix.py:17-51), FP64, scaled for a Gram product:

@@ -27,6 +27,10 @@ _SIGS = {
     'oi_band_spectrum_fft': [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],
     'oi_coarse_to_image_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp,
                                _vp],
+    'oi_spectrum_to_image': [_vp, _i, _i, _i, _vp, _vp, _i, _i, _vp, _vp],
+    'oi_spectrum_to_image_fft': [_vp, _i, _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp],
+    'oi_coherent_adjoint': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _i, _i, _vp, _i, _i, _vp, _vp, _i, _vp, _vp,
+                            _vp],
     'oi_band_spectrum_noalloc': [_vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp],
     'oi_coherent_coarse_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _i, _i, _vp, _vp, _i, _vp, _vp],
 }

@@ -556,3 +556,31 @@ extern "C" int oi_coarse_to_image_fft(float* coarse, int nparts, int count, int 
     default: return rows_inv<64>(v, count, ny, bc, (const float2*)wn_x, out, s);
   }
 }
+
+extern "C" int oi_spectrum_to_image_fft(const void* ihat, int count, int br, int bc, const void* wn_y,
+                                        const void* wn_x, int ny, int nx, void* scratch_v, float* out,
+                                        void* stream) {
+  using namespace oi;
+  if (!ihat || !wn_y || !wn_x || !scratch_v || !out || count <= 0 || br <= 0 || bc <= 0)
+    return fail(OI_EINVAL, "oi_spectrum_to_image_fft: bad arguments");
+  const int nx1 = n1_of(nx), ny1 = n1_of(ny);
+  if (!nx1 || !ny1) return fail(OI_ERANGE, "oi_spectrum_to_image_fft: grid %dx%d is not 256..2048, power of 2", ny, nx);
+  if (2 * br - 1 > ny || 2 * bc - 1 > nx) return fail(OI_ERANGE, "oi_spectrum_to_image_fft: band too wide for grid");
+  cudaStream_t s = (cudaStream_t)stream;
+  const float2* ih = (const float2*)ihat;
+  float2* v = (float2*)scratch_v;
+  int rc;
+  switch (ny1) {
+    case 8: rc = cols_inv<8>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+    case 16: rc = cols_inv<16>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+    case 32: rc = cols_inv<32>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+    default: rc = cols_inv<64>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+  }
+  if (rc) return rc;
+  switch (nx1) {
+    case 8: return rows_inv<8>(v, count, ny, bc, (const float2*)wn_x, out, s);
+    case 16: return rows_inv<16>(v, count, ny, bc, (const float2*)wn_x, out, s);
+    case 32: return rows_inv<32>(v, count, ny, bc, (const float2*)wn_x, out, s);
+    default: return rows_inv<64>(v, count, ny, bc, (const float2*)wn_x, out, s);
+  }
+}

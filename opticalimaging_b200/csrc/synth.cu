@@ -188,3 +188,23 @@ extern "C" int oi_coarse_to_image(float* coarse, int nparts, int count, int mr, 
   }
   return check_launch("oi_coarse_to_image/synth");
 }
+
+extern "C" int oi_spectrum_to_image(const void* ihat, int count, int br, int bc, const void* sy, const void* sx,
+                                    int ny, int nx, float* out, void* stream) {
+  using namespace oi;
+  if (!ihat || !sy || !sx || !out || count <= 0 || br <= 0 || bc <= 0 || ny <= 0 || nx <= 0)
+    return fail(OI_EINVAL, "oi_spectrum_to_image: bad arguments");
+  if (bc > 512 || nx > 2048 || count > 65535)
+    return fail(OI_ERANGE, "oi_spectrum_to_image: sizes out of range (bc=%d nx=%d)", bc, nx);
+  cudaStream_t s = (cudaStream_t)stream;
+  const float2* ih = (const float2*)ihat;
+  switch ((nx + 255) / 256) {
+    case 1: launch_synth<1>(ih, count, br, bc, (const float2*)sy, (const float2*)sx, ny, nx, out, s); break;
+    case 2: launch_synth<2>(ih, count, br, bc, (const float2*)sy, (const float2*)sx, ny, nx, out, s); break;
+    case 3: case 4:
+      launch_synth<4>(ih, count, br, bc, (const float2*)sy, (const float2*)sx, ny, nx, out, s); break;
+    default:
+      launch_synth<8>(ih, count, br, bc, (const float2*)sy, (const float2*)sx, ny, nx, out, s); break;
+  }
+  return check_launch("oi_spectrum_to_image");
+}

@@ -75,10 +75,12 @@ class Plan:
     _cache: dict = {}
     _lock = threading.Lock()
 
-    def __init__(self, ny, nx, band: Band, device):
+    def __init__(self, ny, nx, band: Band, device, coarse=None):
         self.ny, self.nx, self.band, self.device = ny, nx, band, device
         b = band
-        self.mr, self.mc = coarse_size(b.br), coarse_size(b.bc)
+        self.mr, self.mc = coarse if coarse is not None else (coarse_size(b.br), coarse_size(b.bc))
+        if self.mr < 2 * b.br - 1 or self.mc < 2 * b.bc - 1 or self.mc % 64:
+            raise ValueError(f'coarse grid {self.mr}x{self.mc} cannot hold the intensity of band {b.br}x{b.bc}')
         nq = 2 * b.br - 1
         t = lambda *a: twiddle(*a, device=device)  # noqa: E731
         self.wx = t(nx, b.bc, 0, b.m0c, nx, +1)              # [nx][bc]   forward x
@@ -108,12 +110,12 @@ class Plan:
 
 
     @classmethod
-    def get(cls, ny, nx, band: Band, device) -> 'Plan':
-        key = (ny, nx, band, str(device))
+    def get(cls, ny, nx, band: Band, device, coarse=None) -> 'Plan':
+        key = (ny, nx, band, str(device), coarse)
         with cls._lock:
             p = cls._cache.get(key)
             if p is None:
-                p = cls._cache[key] = Plan(ny, nx, band, device)
+                p = cls._cache[key] = Plan(ny, nx, band, device, coarse)
             return p
 
 
