@@ -216,6 +216,25 @@ template <int N1>
 __device__ __forceinline__ void inverse_gather(float2 (&z)[32], const float2* cq, int qmax, const float2* t2,
                                                const float2* t1, int n1) {
   constexpr int N = 32 * N1;
+  if (qmax < 64) {
+    // |q| <= 63: the only non-zero inputs of k2 are q = k2, k2 + 32 (k1 = 0, 1) and q = k2 - 32, k2 - 64
+    // (k1 = N1 - 1, N1 - 2).  Four predicated terms with their twiddles in registers: no runtime loops, so
+    // the 32 independent k2 chains interleave.
+    const float2 w1 = sgn<-1>(t1[1 * N1 + n1]);            // W_N1^{-n1}
+    const float2 wm1 = sgn<-1>(t1[(N1 - 1) * N1 + n1]);    // W_N1^{-(N1-1) n1}
+    const float2 wm2 = sgn<-1>(t1[(N1 - 2) * N1 + n1]);    // W_N1^{-(N1-2) n1}
+    const float2* c0 = cq + qmax;                          // c0[q] = coefficient of frequency q
+#pragma unroll
+    for (int k2 = 0; k2 < 32; ++k2) {
+      float2 acc = k2 <= qmax ? c0[k2] : make_float2(0.f, 0.f);
+      if (k2 + 32 <= qmax) cfma(acc, c0[k2 + 32], w1);
+      if (k2 - 32 >= -qmax) cfma(acc, c0[k2 - 32], wm1);
+      if (k2 - 64 >= -qmax) cfma(acc, c0[k2 - 64], wm2);
+      z[k2] = cmul(acc, sgn<-1>(t2[k2 * N1 + n1]));
+    }
+    fft32<-1>(z);
+    return;
+  }
 #pragma unroll
   for (int k2 = 0; k2 < 32; ++k2) {
     float2 acc = make_float2(0.f, 0.f);
@@ -275,8 +294,8 @@ __global__ void __launch_bounds__(256) fft_rows_inv_kernel(const float2* __restr
   float2* t2 = (float2*)smem_raw;
   float2* t1 = t2 + 32 * N1;
   const int nq = 2 * bc - 1;
-  float2* vs = t1 + N1 * N1;     // [bc][2G]
-  float2* cs = vs + bc * 2 * G;  // [G][nq]
+  float2* vs = t1 + N1 * N1;           // [bc][2G + 1] (padded against bank conflicts)
+  float2* cs = vs + bc * (2 * G + 1);  // [G][nq]
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
   build_tables<N1>(wn_g, t2, t1, tid, 256);
   const long long rblk = (long long)blockIdx.x * (2 * G);
@@ -289,13 +308,13 @@ __global__ void __launch_bounds__(256) fft_rows_inv_kernel(const float2* __restr
       const int y = (int)(r - i * ny);
       c = v[(i * bc + qc) * (long long)ny + y];
     }
-    vs[e] = c;
+    vs[qc * (2 * G + 1) + rr] = c;
   }
   __syncthreads();
   // Hermitian spectra of the row pair packed as F_a + i F_b, q in [-(bc-1), bc-1]
   for (int e = tid; e < G * nq; e += 256) {
     const int gg = e / nq, j = e % nq, q = j - (bc - 1), aq = q < 0 ? -q : q;
-    float2 a = vs[aq * 2 * G + 2 * gg], b = vs[aq * 2 * G + 2 * gg + 1];
+    float2 a = vs[aq * (2 * G + 1) + 2 * gg], b = vs[aq * (2 * G + 1) + 2 * gg + 1];
     const float h = aq == 0 ? 1.0f : 0.5f;
     if (q < 0) {
       a.y = -a.y;
@@ -459,7 +478,7 @@ static int cols_inv(const float2* ihat, int count, int br, int bc, const float2*
 template <int N1>
 static int rows_inv(const float2* v, int count, int ny, int bc, const float2* wn_x, float* out, cudaStream_t s) {
   constexpr int G = 256 / N1;
-  size_t smem = sizeof(float2) * (table_f2<N1>() + bc * 2 * G + G * (2 * bc - 1));
+  size_t smem = sizeof(float2) * (table_f2<N1>() + bc * (2 * G + 1) + G * (2 * bc - 1));
   int rc = set_smem(fft_rows_inv_kernel<N1>, smem, "oi_coarse_to_image_fft/rows");
   if (rc) return rc;
   const long long nrows = (long long)count * ny;
