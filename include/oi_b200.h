@@ -138,8 +138,9 @@ OI_API int oi_coarse_to_image(float* coarse, int nparts, int count, int mr, int 
  * returns 1 when both axes qualify.
  *
  * oi_band_spectrum_fft: as oi_band_spectrum for real float32 / uint8 masks [batch][ny][nx], band rows
- *   m0r .. m0r+br-1 and columns m0c .. m0c+bc-1 (2 max|m_c| < nx, br <= ny).  wn_x / wn_y: oi_twiddle(1, n, 1,
- *   0, n, +1) for n = nx / ny.  scratch: float2 [batch * bc * ny].  band: float2 [batch][br][bc].
+ *   m0r .. m0r+br-1 and columns m0c .. m0c+bc-1 (2 max|m_c| < nx, br <= ny).  wn_x / wn_y: the FFT tables of
+ *   n = nx / ny (n1 = n/32): oi_twiddle(32, n1, 0, 0, n, +1) followed by oi_twiddle(n1, n1, 0, 0, n1, +1) in one
+ *   buffer.  scratch: float2 [batch * bc * ny].  band: float2 [batch][br][bc].
  * oi_coarse_to_image_fft: as oi_coarse_to_image (same gc, gr tables), with the y and x syntheses done as
  *   pruned inverse FFTs; the coarse input holds `nparts` partial sums one after another (count*mr*mc floats
  *   each).  When wm_r / wm_c (oi_twiddle(1, m, 1, 0, m, +1) for m = mr / mc) are given and mr, mc are 64 or

@@ -75,10 +75,12 @@ template <> __device__ __forceinline__ float load_real<OI_FIELD_U8>(const void* 
   return (float)__ldg((const uint8_t*)f + i);
 }
 
-// Per-block twiddle tables, laid out so that a warp reading one k for all n1 touches consecutive entries:
+// Twiddle tables, laid out so that a warp reading one k for all n1 touches consecutive entries:
 //   t2[k2][n1] = W_N^{k2 n1}  (32 x N1)      t1[k1][n1] = W_N1^{k1 n1} = W_N^{32 k1 n1}  (N1 x N1)
-// with W_N = exp(+2 pi i / N), built from the 1-D table wn_g[j] = W_N^j.  (Reading the 1-D table at index
-// k n1 mod N across a warp is a stride-k access, up to 32-way bank conflicts.)
+// with W_N = exp(+2 pi i / N).  The four N-point kernels read them from global memory (one table per N, built
+// by oi_twiddle: warp-coalesced, L1-resident); the coarse-spectrum kernel builds them in shared memory from the
+// 1-D table W_M^j.  (Reading a 1-D table at index k n1 mod N across a warp is a stride-k access, up to 32-way
+// bank conflicts.)
 template <int N1>
 __device__ __forceinline__ void build_tables(const float2* __restrict__ wn_g, float2* t2, float2* t1, int tid,
                                              int nthreads) {
@@ -125,17 +127,16 @@ __device__ __forceinline__ float2 outer_bin(const float2* ys, const float2* t1, 
 // field rows [nrows = batch*ny][N] (real or u8) -> t[b][ic][y], ic over the band m0c .. m0c+bc-1.
 // Z is evaluated on the contiguous frequency range u0 .. u0+nu-1 that holds the band and its mirror.
 template <int N1, int KIND>
-__global__ void __launch_bounds__(256) fft_rows_fwd_kernel(const void* __restrict__ field, long long nrows, int ny,
+__global__ void __launch_bounds__(256, 3) fft_rows_fwd_kernel(const void* __restrict__ field, long long nrows, int ny,
                                                            const float2* __restrict__ wn_g, int m0c, int bc, int u0,
                                                            int nu, float2* __restrict__ t) {
   constexpr int N = 32 * N1, G = 256 / N1;  // G row pairs per block
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* t2 = (float2*)smem_raw;             // [32][N1]
-  float2* t1 = t2 + 32 * N1;                  // [N1][N1]
-  float2* ys = t1 + N1 * N1;                  // [G][32][N1+1]
+  const float2* t2 = wn_g;                    // global [32][N1], read through L1 (warp-coalesced)
+  const float2* t1 = wn_g + 32 * N1;          // global [N1][N1]
+  float2* ys = (float2*)smem_raw;             // [G][32][N1+1]
   float2* zs = ys + G * 32 * (N1 + 1);        // [G][nu]
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
-  build_tables<N1>(wn_g, t2, t1, tid, 256);
   const long long r0 = (long long)blockIdx.x * (2 * G) + 2 * g;
   float2 z[32];
   if (r0 + 1 < nrows) {
@@ -175,16 +176,15 @@ __global__ void __launch_bounds__(256) fft_rows_fwd_kernel(const void* __restric
 // ------------------------------------------------------------------------------ forward, columns
 // t[b][ic][y] (N = ny) -> band[b][ir][ic] = scale * sum_y t exp(+2 pi i (m0r+ir) y / ny)
 template <int N1>
-__global__ void __launch_bounds__(256) fft_cols_fwd_kernel(const float2* __restrict__ t, long long ncols, int bc,
+__global__ void __launch_bounds__(256, 3) fft_cols_fwd_kernel(const float2* __restrict__ t, long long ncols, int bc,
                                                            const float2* __restrict__ wn_g, int m0r, int br,
                                                            float scale, float2* __restrict__ band) {
   constexpr int N = 32 * N1, G = 256 / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* t2 = (float2*)smem_raw;
-  float2* t1 = t2 + 32 * N1;
-  float2* ys = t1 + N1 * N1;
+  const float2* t2 = wn_g;
+  const float2* t1 = wn_g + 32 * N1;
+  float2* ys = (float2*)smem_raw;
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
-  build_tables<N1>(wn_g, t2, t1, tid, 256);
   const long long col = (long long)blockIdx.x * G + g;
   float2 z[32];
   if (col < ncols) {
@@ -250,17 +250,16 @@ __device__ __forceinline__ void inverse_gather(float2 (&z)[32], const float2* cq
 // ------------------------------------------------------------------------------ inverse, columns
 // ihat[i][jr][qc] (qr = jr - (br-1)) -> v[i][qc][y] = sum_qr ihat exp(-2 pi i qr y / ny)
 template <int N1>
-__global__ void __launch_bounds__(256) fft_cols_inv_kernel(const float2* __restrict__ ihat, long long ncols, int br,
+__global__ void __launch_bounds__(256, 3) fft_cols_inv_kernel(const float2* __restrict__ ihat, long long ncols, int br,
                                                            int bc, const float2* __restrict__ wn_g,
                                                            float2* __restrict__ v) {
   constexpr int N = 32 * N1, G = 256 / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* t2 = (float2*)smem_raw;
-  float2* t1 = t2 + 32 * N1;
+  const float2* t2 = wn_g;
+  const float2* t1 = wn_g + 32 * N1;
   const int nq = 2 * br - 1;
-  float2* cs = t1 + N1 * N1;  // [G][nq]
+  float2* cs = (float2*)smem_raw;  // [G][nq]
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
-  build_tables<N1>(wn_g, t2, t1, tid, 256);
   const long long col0 = (long long)blockIdx.x * G;
   for (int e = tid; e < G * nq; e += 256) {
     const int jr = e / G, gg = e % G;
@@ -286,18 +285,17 @@ __global__ void __launch_bounds__(256) fft_cols_inv_kernel(const float2* __restr
 // --------------------------------------------------------------------------------- inverse, rows
 // v[i][qc][y] (qc = 0..bc-1, qc > 0 doubled) -> out[i][y][x] = sum_qc Re(v exp(-2 pi i qc x / nx))
 template <int N1>
-__global__ void __launch_bounds__(256) fft_rows_inv_kernel(const float2* __restrict__ v, long long nrows, int ny,
+__global__ void __launch_bounds__(256, 3) fft_rows_inv_kernel(const float2* __restrict__ v, long long nrows, int ny,
                                                            int bc, const float2* __restrict__ wn_g,
                                                            float* __restrict__ out) {
   constexpr int N = 32 * N1, G = 256 / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* t2 = (float2*)smem_raw;
-  float2* t1 = t2 + 32 * N1;
+  const float2* t2 = wn_g;
+  const float2* t1 = wn_g + 32 * N1;
   const int nq = 2 * bc - 1;
-  float2* vs = t1 + N1 * N1;           // [bc][2G + 1] (padded against bank conflicts)
+  float2* vs = (float2*)smem_raw;      // [bc][2G + 1] (padded against bank conflicts)
   float2* cs = vs + bc * (2 * G + 1);  // [G][nq]
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
-  build_tables<N1>(wn_g, t2, t1, tid, 256);
   const long long rblk = (long long)blockIdx.x * (2 * G);
   for (int e = tid; e < bc * 2 * G; e += 256) {
     const int qc = e / (2 * G), rr = e % (2 * G);
@@ -422,11 +420,9 @@ static int launch_coarse_spec_fft(float* coarse, int count, int br, int bc, cons
 }
 
 template <int N1>
-static size_t smem_rows_fwd(int nu) {
-  return sizeof(float2) * (table_f2<N1>() + (256 / N1) * 32 * (N1 + 1) + (256 / N1) * nu);
-}
+static size_t smem_rows_fwd(int nu) { return sizeof(float2) * ((256 / N1) * 32 * (N1 + 1) + (256 / N1) * nu); }
 template <int N1>
-static size_t smem_cols_fwd() { return sizeof(float2) * (table_f2<N1>() + (256 / N1) * 32 * (N1 + 1)); }
+static size_t smem_cols_fwd() { return sizeof(float2) * ((256 / N1) * 32 * (N1 + 1)); }
 
 
 template <int N1>
@@ -467,7 +463,7 @@ static int cols_fwd(const float2* t, int batch, int bc, const float2* wn_y, int 
 template <int N1>
 static int cols_inv(const float2* ihat, int count, int br, int bc, const float2* wn_y, float2* v, cudaStream_t s) {
   constexpr int G = 256 / N1;
-  size_t smem = sizeof(float2) * (table_f2<N1>() + G * (2 * br - 1));
+  size_t smem = sizeof(float2) * (G * (2 * br - 1));
   int rc = set_smem(fft_cols_inv_kernel<N1>, smem, "oi_coarse_to_image_fft/cols");
   if (rc) return rc;
   const long long ncols = (long long)count * bc;
@@ -478,7 +474,7 @@ static int cols_inv(const float2* ihat, int count, int br, int bc, const float2*
 template <int N1>
 static int rows_inv(const float2* v, int count, int ny, int bc, const float2* wn_x, float* out, cudaStream_t s) {
   constexpr int G = 256 / N1;
-  size_t smem = sizeof(float2) * (table_f2<N1>() + bc * (2 * G + 1) + G * (2 * bc - 1));
+  size_t smem = sizeof(float2) * (bc * (2 * G + 1) + G * (2 * bc - 1));
   int rc = set_smem(fft_rows_inv_kernel<N1>, smem, "oi_coarse_to_image_fft/rows");
   if (rc) return rc;
   const long long nrows = (long long)count * ny;

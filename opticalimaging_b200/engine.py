@@ -48,6 +48,14 @@ def twiddle(rows, cols, a0, b0, n, sign, device, scale=1.0):
     return out
 
 
+def fft_tables(n: int, device) -> torch.Tensor:
+    """Twiddle tables of the n-point four-step FFT (n = 32 n1): t2[k2][j] = exp(+2 pi i k2 j / n) (32 x n1)
+    followed by t1[k1][j] = exp(+2 pi i k1 j / n1) (n1 x n1), one complex64 buffer."""
+    n1 = n // 32
+    return torch.cat([twiddle(32, n1, 0, 0, n, +1, device).reshape(-1),
+                      twiddle(n1, n1, 0, 0, n1, +1, device).reshape(-1)])
+
+
 @dataclass(frozen=True)
 class Band:
     """Centred frequency band: rows m0r .. m0r+br-1, columns m0c .. m0c+bc-1."""
@@ -92,9 +100,9 @@ class Plan:
         self.sy = t(ny, nq, 0, -(b.br - 1), ny, -1)          # [ny][2br-1] spectrum -> image (y)
         self.sx = t(b.bc, nx, 0, 0, nx, -1)                  # [bc][nx]   spectrum -> image (x)
         self.fft = fft_supported(ny, nx, band)
-        if self.fft:                                          # exp(+2 pi i j/n), j < n, for the FFT form
-            self.wn_x = t(1, nx, 1, 0, nx, +1)
-            self.wn_y = t(1, ny, 1, 0, ny, +1)
+        if self.fft:                                          # the FFT form's twiddle tables per axis
+            self.wn_x = fft_tables(nx, device)
+            self.wn_y = fft_tables(ny, device)
         self.coarse_fft = self.mr in (64, 128) and self.mc in (64, 128)
         if self.coarse_fft:                                   # the coarse-grid FFT tables
             self.wm_r = t(1, self.mr, 1, 0, self.mr, +1)
