@@ -9,6 +9,11 @@ eigendecomposition, reported as `setup_s`) and stay resident, as they do in serv
   value  images/s with the masks already in HBM (256 MB of float32 masks per step: larger than L2)
   e2e    images/s through the public batched API from pinned host uint8 masks to host float32 images,
          host<->device copies inside the timed region
+  serving  the same clips as requests through the continuous-batching server, against the plain FP32 path
+         (one request at a time), with p50/p99 latency
+  forms  the precision study: images/s and max / RMS error vs the FP64 oracle of the FP32 FFT form, the FP32
+         DFT form and the split-BF16x3 tensor-core form
+--form picks the form of the timed path (default bf16x3, the split-precision form).
 The path shards by clip with no exchange, so N GPUs run N independent replicas ("scaling": "weak").
 --impl reference times the reference's SOCS algorithm (full-grid FFTs, complex64) on the host cores.
 """
@@ -141,15 +146,15 @@ def build_kernels():
     return sk, time.perf_counter() - t0, (sr, po, nm, T, fg)
 
 
-def stage_times(sk, masks, out, reps=5):
+def stage_times(sk, masks, out, form, reps=5):
     """Average device time of each native stage over `reps` batches (CUDA events on the launching stream).
 
     The output buffer is reused and the first batch is not counted, so no allocation sits between events."""
     acc = {}
-    sk.image(masks, out=out)
+    sk.image(masks, out=out, form=form)
     for _ in range(reps):
         marks = []
-        sk.image(masks, out=out, marks=marks)
+        sk.image(masks, out=out, marks=marks, form=form)
         torch.cuda.synchronize()
         for (_, a), (name, b) in zip(marks[:-1], marks[1:]):
             acc[name] = acc.get(name, 0.0) + a.elapsed_time(b) / reps
@@ -165,7 +170,10 @@ def serve_measure(sk, info, masks_np, dev, args):
     import collections
     import random
     from opticalimaging_b200 import serve
-    spec = serve.ModelSpec(('socs24', N_PIX, PERIOD), N_PIX, N_PIX, 1, build=lambda: serve_model_from(sk))
+    spec = serve.ModelSpec(('socs24', N_PIX, PERIOD, args.form), N_PIX, N_PIX, 1,
+                           build=lambda: serve_model_from(sk, args.form))
+    plain_spec = serve.ModelSpec(('socs24', N_PIX, PERIOD, 'fft'), N_PIX, N_PIX, 1,
+                                 build=lambda: serve_model_from(sk, 'fft'))
     pinned = [torch.from_numpy(m.astype(np.uint8)).pin_memory() for m in masks_np]
     nreq = max(4 * BATCH, args.serve_requests)
     window = 4 * BATCH
@@ -206,20 +214,21 @@ def serve_measure(sk, info, masks_np, dev, args):
     batches = srv.batches
     srv.close()
     nplain = min(32, nreq)
-    _, tp = serve.plain_run([(spec, pinned[i % len(pinned)]) for i in range(nplain)], device=dev)
+    serve.plain_run([(plain_spec, pinned[0])], device=dev)       # build the plain model outside the timing
+    _, tp = serve.plain_run([(plain_spec, pinned[i % len(pinned)]) for i in range(nplain)], device=dev)
     plain = nplain / tp
     return {"images_per_s": served, "p50_ms": poisson.get("p50_ms"), "p99_ms": poisson.get("p99_ms"),
             "latency_at": f"Poisson arrivals at {rate:.0f} requests/s (70 % of the saturated rate)",
             "saturated_p50_ms": sat.get("p50_ms"), "saturated_p99_ms": sat.get("p99_ms"),
-            "requests": nreq, "window": window, "batches": batches, "plain_images_per_s": plain,
+            "requests": nreq, "window": window, "batches": batches, "form": args.form, "plain_images_per_s": plain,
             "served_over_plain": served / plain,
             "plain": "one request at a time: H2D, image (batch 1, FP32 FFT form, no graph), D2H, synchronise",
             "h2d_bytes_per_image": N_PIX * N_PIX, "d2h_bytes_per_image": 4 * N_PIX * N_PIX}
 
 
-def serve_model_from(sk):
+def serve_model_from(sk, form):
     from opticalimaging_b200.engine import CoherentModel
-    return CoherentModel(sk.pupils, sk.weights, sk.band, sk.ny, sk.nx)
+    return CoherentModel(sk.pupils, sk.weights, sk.band, sk.ny, sk.nx, form=form)
 
 
 def cpu_reference_sample(sk_info, masks_np, budget_s, threads):
@@ -242,8 +251,8 @@ def cpu_reference_sample(sk_info, masks_np, budget_s, threads):
     return 1.0 / med, n
 
 
-def accuracy_vs_fp64(sk, masks_np, sk_info, engine_images):
-    """Max and RMS error of the engine image vs the FP64 oracle SOCS image with the same K (one clip)."""
+def fp64_image(sk_info, mask):
+    """FP64 oracle SOCS image of one clip with the engine's K kernels (the precision reference)."""
     from oracle import optics64 as O
     from opticalimaging_b200 import imaging, workloads as W
     from opticalimaging_b200.params import Scatter
@@ -251,12 +260,32 @@ def accuracy_vs_fp64(sk, masks_np, sk_info, engine_images):
     kern = imaging.DecomposeTCC_SOCS(T, fg, [N_PIX, N_PIX], nm).cpu().numpy().astype(np.complex128)
     sc = Scatter()
     sc.Period_X = sc.Period_Y = PERIOD
-    sc.ScatterField = W.thin_field(masks_np[0])
-    ref = O.socs(sc, kern, sr, po)
-    d = engine_images[0].astype(np.float64) - ref
+    sc.ScatterField = W.thin_field(mask)
+    return O.socs(sc, kern, sr, po)
+
+
+def precision_study(sk, masks, ref, steps=5):
+    """Per form: images/s on the HBM-resident batch and max / RMS error of clip 0 vs the FP64 image, both
+    relative to the FP64 image's peak."""
+    from opticalimaging_b200.engine import FORMS
+    out = torch.empty((masks.shape[0], N_PIX, N_PIX), dtype=torch.float32, device=masks.device)
     peak = float(np.max(np.abs(ref)))
-    return {"max": float(np.max(np.abs(d)) / peak), "rms": float(np.sqrt(np.mean(d ** 2)) / peak),
-            "relative_to": "peak of the FP64 SOCS-24 image (same kernels)"}
+    res = {}
+    for form in FORMS:
+        for _ in range(2):
+            sk.image(masks, out=out, form=form)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            sk.image(masks, out=out, form=form)
+        b.record()
+        torch.cuda.synchronize()
+        d = out[0].cpu().numpy().astype(np.float64) - ref
+        res[form] = {"images_per_s": masks.shape[0] * steps / (a.elapsed_time(b) / 1e3),
+                     "max": float(np.max(np.abs(d)) / peak), "rms": float(np.sqrt(np.mean(d ** 2)) / peak)}
+    res["relative_to"] = "peak of the FP64 SOCS-24 image of clip 0 (same kernels, FP64 transforms)"
+    return res
 
 
 def run_reference(args, world, rank):
@@ -297,7 +326,7 @@ def run_reference(args, world, rank):
 
 
 def run_engine(args, world, rank, local):
-    from opticalimaging_b200 import workloads as W
+    from opticalimaging_b200 import workloads as W, _native as N
     dev = torch.device('cuda', local)
     sk, setup_s, info = build_kernels()
     masks_np = W.config3_masks(count=BATCH, n=N_PIX, seed=3 + 1000 * rank)
@@ -308,14 +337,16 @@ def run_engine(args, world, rank, local):
     with ClockSampler(local) as clk:
         clk.wait_samples(1)
         for _ in range(max(args.warmup, 3)):
-            sk.image(masks, out=out)
+            sk.image(masks, out=out, form=args.form)
         torch.cuda.synchronize()
         barrier(world)
         torch.cuda.synchronize()
+        n0 = N.launch_count()
         start.record()
         for _ in range(args.steps):
-            sk.image(masks, out=out)
+            sk.image(masks, out=out, form=args.form)
         end.record()
+        launches = N.launch_count() - n0
         torch.cuda.synchronize()
         barrier(world)
         clk.wait_samples(len(clk.lines) + 1, timeout=0.5)
@@ -327,7 +358,7 @@ def run_engine(args, world, rank, local):
 
     def e2e_step():
         d_in = host_in.to(dev, non_blocking=True)
-        img = sk.image(d_in, out=out)
+        img = sk.image(d_in, out=out, form=args.form)
         host_out.copy_(img, non_blocking=True)
 
     for _ in range(max(args.warmup, 3)):
@@ -347,7 +378,7 @@ def run_engine(args, world, rank, local):
     # host float32 images out), saturated arrival; and the plain one-request-at-a-time path
     serving = serve_measure(sk, info, masks_np, dev, args)
     # ---- per-stage device times (outside the timed region) and the roofline of the dominant stage
-    st = stage_times(sk, masks, out)
+    st = stage_times(sk, masks, out, args.form)
     hbm, bf16, src = peaks()
     dominant = max(st, key=st.get)
     px = BATCH * N_PIX * N_PIX
@@ -355,28 +386,40 @@ def run_engine(args, world, rank, local):
     if dominant in alg_bytes:
         ach = alg_bytes[dominant] / (st[dominant] / 1e3) / 1e9
         roof = {"kernel": dominant, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "traffic": None, "peak_source": src}
+                "frac": ach / hbm, "traffic": None, "peak_source": src,
+                "algorithmic": "4 bytes per pixel (float32 mask read / image written)"}
     else:
         b = sk.band
-        flops = 8.0 * BATCH * sk.count * (sk.plan.mr * b.br * b.bc + sk.plan.mr * b.bc * sk.plan.mc)
+        m = 128 if args.form == 'bf16x3' else sk.plan.mr
+        fields = BATCH * sk.count
+        flops = 8.0 * fields * (m * b.br * b.bc + m * m * b.br)
         ach = flops / (st[dominant] / 1e3) / 1e12
         roof = {"kernel": dominant, "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
-                "frac": ach / bf16, "traffic": None, "peak_source": src}
+                "frac": ach / bf16, "traffic": None, "peak_source": src,
+                "algorithmic": f"8 (M br bc + M M br) flops per field, M={m} coarse grid, {fields} fields"}
+        if args.form == 'bf16x3':
+            exe = 3 * 8.0 * fields * (m * 64 * 64 + m * m * 64) / (st[dominant] / 1e3) / 1e12
+            roof["executed_tflops"] = exe
+            roof["executed_frac"] = exe / bf16
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "batch_per_gpu": BATCH, "kernels": sk.count, "band": [sk.band.br,
-                       sk.band.bc], "coarse": [sk.plan.mr, sk.plan.mc], "l2": "inputs larger than L2 "
-                       "(256 MB float32 masks + 256 MB images per step)", "parallelism": f"replicas x{world}"},
+            "vs_baseline": None, "dtype": "bf16x3" if args.form == 'bf16x3' else "fp32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "batch_per_gpu": BATCH, "kernels": sk.count,
+                       "band": [sk.band.br, sk.band.bc], "form": args.form,
+                       "coarse": [128, 128] if args.form == 'bf16x3' else [sk.plan.mr, sk.plan.mc],
+                       "l2": "inputs larger than L2 (256 MB float32 masks + 256 MB images per step)",
+                       "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_in.numel()),
                     "d2h_bytes_per_step": int(host_out.numel() * 4)},
-            "gpu_launches": 5 * args.steps, "setup_s": setup_s, "serving": serving,
+            "gpu_launches": launches, "setup_s": setup_s, "serving": serving,
             "stage_ms": {k: round(v, 4) for k, v in st.items()}, "roofline": roof, "clocks": clk.summary()}
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
         torch.set_num_threads(threads)
-        imgs = out[:1].cpu().numpy()
-        line["accuracy_vs_fp64"] = accuracy_vs_fp64(sk, masks_np, info, imgs)
+        ref = fp64_image(info, masks_np[0])
+        forms = precision_study(sk, masks, ref)
+        line["forms"] = forms
+        line["accuracy_vs_fp64"] = dict(forms[args.form], relative_to=forms["relative_to"])
         v, n = cpu_reference_sample(info, masks_np, args.cpu_budget, threads)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{n} clips of 1024x1024 through the reference's SOCS algorithm "
@@ -395,6 +438,8 @@ def main():
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--batch', type=int, default=64, help='clips per step (64 in the benchmark configuration)')
     ap.add_argument('--serve-requests', type=int, default=512, help='requests in the served measurement')
+    ap.add_argument('--form', default='bf16x3', choices=['fft', 'dft', 'bf16x3'],
+                    help='transform form of the timed path (bf16x3: split-BF16x3 contraction on tensor cores)')
     args = ap.parse_args()
     global BATCH
     BATCH = args.batch

@@ -16,6 +16,7 @@
  *   oi_band_spectrum_fft / oi_coherent_coarse_fft / oi_coarse_to_image_fft
  *                         <- the same three stages in FFT form (power-of-two grids)
  *   oi_spectrum_to_image(_fft) <- the synthesis half of the two above
+ *   oi_coherent_coarse_tc <- the |fft2(.)|^2 accumulation again, split-BF16x3 on tensor cores (tcgen05)
  *   oi_coherent_adjoint   <- (no counterpart: the reference differentiates through torch autograd)
  *   oi_twiddle            <- (no counterpart: fills the phase tables the transforms read)
  *
@@ -166,6 +167,31 @@ OI_API int oi_coherent_coarse_fft(const void* band, int batch, int nch, int m0r,
                                   const void* pupil, long long pupil_batch_stride, const float* weight, int nz,
                                   int nk, int mr, int mc, const void* wr, const void* wc, int nsplit, float* coarse,
                                   void* stream);
+
+/*
+ * Split-BF16x3 form of oi_coherent_coarse_fft on the 5th-generation tensor cores, coarse grid 128 x 128,
+ * band at most 64 x 64.  Each real operand x is split into bf16 hi = bf16(x), lo = bf16(x - hi) and a product
+ * is hi*hi + hi*lo + lo*hi accumulated in FP32 (about 16 significant bits).  Same arguments and result as
+ * oi_coherent_coarse_fft, except that the work is cut by task: the batch*nz*nk*nch fields run as `ctas`
+ * contiguous ranges and `coarse` holds `nparts` partial sums, [nparts][batch][nz][128][128], added in order
+ * by oi_coarse_to_image(_fft) with the same nparts.  oi_coherent_tc_layout gives ctas (one per SM) and the
+ * nparts that cut needs; a smaller nparts is OI_ERANGE.  wr / wc: oi_twiddle(1, 128, 1, 0, 128, +1).
+ * A wait on the tensor pipe that exceeds 2 s ends the kernel early and sets the device status
+ * (oi_device_status) to 1; the result is then invalid.
+ */
+OI_API int oi_coherent_tc_layout(long long images, int fields, int* ctas, int* nparts);
+OI_API int oi_coherent_coarse_tc(const void* band, int batch, int nch, int m0r, int br, int m0c, int bc,
+                                 const void* pupil, long long pupil_batch_stride, const float* weight, int nz,
+                                 int nk, const void* wr, const void* wc, int ctas, int nparts, float* coarse,
+                                 void* stream);
+
+/* Kernel launches this library has enqueued since it was loaded (launches captured into a CUDA graph are
+ * counted once, at capture). */
+OI_API int oi_launch_count(long long* count);
+
+/* The device status word (0 = no error) set by kernels whose bounded waits expired; optionally cleared.
+ * Synchronous (reads device memory). */
+OI_API int oi_device_status(int* status, int reset);
 
 /*
  * The synthesis half of oi_coarse_to_image(_fft) on its own: a real image from the Hermitian half of its

@@ -33,6 +33,10 @@ _SIGS = {
                             _vp],
     'oi_band_spectrum_noalloc': [_vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp],
     'oi_coherent_coarse_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _i, _i, _vp, _vp, _i, _vp, _vp],
+    'oi_coherent_tc_layout': [_ll, _i, _vp, _vp],
+    'oi_coherent_coarse_tc': [_vp, _i, _i, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _vp],
+    'oi_device_status': [_vp, _i],
+    'oi_launch_count': [_vp],
 }
 
 FIELD_REAL_F32, FIELD_COMPLEX_C64, FIELD_U8 = 0, 1, 2
@@ -97,3 +101,24 @@ def stream_handle(device=None):
 def host_doubles(values):
     arr = (ctypes.c_double * len(values))(*[float(v) for v in values])
     return arr
+
+
+def tc_layout(images: int, fields: int):
+    """(ctas, nparts) of oi_coherent_coarse_tc for `images` coarse images of `fields` fields each."""
+    ctas, nparts = ctypes.c_int(0), ctypes.c_int(0)
+    call('oi_coherent_tc_layout', int(images), int(fields), ctypes.byref(ctas), ctypes.byref(nparts))
+    return ctas.value, nparts.value
+
+
+def device_status(reset: bool = False) -> int:
+    """The device status word set by kernels whose bounded waits expired (0 = none); synchronous."""
+    st = ctypes.c_int(0)
+    call('oi_device_status', ctypes.byref(st), int(reset))
+    return st.value
+
+
+def launch_count() -> int:
+    """Kernel launches the library has enqueued so far (graph replays are not counted)."""
+    n = ctypes.c_longlong(0)
+    call('oi_launch_count', ctypes.byref(n))
+    return n.value

@@ -13,70 +13,12 @@
 // One block per (field split, plane, image): for each of its fields it recomputes E^c (row and column inverse
 // FFTs, as the forward kernel), multiplies by g^c, and takes the product back to the band with two direct DFTs
 // (column then row; the band is small), accumulating W in registers.  Nothing per field reaches global memory.
-#include "oi_common.cuh"
+#include "fft_common.cuh"
 
 namespace oi {
 
-__host__ __device__ constexpr float ca32(int t) {
-  return t == 0 ? 1.0f : t == 1 ? 0.980785280403230449f : t == 2 ? 0.923879532511286756f
-       : t == 3 ? 0.831469612302545237f : t == 4 ? 0.707106781186547524f : t == 5 ? 0.555570233019602225f
-       : t == 6 ? 0.382683432365089772f : t == 7 ? 0.195090322016128268f : t == 8 ? 0.0f
-       : t == 9 ? -0.195090322016128268f : t == 10 ? -0.382683432365089772f : t == 11 ? -0.555570233019602225f
-       : t == 12 ? -0.707106781186547524f : t == 13 ? -0.831469612302545237f : t == 14 ? -0.923879532511286756f
-       : -0.980785280403230449f;
-}
-__host__ __device__ constexpr float sa32(int t) { return t <= 8 ? ca32(8 - t) : ca32(t - 8); }
-__host__ __device__ constexpr int rev5(int i) {
-  return ((i & 1) << 4) | ((i & 2) << 2) | (i & 4) | ((i & 8) >> 2) | ((i & 16) >> 4);
-}
-
-// 32-point DFT with exp(-2 pi i k n / 32), decimation in frequency; v[i] = X[rev5(i)].
-__device__ __forceinline__ void ifft32a(float2 (&v)[32]) {
-#pragma unroll
-  for (int len = 32; len >= 2; len >>= 1) {
-    const int half = len >> 1, step = 32 / len;
-#pragma unroll
-    for (int blk = 0; blk < 32; blk += len) {
-#pragma unroll
-      for (int j = 0; j < half; ++j) {
-        float2 u = v[blk + j], w = v[blk + j + half];
-        v[blk + j] = make_float2(u.x + w.x, u.y + w.y);
-        float2 d = make_float2(u.x - w.x, u.y - w.y);
-        const int t = j * step;
-        if (t == 0) {
-          v[blk + j + half] = d;
-        } else if (t == 8) {
-          v[blk + j + half] = make_float2(d.y, -d.x);
-        } else {
-          const float c = ca32(t), s = -sa32(t);
-          v[blk + j + half] = make_float2(d.x * c - d.y * s, d.x * s + d.y * c);
-        }
-      }
-    }
-  }
-}
-
-// Inverse four-step gather (as coherent_fft.cu): z[k2] = W_M^{-k2 n1} sum_k1 x[k2 + 32 k1] W_N1^{-k1 n1}.
-template <int N1>
-__device__ __forceinline__ void gather_ifft_a(float2 (&z)[32], const float2* src, int stride, int m0, int b,
-                                              const float2* w, int n1) {
-  constexpr int M = 32 * N1;
-#pragma unroll
-  for (int k2 = 0; k2 < 32; ++k2) {
-    float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int k1 = 0; k1 < N1; ++k1) {
-      const int idx = (k2 + 32 * k1 - m0) & (M - 1);
-      if (idx < b) {
-        const float2 tw = w[(32 * k1 * n1) & (M - 1)];
-        cfma(acc, src[idx * stride], make_float2(tw.x, -tw.y));
-      }
-    }
-    const float2 tw = w[(k2 * n1) & (M - 1)];
-    z[k2] = cmul(acc, make_float2(tw.x, -tw.y));
-  }
-  ifft32a(z);
-}
+using cg::brev5;
+using cg::gather_ifft;
 
 constexpr int ADJ_T = 512;
 constexpr int ADJ_RB = 16;  // band-rows x columns tasks per thread in the column DFT: br * MC <= 16 * 512
@@ -133,18 +75,18 @@ __global__ void __launch_bounds__(ADJ_T) coherent_adjoint_kernel(AdjointArgs a) 
       for (int task = tid; task < br * N1C; task += T) {
         const int ir = task / N1C, n1 = task % N1C;
         float2 zr[32];
-        gather_ifft_a<N1C>(zr, as + ir * bc, 1, a.m0c, bc, wc, n1);
+        gather_ifft<N1C>(zr, as + ir * bc, 1, a.m0c, bc, wc, n1);
 #pragma unroll
-        for (int i = 0; i < 32; ++i) x[ir * (MC + 1) + n1 + N1C * rev5(i)] = zr[i];
+        for (int i = 0; i < 32; ++i) x[ir * (MC + 1) + n1 + N1C * brev5(i)] = zr[i];
       }
       __syncthreads();
       float2 zc[32];
-      gather_ifft_a<N1R>(zc, x + sc, MC + 1, a.m0r, br, wr, n1r);
+      gather_ifft<N1R>(zc, x + sc, MC + 1, a.m0r, br, wr, n1r);
       __syncthreads();  // every column task has read its band rows: x may now hold Y = g^c E^c
       float dot = 0.f;
 #pragma unroll
       for (int i = 0; i < 32; ++i) {
-        const int sr = n1r + N1R * rev5(i);
+        const int sr = n1r + N1R * brev5(i);
         const float g = __ldg(gc + sr * MC + sc);
         dot = fmaf(g, fmaf(zc[i].x, zc[i].x, zc[i].y * zc[i].y), dot);
         x[sr * (MC + 1) + sc] = make_float2(g * zc[i].x, g * zc[i].y);
@@ -215,6 +157,7 @@ static int launch_adjoint(const AdjointArgs& a, int batch, cudaStream_t s) {
   if (rc) return rc;
   dim3 grid((unsigned)a.nsplit, (unsigned)a.nz, (unsigned)batch);
   kern<<<grid, ADJ_T, smem, s>>>(a);
+  oi::note_launch();
   return check_launch("oi_coherent_adjoint");
 }
 

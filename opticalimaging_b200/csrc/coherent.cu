@@ -151,6 +151,7 @@ static int launch_coherent(const CoherentArgs& a, int batch, cudaStream_t s) {
   }
   dim3 grid((unsigned)ceil_div(a.mr, CO_TR), (unsigned)a.nz, (unsigned)batch);
   kern<<<grid, 256, smem, s>>>(a);
+  oi::note_launch();
   return check_launch("oi_coherent_coarse");
 }
 

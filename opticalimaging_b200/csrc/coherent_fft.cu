@@ -12,49 +12,12 @@
 //
 // Fields of one (b, z) are split over `nsplit` blocks; block s writes its partial sum to
 // coarse[s][b][z][sr][sc] and the coarse-spectrum stage adds the partials (a fixed order: deterministic).
-#include "oi_common.cuh"
+#include "fft_common.cuh"
 
 namespace oi {
 
-__host__ __device__ constexpr float cf32(int t) {
-  return t == 0 ? 1.0f : t == 1 ? 0.980785280403230449f : t == 2 ? 0.923879532511286756f
-       : t == 3 ? 0.831469612302545237f : t == 4 ? 0.707106781186547524f : t == 5 ? 0.555570233019602225f
-       : t == 6 ? 0.382683432365089772f : t == 7 ? 0.195090322016128268f : t == 8 ? 0.0f
-       : t == 9 ? -0.195090322016128268f : t == 10 ? -0.382683432365089772f : t == 11 ? -0.555570233019602225f
-       : t == 12 ? -0.707106781186547524f : t == 13 ? -0.831469612302545237f : t == 14 ? -0.923879532511286756f
-       : -0.980785280403230449f;
-}
-__host__ __device__ constexpr float sf32(int t) { return t <= 8 ? cf32(8 - t) : cf32(t - 8); }
-__host__ __device__ constexpr int brev5(int i) {
-  return ((i & 1) << 4) | ((i & 2) << 2) | (i & 4) | ((i & 8) >> 2) | ((i & 16) >> 4);
-}
-
-// 32-point inverse-sign DFT in registers, decimation in frequency: v[i] = X[brev5(i)],
-// X[n] = sum_k v[k] exp(-2 pi i k n / 32).
-__device__ __forceinline__ void ifft32(float2 (&v)[32]) {
-#pragma unroll
-  for (int len = 32; len >= 2; len >>= 1) {
-    const int half = len >> 1, step = 32 / len;
-#pragma unroll
-    for (int blk = 0; blk < 32; blk += len) {
-#pragma unroll
-      for (int j = 0; j < half; ++j) {
-        float2 u = v[blk + j], w = v[blk + j + half];
-        v[blk + j] = make_float2(u.x + w.x, u.y + w.y);
-        float2 d = make_float2(u.x - w.x, u.y - w.y);
-        const int t = j * step;
-        if (t == 0) {
-          v[blk + j + half] = d;
-        } else if (t == 8) {
-          v[blk + j + half] = make_float2(d.y, -d.x);  // * (-i)
-        } else {
-          const float c = cf32(t), s = -sf32(t);
-          v[blk + j + half] = make_float2(d.x * c - d.y * s, d.x * s + d.y * c);
-        }
-      }
-    }
-  }
-}
+using cg::brev5;
+using cg::gather_ifft;
 
 struct CoherentFftArgs {
   const float2* band;
@@ -69,29 +32,6 @@ struct CoherentFftArgs {
   float* coarse;     // [nsplit][batch][nz][mr][mc]
   long long split_stride;
 };
-
-// Inverse four-step gather for one task: z[k2] = W_M^{-k2 n1} sum_k1 x[k2 + 32 k1] W_N1^{-k1 n1}, then the
-// 32-point transform.  x[k] = src[(k - m0) mod M * stride] when (k - m0) mod M < B, else 0.
-template <int N1>
-__device__ __forceinline__ void gather_ifft(float2 (&z)[32], const float2* src, int stride, int m0, int b,
-                                            const float2* w, int n1) {
-  constexpr int M = 32 * N1;
-#pragma unroll
-  for (int k2 = 0; k2 < 32; ++k2) {
-    float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int k1 = 0; k1 < N1; ++k1) {
-      const int idx = (k2 + 32 * k1 - m0) & (M - 1);
-      if (idx < b) {
-        const float2 tw = w[(32 * k1 * n1) & (M - 1)];
-        cfma(acc, src[idx * stride], make_float2(tw.x, -tw.y));
-      }
-    }
-    const float2 tw = w[(k2 * n1) & (M - 1)];
-    z[k2] = cmul(acc, make_float2(tw.x, -tw.y));
-  }
-  ifft32(z);
-}
 
 // grid (nsplit, nz, batch); block = mc * N1R threads (column tasks); mr = 32 N1R, mc = 32 N1C.
 template <int N1R, int N1C>
@@ -153,6 +93,7 @@ static int launch_cfft(const CoherentFftArgs& a, int batch, cudaStream_t s) {
   }
   dim3 grid((unsigned)a.nsplit, (unsigned)a.nz, (unsigned)batch);
   kern<<<grid, T, smem, s>>>(a);
+  oi::note_launch();
   return check_launch("oi_coherent_coarse_fft");
 }
 

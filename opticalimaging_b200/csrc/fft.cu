@@ -416,6 +416,7 @@ static int launch_coarse_spec_fft(float* coarse, int count, int br, int bc, cons
   int rc = set_smem(kern, smem, "coarse spectrum fft");
   if (rc) return rc;
   kern<<<count, 512, smem, s>>>(coarse, br, bc, wr, wc, area_f2, ihat);
+  oi::note_launch();
   return check_launch("coarse spectrum fft");
 }
 
@@ -439,11 +440,13 @@ static int band_fft(const void* field, int kind, int batch, int ny, int nx, int 
     if (rc) return rc;
     fft_rows_fwd_kernel<N1, OI_FIELD_U8><<<(unsigned)ceil_div(nrows, 2 * G), 256, smem, s>>>(
         field, nrows, ny, wn_x, m0c, bc, u0, nu, t);
+    oi::note_launch();
   } else {
     rc = set_smem(fft_rows_fwd_kernel<N1, OI_FIELD_REAL_F32>, smem, "oi_band_spectrum_fft/rows");
     if (rc) return rc;
     fft_rows_fwd_kernel<N1, OI_FIELD_REAL_F32><<<(unsigned)ceil_div(nrows, 2 * G), 256, smem, s>>>(
         field, nrows, ny, wn_x, m0c, bc, u0, nu, t);
+    oi::note_launch();
   }
   return check_launch("oi_band_spectrum_fft/rows");
 }
@@ -457,6 +460,7 @@ static int cols_fwd(const float2* t, int batch, int bc, const float2* wn_y, int 
   if (rc) return rc;
   const long long ncols = (long long)batch * bc;
   fft_cols_fwd_kernel<N1><<<(unsigned)ceil_div(ncols, G), 256, smem, s>>>(t, ncols, bc, wn_y, m0r, br, scale, band);
+  oi::note_launch();
   return check_launch("oi_band_spectrum_fft/cols");
 }
 
@@ -468,6 +472,7 @@ static int cols_inv(const float2* ihat, int count, int br, int bc, const float2*
   if (rc) return rc;
   const long long ncols = (long long)count * bc;
   fft_cols_inv_kernel<N1><<<(unsigned)ceil_div(ncols, G), 256, smem, s>>>(ihat, ncols, br, bc, wn_y, v);
+  oi::note_launch();
   return check_launch("oi_coarse_to_image_fft/cols");
 }
 
@@ -479,6 +484,7 @@ static int rows_inv(const float2* v, int count, int ny, int bc, const float2* wn
   if (rc) return rc;
   const long long nrows = (long long)count * ny;
   fft_rows_inv_kernel<N1><<<(unsigned)ceil_div(nrows, 2 * G), 256, smem, s>>>(v, nrows, ny, bc, wn_x, out);
+  oi::note_launch();
   return check_launch("oi_coarse_to_image_fft/rows");
 }
 

@@ -10,6 +10,9 @@ namespace oi {
 // Records a formatted message as the calling thread's last error and returns `code`.
 int fail(int code, const char* fmt, ...);
 
+// Counts one kernel launch (oi_launch_count reports the total, for launch accounting in benchmarks).
+void note_launch();
+
 // Checks the launch just enqueued; returns OI_OK or OI_ECUDA with the CUDA error text recorded.
 int check_launch(const char* what);
 

@@ -209,6 +209,7 @@ extern "C" int oi_abbe_pupils(const float* fr, const float* fc, int br, int bc, 
   dim3 grid((unsigned)ceil_div(plane, 128), (unsigned)nsrc, (unsigned)nz);
   abbe_pupil_kernel<<<grid, 128, 0, s>>>(o, fr, fc, br, bc, sx, sy, sv, nsrc, focus, index_image / weight_sum,
                                          (float2*)pupil, weight);
+  oi::note_launch();
   return check_launch("oi_abbe_pupils");
 }
 
@@ -225,5 +226,6 @@ extern "C" int oi_tcc_pupils64(const float* ff, int lf, const float* gg, int lg,
   long long total = (long long)lf * lg * nsrc;
   tcc_pupil_kernel<<<(unsigned)ceil_div(total, 128), 128, 0, s>>>(o, ff, lf, gg, lg, sx, sy, sv, nsrc, focus,
                                                                    index_image / weight_sum, (double2*)h);
+  oi::note_launch();
   return check_launch("oi_tcc_pupils64");
 }

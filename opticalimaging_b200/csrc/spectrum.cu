@@ -186,14 +186,17 @@ extern "C" int oi_band_spectrum(const void* field, int kind, int batch, int ny, 
     case OI_FIELD_REAL_F32:
       band_x_kernel<OI_FIELD_REAL_F32><<<gx, 256, 0, s>>>(field, ny, nx, nch, nrows, bc, (const float2*)wx,
                                                            (float2*)scratch);
+      oi::note_launch();
       break;
     case OI_FIELD_U8:
       band_x_kernel<OI_FIELD_U8><<<gx, 256, 0, s>>>(field, ny, nx, nch, nrows, bc, (const float2*)wx,
                                                      (float2*)scratch);
+      oi::note_launch();
       break;
     case OI_FIELD_COMPLEX_C64:
       band_x_kernel<OI_FIELD_COMPLEX_C64><<<gx, 256, 0, s>>>(field, ny, nx, nch, nrows, bc, (const float2*)wx,
                                                               (float2*)scratch);
+      oi::note_launch();
       break;
     default:
       return fail(OI_EINVAL, "oi_band_spectrum: unknown field kind %d", kind);
@@ -202,6 +205,7 @@ extern "C" int oi_band_spectrum(const void* field, int kind, int batch, int ny, 
   if (rc) return rc;
   dim3 gy((unsigned)ceil_div(bc, YB_N), (unsigned)ceil_div(br, YB_M), (unsigned)(batch * nch));
   band_y_kernel<<<gy, 256, 0, s>>>((const float2*)scratch, ny, br, bc, (const float2*)wy, scale, (float2*)band);
+  oi::note_launch();
   return check_launch("oi_band_spectrum/y");
 }
 

@@ -130,6 +130,7 @@ int fold_parts(float* coarse, int nparts, long long n, cudaStream_t s) {
   if (nparts <= 1) return OI_OK;
   if (n % 4 != 0) return fail(OI_EINVAL, "partial sums of %lld floats are not float4 aligned", n);
   sum_parts_kernel<<<(unsigned)ceil_div(n / 4, 256), 256, 0, s>>>(coarse, nparts, n);
+  oi::note_launch();
   return check_launch("coarse spectrum/sum parts");
 }
 
@@ -149,6 +150,7 @@ int coarse_spectrum(float* coarse, int count, int mr, int mc, int br, int bc, co
   dim3 g1((unsigned)ceil_div(bc, SP_QT), (unsigned)count);
   coarse_spec_kernel<<<g1, 256, smem, s>>>(coarse, nparts, (long long)count * mr * mc, mr, mc, br, bc,
                                            (const float2*)gc, (const float2*)gr, (float2*)ihat);
+  oi::note_launch();
   return check_launch("coarse spectrum");
 }
 
@@ -157,6 +159,7 @@ static void launch_synth(const float2* ihat, int count, int br, int bc, const fl
                          int nx, float* out, cudaStream_t s) {
   dim3 grid((unsigned)ceil_div(ny, SY_TY), (unsigned)count);
   synth_kernel<NV><<<grid, 256, sizeof(float2) * SY_TY * bc, s>>>(ihat, br, bc, sy, sx, ny, nx, out);
+  oi::note_launch();
 }
 
 }  // namespace oi

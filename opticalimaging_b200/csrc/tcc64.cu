@@ -77,5 +77,6 @@ extern "C" int oi_tcc_assemble64(const void* h, int ne, int fg, int nsrc, void* 
   if (tiles > 0x7fffffffLL) return fail(OI_ERANGE, "oi_tcc_assemble64: fg=%d too large", fg);
   tcc_assemble_kernel<<<(unsigned)tiles, 256, 0, (cudaStream_t)stream>>>((const double2*)h, ne, fg, nsrc,
                                                                           (double2*)tcc);
+  oi::note_launch();
   return check_launch("oi_tcc_assemble64");
 }

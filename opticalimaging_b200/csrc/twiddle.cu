@@ -1,4 +1,5 @@
 // Phase tables, status reporting and version of liboi_b200.
+#include <atomic>
 #include "oi_common.cuh"
 #include <cstring>
 #include <mutex>
@@ -37,6 +38,10 @@ int ensure_smem(const void* kern, size_t bytes, const char* what) {
   return OI_OK;
 }
 
+static std::atomic<long long> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 int check_launch(const char* what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(OI_ECUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -73,5 +78,12 @@ extern "C" int oi_twiddle(void* out, int rows, int cols, long long a0, long long
   long long blocks = (total + threads - 1) / threads;
   oi::twiddle_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>((float2*)out, rows, cols, a0, b0, n,
                                                                              sign, scale);
+  oi::note_launch();
   return oi::check_launch("oi_twiddle");
+}
+
+extern "C" int oi_launch_count(long long* count) {
+  if (!count) return oi::fail(OI_EINVAL, "oi_launch_count: null count");
+  *count = oi::g_launches.load(std::memory_order_relaxed);
+  return OI_OK;
 }

@@ -65,7 +65,13 @@ class Band:
     bc: int
 
 
-FORMS = ('fft', 'dft')
+FORMS = ('fft', 'dft', 'bf16x3')
+TC_COARSE = (128, 128)      # the coarse grid of the tensor-core (split-BF16x3) coherent contraction
+
+
+def tc_supported(band: Band) -> bool:
+    """The split-BF16x3 contraction covers bands of at most 64 x 64 (coarse grid 128 x 128)."""
+    return band.br <= 64 and band.bc <= 64
 
 
 def fft_supported(ny: int, nx: int, band: Band) -> bool:
@@ -130,6 +136,13 @@ class Plan:
 SM_COUNT = 148
 
 
+def tc_parts_bound(images: int, fields: int, ctas: int = SM_COUNT) -> int:
+    """Upper bound of the partial-sum slots oi_coherent_coarse_tc needs (for workspace estimates)."""
+    tasks = images * fields
+    g = min(ctas, tasks)
+    return min(fields, -(-fields * g // tasks) + 1)
+
+
 def field_split(nfields: int, blocks: int) -> int:
     """Smallest divisor d of nfields with blocks * d >= 3 waves of one block per SM (nfields if none)."""
     target = 3 * SM_COUNT
@@ -185,7 +198,17 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
     nz, nk = pupils.shape[-4], pupils.shape[-3]
     dev = plan.device
     s = N.stream_handle(dev)
-    if plan.use_coarse_fft(form):
+    if form == 'bf16x3':
+        if not tc_supported(b):
+            raise ValueError(f'the bf16x3 form covers bands up to 64 x 64 (this one is {b.br} x {b.bc})')
+        if (plan.mr, plan.mc) != TC_COARSE:
+            plan = Plan.get(plan.ny, plan.nx, b, dev, coarse=TC_COARSE)
+        ctas, nsplit = N.tc_layout(batch * nz, nk * nch)
+        coarse = torch.empty((nsplit, batch, nz, plan.mr, plan.mc), dtype=torch.float32, device=dev)
+        N.call('oi_coherent_coarse_tc', N.ptr(band), batch, nch, b.m0r, b.br, b.m0c, b.bc, N.ptr(pupils),
+               int(pupil_batch_stride), N.ptr(weights), nz, nk, N.ptr(plan.wm_r), N.ptr(plan.wm_c), ctas, nsplit,
+               N.ptr(coarse), s)
+    elif plan.use_coarse_fft(form):
         nsplit = field_split(nk * nch, batch * nz)
         coarse = torch.empty((nsplit, batch, nz, plan.mr, plan.mc), dtype=torch.float32, device=dev)
         N.call('oi_coherent_coarse_fft', N.ptr(band), batch, nch, b.m0r, b.br, b.m0c, b.bc, N.ptr(pupils),
@@ -265,7 +288,8 @@ class CoherentModel:
     (source point, field component) (w = n v_j / sum v, CalculateAerialImage.py:46-92).
     """
 
-    def __init__(self, pupils: torch.Tensor, weights: torch.Tensor, band: Band, ny: int, nx: int, kind: str = 'socs'):
+    def __init__(self, pupils: torch.Tensor, weights: torch.Tensor, band: Band, ny: int, nx: int, kind: str = 'socs',
+                 form: str | None = None):
         if pupils.dim() != 4 or pupils.shape[2:] != (band.br, band.bc):
             raise ValueError('pupils must be [Z, K, br, bc] on the band')
         if weights.shape != pupils.shape[:2]:
@@ -275,7 +299,11 @@ class CoherentModel:
         self.device = require_cuda(pupils.device)
         self.pupils = pupils.to(self.device, torch.complex64).contiguous()
         self.weights = weights.to(self.device, torch.float32).contiguous()
-        self.band, self.ny, self.nx, self.kind = band, ny, nx, kind
+        if form not in (None,) + FORMS:
+            raise ValueError(f'form must be one of {FORMS}')
+        if form == 'bf16x3' and not tc_supported(band):
+            raise ValueError(f'the bf16x3 form covers bands up to 64 x 64 (this one is {band.br} x {band.bc})')
+        self.band, self.ny, self.nx, self.kind, self.form = band, ny, nx, kind, form
         self.plan = Plan.get(ny, nx, band, self.device)
 
     @property
@@ -290,11 +318,15 @@ class CoherentModel:
     def nbytes(self):
         return self.pupils.numel() * 8 + self.weights.numel() * 4
 
-    def workspace_bytes(self, batch: int, nch: int = 1) -> int:
+    def workspace_bytes(self, batch: int, nch: int = 1, form: str | None = None) -> int:
         """Device bytes one image() call of `batch` masks allocates besides its input and output."""
         b, p = self.band, self.plan
         nz = self.planes
+        form = self.form if form is None else form
         split = field_split(self.count * nch, batch * nz) if p.use_coarse_fft(None) else 1
+        if form == 'bf16x3':
+            split = tc_parts_bound(batch * nz, self.count * nch)
+            p = Plan.get(self.ny, self.nx, b, self.device, coarse=TC_COARSE)
         return 8 * (batch * nch * p.ny * b.bc + batch * nch * b.br * b.bc + batch * nz * (2 * b.br - 1) * b.bc
                     + batch * nz * b.bc * p.ny) + 4 * split * batch * nz * p.mr * p.mc
 
@@ -308,10 +340,14 @@ class CoherentModel:
 
         masks: float32 [B, ny, nx] (real transmission), uint8 [B, ny, nx] or complex64 [B, ny, nx, nch].
         `marks`, if a list, receives (stage name, CUDA event) pairs recorded after each native stage.
-        `form` picks the transform form of the two N-point stages: 'fft' (default where supported) or 'dft'.
+        `form`: 'fft' (default where supported) or 'dft' picks the transform form of every stage; 'bf16x3' runs
+        the coherent contraction in split BF16x3 on the tensor cores (bands up to 64 x 64) and the N-point
+        stages in FFT form where supported.  None takes the model's own form (set at construction).
         """
         if kind is None:
             kind = self._kind(masks)
+        if form is None:
+            form = self.form
         if masks.shape[1] != self.ny or masks.shape[2] != self.nx:
             raise ValueError(f'mask grid {tuple(masks.shape[1:3])} != model grid {(self.ny, self.nx)}')
         _mark(marks, 'start')

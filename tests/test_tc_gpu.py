@@ -1,0 +1,131 @@
+"""Split-BF16x3 coherent contraction on the tensor cores (oi_coherent_coarse_tc) against the FP64 oracle, the
+reference's own outputs and the FP32 forms.
+
+Stated bound of the split form: 1e-4 of the peak of the FP64 image (each real operand carries ~16 significant
+bits as bf16 hi + lo; products hi*hi + hi*lo + lo*hi in FP32).  Every case also reports max and RMS error.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import optics64 as O
+from tests.fixtures import build, load, rel_err
+
+pytestmark = pytest.mark.gpu
+
+BF16X3_VS_FP64 = 1e-4
+
+
+def rms_rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.sqrt(np.mean((a - b) ** 2)) / np.max(np.abs(b)))
+
+
+@pytest.fixture(scope='module')
+def oi():
+    import opticalimaging_b200.imaging as imaging
+    from opticalimaging_b200 import _native
+    _native.load()
+    _native.device_status(reset=True)
+    return imaging
+
+
+def test_tc_layout_and_range_errors(oi):
+    from opticalimaging_b200 import _native as N
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert N.tc_layout(64, 24) == (sms, N.tc_layout(64, 24)[1])
+    assert N.tc_layout(2, 3) == (6, 3)                     # fewer tasks than SMs: one task per CTA
+    dev = torch.device('cuda')
+    band = torch.zeros((1, 1, 8, 8), dtype=torch.complex64, device=dev)
+    pup = torch.zeros((1, 4, 8, 8), dtype=torch.complex64, device=dev)
+    w = torch.ones((1, 4), device=dev)
+    tw = torch.zeros(128, dtype=torch.complex64, device=dev)
+    coarse = torch.zeros((4, 1, 1, 128, 128), device=dev)
+    s = N.stream_handle(dev)
+    with pytest.raises(N.NativeError, match='partial slots'):
+        N.call('oi_coherent_coarse_tc', N.ptr(band), 1, 1, -4, 8, -4, 8, N.ptr(pup), 0, N.ptr(w), 1, 4, N.ptr(tw),
+               N.ptr(tw), 4, 3, N.ptr(coarse), s)
+    big = torch.zeros((1, 1, 65, 8), dtype=torch.complex64, device=dev)
+    with pytest.raises(N.NativeError, match='exceeds 64x64'):
+        N.call('oi_coherent_coarse_tc', N.ptr(big), 1, 1, -32, 65, -4, 8, N.ptr(pup), 0, N.ptr(w), 1, 4, N.ptr(tw),
+               N.ptr(tw), 4, 4, N.ptr(coarse), s)
+
+
+@pytest.mark.parametrize('name', ['cfg1', 'vec_small', 'odd_scalar'])
+def test_abbe_bf16x3_vs_fp64(oi, name):
+    from opticalimaging_b200 import _native as N
+    meta, a = load(name)
+    sr, sc, po, nm = build(meta, a)
+    h = torch.from_numpy(a['field']).cuda().to(torch.complex64)
+    ny, nx = h.shape[0], h.shape[1]
+    model = oi.abbe_model(sr, po, nm, sc.Period_Y, sc.Period_X, ny, nx)
+    got = model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=3, form='bf16x3')[0].cpu().numpy()
+    fp32 = model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=3)[0].cpu().numpy()
+    want = O.abbe(sr, sc, po, nm)
+    err, rms = rel_err(got, want), rms_rel(got, want)
+    print(f'{name}: bf16x3 vs FP64 max {err:.2e} rms {rms:.2e}; fp32 vs FP64 max {rel_err(fp32, want):.2e}')
+    assert err < BF16X3_VS_FP64
+    assert rel_err(got, a['abbe']) < BF16X3_VS_FP64
+    assert N.device_status() == 0
+
+
+@pytest.mark.parametrize('name', ['vec_small', 'odd_scalar', 'cfg3_small'])
+def test_hopkins_bf16x3_vs_reference(oi, name):
+    from opticalimaging_b200 import _native as N
+    meta, a = load(name)
+    sr, sc, po, nm = build(meta, a)
+    h = torch.from_numpy(a['field']).cuda().to(torch.complex64)
+    ny, nx = h.shape[0], h.shape[1]
+    model = oi.socs_model(sr, po, nm, sc.Period_Y, sc.Period_X, ny, nx)
+    got = model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=3, form='bf16x3')[0].cpu().numpy()
+    fp32 = model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=3)[0].cpu().numpy()
+    print(f'{name}: bf16x3 vs fp32 max {rel_err(got, fp32):.2e} rms {rms_rel(got, fp32):.2e}; '
+          f'vs reference max {rel_err(got, a["hopkins"]):.2e}')
+    assert rel_err(got, fp32) < BF16X3_VS_FP64
+    assert rel_err(got, a['hopkins']) < BF16X3_VS_FP64
+
+
+def test_socs24_1024_bf16x3_vs_fp64(oi):
+    """The headline workload: SOCS-24 from the vector annular TCC at 1024 x 1024 (2 nm pixels)."""
+    from opticalimaging_b200 import workloads as W
+    from opticalimaging_b200.params import Scatter
+    sr, po, nm = W.config3_optics(order=24)
+    T, fg = oi.CalculateTCCMatrix(sr, [2048.0, 2048.0], po, 0.0, nm)
+    sk = oi.socs_kernels_from_tcc(T, fg, [1024, 1024], nm)
+    masks = W.config3_masks(4, seed=11)
+    md = torch.from_numpy(masks).cuda()
+    got = sk.image(md, form='bf16x3').cpu().numpy()
+    fp32 = sk.image(md, form='fft').cpu().numpy()
+    assert rel_err(got, fp32) < BF16X3_VS_FP64
+    s = Scatter()
+    s.Period_X = s.Period_Y = 2048.0
+    s.ScatterField = W.thin_field(masks[0])
+    K = oi.DecomposeTCC_SOCS(T, fg, [1024, 1024], nm).cpu().numpy().astype(np.complex128)
+    want = O.socs(s, K, sr, po)
+    err, rms = rel_err(got[0], want), rms_rel(got[0], want)
+    print(f'SOCS-24 1024^2: bf16x3 vs FP64 max {err:.2e} rms {rms:.2e}; fp32 max {rel_err(fp32[0], want):.2e}')
+    assert err < BF16X3_VS_FP64
+
+
+@pytest.mark.parametrize('batch', [3, 7])
+def test_tc_ranges_cross_images_deterministic(oi, batch):
+    """Two planes x 5 fields x 3 channels: task ranges that start and end inside images, partial slots
+    zero-filled; the result is bit-identical run to run and matches the FP32 form."""
+    from opticalimaging_b200 import _native as N
+    from opticalimaging_b200.engine import Band, CoherentModel
+    g = torch.Generator().manual_seed(batch)
+    band = Band(-20, 41, -13, 27)
+    pupils = torch.randn((2, 5, band.br, band.bc), dtype=torch.complex64, generator=g)
+    weights = torch.rand((2, 5), generator=g) + 0.5
+    model = CoherentModel(pupils.cuda(), weights.cuda(), band, 256, 256)
+    field = (torch.rand((batch, 256, 256, 3), generator=g) > 0.5).to(torch.complex64).cuda()
+    field[..., 1] *= 0.3j
+    one = model.image(field, kind=N.FIELD_COMPLEX_C64, nch=3, form='bf16x3')
+    two = model.image(field, kind=N.FIELD_COMPLEX_C64, nch=3, form='bf16x3')
+    ref = model.image(field, kind=N.FIELD_COMPLEX_C64, nch=3, form='fft')
+    assert torch.equal(one, two)
+    assert rel_err(one.cpu().numpy(), ref.cpu().numpy()) < BF16X3_VS_FP64
+    for b in range(batch):   # every image on its own gives the same result as in the batch
+        solo = model.image(field[b:b + 1].contiguous(), kind=N.FIELD_COMPLEX_C64, nch=3, form='bf16x3')
+        assert rel_err(solo.cpu().numpy(), ref[b:b + 1].cpu().numpy()) < BF16X3_VS_FP64
+    assert N.device_status() == 0
