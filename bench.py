@@ -376,7 +376,7 @@ def run_engine(args, world, rank, local):
     e2e_value = world * BATCH * args.steps / (ms_e2e / 1000.0)
     # ---- served: the same clips as requests through the continuous-batching server (pinned uint8 in,
     # host float32 images out), saturated arrival; and the plain one-request-at-a-time path
-    serving = serve_measure(sk, info, masks_np, dev, args)
+    serving = serve_measure(sk, info, masks_np, dev, args) if not args.no_serve else None
     # ---- per-stage device times (outside the timed region) and the roofline of the dominant stage
     st = stage_times(sk, masks, out, args.form)
     hbm, bf16, src = peaks()
@@ -435,7 +435,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='engine', choices=['engine', 'reference'])
     ap.add_argument('--cpu-budget', type=float, default=15.0)
-    ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline and the precision study')
+    ap.add_argument('--no-serve', action='store_true', help='skip the served measurement (profiling runs)')
     ap.add_argument('--batch', type=int, default=64, help='clips per step (64 in the benchmark configuration)')
     ap.add_argument('--serve-requests', type=int, default=512, help='requests in the served measurement')
     ap.add_argument('--form', default='bf16x3', choices=['fft', 'dft', 'bf16x3'],

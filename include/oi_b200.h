@@ -175,23 +175,31 @@ OI_API int oi_coherent_coarse_fft(const void* band, int batch, int nch, int m0r,
  * oi_coherent_coarse_fft, except that the work is cut by task: the batch*nz*nk*nch fields run as `ctas`
  * contiguous ranges and `coarse` holds `nparts` partial sums, [nparts][batch][nz][128][128], added in order
  * by oi_coarse_to_image(_fft) with the same nparts.  oi_coherent_tc_layout gives ctas (one per SM) and the
- * nparts that cut needs; a smaller nparts is OI_ERANGE.  wr / wc: oi_twiddle(1, 128, 1, 0, 128, +1).
- * A wait on the tensor pipe that exceeds 2 s ends the kernel early and sets the device status
- * (oi_device_status) to 1; the result is then invalid.
+ * nparts that cut needs; a smaller nparts is OI_ERANGE.  `consts` is the band's constant operand image written
+ * by oi_tc_constants (16-byte aligned).  A wait on the tensor pipe or a copy that exceeds 2 s ends the kernel
+ * early and sets the device status (oi_device_status) to 1; the result is then invalid.
  */
 OI_API int oi_coherent_tc_layout(long long images, int fields, int* ctas, int* nparts);
 OI_API int oi_coherent_coarse_tc(const void* band, int batch, int nch, int m0r, int br, int m0c, int bc,
                                  const void* pupil, long long pupil_batch_stride, const float* weight, int nz,
-                                 int nk, const void* wr, const void* wc, int ctas, int nparts, float* coarse,
-                                 void* stream);
+                                 int nk, const void* consts, int ctas, int nparts, float* coarse, void* stream);
+
+/*
+ * The constant operand image of oi_coherent_coarse_tc for a band starting at (m0r, m0c): the split DFT
+ * matrices exp(-2 pi i (m0+i) s / 128), s < 128, i < 64, in the kernel's swizzled shared-memory layout.
+ * 98304 bytes when m0r == m0c, else 163840.  wr / wc: oi_twiddle(1, 128, 1, 0, 128, +1).
+ */
+OI_API int oi_tc_constants(int m0r, int m0c, const void* wr, const void* wc, void* image, long long bytes,
+                           void* stream);
+
+/* The device status word (0 = no error) set by kernels whose bounded waits expired; optionally cleared.
+ * Synchronous (reads device memory). */
+OI_API int oi_device_status(int* status, int reset);
 
 /* Kernel launches this library has enqueued since it was loaded (launches captured into a CUDA graph are
  * counted once, at capture). */
 OI_API int oi_launch_count(long long* count);
 
-/* The device status word (0 = no error) set by kernels whose bounded waits expired; optionally cleared.
- * Synchronous (reads device memory). */
-OI_API int oi_device_status(int* status, int reset);
 
 /*
  * The synthesis half of oi_coarse_to_image(_fft) on its own: a real image from the Hermitian half of its

@@ -34,7 +34,8 @@ _SIGS = {
     'oi_band_spectrum_noalloc': [_vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp],
     'oi_coherent_coarse_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _i, _i, _vp, _vp, _i, _vp, _vp],
     'oi_coherent_tc_layout': [_ll, _i, _vp, _vp],
-    'oi_coherent_coarse_tc': [_vp, _i, _i, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _vp],
+    'oi_coherent_coarse_tc': [_vp, _i, _i, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _vp, _i, _i, _vp, _vp],
+    'oi_tc_constants': [_i, _i, _vp, _vp, _vp, _ll, _vp],
     'oi_device_status': [_vp, _i],
     'oi_launch_count': [_vp],
 }

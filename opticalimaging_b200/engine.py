@@ -114,6 +114,18 @@ class Plan:
             self.wm_r = t(1, self.mr, 1, 0, self.mr, +1)
             self.wm_c = t(1, self.mc, 1, 0, self.mc, +1)
 
+    def tc_constants(self) -> torch.Tensor:
+        """The split DFT operand image of the tensor-core form (built once per plan; coarse grid 128 x 128)."""
+        c = getattr(self, '_tc_consts', None)
+        if c is None:
+            b = self.band
+            nbytes = 98304 if b.m0r == b.m0c else 163840
+            c = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            N.call('oi_tc_constants', b.m0r, b.m0c, N.ptr(self.wm_r), N.ptr(self.wm_c), N.ptr(c), nbytes,
+                   N.stream_handle(self.device))
+            self._tc_consts = c
+        return c
+
     def use_fft(self, form):
         if form not in (None,) + FORMS:
             raise ValueError(f'form must be one of {FORMS}')
@@ -206,7 +218,7 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
         ctas, nsplit = N.tc_layout(batch * nz, nk * nch)
         coarse = torch.empty((nsplit, batch, nz, plan.mr, plan.mc), dtype=torch.float32, device=dev)
         N.call('oi_coherent_coarse_tc', N.ptr(band), batch, nch, b.m0r, b.br, b.m0c, b.bc, N.ptr(pupils),
-               int(pupil_batch_stride), N.ptr(weights), nz, nk, N.ptr(plan.wm_r), N.ptr(plan.wm_c), ctas, nsplit,
+               int(pupil_batch_stride), N.ptr(weights), nz, nk, N.ptr(plan.tc_constants()), ctas, nsplit,
                N.ptr(coarse), s)
     elif plan.use_coarse_fft(form):
         nsplit = field_split(nk * nch, batch * nz)

@@ -39,16 +39,19 @@ def test_tc_layout_and_range_errors(oi):
     band = torch.zeros((1, 1, 8, 8), dtype=torch.complex64, device=dev)
     pup = torch.zeros((1, 4, 8, 8), dtype=torch.complex64, device=dev)
     w = torch.ones((1, 4), device=dev)
-    tw = torch.zeros(128, dtype=torch.complex64, device=dev)
+    consts = torch.zeros(98304, dtype=torch.uint8, device=dev)
     coarse = torch.zeros((4, 1, 1, 128, 128), device=dev)
     s = N.stream_handle(dev)
     with pytest.raises(N.NativeError, match='partial slots'):
-        N.call('oi_coherent_coarse_tc', N.ptr(band), 1, 1, -4, 8, -4, 8, N.ptr(pup), 0, N.ptr(w), 1, 4, N.ptr(tw),
-               N.ptr(tw), 4, 3, N.ptr(coarse), s)
+        N.call('oi_coherent_coarse_tc', N.ptr(band), 1, 1, -4, 8, -4, 8, N.ptr(pup), 0, N.ptr(w), 1, 4,
+               N.ptr(consts), 4, 3, N.ptr(coarse), s)
     big = torch.zeros((1, 1, 65, 8), dtype=torch.complex64, device=dev)
     with pytest.raises(N.NativeError, match='exceeds 64x64'):
-        N.call('oi_coherent_coarse_tc', N.ptr(big), 1, 1, -32, 65, -4, 8, N.ptr(pup), 0, N.ptr(w), 1, 4, N.ptr(tw),
-               N.ptr(tw), 4, 4, N.ptr(coarse), s)
+        N.call('oi_coherent_coarse_tc', N.ptr(big), 1, 1, -32, 65, -4, 8, N.ptr(pup), 0, N.ptr(w), 1, 4,
+               N.ptr(consts), 4, 4, N.ptr(coarse), s)
+    tw = torch.zeros(128, dtype=torch.complex64, device=dev)
+    with pytest.raises(N.NativeError, match='bytes given'):
+        N.call('oi_tc_constants', -4, -3, N.ptr(tw), N.ptr(tw), N.ptr(consts), 98304, s)
 
 
 @pytest.mark.parametrize('name', ['cfg1', 'vec_small', 'odd_scalar'])
