@@ -427,17 +427,30 @@ def plain_run(spec_masks, device=None):
 
 
 # ------------------------------------------------------------------------------------------- specs
-def socs_spec(source, projector, numerics, period, n, focus=(0.0,), name='socs'):
-    """SOCS model of an n x n clip of `period` nm with the kernels of every focus plane."""
+def _with_form(model, form):
+    """Give a built model its serving form: 'bf16x3' where the band allows it (<= 64 x 64), else the FP32 FFT
+    form; None keeps the model's default."""
+    from .engine import tc_supported
+    if model is not None and form is not None:
+        model.form = form if form != 'bf16x3' or tc_supported(model.band) else 'fft'
+    return model
+
+
+def socs_spec(source, projector, numerics, period, n, focus=(0.0,), name='socs', form=None):
+    """SOCS model of an n x n clip of `period` nm with the kernels of every focus plane; `form` as in
+    _with_form."""
     from .imaging import socs_model
-    key = (name, n, float(period), tuple(float(z) for z in focus))
+    key = (name, n, float(period), tuple(float(z) for z in focus), form)
     return ModelSpec(key, n, n, len(focus),
-                     lambda: socs_model(source, projector, numerics, period, period, n, n, focus=list(focus)))
+                     lambda: _with_form(socs_model(source, projector, numerics, period, period, n, n,
+                                                   focus=list(focus)), form))
 
 
-def abbe_spec(source, projector, numerics, period, n, focus=(0.0,), name='abbe'):
-    """Abbe model (resident pupils of every source point) of an n x n clip of `period` nm."""
+def abbe_spec(source, projector, numerics, period, n, focus=(0.0,), name='abbe', form=None):
+    """Abbe model (resident pupils of every source point) of an n x n clip of `period` nm; `form` as in
+    _with_form."""
     from .imaging import abbe_model
-    key = (name, n, float(period), tuple(float(z) for z in focus))
+    key = (name, n, float(period), tuple(float(z) for z in focus), form)
     return ModelSpec(key, n, n, len(focus),
-                     lambda: abbe_model(source, projector, numerics, period, period, n, n, focus=list(focus)))
+                     lambda: _with_form(abbe_model(source, projector, numerics, period, period, n, n,
+                                                   focus=list(focus)), form))

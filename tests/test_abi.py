@@ -40,3 +40,25 @@ def test_errors_are_reported_not_raised_in_c():
     assert rc == -1
     assert b'oi_twiddle' in lib.oi_last_error()
     assert lib.oi_version() >= 1
+
+
+def test_every_literal_call_matches_its_signature():
+    """Each N.call('oi_...', ...) in the package, the bench and the tests passes as many arguments as the
+    entry point's ctypes signature (and so as include/oi_b200.h) declares."""
+    import ast
+    import glob
+    import os
+    from opticalimaging_b200 import _native as N
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    files = glob.glob(os.path.join(root, 'opticalimaging_b200', '*.py')) + glob.glob(os.path.join(root, 'tests', '*.py'))
+    files.append(os.path.join(root, 'bench.py'))
+    seen = 0
+    for f in files:
+        for node in ast.walk(ast.parse(open(f).read())):
+            if (isinstance(node, ast.Call) and getattr(node.func, 'attr', None) == 'call' and node.args
+                    and isinstance(node.args[0], ast.Constant) and node.args[0].value in N._SIGS
+                    and not any(isinstance(a, ast.Starred) for a in node.args)):
+                name = node.args[0].value
+                assert len(node.args) - 1 == len(N._SIGS[name]), f'{f}:{node.lineno} {name}'
+                seen += 1
+    assert seen > 10

@@ -10,7 +10,7 @@ pytestmark = pytest.mark.gpu
 TOL = 2e-6   # same kernels; only the batch composition (and so the summation split) differs
 
 
-def _specs():
+def _specs(form=None):
     import math
     from opticalimaging_b200 import serve, workloads as W
     from opticalimaging_b200.params import Numerics, Projection, Source
@@ -19,16 +19,18 @@ def _specs():
     q.Shape, q.PntNum, q.SigmaIn, q.SigmaOut, q.OpenAngle = 'quasar', 15, 0.5, 0.85, math.pi / 6
     W.mapped_optics(qp, q)
     qn.ImageCalculationMode = 'vector'
-    return [serve.socs_spec(sr, po, nm, 512.0, 256),
-            serve.socs_spec(sr, po, nm, 1024.0, 512),
-            serve.socs_spec(sr, po, nm, 512.0, 256, focus=(-40.0, 0.0, 40.0), name='socs3'),
-            serve.abbe_spec(q, qp, qn, 512.0, 256)]
+    return [serve.socs_spec(sr, po, nm, 512.0, 256, form=form),
+            serve.socs_spec(sr, po, nm, 1024.0, 512, form=form),
+            serve.socs_spec(sr, po, nm, 512.0, 256, focus=(-40.0, 0.0, 40.0), name='socs3', form=form),
+            serve.abbe_spec(q, qp, qn, 512.0, 256, form=form)]
 
 
-@pytest.mark.parametrize('graphs', [True, False])
-def test_mixed_stream_matches_alone(graphs):
+@pytest.mark.parametrize('graphs,form', [(True, None), (False, None), (True, 'bf16x3')])
+def test_mixed_stream_matches_alone(graphs, form):
+    """Also for the split-BF16x3 form: the tensor-core kernel's task cut depends on the batch, which only
+    changes the FP32 summation order of the partial sums."""
     from opticalimaging_b200 import serve, workloads as W
-    specs = _specs()
+    specs = _specs(form)
     rng = np.random.default_rng(7)
     reqs = []
     for i in range(40):
