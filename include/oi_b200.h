@@ -17,6 +17,8 @@
  *                         <- the same three stages in FFT form (power-of-two grids)
  *   oi_spectrum_to_image(_fft) <- the synthesis half of the two above
  *   oi_coherent_coarse_tc <- the |fft2(.)|^2 accumulation again, split-BF16x3 on tensor cores (tcgen05)
+ *   oi_band_spectrum_tc / oi_coarse_to_image_tc / oi_rows_fwd_tc / oi_rows_inv_tc
+ *                         <- the N-point stages with their row passes on the tensor cores (split-BF16x3 form)
  *   oi_coherent_adjoint   <- (no counterpart: the reference differentiates through torch autograd)
  *   oi_twiddle            <- (no counterpart: fills the phase tables the transforms read)
  *
@@ -191,6 +193,31 @@ OI_API int oi_coherent_coarse_tc(const void* band, int batch, int nch, int m0r, 
  */
 OI_API int oi_tc_constants(int m0r, int m0c, const void* wr, const void* wc, void* image, long long bytes,
                            void* stream);
+
+/*
+ * The N-point row passes of the split-BF16x3 form on the tensor cores (dense DFT contractions, bf16 hi / lo
+ * operands, FP32 accumulate).  Grids: ny a multiple of 128 (the row blocks), nx a multiple of 128 up to 4096;
+ * band width bc <= 64.
+ *   oi_rows_fwd_tc  t[b][ic][y] = sum_x field[b][y][x] exp(+2 pi i (m0c+ic) x / nx)  (float32 or uint8 masks;
+ *                   t as the scratch of oi_band_spectrum_fft, float2 [batch][bc][ny])
+ *   oi_rows_inv_tc  out[i][y][x] = sum_{qc<bc} Re(v[i][qc][y] exp(-2 pi i qc x / nx))  (v float2 [count][bc][ny])
+ * `consts` is the constant operand image from oi_rows_tc_constants: which = 0 (forward; depends on nx, m0c, bc;
+ * nx/64 * 32768 bytes) or 1 (inverse; depends on nx, bc; nx/128 * 65536 bytes).  A wait that exceeds 2 s ends
+ * the kernel early and sets the device status.
+ * oi_band_spectrum_tc and oi_coarse_to_image_tc are oi_band_spectrum_fft and oi_coarse_to_image_fft (coarse grid
+ * 128 x 128) with these row passes.
+ */
+OI_API int oi_rows_tc_constants(int which, int nx, int m0c, int bc, void* image, long long bytes, void* stream);
+OI_API int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, int nx, int m0c, int bc,
+                          const void* consts, void* t, void* stream);
+OI_API int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, const void* consts, float* out,
+                          void* stream);
+OI_API int oi_band_spectrum_tc(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c,
+                               int bc, const void* wconsts, const void* wn_y, float scale, void* scratch,
+                               void* band, void* stream);
+OI_API int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int br, int bc, const void* wm_r,
+                                 const void* wm_c, const void* wn_y, const void* cconsts, int ny, int nx,
+                                 void* scratch_ihat, void* scratch_v, float* out, void* stream);
 
 /* The device status word (0 = no error) set by kernels whose bounded waits expired; optionally cleared.
  * Synchronous (reads device memory). */

@@ -605,3 +605,57 @@ extern "C" int oi_spectrum_to_image_fft(const void* ihat, int count, int br, int
     default: return rows_inv<64>(v, count, ny, bc, (const float2*)wn_x, out, s);
   }
 }
+
+// Split-BF16x3 tensor-core form of oi_band_spectrum_fft: the row pass is oi_rows_fwd_tc (a DFT contraction
+// on the tensor cores against the constant image `wconsts` of oi_rows_tc_constants(0, ...)), the column pass
+// the FFT above.
+extern "C" int oi_band_spectrum_tc(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c,
+                                   int bc, const void* wconsts, const void* wn_y, float scale, void* scratch,
+                                   void* band, void* stream) {
+  using namespace oi;
+  if (!field || !wconsts || !wn_y || !scratch || !band || batch <= 0 || br <= 0 || bc <= 0)
+    return fail(OI_EINVAL, "oi_band_spectrum_tc: bad arguments");
+  const int ny1 = n1_of(ny);
+  if (!ny1 || nx % 128 != 0 || nx > 4096)
+    return fail(OI_ERANGE, "oi_band_spectrum_tc: grid %dx%d unsupported", ny, nx);
+  if (bc > 64 || br > ny) return fail(OI_ERANGE, "oi_band_spectrum_tc: band %dx%d unsupported", br, bc);
+  int rc = oi_rows_fwd_tc(field, kind, batch, ny, nx, m0c, bc, wconsts, scratch, stream);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const float2* t = (const float2*)scratch;
+  switch (ny1) {
+    case 8: return cols_fwd<8>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+    case 16: return cols_fwd<16>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+    case 32: return cols_fwd<32>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+    default: return cols_fwd<64>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+  }
+}
+
+// Split-BF16x3 tensor-core form of oi_coarse_to_image_fft on the 128 x 128 coarse grid: fold, coarse spectrum
+// and column pass as there; the row pass is oi_rows_inv_tc against `cconsts` of oi_rows_tc_constants(1, ...).
+extern "C" int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int br, int bc, const void* wm_r,
+                                     const void* wm_c, const void* wn_y, const void* cconsts, int ny, int nx,
+                                     void* scratch_ihat, void* scratch_v, float* out, void* stream) {
+  using namespace oi;
+  if (!coarse || !wm_r || !wm_c || !wn_y || !cconsts || !scratch_ihat || !scratch_v || !out || count <= 0 ||
+      nparts <= 0 || br <= 0 || bc <= 0)
+    return fail(OI_EINVAL, "oi_coarse_to_image_tc: bad arguments");
+  const int ny1 = n1_of(ny);
+  if (!ny1 || nx % 128 != 0 || nx > 4096 || bc > 64 || 2 * br - 1 > 128 || 2 * br - 1 > ny)
+    return fail(OI_ERANGE, "oi_coarse_to_image_tc: grid %dx%d / band %dx%d unsupported", ny, nx, br, bc);
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = fold_parts(coarse, nparts, (long long)count * 128 * 128, s);
+  if (rc) return rc;
+  float2* ih = (float2*)scratch_ihat;
+  rc = launch_coarse_spec_fft<4, 4>(coarse, count, br, bc, (const float2*)wm_r, (const float2*)wm_c, ih, s);
+  if (rc) return rc;
+  float2* v = (float2*)scratch_v;
+  switch (ny1) {
+    case 8: rc = cols_inv<8>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+    case 16: rc = cols_inv<16>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+    case 32: rc = cols_inv<32>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+    default: rc = cols_inv<64>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+  }
+  if (rc) return rc;
+  return oi_rows_inv_tc(v, count, ny, nx, bc, cconsts, out, stream);
+}

@@ -126,6 +126,24 @@ class Plan:
             self._tc_consts = c
         return c
 
+    def tc_rows(self, form) -> bool:
+        """The split-BF16x3 form runs the N-point row passes on the tensor cores too (FFT grids, band <= 64)."""
+        b = self.band
+        return (form == 'bf16x3' and self.fft and self.ny % 128 == 0 and self.nx % 128 == 0 and b.bc <= 64
+                and b.br <= 64)
+
+    def rows_consts(self, which: int) -> torch.Tensor:
+        """Constant operand image of the tensor-core row pass: 0 forward (band columns), 1 inverse (synthesis)."""
+        attr = '_rows_consts_%d' % which
+        c = getattr(self, attr, None)
+        if c is None:
+            b = self.band
+            nbytes = (self.nx // 64) * 32768 if which == 0 else (self.nx // 128) * 65536
+            c = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            N.call('oi_rows_tc_constants', which, self.nx, b.m0c, b.bc, N.ptr(c), nbytes, N.stream_handle(self.device))
+            setattr(self, attr, c)
+        return c
+
     def use_fft(self, form):
         if form not in (None,) + FORMS:
             raise ValueError(f'form must be one of {FORMS}')
@@ -181,7 +199,10 @@ def band_spectrum(field: torch.Tensor, kind: int, plan: Plan, nch: int = 1, scal
     band = torch.empty((batch, nch, b.br, b.bc), dtype=torch.complex64, device=plan.device)
     s = N.stream_handle(plan.device)
     sc = float(scale / (plan.ny * plan.nx))
-    if plan.use_fft(form) and kind != N.FIELD_COMPLEX_C64 and nch == 1:
+    if plan.tc_rows(form) and kind != N.FIELD_COMPLEX_C64 and nch == 1:
+        N.call('oi_band_spectrum_tc', N.ptr(field), kind, batch, plan.ny, plan.nx, b.m0r, b.br, b.m0c, b.bc,
+               N.ptr(plan.rows_consts(0)), N.ptr(plan.wn_y), sc, N.ptr(scratch), N.ptr(band), s)
+    elif plan.use_fft(form) and kind != N.FIELD_COMPLEX_C64 and nch == 1:
         N.call('oi_band_spectrum_fft', N.ptr(field), kind, batch, plan.ny, plan.nx, b.m0r, b.br, b.m0c, b.bc,
                N.ptr(plan.wn_x), N.ptr(plan.wn_y), sc, N.ptr(scratch), N.ptr(band), s)
     else:
@@ -235,7 +256,12 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
     if out is None:
         out = torch.empty((batch, nz, plan.ny, plan.nx), dtype=torch.float32, device=dev)
     ihat = torch.empty(batch * nz * (2 * b.br - 1) * b.bc, dtype=torch.complex64, device=dev)
-    if plan.use_fft(form):
+    if form == 'bf16x3' and plan.tc_rows(form):
+        v = torch.empty(batch * nz * b.bc * plan.ny, dtype=torch.complex64, device=dev)
+        N.call('oi_coarse_to_image_tc', N.ptr(coarse), nsplit, batch * nz, b.br, b.bc, N.ptr(plan.wm_r),
+               N.ptr(plan.wm_c), N.ptr(plan.wn_y), N.ptr(plan.rows_consts(1)), plan.ny, plan.nx, N.ptr(ihat),
+               N.ptr(v), N.ptr(out), s)
+    elif plan.use_fft(form):
         v = torch.empty(batch * nz * b.bc * plan.ny, dtype=torch.complex64, device=dev)
         wm_r, wm_c = (plan.wm_r, plan.wm_c) if plan.coarse_fft else (None, None)
         N.call('oi_coarse_to_image_fft', N.ptr(coarse), nsplit, batch * nz, plan.mr, plan.mc, b.br, b.bc,

@@ -8,6 +8,11 @@ from tests.fixtures import rel_err
 pytestmark = pytest.mark.gpu
 
 TOL = 2e-6   # same kernels; only the batch composition (and so the summation split) differs
+# The split-BF16x3 form cuts a batch's fields into per-SM task ranges that depend on the batch, so the FP32 fold of
+# the partial coarse sums runs in a different order alone and in a mix (differences of a few ulp); the bf16 hi/lo
+# split of the tensor-core synthesis then resolves values to ~2^-16, so results agree to the form's resolution
+# (measured <= 1.1e-5 of peak), well inside its stated bound of 1e-4.
+TOL_SPLIT = 5e-5
 
 
 def _specs(form=None):
@@ -49,7 +54,7 @@ def test_mixed_stream_matches_alone(graphs, form):
         m = models.setdefault(sp.key, ex.models[sp.key])
         alone = m.image(t.cuda().unsqueeze(0))[0].cpu()
         assert got.shape == (sp.planes, sp.ny, sp.nx)
-        assert rel_err(got.numpy(), alone.numpy()) < TOL
+        assert rel_err(got.numpy(), alone.numpy()) < (TOL_SPLIT if form == 'bf16x3' else TOL)
     lat = srv.latency_ms()
     assert lat['count'] == len(reqs)
 

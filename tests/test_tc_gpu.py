@@ -132,3 +132,38 @@ def test_tc_ranges_cross_images_deterministic(oi, batch):
         solo = model.image(field[b:b + 1].contiguous(), kind=N.FIELD_COMPLEX_C64, nch=3, form='bf16x3')
         assert rel_err(solo.cpu().numpy(), ref[b:b + 1].cpu().numpy()) < BF16X3_VS_FP64
     assert N.device_status() == 0
+
+
+@pytest.mark.parametrize('ny,nx,band', [
+    (256, 256, (-15, 31, -15, 31)),
+    (512, 1024, (-29, 59, -29, 59)),
+    (1024, 1024, (-29, 59, -20, 41)),
+    (2048, 512, (-31, 63, 0, 64)),
+])
+def test_tc_row_passes_vs_fft(oi, ny, nx, band):
+    """Band spectrum (tensor-core row pass + FFT columns) of float32 and uint8 masks, and the synthesis
+    (FFT columns + tensor-core row pass), against the FP32 FFT form."""
+    from opticalimaging_b200 import _native as N
+    from opticalimaging_b200.engine import Band, CoherentModel, Plan, band_spectrum
+    dev = torch.device('cuda')
+    b = Band(*band)
+    plan = Plan.get(ny, nx, b, dev)
+    assert plan.tc_rows('bf16x3')
+    rng = np.random.default_rng(ny + nx)
+    m = (rng.random((3, ny, nx)) > 0.6).astype(np.float32)
+    m[1] *= rng.random((ny, nx)).astype(np.float32)          # a grey mask too
+    md = torch.from_numpy(m).to(dev)
+    want = band_spectrum(md, N.FIELD_REAL_F32, plan, form='fft').cpu().numpy()
+    got = band_spectrum(md, N.FIELD_REAL_F32, plan, form='bf16x3').cpu().numpy()
+    assert rel_err(got, want) < 2e-5
+    u8 = torch.from_numpy((m[[0, 2]] > 0).astype(np.uint8)).to(dev)
+    got8 = band_spectrum(u8, N.FIELD_U8, plan, form='bf16x3').cpu().numpy()
+    assert rel_err(got8, want[[0, 2]]) < 2e-5
+    g = torch.Generator().manual_seed(ny)
+    pupils = torch.randn((1, 3, b.br, b.bc), dtype=torch.complex64, generator=g)
+    model = CoherentModel(pupils.to(dev), torch.ones((1, 3), device=dev), b, ny, nx)
+    img = model.image(md, form='bf16x3').cpu().numpy()
+    ref = model.image(md, form='fft').cpu().numpy()
+    print(f'{ny}x{nx}: band max {rel_err(got, want):.2e}, image max {rel_err(img, ref):.2e} rms {rms_rel(img, ref):.2e}')
+    assert rel_err(img, ref) < BF16X3_VS_FP64
+    assert N.device_status() == 0
