@@ -226,6 +226,138 @@ def serve_measure(sk, info, masks_np, dev, args):
             "h2d_bytes_per_image": N_PIX * N_PIX, "d2h_bytes_per_image": 4 * N_PIX * N_PIX}
 
 
+def serve_mix(dev, args, state):
+    """Configuration 5: a Poisson stream of mixed requests (clip sizes 256..2048, SOCS-24 / vector Abbe /
+    three-plane SOCS) through the server with a 150 GB HBM budget, against the plain FP32 path on a sample of the
+    same requests, with the served form's error against the FP32 form (every model) and the FP64 oracle."""
+    import collections
+    import random
+    from opticalimaging_b200 import serve, workloads as W
+    from tests.fixtures import rel_err
+    t_setup = time.perf_counter()
+    specs = W.config5_specs('bf16x3')
+    plain_specs = W.config5_specs(None)
+    stream = W.config5_stream(args.mix_requests)
+    pool = {n: [torch.from_numpy(m.astype(np.uint8)).pin_memory()
+                for m in W.manhattan_masks(4, n, 2.0 * n, seed=50 + n)] for n in W.CONFIG5_SIZES}
+    ex = serve.CudaExecutor(device=dev, nslots=3, max_batch=BATCH)
+    srv = serve.Server(ex, hbm_budget=150e9, max_batch=BATCH)
+
+    # caller-provided pinned result buffers, recycled when their request completes (as a client that consumes
+    # each image would): no pinned allocation per batch, bounded host memory
+    free = collections.defaultdict(list)
+    lock = threading.Lock()
+
+    def submit(k, n, i):
+        sp = specs[(k, n)]
+        shape = (sp.planes, sp.ny, sp.nx)
+        with lock:
+            buf = free[shape].pop() if free[shape] else None
+        if buf is None:
+            buf = torch.empty(shape, dtype=torch.float32).pin_memory()
+        f = srv.submit(sp, pool[n][i % len(pool[n])], out=buf)
+
+        def recycle(_f, buf=buf, shape=shape):
+            with lock:
+                free[shape].append(buf)
+        f.add_done_callback(recycle)
+        return f
+
+    # every model built and the graph of every batch bucket captured before any timing; then a short warm-up
+    for sp in specs.values():
+        ex.prepare(sp, torch.uint8, srv.batch_limit(sp))
+    futs = [submit(k, n, i) for k, n, i in stream[:min(len(stream), 300)]]
+    for f in futs:
+        f.result()
+    del futs
+    setup_s = time.perf_counter() - t_setup
+    # saturated throughput: a closed loop keeping 256 requests outstanding
+    srv.completed.clear()
+    q = collections.deque()
+    t0 = time.perf_counter()
+    for k, n, i in stream:
+        if len(q) >= 256:
+            q.popleft().result()
+        q.append(submit(k, n, i))
+    while q:
+        q.popleft().result()
+    sat_rate = len(stream) / (time.perf_counter() - t0)
+    # Poisson arrivals at 70 % of the saturated rate: latency under load
+    srv.completed.clear()
+    rng = random.Random(11)
+    rate = 0.7 * sat_rate
+    futs = []
+    t_next = t0 = time.perf_counter()
+    for k, n, i in stream:
+        t_next += rng.expovariate(rate)
+        while time.perf_counter() < t_next:
+            pass
+        futs.append(submit(k, n, i))
+    for f in futs:
+        f.result()
+    del futs
+    served_rate = len(stream) / (time.perf_counter() - t0)
+    lat = srv.latency_ms()
+    batches = srv.batches
+    resident = ex.resident_bytes()
+    srv.close()
+    # plain FP32 path, one request at a time, on a sample with the same mix (models built outside the timing)
+    sample = stream[:min(len(stream), 60)]
+    serve.plain_run([(plain_specs[(k, n)], pool[n][0]) for k, n in {(k, n) for k, n, _ in sample}], device=dev)
+    _, tp = serve.plain_run([(plain_specs[(k, n)], pool[n][i % len(pool[n])]) for k, n, i in sample], device=dev)
+    plain_rate = len(sample) / tp
+    # accuracy of the served form: against the FP32 form on every model, against the FP64 oracle on two
+    worst = 0.0
+    for key, sp in specs.items():
+        m = ex.models.get(sp.key) or sp.build()
+        mask = pool[key[1]][0].to(dev).unsqueeze(0)
+        a = m.image(mask).cpu().numpy()
+        b = m.image(mask, form='fft' if m.plan.fft else 'dft').cpu().numpy()
+        worst = max(worst, rel_err(a, b))
+    state["specs"], state["ex"], state["pool"] = specs, ex, pool
+    return {"requests": len(stream), "mix": "50 % SOCS-24, 30 % vector Abbe (quasar PntNum 31), 20 % SOCS-24 x 3 "
+            "focus planes; clip sizes uniform over 256, 512, 1024, 2048 (2 nm/pixel); binary Manhattan masks "
+            "(~35 % fill) as uint8; float32 images returned to the host",
+            "images_per_s": served_rate, "saturated_images_per_s": sat_rate,
+            "latency_at": f"Poisson arrivals at {rate:.0f} requests/s (70 % of the saturated rate)",
+            "p50_ms": lat.get("p50_ms"), "p99_ms": lat.get("p99_ms"), "batches": batches,
+            "plain_images_per_s": plain_rate, "served_over_plain": served_rate / plain_rate,
+            "plain": f"{len(sample)} requests of the same stream one at a time, FP32 form, no batching or graphs",
+            "hbm_budget_gb": 150, "resident_gb": resident / 1e9, "setup_s": setup_s,
+            "max_err_vs_fp32_form": worst}
+
+
+def mix_fp64_check(specs, ex, pool, dev):
+    """Served-form images of the 256 x 256 SOCS-24 and Abbe models against the FP64 oracle (relative to peak)."""
+    from oracle import optics64 as O
+    from opticalimaging_b200 import imaging, workloads as W
+    from opticalimaging_b200.params import Scatter
+    from tests.fixtures import rel_err
+    out = {}
+    mask = pool[256][0].float().numpy()
+    sc = Scatter()
+    sc.Period_X = sc.Period_Y = 512.0
+    sc.ScatterField = W.thin_field(mask)
+    md = torch.from_numpy(mask).to(dev).unsqueeze(0)
+    sr, po, nm = W.config3_optics(order=24)
+    T, fg = imaging.CalculateTCCMatrix(sr, [512.0, 512.0], po, 0.0, nm)
+    K = imaging.DecomposeTCC_SOCS(T, fg, [256, 256], nm).cpu().numpy().astype(np.complex128)
+    m = ex.models.get(specs[('socs24', 256)].key) or specs[('socs24', 256)].build()
+    out["socs24_256"] = rel_err(m.image(md)[0, 0].cpu().numpy(), O.socs(sc, K, sr, po))
+    q = specs[('abbe', 256)]
+    m = ex.models.get(q.key) or q.build()
+    import math
+    from opticalimaging_b200.params import Numerics, Projection, Source
+    s2, p2, n2 = Source(), Projection(), Numerics()
+    s2.Shape, s2.PntNum, s2.SigmaIn, s2.SigmaOut, s2.OpenAngle = 'quasar', 31, 0.5, 0.85, math.pi / 6
+    s2.PolarizationVector = [1.0, 0.0]
+    W.mapped_optics(p2, s2)
+    n2.ImageCalculationMode = 'vector'
+    p2.FocusRange = torch.tensor([0.0])
+    out["abbe_256"] = rel_err(m.image(md)[0, 0].cpu().numpy(), O.abbe(s2, sc, p2, n2)[0])
+    return out
+
+
 def serve_model_from(sk, form):
     from opticalimaging_b200.engine import CoherentModel
     return CoherentModel(sk.pupils, sk.weights, sk.band, sk.ny, sk.nx, form=form)
@@ -377,6 +509,12 @@ def run_engine(args, world, rank, local):
     # ---- served: the same clips as requests through the continuous-batching server (pinned uint8 in,
     # host float32 images out), saturated arrival; and the plain one-request-at-a-time path
     serving = serve_measure(sk, info, masks_np, dev, args) if not args.no_serve else None
+    mix, mix_state = None, {}
+    if not args.no_serve and args.mix_requests > 0:
+        try:
+            mix = serve_mix(dev, args, mix_state)
+        except Exception as e:  # the configuration-3 line must still print
+            mix = {"error": f"{type(e).__name__}: {e}"}
     # ---- per-stage device times (outside the timed region) and the roofline of the dominant stage
     st = stage_times(sk, masks, out, args.form)
     hbm, bf16, src = peaks()
@@ -411,7 +549,7 @@ def run_engine(args, world, rank, local):
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_in.numel()),
                     "d2h_bytes_per_step": int(host_out.numel() * 4)},
-            "gpu_launches": launches, "setup_s": setup_s, "serving": serving,
+            "gpu_launches": launches, "setup_s": setup_s, "serving": serving, "serving_mix": mix,
             "stage_ms": {k: round(v, 4) for k, v in st.items()}, "roofline": roof, "clocks": clk.summary()}
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -420,6 +558,8 @@ def run_engine(args, world, rank, local):
         forms = precision_study(sk, masks, ref)
         line["forms"] = forms
         line["accuracy_vs_fp64"] = dict(forms[args.form], relative_to=forms["relative_to"])
+        if mix is not None and "error" not in mix:
+            mix["err_vs_fp64"] = mix_fp64_check(mix_state["specs"], mix_state["ex"], mix_state["pool"], dev)
         v, n = cpu_reference_sample(info, masks_np, args.cpu_budget, threads)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{n} clips of 1024x1024 through the reference's SOCS algorithm "
@@ -436,7 +576,9 @@ def main():
     ap.add_argument('--impl', default='engine', choices=['engine', 'reference'])
     ap.add_argument('--cpu-budget', type=float, default=15.0)
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline and the precision study')
-    ap.add_argument('--no-serve', action='store_true', help='skip the served measurement (profiling runs)')
+    ap.add_argument('--no-serve', action='store_true', help='skip the served measurements (profiling runs)')
+    ap.add_argument('--mix-requests', type=int, default=2000,
+                    help='requests of the mixed serving stream (configuration 5); 0 skips it')
     ap.add_argument('--batch', type=int, default=64, help='clips per step (64 in the benchmark configuration)')
     ap.add_argument('--serve-requests', type=int, default=512, help='requests in the served measurement')
     ap.add_argument('--form', default='bf16x3', choices=['fft', 'dft', 'bf16x3'],

@@ -117,11 +117,13 @@ OI_API int oi_abbe_pupils(const float* fr, const float* fc, int br, int bc, cons
  * fr  = oi_twiddle(mr x br, sign -1) row phases, fcs = oi_twiddle(bc x mc, sign -1) column phases.
  * mc must be a multiple of 64 and at most 256; br, bc at most 256.
  * `pupil_batch_stride` = 0 shares the pupils across the batch (SOCS kernels), else it is the element stride
- * between images' pupil sets.
+ * between images' pupil sets.  The fields (k, c), f = k*nch + c, are split over `nsplit` partial sums:
+ * f = s, s + nsplit, ... go to coarse[s][b][z][sr][sc] (float [nsplit][batch][nz][mr][mc]); the coarse-to-image
+ * stage adds them with nparts = nsplit.
  */
 OI_API int oi_coherent_coarse(const void* band, int batch, int nch, int br, int bc, const void* pupil,
                               long long pupil_batch_stride, const float* weight, int nz, int nk, int mr, int mc,
-                              const void* frow, const void* fcol, float* coarse, void* stream);
+                              const void* frow, const void* fcol, int nsplit, float* coarse, void* stream);
 
 /*
  * Exact band-limited resampling of the coarse intensity to the output grid:

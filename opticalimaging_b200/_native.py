@@ -19,7 +19,7 @@ _SIGS = {
     'oi_band_spectrum': [_vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],
     'oi_abbe_pupils': [_vp, _vp, _i, _i, _vp, _vp, _vp, _i, _d, _vp, _i, _vp, _i, _vp, _d, _d, _d, _d, _vp, _vp,
                        _vp],
-    'oi_coherent_coarse': [_vp, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp],
+    'oi_coherent_coarse': [_vp, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _i, _i, _vp, _vp, _i, _vp, _vp],
     'oi_coarse_to_image': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp],
     'oi_tcc_pupils64': [_vp, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _d, _vp, _i, _vp, _d, _d, _d, _d, _vp, _vp],
     'oi_tcc_assemble64': [_vp, _i, _i, _i, _vp, _vp],

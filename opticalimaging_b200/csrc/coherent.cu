@@ -27,7 +27,9 @@ struct CoherentArgs {
   int nz, nk, mr, mc;
   const float2* frow;  // [mr][br]
   const float2* fcol;  // [bc][mc]
-  float* coarse;       // [batch][nz][mr][mc]
+  float* coarse;       // [nsplit][batch][nz][mr][mc]
+  int nsplit;          // fields f = split, split + nsplit, ... go to partial sum `split`
+  long long split_stride;
 };
 
 // NU = ceil(bc / 64) column groups of stage 1, NJ = mc / 64 column groups of stage 2.
@@ -41,7 +43,8 @@ __global__ void __launch_bounds__(256) coherent_coarse_kernel(CoherentArgs a) {
   float2* c_chunk = gs + CO_TR * bcp;           // [CO_CC][mc]
 
   const int tid = threadIdx.x, lane64 = tid & 63, grp = tid >> 6;  // grp 0..3 -> 4 coarse rows each
-  const int sr0 = blockIdx.x * CO_TR, z = blockIdx.y;
+  const int rblocks = (a.mr + CO_TR - 1) / CO_TR;
+  const int split = blockIdx.x / rblocks, sr0 = (blockIdx.x % rblocks) * CO_TR, z = blockIdx.y;
   const long long b = blockIdx.z;
   const int br = a.br, bc = a.bc, mr = a.mr, mc = a.mc;
 
@@ -52,10 +55,11 @@ __global__ void __launch_bounds__(256) coherent_coarse_kernel(CoherentArgs a) {
     for (int j = 0; j < NJ; ++j) acc[i][j] = 0.f;
 
   const float2* pup_base = a.pupil + b * a.pupil_batch_stride + (long long)z * a.nk * br * bc;
-  for (int k = 0; k < a.nk; ++k) {
+  for (int f = split; f < a.nk * a.nch; f += a.nsplit) {
+    const int k = f / a.nch, c = f % a.nch;
     const float2* pk = pup_base + (long long)k * br * bc;
     const float w = __ldg(a.weight + (long long)z * a.nk + k);
-    for (int c = 0; c < a.nch; ++c) {
+    {
       const float2* hc = a.band + b * a.band_img_stride + (long long)c * br * bc;
       // ---- stage 1: G[r][ic] = sum_ir frow[sr0+r][ir] * P[ir][ic] * band[ir][ic]
       float2 g[4][NU];
@@ -130,7 +134,7 @@ __global__ void __launch_bounds__(256) coherent_coarse_kernel(CoherentArgs a) {
         for (int j = 0; j < NJ; ++j) acc[i][j] = fmaf(w, fmaf(e2[i][j].x, e2[i][j].x, e2[i][j].y * e2[i][j].y), acc[i][j]);
     }
   }
-  float* out = a.coarse + ((b * a.nz + z) * (long long)mr) * mc;
+  float* out = a.coarse + split * a.split_stride + ((b * a.nz + z) * (long long)mr) * mc;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     int sr = sr0 + grp * 4 + i;
@@ -149,7 +153,7 @@ static int launch_coherent(const CoherentArgs& a, int batch, cudaStream_t s) {
     int rc_smem = ensure_smem((const void*)kern, smem, "oi_coherent_coarse");
     if (rc_smem) return rc_smem;
   }
-  dim3 grid((unsigned)ceil_div(a.mr, CO_TR), (unsigned)a.nz, (unsigned)batch);
+  dim3 grid((unsigned)(ceil_div(a.mr, CO_TR) * a.nsplit), (unsigned)a.nz, (unsigned)batch);
   kern<<<grid, 256, smem, s>>>(a);
   oi::note_launch();
   return check_launch("oi_coherent_coarse");
@@ -170,15 +174,17 @@ static int dispatch_nj(const CoherentArgs& a, int batch, cudaStream_t s) {
 
 extern "C" int oi_coherent_coarse(const void* band, int batch, int nch, int br, int bc, const void* pupil,
                                   long long pupil_batch_stride, const float* weight, int nz, int nk, int mr, int mc,
-                                  const void* frow, const void* fcol, float* coarse, void* stream) {
+                                  const void* frow, const void* fcol, int nsplit, float* coarse, void* stream) {
   using namespace oi;
   if (!band || !pupil || !weight || !frow || !fcol || !coarse || batch <= 0 || nch <= 0 || br <= 0 || bc <= 0 ||
-      nz <= 0 || nk <= 0 || mr <= 0 || mc <= 0 || pupil_batch_stride < 0)
+      nz <= 0 || nk <= 0 || mr <= 0 || mc <= 0 || pupil_batch_stride < 0 || nsplit <= 0)
     return fail(OI_EINVAL, "oi_coherent_coarse: bad arguments");
-  if (mc % 64 != 0 || mc > 256 || br > CO_BMAX || bc > CO_BMAX || nz > 65535 || batch > 65535)
-    return fail(OI_ERANGE, "oi_coherent_coarse: sizes out of range (br=%d bc=%d mc=%d)", br, bc, mc);
+  if (mc % 64 != 0 || mc > 256 || br > CO_BMAX || bc > CO_BMAX || nz > 65535 || batch > 65535 ||
+      nsplit > nk * nch || (long long)ceil_div(mr, CO_TR) * nsplit > 2147483647LL)
+    return fail(OI_ERANGE, "oi_coherent_coarse: sizes out of range (br=%d bc=%d mc=%d nsplit=%d)", br, bc, mc, nsplit);
   CoherentArgs a{(const float2*)band, (long long)nch * br * bc, nch, br, bc, (const float2*)pupil,
-                 pupil_batch_stride, weight, nz, nk, mr, mc, (const float2*)frow, (const float2*)fcol, coarse};
+                 pupil_batch_stride, weight, nz, nk, mr, mc, (const float2*)frow, (const float2*)fcol, coarse,
+                 nsplit, (long long)batch * nz * mr * mc};
   cudaStream_t s = (cudaStream_t)stream;
   switch ((bc + 63) / 64) {
     case 1: return dispatch_nj<1>(a, batch, s);

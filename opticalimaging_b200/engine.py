@@ -144,6 +144,19 @@ class Plan:
             setattr(self, attr, c)
         return c
 
+    def coarse_fft_tables(self):
+        """Four-step FFT tables of the coarse grid (for coarse grids of 256..2048 points per axis)."""
+        t = getattr(self, '_coarse_fft_tables', None)
+        if t is None:
+            t = self._coarse_fft_tables = (fft_tables(self.mr, self.device), fft_tables(self.mc, self.device))
+        return t
+
+    def big_coarse_fft(self, form) -> bool:
+        """Coarse grids above 128 (bands over 64) on FFT output grids: the coarse spectrum by the FFT band pass."""
+        lib = N.load()
+        return (form != 'dft' and self.fft and not self.coarse_fft and lib.oi_fft_supported(self.mr, self.mc) == 1
+                and 2 * (self.band.bc - 1) < self.mc and 2 * self.band.br - 1 <= self.mr)
+
     def use_fft(self, form):
         if form not in (None,) + FORMS:
             raise ValueError(f'form must be one of {FORMS}')
@@ -248,10 +261,11 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
                int(pupil_batch_stride), N.ptr(weights), nz, nk, plan.mr, plan.mc, N.ptr(plan.wm_r),
                N.ptr(plan.wm_c), nsplit, N.ptr(coarse), s)
     else:
-        nsplit = 1
-        coarse = torch.empty((batch, nz, plan.mr, plan.mc), dtype=torch.float32, device=dev)
+        nsplit = field_split(nk * nch, batch * nz * ((plan.mr + 15) // 16))
+        coarse = torch.empty((nsplit, batch, nz, plan.mr, plan.mc), dtype=torch.float32, device=dev)
         N.call('oi_coherent_coarse', N.ptr(band), batch, nch, b.br, b.bc, N.ptr(pupils), int(pupil_batch_stride),
-               N.ptr(weights), nz, nk, plan.mr, plan.mc, N.ptr(plan.frow), N.ptr(plan.fcol), N.ptr(coarse), s)
+               N.ptr(weights), nz, nk, plan.mr, plan.mc, N.ptr(plan.frow), N.ptr(plan.fcol), nsplit, N.ptr(coarse),
+               s)
     _mark(marks, 'coherent_coarse')
     if out is None:
         out = torch.empty((batch, nz, plan.ny, plan.nx), dtype=torch.float32, device=dev)
@@ -261,6 +275,19 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
         N.call('oi_coarse_to_image_tc', N.ptr(coarse), nsplit, batch * nz, b.br, b.bc, N.ptr(plan.wm_r),
                N.ptr(plan.wm_c), N.ptr(plan.wn_y), N.ptr(plan.rows_consts(1)), plan.ny, plan.nx, N.ptr(ihat),
                N.ptr(v), N.ptr(out), s)
+    elif plan.big_coarse_fft(form):
+        # the coarse intensity's Hermitian half-spectrum by the FFT band pass, then the FFT synthesis
+        count, nq = batch * nz, 2 * b.br - 1
+        cimg = (coarse[0] if nsplit == 1 else coarse.sum(dim=0)).reshape(count, plan.mr, plan.mc)
+        wn_r, wn_c = plan.coarse_fft_tables()
+        t = torch.empty(count * plan.mr * b.bc, dtype=torch.complex64, device=dev)
+        ih = ihat.view(count, 1, nq, b.bc)
+        N.call('oi_band_spectrum_fft', N.ptr(cimg), N.FIELD_REAL_F32, count, plan.mr, plan.mc, -(b.br - 1), nq, 0,
+               b.bc, N.ptr(wn_c), N.ptr(wn_r), 1.0 / (plan.mr * plan.mc), N.ptr(t), N.ptr(ih), s)
+        ih[..., 1:] *= 2.0
+        v = torch.empty(count * b.bc * plan.ny, dtype=torch.complex64, device=dev)
+        N.call('oi_spectrum_to_image_fft', N.ptr(ih), count, b.br, b.bc, N.ptr(plan.wn_y), N.ptr(plan.wn_x), plan.ny,
+               plan.nx, N.ptr(v), N.ptr(out), s)
     elif plan.use_fft(form):
         v = torch.empty(batch * nz * b.bc * plan.ny, dtype=torch.complex64, device=dev)
         wm_r, wm_c = (plan.wm_r, plan.wm_c) if plan.coarse_fft else (None, None)
@@ -361,7 +388,8 @@ class CoherentModel:
         b, p = self.band, self.plan
         nz = self.planes
         form = self.form if form is None else form
-        split = field_split(self.count * nch, batch * nz) if p.use_coarse_fft(None) else 1
+        split = (field_split(self.count * nch, batch * nz) if p.use_coarse_fft(None)
+                 else field_split(self.count * nch, batch * nz * ((p.mr + 15) // 16)))
         if form == 'bf16x3':
             split = tc_parts_bound(batch * nz, self.count * nch)
             p = Plan.get(self.ny, self.nx, b, self.device, coarse=TC_COARSE)

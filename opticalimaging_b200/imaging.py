@@ -306,6 +306,29 @@ def socs_kernels_from_tcc(tcc, FG_ValidSize, Nfg, numerics) -> SocsKernels:
     return SocsKernels(kb.to(torch.complex64), band, ng, nf)
 
 
+def socs_kernels_from_pupils(h, FG_ValidSize, Nfg, numerics) -> SocsKernels:
+    """Top-K SOCS kernels from the pupil matrix h [ne, FG, S] of TCC = sum_e h_e h_e^H, without forming the TCC
+    when its rank bound ne*S is below FG: with H = [h_0 | .. | h_ne-1] (FG x ne*S), the Gram matrix H^H H has the
+    TCC's non-zero eigenvalues, and its eigenvectors v give the kernels sqrt(lambda) u = H v (FP64 on the device).
+    Kernels equal socs_kernels_from_tcc's up to a phase per kernel (images are unchanged)."""
+    ne, fg, s = h.shape
+    if ne * s >= fg:
+        tcc = torch.empty((fg, fg), dtype=torch.complex128, device=h.device)
+        N.call('oi_tcc_assemble64', N.ptr(h), ne, fg, s, N.ptr(tcc), N.stream_handle(h.device))
+        return socs_kernels_from_tcc(tcc, FG_ValidSize, Nfg, numerics)
+    nf, ng = Nfg
+    lg, lf = FG_ValidSize
+    if lf > ng or lg > nf:
+        raise ValueError(f'TCC grid {lf}x{lg} does not fit the {ng}x{nf} image grid')
+    H = h.permute(1, 0, 2).reshape(fg, ne * s)
+    lam, V = torch.linalg.eigh(H.conj().T @ H)
+    lam, V = torch.clamp(lam.flip(0), min=0), V.flip(1)
+    k = min(_socs_count(numerics, lam, fg), V.shape[1])   # kernels past the rank bound are zero
+    kb = (H @ V[:, :k]).T.reshape(k, lf, lg)
+    band = Band(_placement(ng, lf), lf, _placement(nf, lg), lg)
+    return SocsKernels(kb.to(torch.complex64).contiguous(), band, ng, nf)
+
+
 def DecomposeTCC_SOCS(TCCMatrix_Stacked, FG_ValidSize, Nfg, numerics):
     """Full-grid SOCS kernels [Ny, Nx, K] complex64 on the device (DecomposeTCC_SOCS.py:3-37)."""
     dev = require_cuda()
@@ -338,8 +361,8 @@ def socs_model(source, projector, numerics, period_y, period_x, ny, nx, focus=No
     zs = _focus_list(projector) if focus is None else [float(z) for z in focus]
     sets = []
     for z in zs:
-        tcc, fg = CalculateTCCMatrix(source, [period_y, period_x], projector, z, numerics)
-        sets.append(socs_kernels_from_tcc(tcc, fg, [nx, ny], numerics))
+        h, fg = tcc_pupil_matrix(source, [period_y, period_x], projector, z, numerics)
+        sets.append(socs_kernels_from_pupils(h, fg, [nx, ny], numerics))
     k = max(s.count for s in sets)   # 'threshold' may keep a different count per plane: pad with zero kernels
     pupils = torch.zeros((len(zs), k, sets[0].band.br, sets[0].band.bc), dtype=torch.complex64,
                          device=sets[0].kernels.device)

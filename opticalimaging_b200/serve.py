@@ -144,6 +144,10 @@ class Server:
     def _max_batch(self, spec: ModelSpec) -> int:
         return max(1, min(self.max_batch, self.max_batch_pixels // spec.pixels, self.ex.max_batch(spec)))
 
+    def batch_limit(self, spec: ModelSpec) -> int:
+        """The largest batch this server forms for `spec` (by max_batch and max_batch_pixels)."""
+        return self._max_batch(spec)
+
     def _run(self):
         init = getattr(self.ex, 'thread_init', None)
         if init is not None:
@@ -345,6 +349,19 @@ class CudaExecutor:
             g = self.graphs[gk] = (graph, used)
             self._bytes[spec.key] = self._bytes.get(spec.key, 0) + used
         return g[0]
+
+    def prepare(self, spec, dtype=torch.uint8, max_batch: int | None = None):
+        """Build `spec`'s model, the slot buffers and the CUDA graph of every batch bucket up to `max_batch` on
+        every slot, so that no capture -- and no device-wide synchronisation -- happens while serving.  Call it
+        before the first request of a model (not while batches run)."""
+        model = self._model(spec)
+        top = bucket(max_batch or self._max_batch)
+        for slot in range(self.nslots):
+            d_in, d_out = self._buffers(spec, slot, dtype, top)
+            b = 1
+            while self.use_graphs and b <= top:
+                self._graph(spec, model, slot, dtype, b, d_in, d_out)
+                b *= 2
 
     def launch(self, slot, spec, reqs):
         model = self._model(spec)

@@ -132,3 +132,37 @@ def config4(seed=4, n=1024, order=16):
     logits = rng.standard_normal((n, n)).astype(np.float32)
     target = rect_mask(n, n, 2048, 2048, 40, 60.0, 400.0, rng)
     return sr, po, nm, logits, target
+
+
+CONFIG5_SIZES = (256, 512, 1024, 2048)
+
+
+def config5_specs(form='bf16x3'):
+    """The resident models of the serving stream, keyed (kind, n): SOCS-24 (annular 0.7/0.95 PntNum 41 vector
+    TCC), vector Abbe (quasar 0.5/0.85/30deg PntNum 31, x_pol) and SOCS-24 at three focus planes (-40, 0, 40 nm),
+    each for clips n x n at 2 nm/pixel (period 2n nm).  `form` is the serving form ('bf16x3' where the band
+    allows it, FP32 FFT otherwise; None for the plain FP32 path)."""
+    from . import serve
+    sr, po, nm = config3_optics(order=24)
+    q, qp, qn = Source(), Projection(), Numerics()
+    q.Shape, q.PntNum, q.SigmaIn, q.SigmaOut, q.OpenAngle = 'quasar', 31, 0.5, 0.85, math.pi / 6
+    q.PolarizationVector = [1.0, 0.0]
+    mapped_optics(qp, q)
+    qn.ImageCalculationMode, qn.ImageCalculationMethod = 'vector', 'abbe'
+    specs = {}
+    for n in CONFIG5_SIZES:
+        period = 2.0 * n
+        specs[('socs24', n)] = serve.socs_spec(sr, po, nm, period, n, name='socs24', form=form)
+        specs[('abbe', n)] = serve.abbe_spec(q, qp, qn, period, n, name='abbe-quasar', form=form)
+        specs[('socs24x3', n)] = serve.socs_spec(sr, po, nm, period, n, focus=(-40.0, 0.0, 40.0), name='socs24x3',
+                                                 form=form)
+    return specs
+
+
+def config5_stream(count, seed=5):
+    """`count` requests (kind, n, mask index): sizes uniform over CONFIG5_SIZES, kinds 50 % SOCS-24, 30 % Abbe,
+    20 % three-plane SOCS."""
+    rng = np.random.default_rng(seed)
+    kinds = rng.choice(['socs24', 'abbe', 'socs24x3'], size=count, p=[0.5, 0.3, 0.2])
+    sizes = rng.choice(CONFIG5_SIZES, size=count)
+    return [(str(k), int(n), i) for i, (k, n) in enumerate(zip(kinds, sizes))]

@@ -196,3 +196,26 @@ def test_clear_field_is_uniform(oi):
     sc.ScatterField = W.thin_field(np.ones((256, 256), np.float32))
     img, _ = oi.CalculateAbbeImage(sr, sc, po, nm)
     np.testing.assert_allclose(img.Intensity.numpy(), 1.0, rtol=0, atol=5e-6)
+
+
+@pytest.mark.parametrize('order,threshold', [(24, None), (None, 0.99)])
+def test_gram_kernels_match_tcc_kernels(oi, order, threshold):
+    """SOCS kernels from the Gram matrix of the pupil matrix (rank 3S < FG) give the same images as the
+    eigendecomposition of the assembled TCC, for 'order' and 'threshold' truncation."""
+    from opticalimaging_b200 import _native as N, workloads as W
+    sr, po, nm = W.config3_optics(order=order or 24)
+    if threshold is not None:
+        nm.Hopkins_SettingType, nm.Hopkins_Threshold = 'threshold', threshold
+    h, fg = oi.tcc_pupil_matrix(sr, [2048.0, 2048.0], po, 0.0, nm)   # FG = 59^2 > 3 S = 1560
+    assert h.shape[0] * h.shape[2] < h.shape[1]          # the Gram path is taken
+    gram = oi.socs_kernels_from_pupils(h, fg, [256, 256], nm)
+    T, fg2 = oi.CalculateTCCMatrix(sr, [2048.0, 2048.0], po, 0.0, nm)
+    full = oi.socs_kernels_from_tcc(T, fg2, [256, 256], nm)
+    assert gram.count == full.count and gram.band == full.band
+    rng = np.random.default_rng(5)
+    masks = torch.from_numpy(np.stack([W.rect_mask(256, 256, 2048.0, 2048.0, 20, 30, 400, rng)
+                                       for _ in range(2)])).cuda()
+    a = gram.image(masks).cpu().numpy()
+    b = full.image(masks).cpu().numpy()
+    assert rel_err(a, b) < 2e-6
+    assert N.device_status() == 0

@@ -75,3 +75,28 @@ def test_fft_rejects_unsupported_grid(eng):
     assert lib.oi_fft_supported(128, 1024) == 0
     plan = eng.Plan.get(45, 63, eng.Band(-5, 11, -5, 11), torch.device('cuda'))
     assert not plan.fft   # odd grids take the DFT form
+
+
+def test_large_band_coarse_256_fft_vs_dft_and_oracle(eng):
+    """Band 117 (> 64): coarse grid 256 x 256, DFT coherent sum split over fields, coarse spectrum by the FFT
+    band pass and FFT synthesis; against the all-DFT form and the FP64 oracle (kernels from the Gram path)."""
+    from opticalimaging_b200 import imaging, workloads as W, _native as N
+    from opticalimaging_b200.params import Scatter
+    sr, po, nm = W.config3_optics(order=8)
+    model = imaging.socs_model(sr, po, nm, 4096.0, 4096.0, 1024, 1024)
+    assert model.band.br > 64 and model.plan.mr == 256 and model.plan.big_coarse_fft(None)
+    rng = np.random.default_rng(9)
+    masks = np.stack([W.rect_mask(1024, 1024, 4096.0, 4096.0, 30, 40, 600, rng) for _ in range(3)])
+    md = torch.from_numpy(masks).cuda()
+    fft = model.image(md)[:, 0].cpu().numpy()
+    dft = model.image(md, form='dft')[:, 0].cpu().numpy()
+    assert rel_err(fft, dft) < 5e-6
+    b = model.band
+    full = torch.zeros((1024, 1024, model.count), dtype=torch.complex64, device=model.device)
+    full[:b.br, :b.bc, :] = model.pupils[0].permute(1, 2, 0)
+    K = torch.roll(full, shifts=(b.m0r, b.m0c), dims=(0, 1)).cpu().numpy().astype(np.complex128)
+    sc = Scatter()
+    sc.Period_X = sc.Period_Y = 4096.0
+    sc.ScatterField = W.thin_field(masks[0])
+    assert rel_err(fft[0], O.socs(sc, K, sr, po)) < 1e-5
+    assert N.device_status() == 0

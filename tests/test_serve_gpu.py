@@ -72,3 +72,21 @@ def test_plain_path_matches_served():
     assert seconds > 0
     for a, b in zip(plain, served):
         assert rel_err(b.numpy(), a.numpy()) < TOL
+
+
+def test_prepare_captures_every_bucket():
+    """After prepare(), serving a model launches no further capture."""
+    from opticalimaging_b200 import serve, workloads as W
+    sp = _specs('bf16x3')[0]
+    ex = serve.CudaExecutor(nslots=2)
+    srv = serve.Server(ex, hbm_budget=40e9, max_batch=8)
+    ex.prepare(sp, torch.uint8, srv.batch_limit(sp))
+    n0 = len(ex.graphs)
+    assert n0 == 2 * 4                                      # buckets 1, 2, 4, 8 on two slots
+    rng = np.random.default_rng(1)
+    masks = [torch.from_numpy((W.rect_mask(sp.ny, sp.nx, 2.0 * sp.ny, 2.0 * sp.nx, 20, 30, 300, rng) > 0)
+                              .astype(np.uint8)).pin_memory() for _ in range(13)]
+    for f in [srv.submit(sp, m) for m in masks]:
+        f.result(timeout=120)
+    srv.close()
+    assert len(ex.graphs) == n0
