@@ -202,7 +202,8 @@ OI_API int oi_tc_constants(int m0r, int m0c, const void* wr, const void* wc, voi
  * band width bc <= 64.
  *   oi_rows_fwd_tc  t[b][ic][y] = sum_x field[b][y][x] exp(+2 pi i (m0c+ic) x / nx)  (float32 or uint8 masks;
  *                   t as the scratch of oi_band_spectrum_fft, float2 [batch][bc][ny])
- *   oi_rows_inv_tc  out[i][y][x] = sum_{qc<bc} Re(v[i][qc][y] exp(-2 pi i qc x / nx))  (v float2 [count][bc][ny])
+ *   oi_rows_inv_tc  out[i][y][x] = sum_{qc<bc} Re(v[i][qc][y] exp(-2 pi i qc x / nx))  (v float2 [count][bc][ny];
+ *                   vtiles: scratch of count * ny * 512 bytes that receives v as bf16 operand tiles)
  * `consts` is the constant operand image from oi_rows_tc_constants: which = 0 (forward; depends on nx, m0c, bc;
  * nx/64 * 32768 bytes) or 1 (inverse; depends on nx, bc; nx/128 * 65536 bytes).  A wait that exceeds 2 s ends
  * the kernel early and sets the device status.
@@ -212,14 +213,14 @@ OI_API int oi_tc_constants(int m0r, int m0c, const void* wr, const void* wc, voi
 OI_API int oi_rows_tc_constants(int which, int nx, int m0c, int bc, void* image, long long bytes, void* stream);
 OI_API int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, int nx, int m0c, int bc,
                           const void* consts, void* t, void* stream);
-OI_API int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, const void* consts, float* out,
-                          void* stream);
+OI_API int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, const void* consts, void* vtiles,
+                          float* out, void* stream);
 OI_API int oi_band_spectrum_tc(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c,
                                int bc, const void* wconsts, const void* wn_y, float scale, void* scratch,
                                void* band, void* stream);
 OI_API int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int br, int bc, const void* wm_r,
                                  const void* wm_c, const void* wn_y, const void* cconsts, int ny, int nx,
-                                 void* scratch_ihat, void* scratch_v, float* out, void* stream);
+                                 void* scratch_ihat, void* scratch_v, void* scratch_tiles, float* out, void* stream);
 
 /* The device status word (0 = no error) set by kernels whose bounded waits expired; optionally cleared.
  * Synchronous (reads device memory). */

@@ -635,9 +635,11 @@ extern "C" int oi_band_spectrum_tc(const void* field, int kind, int batch, int n
 // and column pass as there; the row pass is oi_rows_inv_tc against `cconsts` of oi_rows_tc_constants(1, ...).
 extern "C" int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int br, int bc, const void* wm_r,
                                      const void* wm_c, const void* wn_y, const void* cconsts, int ny, int nx,
-                                     void* scratch_ihat, void* scratch_v, float* out, void* stream) {
+                                     void* scratch_ihat, void* scratch_v, void* scratch_tiles, float* out,
+                                     void* stream) {
   using namespace oi;
-  if (!coarse || !wm_r || !wm_c || !wn_y || !cconsts || !scratch_ihat || !scratch_v || !out || count <= 0 ||
+  if (!coarse || !wm_r || !wm_c || !wn_y || !cconsts || !scratch_ihat || !scratch_v || !scratch_tiles || !out ||
+      count <= 0 ||
       nparts <= 0 || br <= 0 || bc <= 0)
     return fail(OI_EINVAL, "oi_coarse_to_image_tc: bad arguments");
   const int ny1 = n1_of(ny);
@@ -657,5 +659,5 @@ extern "C" int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int b
     default: rc = cols_inv<64>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
   }
   if (rc) return rc;
-  return oi_rows_inv_tc(v, count, ny, nx, bc, cconsts, out, stream);
+  return oi_rows_inv_tc(v, count, ny, nx, bc, cconsts, scratch_tiles, out, stream);
 }

@@ -13,8 +13,9 @@
 // resident per x tile), V = v converted to bf16 hi / lo.  The accumulator's lanes are the rows (forward) or
 // the columns (inverse), so every warp store of the result is one coalesced segment.
 //
-// Roles (320 threads): warps 0-7 convert the staged inputs into the K-major, 128-byte swizzled bf16 operand
-// and drain finished accumulators to global memory (two warps per tensor-memory lane quarter); warp 8 issues
+// Roles (320 threads; the forward kernel has an 11th warp issuing its W loads apart from the mask loads):
+// warps 0-7 convert the staged inputs into the bf16 operand and drain finished accumulators to global memory
+// (two warps per tensor-memory lane quarter); warp 8 issues
 // the loads into the staging buffers (one 2-D tensor-map box per tile and 1-D bulk copies of the constants; no
 // multicast); warp 9 lane 0 issues the MMAs and
 // commits them to mbarriers.  Staging and operands are double-buffered (forward) or single (inverse); the
@@ -68,45 +69,57 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
 }
 
 // ------------------------------------------------------------------------------------------ forward
-// Shared memory: two stages of { staging (mask rows: 128 x 64 f32 or u8), W chunk (hi, lo), A operand (hi, lo) }.
-constexpr uint32_t F_STG = 128 * 64 * 4;
-constexpr uint32_t F_STAGE = F_STG + 2 * OPER + 2 * OPER;
-constexpr uint32_t F_MISC = 2 * F_STAGE;
-constexpr uint32_t F_SMEM = F_MISC + 128 + 1024;
+// Shared memory: a ring of 4 staging slots (a 64-column chunk of 128 mask rows, as two 128-byte-swizzled
+// [128][32] float boxes, or one 64-byte-swizzled [128][64] uint8 box) and a ring of 2 W chunks (hi, lo).  The A
+// operand (the chunk as bf16 hi / lo) goes to tensor memory, two slots of 64 columns, and the MMA reads it there.
+constexpr int F_NS = 4;                              // staging slots
+constexpr uint32_t F_STG = 128 * 64 * 4;             // one staging slot (float)
+constexpr uint32_t F_W = 2 * OPER;                   // one W chunk (hi, lo)
+constexpr uint32_t F_WOFF = F_NS * F_STG;
+constexpr uint32_t F_MISC = F_WOFF + 2 * F_W;
+constexpr uint32_t F_SMEM = F_MISC + 256 + 1024;
+constexpr uint32_t F_COL_A = 2 * ACC_COLS;           // A slot s at columns 256 + 64 s: hi [0,32), lo [32,64)
+constexpr uint32_t F_TMEM_COLS = 512;
 
 struct FwdArgs {
-  const void* field;        // [rows][nx] float32 or uint8
   long long rows;           // batch * ny (a multiple of 128)
-  int ny, nx, bc, kind;
+  int ny, nx, bc;
   const unsigned char* w;   // constant image: per 64-column chunk, [hi | lo] x [128 rows][64]
   float2* t;                // [batch][bc][ny]
 };
 
+constexpr int F_NT = NT + 32;   // + a warp issuing the W loads
+
 template <int KIND>
-__global__ void __launch_bounds__(NT, 1) rows_fwd_tc_kernel(FwdArgs a, const __grid_constant__ CUtensorMap mask_map) {
+__global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const __grid_constant__ CUtensorMap mask_map) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* gbase = smem_raw + (base - raw);
   const uint32_t misc = base + F_MISC;
-  // barriers: full[2] (staging + W landed), conv[2] (A operand written), done[2] (MMAs of the stage finished),
-  // accf[2] (accumulator complete), acce[2] (accumulator drained)
-  const uint32_t full = misc, conv = misc + 16, done = misc + 32, accf = misc + 48, acce = misc + 64;
-  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + F_MISC + 96);
+  // barriers: sfull[4] (staging landed), sfree[4] (staging read), wfull[2] (W landed), conv[2] (A slot written),
+  // adone[2] (MMAs of the A / W slot finished), accf[2] (accumulator complete), acce[2] (accumulator drained)
+  const uint32_t sfull = misc, sfree = misc + 32, wfull = misc + 64, conv = misc + 80, adone = misc + 96,
+                 accf = misc + 112, acce = misc + 128;
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + F_MISC + 160);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int KC = a.nx / 64;
   const long long items = a.rows / 128;
   const long long G = gridDim.x;
   const long long i0 = (long long)blockIdx.x * items / G, i1 = ((long long)blockIdx.x + 1) * items / G;
   const long long nchunks = (i1 - i0) * KC;
-  const uint32_t stg_bytes = KIND == OI_FIELD_U8 ? 128 * 64 : F_STG;
+  constexpr bool U8 = KIND == OI_FIELD_U8;
 
-  if (warp == 0) tmem_alloc(misc + 96, TMEM_COLS);
+  if (warp == 0) tmem_alloc(misc + 160, F_TMEM_COLS);
   if (tid == 0) {
+    for (int s = 0; s < F_NS; ++s) {
+      mbar_init(sfull + 8 * s, 1);
+      mbar_init(sfree + 8 * s, 8);
+    }
     for (int s = 0; s < 2; ++s) {
-      mbar_init(full + 8 * s, 1);
+      mbar_init(wfull + 8 * s, 1);
       mbar_init(conv + 8 * s, 8);
-      mbar_init(done + 8 * s, 1);
+      mbar_init(adone + 8 * s, 1);
       mbar_init(accf + 8 * s, 1);
       mbar_init(acce + 8 * s, 8);
     }
@@ -118,55 +131,70 @@ __global__ void __launch_bounds__(NT, 1) rows_fwd_tc_kernel(FwdArgs a, const __g
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 8) {
-    // ---- producer: staging rows and the W chunk of chunk g into stage g & 1
-    for (long long g = 0; g < nchunks; ++g) {
-      const int s = (int)(g & 1);
-      if (g >= 2 && !warp_wait(done + 8 * s, (uint32_t)(((g - 2) >> 1) & 1))) {
-        if (lane == 0) fail_status();
-        break;
+    // ---- mask producer: chunk g into staging slot g % 4 as soon as the slot has been read
+    if (lane == 0) {
+      for (long long g = 0; g < nchunks; ++g) {
+        const int s4 = (int)(g & 3);
+        if (g >= F_NS && !wait_bar(sfree + 8 * s4, (uint32_t)(((g - F_NS) >> 2) & 1))) {
+          fail_status();
+          break;
+        }
+        const long long item = i0 + g / KC;
+        const int c = (int)(g % KC), y = (int)(item * 128);
+        const uint32_t st = base + s4 * F_STG;
+        expect_tx(sfull + 8 * s4, U8 ? 128 * 64 : F_STG);
+        tma_load_2d(st, &mask_map, 64 * c, y, sfull + 8 * s4);
+        if (!U8) tma_load_2d(st + F_STG / 2, &mask_map, 64 * c + 32, y, sfull + 8 * s4);
       }
-      const long long item = i0 + g / KC;
-      const int c = (int)(g % KC);
-      const uint32_t st = base + s * F_STAGE;
-      if (lane == 0) {
-        // the 128 x 64 mask box (one tensor-map load) and the W chunk (one bulk copy)
-        expect_tx(full + 8 * s, stg_bytes + 2 * OPER);
-        tma_load_2d(st, &mask_map, 64 * c, (int)(item * 128), full + 8 * s);
-        bulk_g2s(st + F_STG, a.w + (long long)c * 2 * OPER, 2 * OPER, full + 8 * s);
+    }
+  } else if (warp == 10) {
+    // ---- W producer: chunk g's W into slot g % 2 once the MMAs of chunk g-2 have finished
+    if (lane == 0) {
+      for (long long g = 0; g < nchunks; ++g) {
+        const int s2 = (int)(g & 1);
+        if (g >= 2 && !wait_bar(adone + 8 * s2, (uint32_t)(((g - 2) >> 1) & 1))) {
+          fail_status();
+          break;
+        }
+        const int c = (int)(g % KC);
+        expect_tx(wfull + 8 * s2, F_W);
+        bulk_g2s(base + F_WOFF + s2 * F_W, a.w + (long long)c * F_W, F_W, wfull + 8 * s2);
       }
     }
   } else if (warp == 9) {
-    // ---- MMA issue: D[buf] += A_s x W_s^T over the 64-column chunk (K steps of 16), split BF16x3
+    // ---- MMA issue: D[buf] += A(tmem slot) x W^T over the chunk (K steps of 16), split BF16x3
     if (lane == 0) {
       constexpr uint32_t ID = idesc(128, false);
       for (long long g = 0; g < nchunks; ++g) {
-        const int s = (int)(g & 1);
+        const int s2 = (int)(g & 1);
         const long long n = g / KC;
         const int c = (int)(g % KC), buf = (int)(n & 1);
-        bool ok = wait_bar(conv + 8 * s, (uint32_t)((g >> 1) & 1));
+        bool ok = wait_bar(conv + 8 * s2, (uint32_t)((g >> 1) & 1));
+        if (ok) ok = wait_bar(wfull + 8 * s2, (uint32_t)((g >> 1) & 1));
         if (ok && c == 0 && n >= 2) ok = wait_bar(acce + 8 * buf, (uint32_t)(((n - 2) >> 1) & 1));
         if (!ok) {
           fail_status();
           break;
         }
         fence_after();
-        const uint32_t st = base + s * F_STAGE, wch = st + F_STG, aop = wch + 2 * OPER;
+        const uint32_t wch = base + F_WOFF + s2 * F_W, at = tmem + F_COL_A + 64 * s2;
         const uint32_t d = tmem + buf * ACC_COLS;
 #pragma unroll
         for (int ks = 0; ks < 4; ++ks) {
           const uint32_t ko = 32 * ks;
-          mma_ss(d, sdesc(aop + ko), sdesc(wch + ko), ID, (c | ks) ? 1u : 0u);        // hi hi
-          mma_ss(d, sdesc(aop + ko), sdesc(wch + OPER + ko), ID, 1);                  // hi lo
-          if (KIND != OI_FIELD_U8) mma_ss(d, sdesc(aop + OPER + ko), sdesc(wch + ko), ID, 1);  // lo hi
+          mma_ts(d, at + 8 * ks, sdesc(wch + ko), ID, (c | ks) ? 1u : 0u);            // hi hi
+          mma_ts(d, at + 8 * ks, sdesc(wch + OPER + ko), ID, 1);                     // hi lo
+          if (!U8) mma_ts(d, at + 32 + 8 * ks, sdesc(wch + ko), ID, 1);              // lo hi
         }
-        commit(done + 8 * s);
+        commit(adone + 8 * s2);
         if (c == KC - 1) commit(accf + 8 * buf);
       }
     }
   } else {
-    // ---- converters (warps 0-7): staging -> A operand; drain finished accumulators
+    // ---- converters (warps 0-7): staging -> A slot in tensor memory; drain finished accumulators.
+    // Warp w converts rows 32 (w & 3) .. +31 (its tensor-memory lane quarter), columns 32 (w >> 2) .. +31.
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
-    const int half = warp >> 2;
+    const int half = warp >> 2, r = 32 * (warp & 3) + lane;
     bool ok = true;
     auto drain = [&](long long n) {
       // accumulator of item n: lanes = rows, columns re [0,64) / im [64,128) of band column ic
@@ -179,7 +207,7 @@ __global__ void __launch_bounds__(NT, 1) rows_fwd_tc_kernel(FwdArgs a, const __g
       fence_before();
       __syncwarp();
       if (lane == 0) arrive(acce + 8 * buf);
-      const long long row = (i0 + n) * 128 + 32 * (warp & 3) + lane;
+      const long long row = (i0 + n) * 128 + r;
       const long long b = row / a.ny;
       const int y = (int)(row - b * a.ny);
       float2* dst = a.t + (b * a.bc + 32 * half) * (long long)a.ny + y;
@@ -189,43 +217,40 @@ __global__ void __launch_bounds__(NT, 1) rows_fwd_tc_kernel(FwdArgs a, const __g
       return true;
     };
     for (long long g = 0; g < nchunks && ok; ++g) {
-      const int s = (int)(g & 1);
-      ok = warp_wait(full + 8 * s, (uint32_t)((g >> 1) & 1));
-      if (ok && g >= 2) ok = warp_wait(done + 8 * s, (uint32_t)(((g - 2) >> 1) & 1));
+      const int s4 = (int)(g & 3), s2 = (int)(g & 1);
+      ok = warp_wait(sfull + 8 * s4, (uint32_t)((g >> 2) & 1));
+      if (ok && g >= 2) ok = warp_wait(adone + 8 * s2, (uint32_t)(((g - 2) >> 1) & 1));   // A slot free
       if (!ok) break;
-      const uint32_t st = base + s * F_STAGE, aop = st + F_STG + 2 * OPER;
-      const unsigned char* gst = gbase + s * F_STAGE;
-      if (KIND == OI_FIELD_U8) {
+      float v[32];
+      if (U8) {
+        const unsigned char* row = gbase + s4 * F_STG + r * 64;   // 64-byte swizzle: chunk j at j ^ ((r >> 1) & 3)
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
-          const int id = tid + NCONV * p, r = id >> 3, q = id & 7;   // row r, columns 8q .. 8q+7 (exact in bf16)
-          const uint2 u = *(const uint2*)(gst + r * 64 + 8 * q);
-          float v[8];
+        for (int jj = 0; jj < 2; ++jj) {
+          const uint4 u = *(const uint4*)(row + (((2 * half + jj) ^ ((r >> 1) & 3)) << 4));
+          const uint32_t w4[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            v[e] = (float)((u.x >> (8 * e)) & 0xFF);
-            v[4 + e] = (float)((u.y >> (8 * e)) & 0xFF);
-          }
-          uint32_t hi[4], lo[4];
-          split8(v, hi, lo);
-          st_shared_v4(aop + swz(r, q), hi[0], hi[1], hi[2], hi[3]);
+          for (int e = 0; e < 16; ++e) v[16 * jj + e] = (float)((w4[e >> 2] >> (8 * (e & 3))) & 0xFF);
         }
       } else {
+        const unsigned char* row = gbase + s4 * F_STG + half * (F_STG / 2) + r * 128;   // 128-byte swizzle
 #pragma unroll
-        for (int p = 0; p < 8; ++p) {
-          const int id = tid + NCONV * p, r = id >> 4, k = id & 15;  // row r, columns 4k .. 4k+3
-          const float4 x = *(const float4*)(gst + r * 256 + 16 * k);
-          uint32_t h0, l0, h1, l1;
-          split2(x.x, x.y, h0, l0);
-          split2(x.z, x.w, h1, l1);
-          const uint32_t o = aop + swz(r, k >> 1) + 8 * (k & 1);
-          asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(o), "r"(h0), "r"(h1) : "memory");
-          asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(o + OPER), "r"(l0), "r"(l1) : "memory");
+        for (int j = 0; j < 8; ++j) {
+          const float4 x = *(const float4*)(row + ((j ^ (r & 7)) << 4));
+          v[4 * j] = x.x, v[4 * j + 1] = x.y, v[4 * j + 2] = x.z, v[4 * j + 3] = x.w;
         }
       }
-      fence_async_smem();
       __syncwarp();
-      if (lane == 0) arrive(conv + 8 * s);
+      if (lane == 0) arrive(sfree + 8 * s4);          // the staging slot may be refilled
+      uint32_t hi[16], lo[16];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) split2(v[2 * e], v[2 * e + 1], hi[e], lo[e]);
+      const uint32_t at = tmem + lane_base + F_COL_A + 64 * s2 + 16 * half;
+      tmem_st16(at, hi);
+      if (!U8) tmem_st16(at + 32, lo);
+      wait_st();
+      fence_before();
+      __syncwarp();
+      if (lane == 0) arrive(conv + 8 * s2);
       // the previous item's accumulator is complete once this item's first chunk is converted
       const long long n = g / KC;
       if (g % KC == 0 && n >= 1) ok = drain(n - 1);
@@ -237,29 +262,77 @@ __global__ void __launch_bounds__(NT, 1) rows_fwd_tc_kernel(FwdArgs a, const __g
   __syncthreads();
   if (warp == 0) {
     fence_after();
-    tmem_dealloc(tmem, TMEM_COLS);
+    tmem_dealloc(tmem, F_TMEM_COLS);
   }
 }
 
 // ------------------------------------------------------------------------------------------ inverse
-// Shared memory: C tile of the current x tile (hi, lo: [kc][128 rows][64]), V operand (hi, lo), staging of v
-// ([bc][128] float2).
+// v -> V operand tiles: for each block of 128 rows (image i, rows y0 .. y0+127) the bf16 hi / lo operand
+// [hi: kc 0 (re of band column qc < 64), kc 1 (im)][lo: kc 0, kc 1] x [128 rows y][64], in the swizzled shared-
+// memory layout, so that the row kernel loads it with one bulk copy.  One block per tile; v is read coalesced
+// (128 consecutive y of one band column) into shared memory and written as 16-byte chunks.
+constexpr uint32_t VT_BYTES = 4 * OPER;   // one V tile (64 KB)
+
+__global__ void __launch_bounds__(256) v_tiles_kernel(const float2* __restrict__ v, int ny, int bc,
+                                                       unsigned char* __restrict__ tiles) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* st = (float2*)smem_raw;   // [bc][128]
+  const int tid = threadIdx.x;
+  const long long r = blockIdx.x, row0 = r * 128, i = row0 / ny;
+  const int y0 = (int)(row0 - i * ny);
+  // bc rows of 128 complex = 64 float4 each; all loads of a thread issued before any store (16 in flight)
+  constexpr int PER = 16;   // 16 x 256 float4 >= 64 x 64
+  float4 buf[PER];
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int e = tid + 256 * p, qc = e >> 6, y2 = e & 63;
+    buf[p] = qc < bc ? __ldg((const float4*)(v + (i * bc + qc) * (long long)ny + y0) + y2) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int e = tid + 256 * p, qc = e >> 6;
+    if (qc < bc) ((float4*)st)[e] = buf[p];
+  }
+  __syncthreads();
+  unsigned char* out = tiles + r * VT_BYTES;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int id = tid + 256 * p, y = id & 127, q = id >> 7;   // row y, band columns 8q .. 8q+7
+    float re[8], im[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int qc = 8 * q + e;
+      const float2 x = qc < bc ? st[qc * 128 + y] : make_float2(0.f, 0.f);
+      re[e] = x.x;
+      im[e] = x.y;
+    }
+    uint32_t hi[4], lo[4];
+    const uint32_t o = swz(y, q);
+    split8(re, hi, lo);
+    *(uint4*)(out + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *(uint4*)(out + 2 * OPER + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    split8(im, hi, lo);
+    *(uint4*)(out + OPER + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *(uint4*)(out + 3 * OPER + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  }
+}
+
+// Shared memory: C tile of the current x tile (hi, lo: [kc][128 rows][64]) and two V tiles.
 constexpr uint32_t I_CX = 0;
-constexpr uint32_t I_VOP = 4 * OPER;
-constexpr uint32_t I_STG = 8 * OPER;
-constexpr uint32_t I_MISC = I_STG + 64 * 128 * 8;
+constexpr uint32_t I_V = 4 * OPER;
+constexpr uint32_t I_MISC = I_V + 2 * VT_BYTES;
 constexpr uint32_t I_SMEM = I_MISC + 128 + 1024;
 
 struct InvArgs {
-  const float2* v;          // [count][bc][ny]
+  const unsigned char* vt;  // V tiles (v_tiles_kernel), [rows / 128][64 KB]
   long long rows;           // count * ny (a multiple of 128)
-  int ny, nx, bc;
+  int ny, nx;
   const unsigned char* c;   // constant image: per 128-column x tile, [hi | lo] x [kc][128 rows][64]
   float* out;               // [count][ny][nx]
 };
 
 // Drain the accumulator of item `it` (tensor-memory buffer `buf`): lanes = x of this warp's quarter, columns =
-// rows y0 .. y0+127 of the block (this warp's half), stored as coalesced 128-byte rows segments.
+// rows y0 .. y0+127 of the block (this warp's half), stored as coalesced 128-byte row segments.
 __device__ __forceinline__ void inv_drain(const InvArgs& a, uint32_t taddr, uint32_t acce, int half, int warp,
                                           int lane, long long it, int buf, long long R) {
   fence_after();
@@ -280,15 +353,17 @@ __device__ __forceinline__ void inv_drain(const InvArgs& a, uint32_t taddr, uint
   if (lane == 0) arrive(acce + 8 * buf);
 }
 
-__global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a, const __grid_constant__ CUtensorMap v_map) {
+// Items (x tile j, row block r), j-major, cut into one contiguous range per CTA.  Producer: the C tile when the x
+// tile changes, V tiles into two slots; MMA: D[buf] = C x V^T (24 MMAs of 128 x 128 x 16); warps 0-7 drain.
+__global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* gbase = smem_raw + (base - raw);
   const uint32_t misc = base + I_MISC;
-  // barriers: full (staging landed), cx (C tile landed), conv (V written), done (MMAs finished),
-  // acce[2] (accumulator drained)
-  const uint32_t full = misc, cxb = misc + 8, conv = misc + 16, done = misc + 24, acce = misc + 32;
+  // barriers: vfull[2] (V tile landed), vdone[2] (MMAs reading the slot finished = accumulator complete),
+  // cxb (C tile landed), acce[2] (accumulator drained)
+  const uint32_t vfull = misc, vdone = misc + 16, cxb = misc + 32, acce = misc + 40;
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + I_MISC + 96);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long long R = a.rows / 128;                // row blocks
@@ -299,12 +374,12 @@ __global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a, const __g
 
   if (warp == 0) tmem_alloc(misc + 96, TMEM_COLS);
   if (tid == 0) {
-    mbar_init(full, 1);
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(vfull + 8 * s, 1);
+      mbar_init(vdone + 8 * s, 1);
+      mbar_init(acce + 8 * s, 8);
+    }
     mbar_init(cxb, 1);
-    mbar_init(conv, 8);
-    mbar_init(done, 1);
-    mbar_init(acce, 8);
-    mbar_init(acce + 8, 8);
     mbar_init_fence();
   }
   fence_before();
@@ -313,43 +388,36 @@ __global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a, const __g
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 8) {
-    // ---- producer: the C tile when the x tile changes, then the staging of v for item n
-    int reloads = 0;
-    for (long long n = 0; n < N; ++n) {
-      const long long it = i0 + n, j = it / R, r = it % R;
-      bool ok = true;
-      if (n >= 1) ok = warp_wait(conv, (uint32_t)((n - 1) & 1));            // staging consumed
-      const bool reload = n == 0 || (it - 1) / R != j;
-      if (ok && reload && n >= 1) ok = warp_wait(done, (uint32_t)((n - 1) & 1));   // old C tile no longer read
-      if (!ok) {
-        if (lane == 0) fail_status();
-        break;
-      }
-      if (reload) {
-        if (lane == 0) {
+    if (lane == 0) {
+      for (long long n = 0; n < N; ++n) {
+        const long long it = i0 + n, j = it / R, r = it % R;
+        const int s = (int)(n & 1);
+        const bool reload = n == 0 || (it - 1) / R != j;
+        bool ok = true;
+        if (n >= 2) ok = wait_bar(vdone + 8 * s, (uint32_t)(((n - 2) >> 1) & 1));           // slot free
+        if (ok && reload && n >= 1) ok = wait_bar(vdone + 8 * ((n - 1) & 1), (uint32_t)(((n - 1) >> 1) & 1));
+        if (!ok) {
+          fail_status();
+          break;
+        }
+        if (reload) {   // the previous C tile is no longer read
           expect_tx(cxb, 4 * OPER);
           for (int q = 0; q < 4; ++q) bulk_g2s(base + I_CX + q * OPER, a.c + j * 4 * OPER + q * OPER, OPER, cxb);
         }
-        ++reloads;
-      }
-      // v of image i, band columns 0 .. bc-1, rows y0 .. y0+127: one [bc][256 float] tensor-map box
-      const long long row0 = r * 128, i = row0 / a.ny;
-      const int y0 = (int)(row0 - i * a.ny);
-      if (lane == 0) {
-        expect_tx(full, (uint32_t)a.bc * 1024);
-        tma_load_2d(base + I_STG, &v_map, 2 * y0, (int)(i * a.bc), full);
+        expect_tx(vfull + 8 * s, VT_BYTES);
+        for (int q = 0; q < 4; ++q)
+          bulk_g2s(base + I_V + s * VT_BYTES + q * OPER, a.vt + r * VT_BYTES + q * OPER, OPER, vfull + 8 * s);
       }
     }
-    (void)reloads;
   } else if (warp == 9) {
     if (lane == 0) {
       constexpr uint32_t ID = idesc(128, false);
       int reloads = 0;
       for (long long n = 0; n < N; ++n) {
         const long long it = i0 + n, j = it / R;
-        const int buf = (int)(n & 1);
+        const int s = (int)(n & 1), buf = s;
         const bool reload = n == 0 || (it - 1) / R != j;
-        bool ok = wait_bar(conv, (uint32_t)(n & 1));
+        bool ok = wait_bar(vfull + 8 * s, (uint32_t)((n >> 1) & 1));
         if (ok && reload) ok = wait_bar(cxb, (uint32_t)(reloads & 1));
         if (ok && n >= 2) ok = wait_bar(acce + 8 * buf, (uint32_t)(((n - 2) >> 1) & 1));
         if (!ok) {
@@ -358,57 +426,28 @@ __global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a, const __g
         }
         if (reload) ++reloads;
         fence_after();
-        const uint32_t d = tmem + buf * ACC_COLS;
+        const uint32_t d = tmem + buf * ACC_COLS, vb = base + I_V + s * VT_BYTES;
 #pragma unroll
         for (int ks = 0; ks < 8; ++ks) {
           const uint32_t ko = (uint32_t)(ks >> 2) * OPER + 32 * (ks & 3);
           const uint32_t ah = base + I_CX + ko, al = ah + 2 * OPER;
-          const uint32_t bh = base + I_VOP + ko, bl = bh + 2 * OPER;
+          const uint32_t bh = vb + ko, bl = bh + 2 * OPER;
           mma_ss(d, sdesc(ah), sdesc(bh), ID, ks ? 1u : 0u);   // hi hi
           mma_ss(d, sdesc(ah), sdesc(bl), ID, 1);              // hi lo
           mma_ss(d, sdesc(al), sdesc(bh), ID, 1);              // lo hi
         }
-        commit(done);
+        commit(vdone + 8 * s);
       }
     }
   } else {
-    // ---- converters: staging [qc][y] float2 -> V operand rows y, K = (re | im) x qc; drain accumulators
+    // ---- warps 0-7: drain each finished accumulator
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
     const int half = warp >> 2;
-    const float2* stg = (const float2*)(gbase + I_STG);
     bool ok = true;
     for (long long n = 0; n < N && ok; ++n) {
-      ok = warp_wait(full, (uint32_t)(n & 1));
-      if (ok && n >= 1) ok = warp_wait(done, (uint32_t)((n - 1) & 1));    // V free, accumulator n-1 complete
-      if (!ok) break;
-#pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        const int id = tid + NCONV * p, y = id & 127, q = id >> 7;    // row y, band columns 8q .. 8q+7
-        float re[8], im[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int qc = 8 * q + e;
-          const float2 x = qc < a.bc ? stg[qc * 128 + y] : make_float2(0.f, 0.f);
-          re[e] = x.x;
-          im[e] = x.y;
-        }
-        uint32_t hi[4], lo[4];
-        split8(re, hi, lo);
-        const uint32_t o = base + I_VOP + swz(y, q);
-        st_shared_v4(o, hi[0], hi[1], hi[2], hi[3]);
-        st_shared_v4(o + 2 * OPER, lo[0], lo[1], lo[2], lo[3]);
-        split8(im, hi, lo);
-        st_shared_v4(o + OPER, hi[0], hi[1], hi[2], hi[3]);
-        st_shared_v4(o + 3 * OPER, lo[0], lo[1], lo[2], lo[3]);
-      }
-      fence_async_smem();
-      __syncwarp();
-      if (lane == 0) arrive(conv);
-      if (n >= 1) inv_drain(a, tmem + lane_base, acce, half, warp, lane, i0 + n - 1, (int)((n - 1) & 1), R);
-    }
-    if (ok && N > 0) {
-      ok = warp_wait(done, (uint32_t)((N - 1) & 1));
-      if (ok) inv_drain(a, tmem + lane_base, acce, half, warp, lane, i0 + N - 1, (int)((N - 1) & 1), R);
+      const int buf = (int)(n & 1);
+      ok = warp_wait(vdone + 8 * buf, (uint32_t)((n >> 1) & 1));
+      if (ok) inv_drain(a, tmem + lane_base, acce, half, warp, lane, i0 + n, buf, R);
     }
     if (!ok && lane == 0) fail_status();
   }
@@ -481,7 +520,8 @@ typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, v
 
 // A 2-D tensor map (dim0 contiguous, rows `stride1` bytes apart) with a box0 x box1 box, no swizzle.
 static int encode_2d(CUtensorMap* map, CUtensorMapDataType type, const void* base, unsigned long long dim0,
-                     unsigned long long dim1, unsigned long long stride1, unsigned box0, unsigned box1) {
+                     unsigned long long dim1, unsigned long long stride1, unsigned box0, unsigned box1,
+                     CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE) {
   static EncodeTiled encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
@@ -493,8 +533,7 @@ static int encode_2d(CUtensorMap* map, CUtensorMapDataType type, const void* bas
   const cuuint64_t dims[2] = {dim0, dim1}, strides[1] = {stride1};
   const cuuint32_t box[2] = {box0, box1}, estr[2] = {1, 1};
   const CUresult r = encode(map, type, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                            swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(OI_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return OI_OK;
 }
@@ -541,48 +580,51 @@ extern "C" int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, in
   const int sms = rt::sm_count();
   if (!sms) return fail(OI_ECUDA, "oi_rows_fwd_tc: no CUDA device");
   const long long ctas = items < sms ? items : sms;
-  rt::FwdArgs a{field, rows, ny, nx, bc, kind, (const unsigned char*)consts, (float2*)t};
+  rt::FwdArgs a{rows, ny, nx, bc, (const unsigned char*)consts, (float2*)t};
   cudaStream_t s = (cudaStream_t)stream;
   const bool u8 = kind == OI_FIELD_U8;
-  CUtensorMap map;
+  CUtensorMap map;   // mask boxes: [128 rows][32 float] with the 128-byte swizzle, or [128][64 uint8], 64-byte
   int rc = rt::encode_2d(&map, u8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, field,
-                         (unsigned long long)nx, (unsigned long long)rows, (unsigned long long)nx * (u8 ? 1 : 4), 64,
-                         128);
+                         (unsigned long long)nx, (unsigned long long)rows, (unsigned long long)nx * (u8 ? 1 : 4),
+                         u8 ? 64 : 32, 128, u8 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B);
   if (rc) return rc;
   if (u8) {
     rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_U8>, rt::F_SMEM, "oi_rows_fwd_tc");
     if (rc) return rc;
-    rt::rows_fwd_tc_kernel<OI_FIELD_U8><<<(unsigned)ctas, rt::NT, rt::F_SMEM, s>>>(a, map);
+    rt::rows_fwd_tc_kernel<OI_FIELD_U8><<<(unsigned)ctas, rt::F_NT, rt::F_SMEM, s>>>(a, map);
     oi::note_launch();
   } else {
     rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32>, rt::F_SMEM, "oi_rows_fwd_tc");
     if (rc) return rc;
-    rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32><<<(unsigned)ctas, rt::NT, rt::F_SMEM, s>>>(a, map);
+    rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32><<<(unsigned)ctas, rt::F_NT, rt::F_SMEM, s>>>(a, map);
     oi::note_launch();
   }
   return check_launch("oi_rows_fwd_tc");
 }
 
-extern "C" int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, const void* consts, float* out,
-                              void* stream) {
+extern "C" int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, const void* consts, void* vtiles,
+                              float* out, void* stream) {
   using namespace oi;
-  if (!v || !consts || !out || count <= 0 || bc <= 0) return fail(OI_EINVAL, "oi_rows_inv_tc: bad arguments");
+  if (!v || !consts || !vtiles || !out || count <= 0 || bc <= 0) return fail(OI_EINVAL, "oi_rows_inv_tc: bad arguments");
   if (ny % 128 != 0 || nx % 128 != 0 || nx > 4096 || bc > 64)
     return fail(OI_ERANGE, "oi_rows_inv_tc: grid %dx%d / band width %d unsupported", ny, nx, bc);
-  if ((uintptr_t)v % 16 || (uintptr_t)consts % 16)
-    return fail(OI_EINVAL, "oi_rows_inv_tc: v and constants must be 16-byte aligned");
-  const long long rows = (long long)count * ny, items = (long long)(nx / 128) * (rows / 128);
+  if ((uintptr_t)consts % 16 || (uintptr_t)vtiles % 16)
+    return fail(OI_EINVAL, "oi_rows_inv_tc: constants and V tiles must be 16-byte aligned");
+  const long long rows = (long long)count * ny, R = rows / 128, items = (long long)(nx / 128) * R;
   const int sms = rt::sm_count();
   if (!sms) return fail(OI_ECUDA, "oi_rows_inv_tc: no CUDA device");
-  const long long ctas = items < sms ? items : sms;
-  rt::InvArgs a{(const float2*)v, rows, ny, nx, bc, (const unsigned char*)consts, out};
-  CUtensorMap map;   // v as float [count * bc][2 ny]: boxes of bc band columns x 128 complex rows
-  int rc = rt::encode_2d(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, v, 2ULL * ny, (unsigned long long)count * bc,
-                         8ULL * ny, 256, (unsigned)bc);
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = ensure_smem((const void*)rt::v_tiles_kernel, (size_t)bc * 128 * 8, "oi_rows_inv_tc/tiles");
   if (rc) return rc;
+  rt::v_tiles_kernel<<<(unsigned)R, 256, (size_t)bc * 128 * 8, s>>>((const float2*)v, ny, bc, (unsigned char*)vtiles);
+  oi::note_launch();
+  rc = check_launch("oi_rows_inv_tc/tiles");
+  if (rc) return rc;
+  const long long ctas = items < sms ? items : sms;
+  rt::InvArgs a{(const unsigned char*)vtiles, rows, ny, nx, (const unsigned char*)consts, out};
   rc = ensure_smem((const void*)rt::rows_inv_tc_kernel, rt::I_SMEM, "oi_rows_inv_tc");
   if (rc) return rc;
-  rt::rows_inv_tc_kernel<<<(unsigned)ctas, rt::NT, rt::I_SMEM, (cudaStream_t)stream>>>(a, map);
+  rt::rows_inv_tc_kernel<<<(unsigned)ctas, rt::NT, rt::I_SMEM, s>>>(a);
   oi::note_launch();
   return check_launch("oi_rows_inv_tc");
 }
