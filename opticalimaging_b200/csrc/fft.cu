@@ -342,7 +342,8 @@ __global__ void __launch_bounds__(256, 3) fft_rows_inv_kernel(const float2* __re
 // for qr = jr - (br-1) in [-(br-1), br-1] and qc in [0, bc).  Row FFTs of the real image in pairs (two rows per
 // complex transform), the band bins of each separated into U[sr][qc]; then column FFTs of U at the qr bins.
 template <int N1R, int N1C>
-__global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __restrict__ coarse, int br, int bc,
+__global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __restrict__ coarse, int nparts,
+                                                              long long part_stride, int br, int bc,
                                                               const float2* __restrict__ wr_g,
                                                               const float2* __restrict__ wc_g, int area_f2,
                                                               float2* __restrict__ ihat) {
@@ -360,7 +361,17 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
   build_tables<N1C>(wc_g, c2, c1, tid, T);
   float* cimg = (float*)area;
   const float4* src = (const float4*)(coarse + img * (long long)MR * MC);
-  for (int j = tid; j < MR * MC / 4; j += T) ((float4*)cimg)[j] = __ldg(src + j);
+  for (int j = tid; j < MR * MC / 4; j += T) {   // the partial sums, added in order
+    float4 v = __ldg(src + j);
+    for (int p = 1; p < nparts; ++p) {
+      const float4 u = __ldg(src + p * (part_stride / 4) + j);
+      v.x += u.x;
+      v.y += u.y;
+      v.z += u.z;
+      v.w += u.w;
+    }
+    ((float4*)cimg)[j] = v;
+  }
   __syncthreads();
   // row pass: pair p = rows (2p, 2p+1), thread n1
   const int p = tid / N1C, n1 = tid % N1C;
@@ -406,8 +417,8 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
 }
 
 template <int N1R, int N1C>
-static int launch_coarse_spec_fft(float* coarse, int count, int br, int bc, const float2* wr, const float2* wc,
-                                  float2* ihat, cudaStream_t s) {
+static int launch_coarse_spec_fft(float* coarse, int nparts, int count, int br, int bc, const float2* wr,
+                                  const float2* wc, float2* ihat, cudaStream_t s) {
   constexpr int MR = 32 * N1R, MC = 32 * N1C;
   const int rows_ys = (MR / 2) * 32 * (N1C + 1), c_f2 = MR * MC / 2, cols_ys = bc * 32 * (N1R + 1);
   const int area_f2 = max(rows_ys, max(c_f2, cols_ys));
@@ -415,7 +426,7 @@ static int launch_coarse_spec_fft(float* coarse, int count, int br, int bc, cons
   auto kern = coarse_spec_fft_kernel<N1R, N1C>;
   int rc = set_smem(kern, smem, "coarse spectrum fft");
   if (rc) return rc;
-  kern<<<count, 512, smem, s>>>(coarse, br, bc, wr, wc, area_f2, ihat);
+  kern<<<count, 512, smem, s>>>(coarse, nparts, (long long)count * MR * MC, br, bc, wr, wc, area_f2, ihat);
   oi::note_launch();
   return check_launch("coarse spectrum fft");
 }
@@ -549,14 +560,12 @@ extern "C" int oi_coarse_to_image_fft(float* coarse, int nparts, int count, int 
   cudaStream_t s = (cudaStream_t)stream;
   int rc;
   if (wm_r && wm_c && (mr == 64 || mr == 128) && (mc == 64 || mc == 128) && bc <= 64) {
-    rc = fold_parts(coarse, nparts, (long long)count * mr * mc, s);
-    if (rc) return rc;
     float2* ih = (float2*)scratch_ihat;
     const float2 *tr = (const float2*)wm_r, *tc = (const float2*)wm_c;
-    if (mr == 128 && mc == 128) rc = launch_coarse_spec_fft<4, 4>(coarse, count, br, bc, tr, tc, ih, s);
-    else if (mr == 64 && mc == 64) rc = launch_coarse_spec_fft<2, 2>(coarse, count, br, bc, tr, tc, ih, s);
-    else if (mr == 128) rc = launch_coarse_spec_fft<4, 2>(coarse, count, br, bc, tr, tc, ih, s);
-    else rc = launch_coarse_spec_fft<2, 4>(coarse, count, br, bc, tr, tc, ih, s);
+    if (mr == 128 && mc == 128) rc = launch_coarse_spec_fft<4, 4>(coarse, nparts, count, br, bc, tr, tc, ih, s);
+    else if (mr == 64 && mc == 64) rc = launch_coarse_spec_fft<2, 2>(coarse, nparts, count, br, bc, tr, tc, ih, s);
+    else if (mr == 128) rc = launch_coarse_spec_fft<4, 2>(coarse, nparts, count, br, bc, tr, tc, ih, s);
+    else rc = launch_coarse_spec_fft<2, 4>(coarse, nparts, count, br, bc, tr, tc, ih, s);
   } else {
     rc = coarse_spectrum(coarse, count, mr, mc, br, bc, gc, gr, scratch_ihat, s, nparts);
   }
@@ -646,10 +655,8 @@ extern "C" int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int b
   if (!ny1 || nx % 128 != 0 || nx > 4096 || bc > 64 || 2 * br - 1 > 128 || 2 * br - 1 > ny)
     return fail(OI_ERANGE, "oi_coarse_to_image_tc: grid %dx%d / band %dx%d unsupported", ny, nx, br, bc);
   cudaStream_t s = (cudaStream_t)stream;
-  int rc = fold_parts(coarse, nparts, (long long)count * 128 * 128, s);
-  if (rc) return rc;
   float2* ih = (float2*)scratch_ihat;
-  rc = launch_coarse_spec_fft<4, 4>(coarse, count, br, bc, (const float2*)wm_r, (const float2*)wm_c, ih, s);
+  int rc = launch_coarse_spec_fft<4, 4>(coarse, nparts, count, br, bc, (const float2*)wm_r, (const float2*)wm_c, ih, s);
   if (rc) return rc;
   float2* v = (float2*)scratch_v;
   switch (ny1) {

@@ -69,14 +69,15 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
 }
 
 // ------------------------------------------------------------------------------------------ forward
-// Shared memory: a ring of 4 staging slots (a 64-column chunk of 128 mask rows, as two 128-byte-swizzled
-// [128][32] float boxes, or one 64-byte-swizzled [128][64] uint8 box) and a ring of 2 W chunks (hi, lo).  The A
+// Shared memory: a ring of 3 staging slots (a 64-column chunk of 128 mask rows, as two 128-byte-swizzled
+// [128][32] float boxes, or one 64-byte-swizzled [128][64] uint8 box) and a ring of 3 W chunks (hi, lo).  The A
 // operand (the chunk as bf16 hi / lo) goes to tensor memory, two slots of 64 columns, and the MMA reads it there.
-constexpr int F_NS = 4;                              // staging slots
+constexpr int F_NS = 3;                              // staging slots
+constexpr int F_NWS = 3;                             // W slots
 constexpr uint32_t F_STG = 128 * 64 * 4;             // one staging slot (float)
 constexpr uint32_t F_W = 2 * OPER;                   // one W chunk (hi, lo)
 constexpr uint32_t F_WOFF = F_NS * F_STG;
-constexpr uint32_t F_MISC = F_WOFF + 2 * F_W;
+constexpr uint32_t F_MISC = F_WOFF + F_NWS * F_W;
 constexpr uint32_t F_SMEM = F_MISC + 256 + 1024;
 constexpr uint32_t F_COL_A = 2 * ACC_COLS;           // A slot s at columns 256 + 64 s: hi [0,32), lo [32,64)
 constexpr uint32_t F_TMEM_COLS = 512;
@@ -97,11 +98,12 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* gbase = smem_raw + (base - raw);
   const uint32_t misc = base + F_MISC;
-  // barriers: sfull[4] (staging landed), sfree[4] (staging read), wfull[2] (W landed), conv[2] (A slot written),
-  // adone[2] (MMAs of the A / W slot finished), accf[2] (accumulator complete), acce[2] (accumulator drained)
-  const uint32_t sfull = misc, sfree = misc + 32, wfull = misc + 64, conv = misc + 80, adone = misc + 96,
-                 accf = misc + 112, acce = misc + 128;
-  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + F_MISC + 160);
+  // barriers: sfull[3] (staging landed), sfree[3] (staging read), wfull[3] (W landed), wdone[3] (MMAs reading
+  // the W slot finished), conv[2] (A slot written), adone[2] (MMAs reading the A slot finished), accf[2]
+  // (accumulator complete), acce[2] (accumulator drained)
+  const uint32_t sfull = misc, sfree = misc + 24, wfull = misc + 48, wdone = misc + 72, conv = misc + 96,
+                 adone = misc + 112, accf = misc + 128, acce = misc + 144;
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + F_MISC + 192);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int KC = a.nx / 64;
   const long long items = a.rows / 128;
@@ -110,14 +112,15 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   const long long nchunks = (i1 - i0) * KC;
   constexpr bool U8 = KIND == OI_FIELD_U8;
 
-  if (warp == 0) tmem_alloc(misc + 160, F_TMEM_COLS);
+  if (warp == 0) tmem_alloc(misc + 192, F_TMEM_COLS);
   if (tid == 0) {
-    for (int s = 0; s < F_NS; ++s) {
+    for (int s = 0; s < 3; ++s) {
       mbar_init(sfull + 8 * s, 1);
       mbar_init(sfree + 8 * s, 8);
+      mbar_init(wfull + 8 * s, 1);
+      mbar_init(wdone + 8 * s, 1);
     }
     for (int s = 0; s < 2; ++s) {
-      mbar_init(wfull + 8 * s, 1);
       mbar_init(conv + 8 * s, 8);
       mbar_init(adone + 8 * s, 1);
       mbar_init(accf + 8 * s, 1);
@@ -131,11 +134,11 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 8) {
-    // ---- mask producer: chunk g into staging slot g % 4 as soon as the slot has been read
+    // ---- mask producer: chunk g into staging slot g % 3 as soon as the slot has been read
     if (lane == 0) {
       for (long long g = 0; g < nchunks; ++g) {
-        const int s4 = (int)(g & 3);
-        if (g >= F_NS && !wait_bar(sfree + 8 * s4, (uint32_t)(((g - F_NS) >> 2) & 1))) {
+        const int s4 = (int)(g % F_NS);
+        if (g >= F_NS && !wait_bar(sfree + 8 * s4, (uint32_t)(((g - F_NS) / F_NS) & 1))) {
           fail_status();
           break;
         }
@@ -148,17 +151,17 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
       }
     }
   } else if (warp == 10) {
-    // ---- W producer: chunk g's W into slot g % 2 once the MMAs of chunk g-2 have finished
+    // ---- W producer: chunk g's W into slot g % 3 once the MMAs of chunk g-3 have finished
     if (lane == 0) {
       for (long long g = 0; g < nchunks; ++g) {
-        const int s2 = (int)(g & 1);
-        if (g >= 2 && !wait_bar(adone + 8 * s2, (uint32_t)(((g - 2) >> 1) & 1))) {
+        const int s3 = (int)(g % F_NWS);
+        if (g >= F_NWS && !wait_bar(wdone + 8 * s3, (uint32_t)(((g - F_NWS) / F_NWS) & 1))) {
           fail_status();
           break;
         }
         const int c = (int)(g % KC);
-        expect_tx(wfull + 8 * s2, F_W);
-        bulk_g2s(base + F_WOFF + s2 * F_W, a.w + (long long)c * F_W, F_W, wfull + 8 * s2);
+        expect_tx(wfull + 8 * s3, F_W);
+        bulk_g2s(base + F_WOFF + s3 * F_W, a.w + (long long)c * F_W, F_W, wfull + 8 * s3);
       }
     }
   } else if (warp == 9) {
@@ -169,15 +172,16 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
         const int s2 = (int)(g & 1);
         const long long n = g / KC;
         const int c = (int)(g % KC), buf = (int)(n & 1);
+        const int s3 = (int)(g % F_NWS);
         bool ok = wait_bar(conv + 8 * s2, (uint32_t)((g >> 1) & 1));
-        if (ok) ok = wait_bar(wfull + 8 * s2, (uint32_t)((g >> 1) & 1));
+        if (ok) ok = wait_bar(wfull + 8 * s3, (uint32_t)((g / F_NWS) & 1));
         if (ok && c == 0 && n >= 2) ok = wait_bar(acce + 8 * buf, (uint32_t)(((n - 2) >> 1) & 1));
         if (!ok) {
           fail_status();
           break;
         }
         fence_after();
-        const uint32_t wch = base + F_WOFF + s2 * F_W, at = tmem + F_COL_A + 64 * s2;
+        const uint32_t wch = base + F_WOFF + s3 * F_W, at = tmem + F_COL_A + 64 * s2;
         const uint32_t d = tmem + buf * ACC_COLS;
 #pragma unroll
         for (int ks = 0; ks < 4; ++ks) {
@@ -187,6 +191,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
           if (!U8) mma_ts(d, at + 32 + 8 * ks, sdesc(wch + ko), ID, 1);              // lo hi
         }
         commit(adone + 8 * s2);
+        commit(wdone + 8 * s3);
         if (c == KC - 1) commit(accf + 8 * buf);
       }
     }
@@ -217,8 +222,8 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
       return true;
     };
     for (long long g = 0; g < nchunks && ok; ++g) {
-      const int s4 = (int)(g & 3), s2 = (int)(g & 1);
-      ok = warp_wait(sfull + 8 * s4, (uint32_t)((g >> 2) & 1));
+      const int s4 = (int)(g % F_NS), s2 = (int)(g & 1);
+      ok = warp_wait(sfull + 8 * s4, (uint32_t)((g / F_NS) & 1));
       if (ok && g >= 2) ok = warp_wait(adone + 8 * s2, (uint32_t)(((g - 2) >> 1) & 1));   // A slot free
       if (!ok) break;
       float v[32];
