@@ -383,6 +383,69 @@ def cpu_reference_sample(sk_info, masks_np, budget_s, threads):
     return 1.0 / med, n
 
 
+# DRAM bytes per launch (read + write) of the three largest kernels at this workload, from the ncu capture
+# summarised in profiles/socs24-1024-bf16x3-step.md
+NCU_TRAFFIC = {"rows_fwd_tc": 286.2e6, "v_tiles+rows_inv_tc": 300.3e6, "coherent_tc": 2.6e6}
+
+
+def kernel_rooflines(sk, masks, reps=10):
+    """Device time of the three largest kernels of the split form, each launched alone through its ABI entry
+    (CUDA events on the launching stream, after warm-up), against the measured peaks."""
+    from opticalimaging_b200 import _native as N
+    from opticalimaging_b200.engine import Plan, TC_COARSE, band_spectrum
+    hbm, bf16, src = peaks()
+    dev = masks.device
+    b, B = sk.band, masks.shape[0]
+    plan = sk.plan
+    tplan = Plan.get(sk.ny, sk.nx, b, dev, coarse=TC_COARSE)
+    s = N.stream_handle(dev)
+    t = torch.empty(B * sk.ny * b.bc, dtype=torch.complex64, device=dev)
+    band = band_spectrum(masks, N.FIELD_REAL_F32, plan, form='bf16x3')
+    ctas, nparts = N.tc_layout(B, sk.count)
+    coarse = torch.empty((nparts, B, 1, 128, 128), device=dev)
+    v = torch.zeros(B * b.bc * sk.ny, dtype=torch.complex64, device=dev)
+    tiles = torch.empty(B * sk.ny * 512, dtype=torch.uint8, device=dev)
+    out = torch.empty((B, sk.ny, sk.nx), device=dev)
+    calls = {
+        "rows_fwd_tc": lambda: N.call('oi_rows_fwd_tc', N.ptr(masks), N.FIELD_REAL_F32, B, sk.ny, sk.nx, b.m0c, b.bc,
+                                      N.ptr(plan.rows_consts(0)), N.ptr(t), s),
+        "coherent_tc": lambda: N.call('oi_coherent_coarse_tc', N.ptr(band), B, 1, b.m0r, b.br, b.m0c, b.bc,
+                                      N.ptr(sk.pupils), 0, N.ptr(sk.weights), 1, sk.count,
+                                      N.ptr(tplan.tc_constants()), ctas, nparts, N.ptr(coarse), s),
+        "v_tiles+rows_inv_tc": lambda: N.call('oi_rows_inv_tc', N.ptr(v), B, sk.ny, sk.nx, b.bc, N.ptr(tplan.rows_consts(1)),
+                                      N.ptr(tiles), N.ptr(out), s),
+    }
+    px = B * sk.ny * sk.nx
+    res = {}
+    for name, fn in calls.items():
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3 / reps
+        if name == "coherent_tc":
+            flops = 8.0 * B * sk.count * (128 * b.br * b.bc + 128 * 128 * b.br)
+            ach = flops / sec / 1e12
+            res[name] = {"bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16,
+                         "traffic": NCU_TRAFFIC[name], "us": sec * 1e6, "peak_source": src,
+                         "algorithmic": "8 (M B^2 + M^2 B) flops per field, M = 128, B = 59, 24 fields per image",
+                         "executed_tflops": 3 * 8.0 * B * sk.count * (128 * 64 * 64 + 128 * 128 * 64) / sec / 1e12}
+        else:
+            ach = 4.0 * px / sec / 1e9
+            res[name] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                         "traffic": NCU_TRAFFIC[name], "us": sec * 1e6, "peak_source": src,
+                         "algorithmic": "4 bytes per pixel: the float32 mask read" if name == "rows_fwd_tc"
+                         else "4 bytes per pixel: the float32 image written (the call converts v to operand tiles "
+                         "first: two kernels)"}
+    res["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch (profiles/)"
+    return res
+
+
 def fp64_image(sk_info, mask):
     """FP64 oracle SOCS image of one clip with the engine's K kernels (the precision reference)."""
     from oracle import optics64 as O
@@ -518,27 +581,18 @@ def run_engine(args, world, rank, local):
     # ---- per-stage device times (outside the timed region) and the roofline of the dominant stage
     st = stage_times(sk, masks, out, args.form)
     hbm, bf16, src = peaks()
-    dominant = max(st, key=st.get)
-    px = BATCH * N_PIX * N_PIX
-    alg_bytes = {'band_spectrum': 4 * px, 'coarse_to_image': 4 * px}
-    if dominant in alg_bytes:
-        ach = alg_bytes[dominant] / (st[dominant] / 1e3) / 1e9
+    if args.form == 'bf16x3':
+        kern = kernel_rooflines(sk, masks)
+        dominant = max((k for k in kern if k != "traffic_source"), key=lambda k: kern[k]["us"])
+        roof = dict(kern[dominant], kernel=dominant)
+    else:
+        kern = None
+        dominant = max(st, key=st.get)
+        px = BATCH * N_PIX * N_PIX
+        ach = 4 * px / (st[dominant] / 1e3) / 1e9
         roof = {"kernel": dominant, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
                 "frac": ach / hbm, "traffic": None, "peak_source": src,
-                "algorithmic": "4 bytes per pixel (float32 mask read / image written)"}
-    else:
-        b = sk.band
-        m = 128 if args.form == 'bf16x3' else sk.plan.mr
-        fields = BATCH * sk.count
-        flops = 8.0 * fields * (m * b.br * b.bc + m * m * b.br)
-        ach = flops / (st[dominant] / 1e3) / 1e12
-        roof = {"kernel": dominant, "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
-                "frac": ach / bf16, "traffic": None, "peak_source": src,
-                "algorithmic": f"8 (M br bc + M M br) flops per field, M={m} coarse grid, {fields} fields"}
-        if args.form == 'bf16x3':
-            exe = 3 * 8.0 * fields * (m * 64 * 64 + m * m * 64) / (st[dominant] / 1e3) / 1e12
-            roof["executed_tflops"] = exe
-            roof["executed_frac"] = exe / bf16
+                "algorithmic": "4 bytes per pixel (float32 mask read / image written), per stage"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16x3" if args.form == 'bf16x3' else "fp32", "data": "synthetic",
@@ -550,7 +604,8 @@ def run_engine(args, world, rank, local):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_in.numel()),
                     "d2h_bytes_per_step": int(host_out.numel() * 4)},
             "gpu_launches": launches, "setup_s": setup_s, "serving": serving, "serving_mix": mix,
-            "stage_ms": {k: round(v, 4) for k, v in st.items()}, "roofline": roof, "clocks": clk.summary()}
+            "stage_ms": {k: round(v, 4) for k, v in st.items()}, "roofline": roof, "roofline_kernels": kern,
+            "clocks": clk.summary()}
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
         torch.set_num_threads(threads)
