@@ -208,7 +208,8 @@ OI_API int oi_tc_constants(int m0r, int m0c, const void* wr, const void* wc, voi
  * nx/64 * 32768 bytes) or 1 (inverse; depends on nx, bc; nx/128 * 65536 bytes).  A wait that exceeds 2 s ends
  * the kernel early and sets the device status.
  * oi_band_spectrum_tc and oi_coarse_to_image_tc are oi_band_spectrum_fft and oi_coarse_to_image_fft (coarse grid
- * 128 x 128) with these row passes.
+ * 128 x 128) with these row passes; oi_coarse_to_image_tc writes the column pass straight into the V operand tiles
+ * (scratch_tiles, count * ny * 512 bytes; scratch_v is unused and may be NULL).
  */
 OI_API int oi_rows_tc_constants(int which, int nx, int m0c, int bc, void* image, long long bytes, void* stream);
 OI_API int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, int nx, int m0c, int bc,

@@ -15,7 +15,7 @@
 // Memory: the forward row pass reads each mask row once (coalesced: thread n1 reads x[n1 + N1 n2]) and writes
 // the band columns transposed, [b][ic][y], so the column pass reads contiguous columns; the inverse passes
 // write [b][qc][y] then rows [b][y][x], again coalesced.
-#include "oi_common.cuh"
+#include "tc_common.cuh"
 #include <cstdint>
 
 namespace oi {
@@ -280,6 +280,72 @@ __global__ void __launch_bounds__(256, 3) fft_cols_inv_kernel(const float2* __re
   float2* dst = v + col * N;
 #pragma unroll
   for (int i = 0; i < 32; ++i) dst[n1 + N1 * bitrev5(i)] = z[i];
+}
+
+// ---------------------------------------------------------------- inverse, columns into V operand tiles
+// The column pass of the tensor-core synthesis: for image i and band columns qc0 .. qc0+G-1 (G = max(8, 256/N1),
+// zero beyond bc) the inverse column FFTs as fft_cols_inv_kernel, kept in shared memory, then written directly as
+// the bf16 hi / lo V operand tiles of the row pass (rows y of 128-row blocks, K = re | im of 64 band columns,
+// 128-byte swizzled: [hi: re | im][lo: re | im] x [128][64]) -- v itself never reaches global memory.
+template <int N1, int G>
+__global__ void __launch_bounds__(G * N1) cols_inv_tiles_kernel(const float2* __restrict__ ihat, int br, int bc,
+                                                              int ny, const float2* __restrict__ wn_g,
+                                                              unsigned char* __restrict__ tiles) {
+  constexpr int N = 32 * N1, T = G * N1;
+  constexpr uint32_t OPER = 128 * 128, TILE = 4 * OPER;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const float2* t2 = wn_g;
+  const float2* t1 = wn_g + 32 * N1;
+  const int nq = 2 * br - 1;
+  float2* cs = (float2*)smem_raw;                        // [G][nq]
+  float2* vs = cs + ((G * nq + 1) & ~1);                 // [N][G] (16-byte aligned)
+  const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
+  const long long i = blockIdx.y;
+  const int qc0 = blockIdx.x * G;
+  for (int e = tid; e < G * nq; e += T) {
+    const int jr = e / G, gg = e % G, qc = qc0 + gg;
+    cs[gg * nq + jr] = qc < bc ? ihat[(i * nq + jr) * (long long)bc + qc] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2 z[32];
+  inverse_gather<N1>(z, cs + g * nq, br - 1, t2, t1, n1);
+#pragma unroll
+  for (int k = 0; k < 32; ++k) vs[(n1 + N1 * bitrev5(k)) * G + g] = z[k];
+  __syncthreads();
+  for (int it = tid; it < N * (G / 8); it += T) {
+    const int y = it % N, gq = it / N, q = (qc0 >> 3) + gq;
+    const float4* src = (const float4*)(vs + y * G + 8 * gq);
+    float re[8], im[8];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const float4 x = src[e];
+      re[2 * e] = x.x, im[2 * e] = x.y, re[2 * e + 1] = x.z, im[2 * e + 1] = x.w;
+    }
+    uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      tc::split2(re[2 * e], re[2 * e + 1], rh[e], rl[e]);
+      tc::split2(im[2 * e], im[2 * e + 1], ih[e], il[e]);
+    }
+    const long long row = i * ny + y;
+    unsigned char* o = tiles + (row >> 7) * TILE + tc::swz((int)(row & 127), q);
+    *(uint4*)o = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+    *(uint4*)(o + OPER) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+    *(uint4*)(o + 2 * OPER) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+    *(uint4*)(o + 3 * OPER) = make_uint4(il[0], il[1], il[2], il[3]);
+  }
+}
+
+template <int N1, int G>
+static int cols_inv_tiles(const float2* ihat, int count, int br, int bc, int ny, const float2* wn_y,
+                          unsigned char* tiles, cudaStream_t s) {
+  const size_t smem = sizeof(float2) * (((size_t)G * (2 * br - 1) + 1) & ~(size_t)1) + sizeof(float2) * 32 * N1 * G;
+  int rc = set_smem(cols_inv_tiles_kernel<N1, G>, smem, "oi_coarse_to_image_tc/cols");
+  if (rc) return rc;
+  dim3 grid(64 / G, (unsigned)count);
+  cols_inv_tiles_kernel<N1, G><<<grid, G * N1, smem, s>>>(ihat, br, bc, ny, wn_y, tiles);
+  oi::note_launch();
+  return check_launch("oi_coarse_to_image_tc/cols");
 }
 
 // --------------------------------------------------------------------------------- inverse, rows
@@ -647,8 +713,8 @@ extern "C" int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int b
                                      void* scratch_ihat, void* scratch_v, void* scratch_tiles, float* out,
                                      void* stream) {
   using namespace oi;
-  if (!coarse || !wm_r || !wm_c || !wn_y || !cconsts || !scratch_ihat || !scratch_v || !scratch_tiles || !out ||
-      count <= 0 ||
+  (void)scratch_v;
+  if (!coarse || !wm_r || !wm_c || !wn_y || !cconsts || !scratch_ihat || !scratch_tiles || !out || count <= 0 ||
       nparts <= 0 || br <= 0 || bc <= 0)
     return fail(OI_EINVAL, "oi_coarse_to_image_tc: bad arguments");
   const int ny1 = n1_of(ny);
@@ -658,13 +724,14 @@ extern "C" int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int b
   float2* ih = (float2*)scratch_ihat;
   int rc = launch_coarse_spec_fft<4, 4>(coarse, nparts, count, br, bc, (const float2*)wm_r, (const float2*)wm_c, ih, s);
   if (rc) return rc;
-  float2* v = (float2*)scratch_v;
+  unsigned char* tiles = (unsigned char*)scratch_tiles;
+  const float2* wy = (const float2*)wn_y;
   switch (ny1) {
-    case 8: rc = cols_inv<8>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
-    case 16: rc = cols_inv<16>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
-    case 32: rc = cols_inv<32>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
-    default: rc = cols_inv<64>(ih, count, br, bc, (const float2*)wn_y, v, s); break;
+    case 8: rc = cols_inv_tiles<8, 32>(ih, count, br, bc, ny, wy, tiles, s); break;
+    case 16: rc = cols_inv_tiles<16, 16>(ih, count, br, bc, ny, wy, tiles, s); break;
+    case 32: rc = cols_inv_tiles<32, 8>(ih, count, br, bc, ny, wy, tiles, s); break;
+    default: rc = cols_inv_tiles<64, 8>(ih, count, br, bc, ny, wy, tiles, s); break;
   }
   if (rc) return rc;
-  return oi_rows_inv_tc(v, count, ny, nx, bc, cconsts, scratch_tiles, out, stream);
+  return rows_inv_from_tiles(tiles, count, ny, nx, cconsts, out, s);
 }

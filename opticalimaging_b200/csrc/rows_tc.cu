@@ -607,6 +607,23 @@ extern "C" int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, in
   return check_launch("oi_rows_fwd_tc");
 }
 
+namespace oi {
+
+int rows_inv_from_tiles(const void* vtiles, int count, int ny, int nx, const void* consts, float* out, cudaStream_t s) {
+  const long long rows = (long long)count * ny, R = rows / 128, items = (long long)(nx / 128) * R;
+  const int sms = rt::sm_count();
+  if (!sms) return fail(OI_ECUDA, "oi_rows_inv_tc: no CUDA device");
+  const long long ctas = items < sms ? items : sms;
+  rt::InvArgs a{(const unsigned char*)vtiles, rows, ny, nx, (const unsigned char*)consts, out};
+  int rc = ensure_smem((const void*)rt::rows_inv_tc_kernel, rt::I_SMEM, "oi_rows_inv_tc");
+  if (rc) return rc;
+  rt::rows_inv_tc_kernel<<<(unsigned)ctas, rt::NT, rt::I_SMEM, s>>>(a);
+  oi::note_launch();
+  return check_launch("oi_rows_inv_tc");
+}
+
+}  // namespace oi
+
 extern "C" int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, const void* consts, void* vtiles,
                               float* out, void* stream) {
   using namespace oi;
@@ -615,9 +632,7 @@ extern "C" int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, 
     return fail(OI_ERANGE, "oi_rows_inv_tc: grid %dx%d / band width %d unsupported", ny, nx, bc);
   if ((uintptr_t)consts % 16 || (uintptr_t)vtiles % 16)
     return fail(OI_EINVAL, "oi_rows_inv_tc: constants and V tiles must be 16-byte aligned");
-  const long long rows = (long long)count * ny, R = rows / 128, items = (long long)(nx / 128) * R;
-  const int sms = rt::sm_count();
-  if (!sms) return fail(OI_ECUDA, "oi_rows_inv_tc: no CUDA device");
+  const long long R = (long long)count * ny / 128;
   cudaStream_t s = (cudaStream_t)stream;
   int rc = ensure_smem((const void*)rt::v_tiles_kernel, (size_t)bc * 128 * 8, "oi_rows_inv_tc/tiles");
   if (rc) return rc;
@@ -625,11 +640,5 @@ extern "C" int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, 
   oi::note_launch();
   rc = check_launch("oi_rows_inv_tc/tiles");
   if (rc) return rc;
-  const long long ctas = items < sms ? items : sms;
-  rt::InvArgs a{(const unsigned char*)vtiles, rows, ny, nx, (const unsigned char*)consts, out};
-  rc = ensure_smem((const void*)rt::rows_inv_tc_kernel, rt::I_SMEM, "oi_rows_inv_tc");
-  if (rc) return rc;
-  rt::rows_inv_tc_kernel<<<(unsigned)ctas, rt::NT, rt::I_SMEM, s>>>(a);
-  oi::note_launch();
-  return check_launch("oi_rows_inv_tc");
+  return rows_inv_from_tiles(vtiles, count, ny, nx, consts, out, s);
 }

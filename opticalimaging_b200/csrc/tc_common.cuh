@@ -13,6 +13,11 @@ namespace oi {
 // expired sets it) and a host reader; oi_device_status combines them.
 int rows_tc_status(int* status, bool reset);
 
+// The tensor-core synthesis row pass (rows_tc.cu) from V operand tiles already in memory: tiles [count*ny/128]
+// [64 KB] (bf16 hi/lo, [hi: re | im][lo: re | im] x [128 rows][64], 128-byte swizzled), consts from
+// oi_rows_tc_constants(1, ...).
+int rows_inv_from_tiles(const void* vtiles, int count, int ny, int nx, const void* consts, float* out, cudaStream_t s);
+
 namespace tc {
 
 constexpr uint32_t SMEM_LIMIT = 232448;                 // opt-in maximum of dynamic shared memory per CTA

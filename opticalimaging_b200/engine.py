@@ -271,11 +271,10 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
         out = torch.empty((batch, nz, plan.ny, plan.nx), dtype=torch.float32, device=dev)
     ihat = torch.empty(batch * nz * (2 * b.br - 1) * b.bc, dtype=torch.complex64, device=dev)
     if form == 'bf16x3' and plan.tc_rows(form):
-        v = torch.empty(batch * nz * b.bc * plan.ny, dtype=torch.complex64, device=dev)
         tiles = torch.empty(batch * nz * plan.ny * 512, dtype=torch.uint8, device=dev)
         N.call('oi_coarse_to_image_tc', N.ptr(coarse), nsplit, batch * nz, b.br, b.bc, N.ptr(plan.wm_r),
                N.ptr(plan.wm_c), N.ptr(plan.wn_y), N.ptr(plan.rows_consts(1)), plan.ny, plan.nx, N.ptr(ihat),
-               N.ptr(v), N.ptr(tiles), N.ptr(out), s)
+               None, N.ptr(tiles), N.ptr(out), s)
     elif plan.big_coarse_fft(form):
         # the coarse intensity's Hermitian half-spectrum by the FFT band pass, then the FFT synthesis
         count, nq = batch * nz, 2 * b.br - 1
