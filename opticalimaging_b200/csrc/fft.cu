@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(256, 3) fft_rows_inv_kernel(const float2* __re
 }
 
 // --------------------------------------------------------------- coarse intensity -> its spectrum
-// One block per coarse image (mr = 32 N1R, mc = 32 N1C, each 64 or 128):
+// Two blocks per coarse image, each for half of the band columns qc (mr = 32 N1R, mc = 32 N1C, each 64 or 128):
 //   ihat[i][jr][qc] = (qc ? 2 : 1) / (mr mc) * sum_{sr,sc} coarse[i][sr][sc] exp(+2 pi i (qr sr/mr + qc sc/mc))
 // for qr = jr - (br-1) in [-(br-1), br-1] and qc in [0, bc).  Row FFTs of the real image in pairs (two rows per
 // complex transform), the band bins of each separated into U[sr][qc]; then column FFTs of U at the qr bins.
@@ -418,26 +418,35 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
   float2* r2 = (float2*)smem_raw;      // row-axis (MR) tables: [32][N1R], [N1R][N1R]
   float2* r1 = r2 + 32 * N1R;
   float2* c2 = r1 + N1R * N1R;         // column-axis (MC) tables: [32][N1C], [N1C][N1C]
-  float2* c1 = c2 + 32 * N1C;
-  float2* area = c1 + N1C * N1C;       // [area_f2] union: coarse image / row transposes / column transposes
+  float2* c1t = c2 + 32 * N1C;
+  float2* area = c1t + N1C * N1C;      // [area_f2] union: coarse image / row transposes / column transposes
   float2* u = area + area_f2;          // [MR][bc]
   const int tid = threadIdx.x;
   const long long img = blockIdx.x;
+  // this block's band columns: blockIdx.y-th of gridDim.y equal ranges of [0, bc)
+  const int cw = (bc + gridDim.y - 1) / gridDim.y, c0 = blockIdx.y * cw, c1 = min(bc, c0 + cw);
   build_tables<N1R>(wr_g, r2, r1, tid, T);
-  build_tables<N1C>(wc_g, c2, c1, tid, T);
+  build_tables<N1C>(wc_g, c2, c1t, tid, T);
   float* cimg = (float*)area;
   const float4* src = (const float4*)(coarse + img * (long long)MR * MC);
-  for (int j = tid; j < MR * MC / 4; j += T) {   // the partial sums, added in order
-    float4 v = __ldg(src + j);
-    for (int p = 1; p < nparts; ++p) {
-      const float4 u = __ldg(src + p * (part_stride / 4) + j);
-      v.x += u.x;
-      v.y += u.y;
-      v.z += u.z;
-      v.w += u.w;
+  constexpr int PER = MR * MC / 4 / T;   // float4 per thread
+  float4 acc[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) acc[k] = __ldg(src + tid + T * k);
+  for (int p = 1; p < nparts; ++p) {   // the partial sums, added in order; all loads of a part in flight together
+    float4 x[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) x[k] = __ldg(src + p * (part_stride / 4) + tid + T * k);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      acc[k].x += x[k].x;
+      acc[k].y += x[k].y;
+      acc[k].z += x[k].z;
+      acc[k].w += x[k].w;
     }
-    ((float4*)cimg)[j] = v;
   }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) ((float4*)cimg)[tid + T * k] = acc[k];
   __syncthreads();
   // row pass: pair p = rows (2p, 2p+1), thread n1
   const int p = tid / N1C, n1 = tid % N1C;
@@ -452,31 +461,31 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
   __syncthreads();  // the image is consumed; the area now holds row transposes
   if (row_task) twiddle_store<+1, N1C>(z, c2, n1, area + p * 32 * (N1C + 1));
   __syncthreads();
-  for (int e = tid; e < (MR / 2) * bc; e += T) {
-    const int pp = e / bc, qc = e % bc;
+  for (int e = tid; e < (MR / 2) * (c1 - c0); e += T) {
+    const int pp = e / (c1 - c0), qc = c0 + e % (c1 - c0);
     const float2* ys = area + pp * 32 * (N1C + 1);
-    const float2 zp = outer_bin<+1, N1C>(ys, c1, qc & (MC - 1));
-    const float2 zm = outer_bin<+1, N1C>(ys, c1, (-qc) & (MC - 1));
+    const float2 zp = outer_bin<+1, N1C>(ys, c1t, qc & (MC - 1));
+    const float2 zm = outer_bin<+1, N1C>(ys, c1t, (-qc) & (MC - 1));
     u[(2 * pp) * bc + qc] = make_float2(0.5f * (zp.x + zm.x), 0.5f * (zp.y - zm.y));
     u[(2 * pp + 1) * bc + qc] = make_float2(0.5f * (zp.y + zm.y), -0.5f * (zp.x - zm.x));
   }
   __syncthreads();
   // column pass: column qc of U, thread n1r
-  const int qc = tid / N1R, n1r = tid % N1R;
-  const bool col_task = qc < bc;
+  const int qc = c0 + tid / N1R, n1r = tid % N1R;
+  const bool col_task = qc < c1;
   if (col_task) {
 #pragma unroll
     for (int n2 = 0; n2 < 32; ++n2) z[n2] = u[(n1r + N1R * n2) * bc + qc];
     fft32<+1>(z);
   }
   __syncthreads();  // row transposes are consumed; the area now holds column transposes
-  if (col_task) twiddle_store<+1, N1R>(z, r2, n1r, area + qc * 32 * (N1R + 1));
+  if (col_task) twiddle_store<+1, N1R>(z, r2, n1r, area + (qc - c0) * 32 * (N1R + 1));
   __syncthreads();
   const int nq = 2 * br - 1;
   const float norm = 1.0f / ((float)MR * (float)MC);
-  for (int e = tid; e < nq * bc; e += T) {
-    const int jr = e / bc, c = e % bc;
-    const float2 v = outer_bin<+1, N1R>(area + c * 32 * (N1R + 1), r1, (jr - (br - 1)) & (MR - 1));
+  for (int e = tid; e < nq * (c1 - c0); e += T) {
+    const int jr = e / (c1 - c0), c = c0 + e % (c1 - c0);
+    const float2 v = outer_bin<+1, N1R>(area + (c - c0) * 32 * (N1R + 1), r1, (jr - (br - 1)) & (MR - 1));
     const float s = (c == 0 ? 1.0f : 2.0f) * norm;
     ihat[(img * nq + jr) * (long long)bc + c] = make_float2(v.x * s, v.y * s);
   }
@@ -492,7 +501,8 @@ static int launch_coarse_spec_fft(float* coarse, int nparts, int count, int br, 
   auto kern = coarse_spec_fft_kernel<N1R, N1C>;
   int rc = set_smem(kern, smem, "coarse spectrum fft");
   if (rc) return rc;
-  kern<<<count, 512, smem, s>>>(coarse, nparts, (long long)count * MR * MC, br, bc, wr, wc, area_f2, ihat);
+  kern<<<dim3((unsigned)count, 2), 512, smem, s>>>(coarse, nparts, (long long)count * MR * MC, br, bc, wr, wc,
+                                                   area_f2, ihat);
   oi::note_launch();
   return check_launch("coarse spectrum fft");
 }
