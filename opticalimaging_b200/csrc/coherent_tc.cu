@@ -153,17 +153,42 @@ struct FieldSrc {
   float w;
 };
 
-__device__ __forceinline__ FieldSrc field_src(const Args& a, long long t) {
-  const int F = a.nk * a.nch;
-  const long long q = t / F;
-  const int f = (int)(t - q * F), k = f / a.nch, c = f - k * a.nch;
-  const long long b = q / a.nz;
-  const int z = (int)(q - b * a.nz);
+// Position of task t = (image q = b * nz + z, kernel k, channel c): divided out once per CTA, then advanced by
+// counters (64-bit division is a long emulated sequence on the device).
+struct TaskPos {
+  long long q, b;
+  int z, k, c;
+  __device__ __forceinline__ void init(const Args& a, long long t) {
+    const int F = a.nk * a.nch;
+    q = t / F;
+    const int f = (int)(t - q * F);
+    k = f / a.nch;
+    c = f - k * a.nch;
+    b = q / a.nz;
+    z = (int)(q - b * a.nz);
+  }
+  __device__ __forceinline__ void next(const Args& a) {
+    if (++c == a.nch) {
+      c = 0;
+      if (++k == a.nk) {
+        k = 0;
+        ++q;
+        if (++z == a.nz) {
+          z = 0;
+          ++b;
+        }
+      }
+    }
+  }
+  __device__ __forceinline__ bool first() const { return k == 0 && c == 0; }   // first field of image q
+};
+
+__device__ __forceinline__ FieldSrc field_src(const Args& a, const TaskPos& p) {
   const long long plane = (long long)a.br * a.bc;
   FieldSrc s;
-  s.pupil = a.pupil + b * a.pupil_batch_stride + ((long long)z * a.nk + k) * plane;
-  s.band = a.band + b * a.band_img_stride + (long long)c * plane;
-  s.w = __ldg(a.weight + (long long)z * a.nk + k);
+  s.pupil = a.pupil + p.b * a.pupil_batch_stride + ((long long)p.z * a.nk + p.k) * plane;
+  s.band = a.band + p.b * a.band_img_stride + (long long)p.c * plane;
+  s.w = __ldg(a.weight + (long long)p.z * a.nk + p.k);
   return s;
 }
 
@@ -314,7 +339,9 @@ __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  FieldSrc cur = field_src(a, t0);
+  TaskPos pt;                                   // position of task t (t0 before the loop)
+  pt.init(a, t0);
+  FieldSrc cur = field_src(a, pt);
   if (tid == 0) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1 + 8 * i) : "memory");
@@ -355,7 +382,9 @@ __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
     }
     pending1 = 1;
     FieldSrc nxt = cur;
-    if (t0 + 1 < t1) nxt = field_src(a, t0 + 1);
+    TaskPos p1 = pt;
+    p1.next(a);
+    if (t0 + 1 < t1) nxt = field_src(a, p1);
     if (L.staged && t0 + 1 < t1) {
       if (tid == 32) stage_copy(a, nxt, stage, L.stage_arr, bar3);
       pending3 = 1;
@@ -369,6 +398,10 @@ __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
 
   for (long long t = t0; t < t1 && !failed; ++t) {
     bad = false;
+    TaskPos p1 = pt, p2;
+    p1.next(a);
+    p2 = p1;
+    p2.next(a);
     // (1) |E|^2 of task t-1 (overlaps stage 1 of t on the tensor pipe)
     if (t > t0) {
       if (warp_wait(bar2, ph2)) {
@@ -379,8 +412,8 @@ __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
       }
       ph2 ^= 1;
       pending2 = 0;
-      const long long qp = (t - 1) / F;
-      if (t / F != qp) {  // task t-1 was the last of its image in this range
+      if (pt.first()) {  // task t-1 was the last of its image in this range
+        const long long qp = pt.q - 1;
         const long long slot = blockIdx.x - cta_of(qp * F, a.tasks, G);
         float* out = a.coarse + (slot * a.images + qp) * (long long)(MR * MC) + sc;
 #pragma unroll
@@ -400,10 +433,10 @@ __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
     ph1 ^= 1;
     pending1 = 0;
     wprev = cur.w;
-    if (t + 1 < t1) cur = field_src(a, t + 1);
+    if (t + 1 < t1) cur = field_src(a, p1);
     // zero-fill the partial slots of this image that no CTA owns (done by the image's first CTA)
-    if (t % F == 0) {
-      const long long q = t / F;
+    if (pt.first()) {
+      const long long q = pt.q;
       const long long first = cta_of(q * F, a.tasks, G), last = cta_of(q * F + F - 1, a.tasks, G);
       for (long long slot = last - first + 1; slot < a.nparts; ++slot) {
         float* out = a.coarse + (slot * a.images + q) * (long long)(MR * MC);
@@ -443,10 +476,11 @@ __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
       }
       pending1 = 1;
       if (L.staged && t + 2 < t1) {
-        if (tid == 32) stage_copy(a, field_src(a, t + 2), stage, L.stage_arr, bar3);
+        if (tid == 32) stage_copy(a, field_src(a, p2), stage, L.stage_arr, bar3);
         pending3 = 1;
       }
     }
+    pt = p1;
   }
   if (!failed) {
     if (warp_wait(bar2, ph2)) {

@@ -54,6 +54,18 @@ __device__ __forceinline__ void arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+// Cursor over a ring of mbarrier-guarded slots: slot index and the parity of its current round.
+struct Ring {
+  int slot;
+  uint32_t phase;
+  __device__ __forceinline__ void next(int n) {
+    if (++slot == n) {
+      slot = 0;
+      phase ^= 1u;
+    }
+  }
+};
+
 // 8 floats -> 4 packed bf16 hi words and 4 lo words
 __device__ __forceinline__ void split8(const float (&v)[8], uint32_t (&hi)[4], uint32_t (&lo)[4]) {
 #pragma unroll
@@ -78,7 +90,7 @@ constexpr uint32_t F_STG = 128 * 64 * 4;             // one staging slot (float)
 constexpr uint32_t F_W = 2 * OPER;                   // one W chunk (hi, lo)
 constexpr uint32_t F_WOFF = F_NS * F_STG;
 constexpr uint32_t F_MISC = F_WOFF + F_NWS * F_W;
-constexpr uint32_t F_SMEM = F_MISC + 256 + 1024;
+constexpr uint32_t F_SMEM = F_MISC + 384 + 1024;
 constexpr uint32_t F_COL_A = 2 * ACC_COLS;           // A slot s at columns 256 + 64 s: hi [0,32), lo [32,64)
 constexpr uint32_t F_TMEM_COLS = 512;
 
@@ -104,6 +116,9 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   const uint32_t sfull = misc, sfree = misc + 24, wfull = misc + 48, wdone = misc + 72, conv = misc + 96,
                  adone = misc + 112, accf = misc + 128, acce = misc + 144;
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + F_MISC + 192);
+  // per A slot and converter warp: 1 when the warp's part of the chunk has a non-zero bf16 lo half (a mask value
+  // not exact in bf16); when no warp sets it the lo x hi products are exactly zero and are not issued
+  volatile uint32_t* lo_flags = (volatile uint32_t*)(gbase + F_MISC + 256);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int KC = a.nx / 64;
   const long long items = a.rows / 128;
@@ -133,66 +148,84 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   fence_after();
   const uint32_t tmem = *tmem_slot;
 
+  // Loop state advances incrementally (ring slot / phase, chunk / item): no integer division per chunk.
+  const int NC = (int)nchunks;
   if (warp == 8) {
     // ---- mask producer: chunk g into staging slot g % 3 as soon as the slot has been read
     if (lane == 0) {
-      for (long long g = 0; g < nchunks; ++g) {
-        const int s4 = (int)(g % F_NS);
-        if (g >= F_NS && !wait_bar(sfree + 8 * s4, (uint32_t)(((g - F_NS) / F_NS) & 1))) {
+      Ring st{0, 0};
+      int c = 0, y = (int)(i0 * 128);
+      for (int g = 0; g < NC; ++g) {
+        if (g >= F_NS && !wait_bar(sfree + 8 * st.slot, st.phase ^ 1u)) {
           fail_status();
           break;
         }
-        const long long item = i0 + g / KC;
-        const int c = (int)(g % KC), y = (int)(item * 128);
-        const uint32_t st = base + s4 * F_STG;
-        expect_tx(sfull + 8 * s4, U8 ? 128 * 64 : F_STG);
-        tma_load_2d(st, &mask_map, 64 * c, y, sfull + 8 * s4);
-        if (!U8) tma_load_2d(st + F_STG / 2, &mask_map, 64 * c + 32, y, sfull + 8 * s4);
+        const uint32_t dst = base + st.slot * F_STG;
+        expect_tx(sfull + 8 * st.slot, U8 ? 128 * 64 : F_STG);
+        tma_load_2d(dst, &mask_map, 64 * c, y, sfull + 8 * st.slot);
+        if (!U8) tma_load_2d(dst + F_STG / 2, &mask_map, 64 * c + 32, y, sfull + 8 * st.slot);
+        st.next(F_NS);
+        if (++c == KC) {
+          c = 0;
+          y += 128;
+        }
       }
     }
   } else if (warp == 10) {
     // ---- W producer: chunk g's W into slot g % 3 once the MMAs of chunk g-3 have finished
     if (lane == 0) {
-      for (long long g = 0; g < nchunks; ++g) {
-        const int s3 = (int)(g % F_NWS);
-        if (g >= F_NWS && !wait_bar(wdone + 8 * s3, (uint32_t)(((g - F_NWS) / F_NWS) & 1))) {
+      Ring ws{0, 0};
+      int c = 0;
+      for (int g = 0; g < NC; ++g) {
+        if (g >= F_NWS && !wait_bar(wdone + 8 * ws.slot, ws.phase ^ 1u)) {
           fail_status();
           break;
         }
-        const int c = (int)(g % KC);
-        expect_tx(wfull + 8 * s3, F_W);
-        bulk_g2s(base + F_WOFF + s3 * F_W, a.w + (long long)c * F_W, F_W, wfull + 8 * s3);
+        expect_tx(wfull + 8 * ws.slot, F_W);
+        bulk_g2s(base + F_WOFF + ws.slot * F_W, a.w + (long long)c * F_W, F_W, wfull + 8 * ws.slot);
+        ws.next(F_NWS);
+        if (++c == KC) c = 0;
       }
     }
   } else if (warp == 9) {
     // ---- MMA issue: D[buf] += A(tmem slot) x W^T over the chunk (K steps of 16), split BF16x3
     if (lane == 0) {
       constexpr uint32_t ID = idesc(128, false);
-      for (long long g = 0; g < nchunks; ++g) {
-        const int s2 = (int)(g & 1);
-        const long long n = g / KC;
-        const int c = (int)(g % KC), buf = (int)(n & 1);
-        const int s3 = (int)(g % F_NWS);
-        bool ok = wait_bar(conv + 8 * s2, (uint32_t)((g >> 1) & 1));
-        if (ok) ok = wait_bar(wfull + 8 * s3, (uint32_t)((g / F_NWS) & 1));
+      Ring as{0, 0}, ws{0, 0};
+      int c = 0, n = 0;
+      for (int g = 0; g < NC; ++g) {
+        const int buf = n & 1;
+        bool ok = wait_bar(conv + 8 * as.slot, as.phase);
+        if (ok) ok = wait_bar(wfull + 8 * ws.slot, ws.phase);
         if (ok && c == 0 && n >= 2) ok = wait_bar(acce + 8 * buf, (uint32_t)(((n - 2) >> 1) & 1));
         if (!ok) {
           fail_status();
           break;
         }
         fence_after();
-        const uint32_t wch = base + F_WOFF + s3 * F_W, at = tmem + F_COL_A + 64 * s2;
+        const uint32_t wch = base + F_WOFF + ws.slot * F_W, at = tmem + F_COL_A + 64 * as.slot;
         const uint32_t d = tmem + buf * ACC_COLS;
+        uint32_t lo_any = 0;
+        if (!U8) {
+#pragma unroll
+          for (int w = 0; w < 8; ++w) lo_any |= lo_flags[8 * as.slot + w];
+        }
 #pragma unroll
         for (int ks = 0; ks < 4; ++ks) {
           const uint32_t ko = 32 * ks;
           mma_ts(d, at + 8 * ks, sdesc(wch + ko), ID, (c | ks) ? 1u : 0u);            // hi hi
           mma_ts(d, at + 8 * ks, sdesc(wch + OPER + ko), ID, 1);                     // hi lo
-          if (!U8) mma_ts(d, at + 32 + 8 * ks, sdesc(wch + ko), ID, 1);              // lo hi
+          if (lo_any) mma_ts(d, at + 32 + 8 * ks, sdesc(wch + ko), ID, 1);           // lo hi
         }
-        commit(adone + 8 * s2);
-        commit(wdone + 8 * s3);
+        commit(adone + 8 * as.slot);
+        commit(wdone + 8 * ws.slot);
         if (c == KC - 1) commit(accf + 8 * buf);
+        as.next(2);
+        ws.next(F_NWS);
+        if (++c == KC) {
+          c = 0;
+          ++n;
+        }
       }
     }
   } else {
@@ -201,9 +234,9 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
     const int half = warp >> 2, r = 32 * (warp & 3) + lane;
     bool ok = true;
-    auto drain = [&](long long n) {
+    auto drain = [&](int n) {
       // accumulator of item n: lanes = rows, columns re [0,64) / im [64,128) of band column ic
-      const int buf = (int)(n & 1);
+      const int buf = n & 1;
       if (!warp_wait(accf + 8 * buf, (uint32_t)((n >> 1) & 1))) return false;
       fence_after();
       float re[32], im[32];
@@ -212,23 +245,23 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
       fence_before();
       __syncwarp();
       if (lane == 0) arrive(acce + 8 * buf);
-      const long long row = (i0 + n) * 128 + r;
-      const long long b = row / a.ny;
-      const int y = (int)(row - b * a.ny);
-      float2* dst = a.t + (b * a.bc + 32 * half) * (long long)a.ny + y;
+      const int row = (int)((i0 + n) * 128) + r;
+      const int b = row / a.ny, y = row - b * a.ny;
+      float2* dst = a.t + ((long long)b * a.bc + 32 * half) * a.ny + y;
 #pragma unroll
       for (int j = 0; j < 32; ++j)
         if (32 * half + j < a.bc) dst[(long long)j * a.ny] = make_float2(re[j], im[j]);
       return true;
     };
-    for (long long g = 0; g < nchunks && ok; ++g) {
-      const int s4 = (int)(g % F_NS), s2 = (int)(g & 1);
-      ok = warp_wait(sfull + 8 * s4, (uint32_t)((g / F_NS) & 1));
-      if (ok && g >= 2) ok = warp_wait(adone + 8 * s2, (uint32_t)(((g - 2) >> 1) & 1));   // A slot free
+    Ring st{0, 0}, as{0, 0};
+    int c = 0, n = 0;
+    for (int g = 0; g < NC && ok; ++g) {
+      ok = warp_wait(sfull + 8 * st.slot, st.phase);
+      if (ok && g >= 2) ok = warp_wait(adone + 8 * as.slot, as.phase ^ 1u);   // A slot free (chunk g-2 done)
       if (!ok) break;
       float v[32];
       if (U8) {
-        const unsigned char* row = gbase + s4 * F_STG + r * 64;   // 64-byte swizzle: chunk j at j ^ ((r >> 1) & 3)
+        const unsigned char* row = gbase + st.slot * F_STG + r * 64;   // 64-byte swizzle: chunk j at j ^ ((r >> 1) & 3)
 #pragma unroll
         for (int jj = 0; jj < 2; ++jj) {
           const uint4 u = *(const uint4*)(row + (((2 * half + jj) ^ ((r >> 1) & 3)) << 4));
@@ -237,7 +270,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
           for (int e = 0; e < 16; ++e) v[16 * jj + e] = (float)((w4[e >> 2] >> (8 * (e & 3))) & 0xFF);
         }
       } else {
-        const unsigned char* row = gbase + s4 * F_STG + half * (F_STG / 2) + r * 128;   // 128-byte swizzle
+        const unsigned char* row = gbase + st.slot * F_STG + half * (F_STG / 2) + r * 128;   // 128-byte swizzle
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const float4 x = *(const float4*)(row + ((j ^ (r & 7)) << 4));
@@ -245,22 +278,36 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
         }
       }
       __syncwarp();
-      if (lane == 0) arrive(sfree + 8 * s4);          // the staging slot may be refilled
+      if (lane == 0) arrive(sfree + 8 * st.slot);          // the staging slot may be refilled
       uint32_t hi[16], lo[16];
 #pragma unroll
       for (int e = 0; e < 16; ++e) split2(v[2 * e], v[2 * e + 1], hi[e], lo[e]);
-      const uint32_t at = tmem + lane_base + F_COL_A + 64 * s2 + 16 * half;
+      const uint32_t at = tmem + lane_base + F_COL_A + 64 * as.slot + 16 * half;
       tmem_st16(at, hi);
-      if (!U8) tmem_st16(at + 32, lo);
+      bool lo_nz = false;
+      if (!U8) {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) lo_nz |= lo[e] != 0u;
+        lo_nz = __any_sync(0xffffffffu, lo_nz);
+        tmem_st16(at + 32, lo);          // always written: another warp's flag may make the MMAs read it
+      }
       wait_st();
       fence_before();
       __syncwarp();
-      if (lane == 0) arrive(conv + 8 * s2);
+      if (lane == 0) {
+        if (!U8) lo_flags[8 * as.slot + warp] = lo_nz ? 1u : 0u;   // read by the MMA thread after `conv`
+        arrive(conv + 8 * as.slot);
+      }
       // the previous item's accumulator is complete once this item's first chunk is converted
-      const long long n = g / KC;
-      if (g % KC == 0 && n >= 1) ok = drain(n - 1);
+      if (c == 0 && n >= 1) ok = drain(n - 1);
+      st.next(F_NS);
+      as.next(2);
+      if (++c == KC) {
+        c = 0;
+        ++n;
+      }
     }
-    if (ok && nchunks > 0) ok = drain(i1 - i0 - 1);
+    if (ok && NC > 0) ok = drain((int)(i1 - i0) - 1);
     if (!ok && lane == 0) fail_status();
   }
   fence_before();
@@ -339,9 +386,8 @@ struct InvArgs {
 // Drain the accumulator of item `it` (tensor-memory buffer `buf`): lanes = x of this warp's quarter, columns =
 // rows y0 .. y0+127 of the block (this warp's half), stored as coalesced 128-byte row segments.
 __device__ __forceinline__ void inv_drain(const InvArgs& a, uint32_t taddr, uint32_t acce, int half, int warp,
-                                          int lane, long long it, int buf, long long R) {
+                                          int lane, long long j, long long r, int buf) {
   fence_after();
-  const long long j = it / R, r = it % R;
   float* dst = a.out + (r * 128 + 64 * half) * (long long)a.nx + j * 128 + 32 * (warp & 3) + lane;
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
@@ -392,12 +438,14 @@ __global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a) {
   fence_after();
   const uint32_t tmem = *tmem_slot;
 
+  // item i0 + n = (x tile j, row block r); counters advance per item (the x tile changes exactly when r wraps)
+  const long long j0 = i0 / R, r0 = i0 - j0 * R;
   if (warp == 8) {
     if (lane == 0) {
+      long long j = j0, r = r0;
       for (long long n = 0; n < N; ++n) {
-        const long long it = i0 + n, j = it / R, r = it % R;
         const int s = (int)(n & 1);
-        const bool reload = n == 0 || (it - 1) / R != j;
+        const bool reload = n == 0 || r == 0;
         bool ok = true;
         if (n >= 2) ok = wait_bar(vdone + 8 * s, (uint32_t)(((n - 2) >> 1) & 1));           // slot free
         if (ok && reload && n >= 1) ok = wait_bar(vdone + 8 * ((n - 1) & 1), (uint32_t)(((n - 1) >> 1) & 1));
@@ -412,16 +460,21 @@ __global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a) {
         expect_tx(vfull + 8 * s, VT_BYTES);
         for (int q = 0; q < 4; ++q)
           bulk_g2s(base + I_V + s * VT_BYTES + q * OPER, a.vt + r * VT_BYTES + q * OPER, OPER, vfull + 8 * s);
+        if (++r == R) {
+          r = 0;
+          ++j;
+        }
       }
     }
   } else if (warp == 9) {
     if (lane == 0) {
       constexpr uint32_t ID = idesc(128, false);
       int reloads = 0;
+      long long r = r0;
       for (long long n = 0; n < N; ++n) {
-        const long long it = i0 + n, j = it / R;
         const int s = (int)(n & 1), buf = s;
-        const bool reload = n == 0 || (it - 1) / R != j;
+        const bool reload = n == 0 || r == 0;
+        if (++r == R) r = 0;
         bool ok = wait_bar(vfull + 8 * s, (uint32_t)((n >> 1) & 1));
         if (ok && reload) ok = wait_bar(cxb, (uint32_t)(reloads & 1));
         if (ok && n >= 2) ok = wait_bar(acce + 8 * buf, (uint32_t)(((n - 2) >> 1) & 1));
@@ -449,10 +502,15 @@ __global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a) {
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
     const int half = warp >> 2;
     bool ok = true;
+    long long j = j0, r = r0;
     for (long long n = 0; n < N && ok; ++n) {
       const int buf = (int)(n & 1);
       ok = warp_wait(vdone + 8 * buf, (uint32_t)((n >> 1) & 1));
-      if (ok) inv_drain(a, tmem + lane_base, acce, half, warp, lane, i0 + n, buf, R);
+      if (ok) inv_drain(a, tmem + lane_base, acce, half, warp, lane, j, r, buf);
+      if (++r == R) {
+        r = 0;
+        ++j;
+      }
     }
     if (!ok && lane == 0) fail_status();
   }
