@@ -9,17 +9,19 @@
 // Forward: D[y][n] (M = 128 rows, N = 128: n < 64 re / n >= 64 im of band column ic = n mod 64, K = x in
 // chunks of 64) = A x W^T, A = the mask rows (converted to bf16 hi / lo), W = [cos; sin] of the band columns
 // (a constant operand image, streamed per chunk).  Inverse: D[x][y] (M = 128 columns x of one x tile,
-// N = 128 rows, K = (re | im) x 64 band columns) = C x V^T, C = [cos | sin] of the x tile (constant image,
-// resident per x tile), V = v converted to bf16 hi / lo.  The accumulator's lanes are the rows (forward) or
-// the columns (inverse), so every warp store of the result is one coalesced segment.
+// N = 256 rows, K = (re | im) x 64 band columns) = C x V^T, C = [cos | sin] of the x tile (constant image,
+// streamed in 16 KB pieces), V = v as bf16 hi / lo operand tiles (resident while the row-block pair lasts).  The
+// accumulator's lanes are the rows (forward) or the columns (inverse), so every warp store of the result is one
+// coalesced segment.  The forward pass takes its A operand (converted on the fly) from tensor memory; the
+// inverse reads both operands from shared memory (at N = 128 an A operand in tensor memory halves the MMA rate,
+// which only the forward pass's conversion justifies).
 //
-// Roles (320 threads; the forward kernel has an 11th warp issuing its W loads apart from the mask loads):
-// warps 0-7 convert the staged inputs into the bf16 operand and drain finished accumulators to global memory
-// (two warps per tensor-memory lane quarter); warp 8 issues
-// the loads into the staging buffers (one 2-D tensor-map box per tile and 1-D bulk copies of the constants; no
-// multicast); warp 9 lane 0 issues the MMAs and
-// commits them to mbarriers.  Staging and operands are double-buffered (forward) or single (inverse); the
-// accumulator is double-buffered in tensor memory so that draining one block overlaps the MMAs of the next.
+// Roles (352 threads): warps 0-7 convert the staged mask chunks into the A operand in tensor memory (forward)
+// and drain finished accumulators to global memory (two warps per tensor-memory lane quarter); warps 8 and 10
+// issue the loads into shared-memory rings (forward: 2-D tensor-map boxes of the masks and 1-D bulk copies of
+// W; inverse: 2-D tensor-map boxes of the C pieces and of the V tiles; no multicast); warp 9 lane 0 issues the
+// MMAs and commits them to mbarriers.  Accumulators are double-buffered so that draining
+// overlaps the MMAs of the next blocks.
 // Every mbarrier wait is bounded (2 s); on expiry the role records the status (oi_device_status) and stops,
 // the others then expire in turn, and the CTA frees tensor memory and exits.
 #include <cuda.h>
@@ -43,10 +45,8 @@ namespace rt {
 using namespace tc;
 
 constexpr int NT = 320;                    // threads: 8 converter warps, producer warp, MMA warp
-constexpr int NCONV = 256;
 constexpr uint32_t OPER = 128 * 128;       // one [128 rows][64 bf16] swizzled operand block (16 KB)
 constexpr uint32_t ACC_COLS = 128;         // one accumulator: 128 lanes x 128 fp32 columns
-constexpr uint32_t TMEM_COLS = 256;        // two accumulators
 
 __device__ __forceinline__ void fail_status() { atomicExch(&g_rows_status, 1); }
 
@@ -369,68 +369,107 @@ __global__ void __launch_bounds__(256) v_tiles_kernel(const float2* __restrict__
   }
 }
 
-// Shared memory: C tile of the current x tile (hi, lo: [kc][128 rows][64]) and two V tiles.
-constexpr uint32_t I_CX = 0;
-constexpr uint32_t I_V = 4 * OPER;
-constexpr uint32_t I_MISC = I_V + 2 * VT_BYTES;
-constexpr uint32_t I_SMEM = I_MISC + 128 + 1024;
+// Items (row-block pair P = rows 256 P .. 256 P + 255, x tile j) in pair-major order, cut into one contiguous
+// range per CTA.  A CTA keeps the V tiles of its pair (128 KB) and streams the C tiles of the nx / 128 x tiles
+// (64 KB each, L2-resident for the whole launch) through a ring of 6 pieces of 16 KB ([128 x][64] blocks: hi or
+// lo of kc 0 or 1), released one by one as soon as the MMAs reading them have finished.  One C tile serves 256
+// output rows (N = 256), so the operand stream is half the output stream, and every V tile is read once.  A pair
+// past the last row block (odd row-block count) reads zeros for its second half and stores nothing there.
+// Tensor memory: two accumulators of 256 columns.
+constexpr int I_NC = 6;                               // C pieces in the ring
+constexpr int I_NT = NT + 32;                         // + a warp loading the V tiles
+constexpr uint32_t I_ACC = 256;                       // accumulator columns (N)
+constexpr uint32_t I_C = 0;
+constexpr uint32_t I_V = I_NC * OPER;                 // V of the pair: block q (hi kc 0, hi kc 1, lo kc 0, lo kc 1)
+                                                      // at 2 q OPER, [256 rows][64]
+constexpr uint32_t I_MISC = I_V + 8 * OPER;
+constexpr uint32_t I_SMEM = I_MISC + 512 + 1024;
+constexpr uint32_t I_TMEM_COLS = 2 * I_ACC;
+static_assert(I_SMEM <= SMEM_LIMIT, "inverse row pass: shared memory");
 
 struct InvArgs {
-  const unsigned char* vt;  // V tiles (v_tiles_kernel), [rows / 128][64 KB]
+  const unsigned char* vt;  // V tiles, [rows / 128][64 KB]: [hi kc 0 | hi kc 1 | lo kc 0 | lo kc 1] x [128 y][64]
   long long rows;           // count * ny (a multiple of 128)
   int ny, nx;
-  const unsigned char* c;   // constant image: per 128-column x tile, [hi | lo] x [kc][128 rows][64]
+  const unsigned char* c;   // constant image: per 128-column x tile, [hi kc 0 | hi kc 1 | lo kc 0 | lo kc 1] x [128 x][64]
   float* out;               // [count][ny][nx]
 };
 
-// Drain the accumulator of item `it` (tensor-memory buffer `buf`): lanes = x of this warp's quarter, columns =
-// rows y0 .. y0+127 of the block (this warp's half), stored as coalesced 128-byte row segments.
+// Block index (in the image layout above) of C piece p of an x tile: p = 0 hi kc 0, 1 lo kc 0, 2 hi kc 1, 3 lo kc 1.
+__host__ __device__ constexpr int piece_block(int p) { return (p & 1) * 2 + (p >> 1); }
+
+// Drain accumulator `buf` (item: pair P, x tile j): lanes = x of this warp's quarter, columns 128 half ..
+// 128 half + 127 = rows of row block 2 P + half, stored as coalesced 128-byte row segments.
 __device__ __forceinline__ void inv_drain(const InvArgs& a, uint32_t taddr, uint32_t acce, int half, int warp,
-                                          int lane, long long j, long long r, int buf) {
+                                          int lane, int j, long long rb, bool store, int buf) {
   fence_after();
-  float* dst = a.out + (r * 128 + 64 * half) * (long long)a.nx + j * 128 + 32 * (warp & 3) + lane;
+  if (store) {
+    float* dst = a.out + rb * 128 * (long long)a.nx + j * 128 + 32 * (warp & 3) + lane;
+    const uint32_t col = taddr + buf * I_ACC + 128 * half;
+#pragma unroll 1
+    for (int p = 0; p < 4; ++p) {
+      float o0[16], o1[16];
+      tmem_ld16x2(col + 32 * p, col + 32 * p + 16, o0, o1);
 #pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    float o0[16], o1[16];
-    tmem_ld16x2(taddr + buf * ACC_COLS + 64 * half + 32 * p, taddr + buf * ACC_COLS + 64 * half + 32 * p + 16, o0,
-                o1);
+      for (int k = 0; k < 16; ++k) __stcs(dst + (long long)(32 * p + k) * a.nx, o0[k]);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) __stcs(dst + (long long)(32 * p + k) * a.nx, o0[k]);
-#pragma unroll
-    for (int k = 0; k < 16; ++k) __stcs(dst + (long long)(32 * p + 16 + k) * a.nx, o1[k]);
+      for (int k = 0; k < 16; ++k) __stcs(dst + (long long)(32 * p + 16 + k) * a.nx, o1[k]);
+    }
   }
   fence_before();
   __syncwarp();
   if (lane == 0) arrive(acce + 8 * buf);
 }
 
-// Items (x tile j, row block r), j-major, cut into one contiguous range per CTA.  Producer: the C tile when the x
-// tile changes, V tiles into two slots; MMA: D[buf] = C x V^T (24 MMAs of 128 x 128 x 16); warps 0-7 drain.
-__global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a) {
+// Wait (bounded) for the last copies of a ring of n slots whose cursor is `c` after `g` issued copies.
+__device__ __forceinline__ void drain_ring(uint32_t full, const Ring& c, int g, int n) {
+  const int last = g < n ? g : n;
+  for (int k = 1; k <= last; ++k) {
+    const int s = (c.slot - k + n) % n;
+    wait_bar(full + 8 * s, s < c.slot ? c.phase : c.phase ^ 1u);
+  }
+}
+
+// Producers: warp 8 the C pieces of every item, warp 10 the V tiles of every pair (after the MMAs of the previous
+// pair have finished).  MMA (warp 9): D[acc] = C x V^T, per C piece the MMAs that read it (C hi: hi x V hi and
+// hi x V lo; C lo: lo x V hi), 24 of 128 x 256 x 16 per item, both operands from shared memory.  Warps 0-7 drain.
+// The C and V images are read through 2-D tensor maps over their 128-byte rows (uint16, no swizzle: the images
+// are stored pre-swizzled, so a box lands in shared memory exactly as the operand layout wants it), one box of
+// 128 rows per 16 KB block.
+__global__ void __launch_bounds__(I_NT, 1) rows_inv_tc_kernel(InvArgs a, const __grid_constant__ CUtensorMap c_map,
+                                                               const __grid_constant__ CUtensorMap v_map) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* gbase = smem_raw + (base - raw);
   const uint32_t misc = base + I_MISC;
-  // barriers: vfull[2] (V tile landed), vdone[2] (MMAs reading the slot finished = accumulator complete),
-  // cxb (C tile landed), acce[2] (accumulator drained)
-  const uint32_t vfull = misc, vdone = misc + 16, cxb = misc + 32, acce = misc + 40;
-  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + I_MISC + 96);
+  // barriers: cfull[6] (piece landed), cfree[6] (MMAs reading the piece finished), vfull (V tiles landed), vfree
+  // (MMAs reading the V tiles finished), accf[2] (accumulator complete), acce[2] (accumulator drained), fin (MMAs
+  // finished, failure path)
+  const uint32_t cfull = misc, cfree = misc + 48, vfull = misc + 96, vfree = misc + 104, accf = misc + 112,
+                 acce = misc + 128, fin = misc + 144;
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + I_MISC + 256);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long long R = a.rows / 128;                // row blocks
-  const long long items = (long long)(a.nx / 128) * R;
+  const int JT = a.nx / 128;                       // x tiles
+  const long long R = a.rows / 128, PR = (R + 1) / 2;
+  const long long items = PR * JT;
   const long long G = gridDim.x;
   const long long i0 = (long long)blockIdx.x * items / G, i1 = ((long long)blockIdx.x + 1) * items / G;
   const long long N = i1 - i0;
 
-  if (warp == 0) tmem_alloc(misc + 96, TMEM_COLS);
+  if (warp == 0) tmem_alloc(misc + 256, I_TMEM_COLS);
   if (tid == 0) {
+    for (int s = 0; s < I_NC; ++s) {
+      mbar_init(cfull + 8 * s, 1);
+      mbar_init(cfree + 8 * s, 1);
+    }
     for (int s = 0; s < 2; ++s) {
-      mbar_init(vfull + 8 * s, 1);
-      mbar_init(vdone + 8 * s, 1);
+      mbar_init(accf + 8 * s, 1);
       mbar_init(acce + 8 * s, 8);
     }
-    mbar_init(cxb, 1);
+    mbar_init(vfull, 1);
+    mbar_init(vfree, 1);
+    mbar_init(fin, 1);
     mbar_init_fence();
   }
   fence_before();
@@ -438,78 +477,116 @@ __global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a) {
   fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  // item i0 + n = (x tile j, row block r); counters advance per item (the x tile changes exactly when r wraps)
-  const long long j0 = i0 / R, r0 = i0 - j0 * R;
+  // item i0 + n = (pair P, x tile j); counters advance per item (the pair changes exactly when j wraps)
+  const long long P0 = i0 / JT;
+  const int j0 = (int)(i0 - P0 * JT);
   if (warp == 8) {
+    // ---- C pieces: piece g of the range into ring slot g % 6 once the MMAs of piece g-6 have finished
     if (lane == 0) {
-      long long j = j0, r = r0;
-      for (long long n = 0; n < N; ++n) {
-        const int s = (int)(n & 1);
-        const bool reload = n == 0 || r == 0;
-        bool ok = true;
-        if (n >= 2) ok = wait_bar(vdone + 8 * s, (uint32_t)(((n - 2) >> 1) & 1));           // slot free
-        if (ok && reload && n >= 1) ok = wait_bar(vdone + 8 * ((n - 1) & 1), (uint32_t)(((n - 1) >> 1) & 1));
-        if (!ok) {
-          fail_status();
+      Ring cs{0, 0};
+      int j = j0, g = 0;
+      bool ok = true;
+      for (long long n = 0; n < N && ok; ++n) {
+        for (int p = 0; p < 4; ++p, ++g) {
+          if (g >= I_NC && !wait_bar(cfree + 8 * cs.slot, cs.phase ^ 1u)) {
+            ok = false;
+            break;
+          }
+          expect_tx(cfull + 8 * cs.slot, OPER);
+          tma_load_2d(base + I_C + cs.slot * OPER, &c_map, 0, (j * 4 + piece_block(p)) * 128, cfull + 8 * cs.slot);
+          cs.next(I_NC);
+        }
+        if (++j == JT) j = 0;
+      }
+      if (!ok) fail_status();
+      drain_ring(cfull, cs, g, I_NC);   // the copies in flight land before shared memory is released
+    }
+  } else if (warp == 10) {
+    // ---- V tiles of pair k of the range, once the MMAs of pair k-1 have finished
+    if (lane == 0) {
+      const long long npairs = N > 0 ? (i1 - 1) / JT - P0 + 1 : 0;
+      int k = 0;
+      bool ok = true;
+      for (; k < npairs; ++k) {
+        if (k >= 1 && !wait_bar(vfree, (uint32_t)((k - 1) & 1))) {
+          ok = false;
           break;
         }
-        if (reload) {   // the previous C tile is no longer read
-          expect_tx(cxb, 4 * OPER);
-          for (int q = 0; q < 4; ++q) bulk_g2s(base + I_CX + q * OPER, a.c + j * 4 * OPER + q * OPER, OPER, cxb);
-        }
-        expect_tx(vfull + 8 * s, VT_BYTES);
+        expect_tx(vfull, 8 * OPER);
+        const long long rb = 2 * (P0 + k);
         for (int q = 0; q < 4; ++q)
-          bulk_g2s(base + I_V + s * VT_BYTES + q * OPER, a.vt + r * VT_BYTES + q * OPER, OPER, vfull + 8 * s);
-        if (++r == R) {
-          r = 0;
-          ++j;
-        }
+          for (int h = 0; h < 2; ++h)   // rows past the tensor's end read as zeros
+            tma_load_2d(base + I_V + (2 * q + h) * OPER, &v_map, 0, (int)(((rb + h) * 4 + q) * 128), vfull);
       }
+      if (!ok) fail_status();
+      if (k > 0) wait_bar(vfull, (uint32_t)((k - 1) & 1));   // the last tiles have landed
     }
   } else if (warp == 9) {
     if (lane == 0) {
-      constexpr uint32_t ID = idesc(128, false);
-      int reloads = 0;
-      long long r = r0;
-      for (long long n = 0; n < N; ++n) {
-        const int s = (int)(n & 1), buf = s;
-        const bool reload = n == 0 || r == 0;
-        if (++r == R) r = 0;
-        bool ok = wait_bar(vfull + 8 * s, (uint32_t)((n >> 1) & 1));
-        if (ok && reload) ok = wait_bar(cxb, (uint32_t)(reloads & 1));
-        if (ok && n >= 2) ok = wait_bar(acce + 8 * buf, (uint32_t)(((n - 2) >> 1) & 1));
-        if (!ok) {
-          fail_status();
-          break;
+      constexpr uint32_t ID = idesc(I_ACC, false);
+      Ring cs{0, 0}, ab{0, 0};
+      uint32_t vph = 0;
+      int j = j0;
+      bool ok = true;
+      int issued = 0;
+      for (long long n = 0; n < N && ok; ++n) {
+        if (n == 0 || j == 0) {   // a new pair: release the previous V tiles, wait for this pair's
+          if (n > 0) commit(vfree);
+          ok = wait_bar(vfull, vph);
+          vph ^= 1u;
         }
-        if (reload) ++reloads;
-        fence_after();
-        const uint32_t d = tmem + buf * ACC_COLS, vb = base + I_V + s * VT_BYTES;
+        if (++j == JT) j = 0;
+        if (ok && n >= 2) ok = wait_bar(acce + 8 * ab.slot, ab.phase ^ 1u);
+        const uint32_t d = tmem + ab.slot * I_ACC;
+        for (int p = 0; p < 4 && ok; ++p) {
+          ok = wait_bar(cfull + 8 * cs.slot, cs.phase);
+          if (!ok) break;
+          fence_after();
+          const uint32_t cp = base + I_C + cs.slot * OPER;
+          const uint32_t vhi = base + I_V + (uint32_t)(p >> 1) * 2 * OPER, vlo = vhi + 4 * OPER;
+          if ((p & 1) == 0) {
 #pragma unroll
-        for (int ks = 0; ks < 8; ++ks) {
-          const uint32_t ko = (uint32_t)(ks >> 2) * OPER + 32 * (ks & 3);
-          const uint32_t ah = base + I_CX + ko, al = ah + 2 * OPER;
-          const uint32_t bh = vb + ko, bl = bh + 2 * OPER;
-          mma_ss(d, sdesc(ah), sdesc(bh), ID, ks ? 1u : 0u);   // hi hi
-          mma_ss(d, sdesc(ah), sdesc(bl), ID, 1);              // hi lo
-          mma_ss(d, sdesc(al), sdesc(bh), ID, 1);              // lo hi
+            for (int ks = 0; ks < 4; ++ks) {
+              mma_ss(d, sdesc(cp + 32 * ks), sdesc(vhi + 32 * ks), ID, (p | ks) ? 1u : 0u);   // hi hi
+              mma_ss(d, sdesc(cp + 32 * ks), sdesc(vlo + 32 * ks), ID, 1);                    // hi lo
+            }
+          } else {
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) mma_ss(d, sdesc(cp + 32 * ks), sdesc(vhi + 32 * ks), ID, 1);   // lo hi
+          }
+          issued = 1;
+          commit(cfree + 8 * cs.slot);
+          cs.next(I_NC);
         }
-        commit(vdone + 8 * s);
+        if (!ok) break;
+        commit(accf + 8 * ab.slot);
+        ab.next(2);
+      }
+      if (!ok) {
+        fail_status();
+        if (issued) {   // every MMA issued has finished before tensor memory is released
+          commit(fin);
+          wait_bar(fin, 0);
+        }
       }
     }
-  } else {
-    // ---- warps 0-7: drain each finished accumulator
-    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
+  } else if (warp < 8) {
+    // ---- warps 0-7: drain each finished accumulator (warps 0-3 the pair's first row block, 4-7 its second)
+    const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
     const int half = warp >> 2;
+    Ring ab{0, 0};
+    long long P = P0;
+    int j = j0;
     bool ok = true;
-    long long j = j0, r = r0;
     for (long long n = 0; n < N && ok; ++n) {
-      const int buf = (int)(n & 1);
-      ok = warp_wait(vdone + 8 * buf, (uint32_t)((n >> 1) & 1));
-      if (ok) inv_drain(a, tmem + lane_base, acce, half, warp, lane, j, r, buf);
-      if (++r == R) {
-        r = 0;
-        ++j;
+      ok = warp_wait(accf + 8 * ab.slot, ab.phase);
+      if (!ok) break;
+      const long long rb = 2 * P + half;
+      inv_drain(a, taddr, acce, half, warp, lane, j, rb, rb < R, ab.slot);
+      ab.next(2);
+      if (++j == JT) {
+        j = 0;
+        ++P;
       }
     }
     if (!ok && lane == 0) fail_status();
@@ -518,7 +595,7 @@ __global__ void __launch_bounds__(NT, 1) rows_inv_tc_kernel(InvArgs a) {
   __syncthreads();
   if (warp == 0) {
     fence_after();
-    tmem_dealloc(tmem, TMEM_COLS);
+    tmem_dealloc(tmem, I_TMEM_COLS);
   }
 }
 
@@ -668,14 +745,19 @@ extern "C" int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, in
 namespace oi {
 
 int rows_inv_from_tiles(const void* vtiles, int count, int ny, int nx, const void* consts, float* out, cudaStream_t s) {
-  const long long rows = (long long)count * ny, R = rows / 128, items = (long long)(nx / 128) * R;
+  const long long rows = (long long)count * ny, R = rows / 128, items = (long long)(nx / 128) * ((R + 1) / 2);
   const int sms = rt::sm_count();
   if (!sms) return fail(OI_ECUDA, "oi_rows_inv_tc: no CUDA device");
+  if ((R + 1) * 512 > 0x7fffffffLL) return fail(OI_ERANGE, "oi_rows_inv_tc: %lld rows exceed the tensor-map range", rows);
   const long long ctas = items < sms ? items : sms;
   rt::InvArgs a{(const unsigned char*)vtiles, rows, ny, nx, (const unsigned char*)consts, out};
-  int rc = ensure_smem((const void*)rt::rows_inv_tc_kernel, rt::I_SMEM, "oi_rows_inv_tc");
+  CUtensorMap c_map, v_map;   // [rows of 128 bytes] of the constant image and of the V tiles
+  int rc = rt::encode_2d(&c_map, CU_TENSOR_MAP_DATA_TYPE_UINT16, consts, 64, (unsigned long long)(nx / 128) * 512, 128,
+                         64, 128);
+  if (!rc) rc = rt::encode_2d(&v_map, CU_TENSOR_MAP_DATA_TYPE_UINT16, vtiles, 64, (unsigned long long)R * 512, 128, 64, 128);
+  if (!rc) rc = ensure_smem((const void*)rt::rows_inv_tc_kernel, rt::I_SMEM, "oi_rows_inv_tc");
   if (rc) return rc;
-  rt::rows_inv_tc_kernel<<<(unsigned)ctas, rt::NT, rt::I_SMEM, s>>>(a);
+  rt::rows_inv_tc_kernel<<<(unsigned)ctas, rt::I_NT, rt::I_SMEM, s>>>(a, c_map, v_map);
   oi::note_launch();
   return check_launch("oi_rows_inv_tc");
 }

@@ -167,3 +167,29 @@ def test_tc_row_passes_vs_fft(oi, ny, nx, band):
     print(f'{ny}x{nx}: band max {rel_err(got, want):.2e}, image max {rel_err(img, ref):.2e} rms {rms_rel(img, ref):.2e}')
     assert rel_err(img, ref) < BF16X3_VS_FP64
     assert N.device_status() == 0
+
+
+@pytest.mark.parametrize('count,ny,nx,bc', [(1, 128, 256, 40), (7, 640, 2048, 33), (5, 1024, 1024, 59)])
+def test_rows_inv_tc_direct(oi, count, ny, nx, bc):
+    """The inverse tensor-core row pass through the C ABI against an FP64 evaluation of
+    out[i][y][x] = sum_qc Re(v[i][qc][y] exp(-2 pi i qc x / nx)): an odd number of 128-row blocks (the last pair of
+    row blocks half empty), more items than CTAs with ranges crossing pairs, and one item per CTA."""
+    from opticalimaging_b200 import _native as N
+    dev = torch.device('cuda')
+    g = torch.Generator().manual_seed(count * ny + nx)
+    v = torch.randn((count, bc, ny), dtype=torch.complex64, generator=g)
+    s = N.stream_handle(dev)
+    consts = torch.empty((nx // 128) * 65536, dtype=torch.uint8, device=dev)
+    N.call('oi_rows_tc_constants', 1, nx, 0, bc, N.ptr(consts), consts.numel(), s)
+    vd = v.to(dev)
+    tiles = torch.empty(count * ny * 512, dtype=torch.uint8, device=dev)
+    out = torch.full((count, ny, nx), float('nan'), device=dev)
+    N.call('oi_rows_inv_tc', N.ptr(vd), count, ny, nx, bc, N.ptr(consts), N.ptr(tiles), N.ptr(out), s)
+    got = out.cpu().numpy()
+    E = np.exp(-2j * np.pi * np.outer(np.arange(bc), np.arange(nx)) / nx)
+    vv = v.numpy().astype(np.complex128)
+    want = np.stack([np.real(vv[i].T @ E) for i in range(count)])
+    err, rms = rel_err(got, want), rms_rel(got, want)
+    print(f'inverse rows {count}x{ny}x{nx} bc {bc}: max {err:.2e} rms {rms:.2e}')
+    assert err < BF16X3_VS_FP64
+    assert N.device_status() == 0
