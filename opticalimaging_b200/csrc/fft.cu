@@ -298,7 +298,8 @@ __global__ void __launch_bounds__(G * N1) cols_inv_tiles_kernel(const float2* __
   const float2* t1 = wn_g + 32 * N1;
   const int nq = 2 * br - 1;
   float2* cs = (float2*)smem_raw;                        // [G][nq]
-  float2* vs = cs + ((G * nq + 1) & ~1);                 // [N][G] (16-byte aligned)
+  float2* vs = cs + ((G * nq + 1) & ~1);                 // [G][N / 2]: one half of the rows, column-major so that
+                                                         // consecutive lanes (rows) hit consecutive banks
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
   const long long i = blockIdx.y;
   const int qc0 = blockIdx.x * G;
@@ -309,37 +310,54 @@ __global__ void __launch_bounds__(G * N1) cols_inv_tiles_kernel(const float2* __
   __syncthreads();
   float2 z[32];
   inverse_gather<N1>(z, cs + g * nq, br - 1, t2, t1, n1);
+  // z[k] is row n1 + N1 bitrev5(k): even k give the first half of the rows, odd k the second.  The rows are
+  // transposed through shared memory one half at a time (half the buffer: more blocks per SM, one wave).
 #pragma unroll
-  for (int k = 0; k < 32; ++k) vs[(n1 + N1 * bitrev5(k)) * G + g] = z[k];
-  __syncthreads();
-  for (int it = tid; it < N * (G / 8); it += T) {
-    const int y = it % N, gq = it / N, q = (qc0 >> 3) + gq;
-    const float4* src = (const float4*)(vs + y * G + 8 * gq);
-    float re[8], im[8];
+  for (int h = 0; h < 2; ++h) {
+    if (h) __syncthreads();   // the first half has been stored
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const float4 x = src[e];
-      re[2 * e] = x.x, im[2 * e] = x.y, re[2 * e + 1] = x.z, im[2 * e + 1] = x.w;
+    for (int k = h; k < 32; k += 2) vs[g * (N / 2) + n1 + N1 * (bitrev5(k) - 16 * h)] = z[k];
+    __syncthreads();
+    // QPT band columns per store: 8 (one 16-byte chunk of the bf16 row) or, for G = 4, 4 (half a chunk)
+    constexpr int QPT = G < 8 ? G : 8;
+    for (int it = tid; it < (N / 2) * (G / QPT); it += T) {
+      const int yh = it % (N / 2), gq = it / (N / 2), y = yh + h * (N / 2);
+      const int qf = qc0 + QPT * gq, q = qf >> 3;
+      const float2* src = vs + (QPT * gq) * (N / 2) + yh;
+      float re[QPT], im[QPT];
+#pragma unroll
+      for (int e = 0; e < QPT; ++e) {
+        const float2 x = src[e * (N / 2)];
+        re[e] = x.x, im[e] = x.y;
+      }
+      uint32_t rh[QPT / 2], rl[QPT / 2], ih[QPT / 2], il[QPT / 2];
+#pragma unroll
+      for (int e = 0; e < QPT / 2; ++e) {
+        tc::split2(re[2 * e], re[2 * e + 1], rh[e], rl[e]);
+        tc::split2(im[2 * e], im[2 * e + 1], ih[e], il[e]);
+      }
+      const long long row = i * ny + y;
+      unsigned char* o = tiles + (row >> 7) * TILE + tc::swz((int)(row & 127), q);
+      if constexpr (QPT == 8) {
+        *(uint4*)o = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+        *(uint4*)(o + OPER) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+        *(uint4*)(o + 2 * OPER) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+        *(uint4*)(o + 3 * OPER) = make_uint4(il[0], il[1], il[2], il[3]);
+      } else {
+        o += 2 * (qf & 7);   // the half of the chunk holding band columns qf .. qf + 3
+        *(uint2*)o = make_uint2(rh[0], rh[1]);
+        *(uint2*)(o + OPER) = make_uint2(ih[0], ih[1]);
+        *(uint2*)(o + 2 * OPER) = make_uint2(rl[0], rl[1]);
+        *(uint2*)(o + 3 * OPER) = make_uint2(il[0], il[1]);
+      }
     }
-    uint32_t rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      tc::split2(re[2 * e], re[2 * e + 1], rh[e], rl[e]);
-      tc::split2(im[2 * e], im[2 * e + 1], ih[e], il[e]);
-    }
-    const long long row = i * ny + y;
-    unsigned char* o = tiles + (row >> 7) * TILE + tc::swz((int)(row & 127), q);
-    *(uint4*)o = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-    *(uint4*)(o + OPER) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-    *(uint4*)(o + 2 * OPER) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-    *(uint4*)(o + 3 * OPER) = make_uint4(il[0], il[1], il[2], il[3]);
   }
 }
 
 template <int N1, int G>
 static int cols_inv_tiles(const float2* ihat, int count, int br, int bc, int ny, const float2* wn_y,
                           unsigned char* tiles, cudaStream_t s) {
-  const size_t smem = sizeof(float2) * (((size_t)G * (2 * br - 1) + 1) & ~(size_t)1) + sizeof(float2) * 32 * N1 * G;
+  const size_t smem = sizeof(float2) * (((size_t)G * (2 * br - 1) + 1) & ~(size_t)1) + sizeof(float2) * 16 * N1 * G;
   int rc = set_smem(cols_inv_tiles_kernel<N1, G>, smem, "oi_coarse_to_image_tc/cols");
   if (rc) return rc;
   dim3 grid(64 / G, (unsigned)count);
@@ -403,10 +421,12 @@ __global__ void __launch_bounds__(256, 3) fft_rows_inv_kernel(const float2* __re
 }
 
 // --------------------------------------------------------------- coarse intensity -> its spectrum
-// Two blocks per coarse image, each for half of the band columns qc (mr = 32 N1R, mc = 32 N1C, each 64 or 128):
+// COARSE_PARTS blocks per coarse image, each for a range of the band columns qc (mr = 32 N1R, mc = 32 N1C, each
+// 64 or 128; U holds the block's columns only, so that two blocks fit an SM):
 //   ihat[i][jr][qc] = (qc ? 2 : 1) / (mr mc) * sum_{sr,sc} coarse[i][sr][sc] exp(+2 pi i (qr sr/mr + qc sc/mc))
 // for qr = jr - (br-1) in [-(br-1), br-1] and qc in [0, bc).  Row FFTs of the real image in pairs (two rows per
 // complex transform), the band bins of each separated into U[sr][qc]; then column FFTs of U at the qr bins.
+constexpr int COARSE_PARTS = 2;
 template <int N1R, int N1C>
 __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __restrict__ coarse, int nparts,
                                                               long long part_stride, int br, int bc,
@@ -420,7 +440,7 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
   float2* c2 = r1 + N1R * N1R;         // column-axis (MC) tables: [32][N1C], [N1C][N1C]
   float2* c1t = c2 + 32 * N1C;
   float2* area = c1t + N1C * N1C;      // [area_f2] union: coarse image / row transposes / column transposes
-  float2* u = area + area_f2;          // [MR][bc]
+  float2* u = area + area_f2;          // [MR][cw]: this block's band columns
   const int tid = threadIdx.x;
   const long long img = blockIdx.x;
   // this block's band columns: blockIdx.y-th of gridDim.y equal ranges of [0, bc)
@@ -466,8 +486,8 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
     const float2* ys = area + pp * 32 * (N1C + 1);
     const float2 zp = outer_bin<+1, N1C>(ys, c1t, qc & (MC - 1));
     const float2 zm = outer_bin<+1, N1C>(ys, c1t, (-qc) & (MC - 1));
-    u[(2 * pp) * bc + qc] = make_float2(0.5f * (zp.x + zm.x), 0.5f * (zp.y - zm.y));
-    u[(2 * pp + 1) * bc + qc] = make_float2(0.5f * (zp.y + zm.y), -0.5f * (zp.x - zm.x));
+    u[(2 * pp) * cw + qc - c0] = make_float2(0.5f * (zp.x + zm.x), 0.5f * (zp.y - zm.y));
+    u[(2 * pp + 1) * cw + qc - c0] = make_float2(0.5f * (zp.y + zm.y), -0.5f * (zp.x - zm.x));
   }
   __syncthreads();
   // column pass: column qc of U, thread n1r
@@ -475,7 +495,7 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
   const bool col_task = qc < c1;
   if (col_task) {
 #pragma unroll
-    for (int n2 = 0; n2 < 32; ++n2) z[n2] = u[(n1r + N1R * n2) * bc + qc];
+    for (int n2 = 0; n2 < 32; ++n2) z[n2] = u[(n1r + N1R * n2) * cw + qc - c0];
     fft32<+1>(z);
   }
   __syncthreads();  // row transposes are consumed; the area now holds column transposes
@@ -495,14 +515,15 @@ template <int N1R, int N1C>
 static int launch_coarse_spec_fft(float* coarse, int nparts, int count, int br, int bc, const float2* wr,
                                   const float2* wc, float2* ihat, cudaStream_t s) {
   constexpr int MR = 32 * N1R, MC = 32 * N1C;
-  const int rows_ys = (MR / 2) * 32 * (N1C + 1), c_f2 = MR * MC / 2, cols_ys = bc * 32 * (N1R + 1);
+  const int cw = (bc + COARSE_PARTS - 1) / COARSE_PARTS;   // band columns per block (as in the kernel)
+  const int rows_ys = (MR / 2) * 32 * (N1C + 1), c_f2 = MR * MC / 2, cols_ys = cw * 32 * (N1R + 1);
   const int area_f2 = max(rows_ys, max(c_f2, cols_ys));
-  const size_t smem = sizeof(float2) * ((size_t)table_f2<N1R>() + table_f2<N1C>() + area_f2 + (size_t)MR * bc);
+  const size_t smem = sizeof(float2) * ((size_t)table_f2<N1R>() + table_f2<N1C>() + area_f2 + (size_t)MR * cw);
   auto kern = coarse_spec_fft_kernel<N1R, N1C>;
   int rc = set_smem(kern, smem, "coarse spectrum fft");
   if (rc) return rc;
-  kern<<<dim3((unsigned)count, 2), 512, smem, s>>>(coarse, nparts, (long long)count * MR * MC, br, bc, wr, wc,
-                                                   area_f2, ihat);
+  kern<<<dim3((unsigned)count, COARSE_PARTS), 512, smem, s>>>(coarse, nparts, (long long)count * MR * MC, br, bc, wr,
+                                                              wc, area_f2, ihat);
   oi::note_launch();
   return check_launch("coarse spectrum fft");
 }
