@@ -385,7 +385,7 @@ def cpu_reference_sample(sk_info, masks_np, budget_s, threads):
 
 # DRAM bytes per launch (read + write) of the three largest kernels at this workload, from the ncu capture
 # summarised in profiles/socs24-1024-bf16x3-step.md
-NCU_TRAFFIC = {"rows_fwd_tc": 286.2e6, "v_tiles+rows_inv_tc": 300.3e6, "coherent_tc": 2.6e6}
+NCU_TRAFFIC = {"rows_fwd_tc": 289.7e6, "rows_inv_tc": 247.9e6, "coherent_tc": 2.6e6}
 
 
 def kernel_rooflines(sk, masks, reps=10):
@@ -412,9 +412,11 @@ def kernel_rooflines(sk, masks, reps=10):
         "coherent_tc": lambda: N.call('oi_coherent_coarse_tc', N.ptr(band), B, 1, b.m0r, b.br, b.m0c, b.bc,
                                       N.ptr(sk.pupils), 0, N.ptr(sk.weights), 1, sk.count,
                                       N.ptr(tplan.tc_constants()), ctas, nparts, N.ptr(coarse), s),
-        "v_tiles+rows_inv_tc": lambda: N.call('oi_rows_inv_tc', N.ptr(v), B, sk.ny, sk.nx, b.bc, N.ptr(tplan.rows_consts(1)),
-                                      N.ptr(tiles), N.ptr(out), s),
+        "rows_inv_tc": lambda: N.call('oi_rows_inv_tc_tiles', N.ptr(tiles), B, sk.ny, sk.nx,
+                                      N.ptr(tplan.rows_consts(1)), N.ptr(out), s),
     }
+    # operand tiles for the synthesis row pass (the image path writes them in its column pass)
+    N.call('oi_rows_inv_tc', N.ptr(v), B, sk.ny, sk.nx, b.bc, N.ptr(tplan.rows_consts(1)), N.ptr(tiles), N.ptr(out), s)
     px = B * sk.ny * sk.nx
     res = {}
     for name, fn in calls.items():
@@ -440,8 +442,7 @@ def kernel_rooflines(sk, masks, reps=10):
             res[name] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                          "traffic": NCU_TRAFFIC[name], "us": sec * 1e6, "peak_source": src,
                          "algorithmic": "4 bytes per pixel: the float32 mask read" if name == "rows_fwd_tc"
-                         else "4 bytes per pixel: the float32 image written (the call converts v to operand tiles "
-                         "first: two kernels)"}
+                         else "4 bytes per pixel: the float32 image written"}
     res["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch (profiles/)"
     return res
 

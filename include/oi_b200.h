@@ -216,6 +216,10 @@ OI_API int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, int nx
                           const void* consts, void* t, void* stream);
 OI_API int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, const void* consts, void* vtiles,
                           float* out, void* stream);
+/* The synthesis row pass alone, from V operand tiles already written (by oi_rows_inv_tc's conversion or by the
+ * column pass of oi_coarse_to_image_tc): the second half of oi_rows_inv_tc. */
+OI_API int oi_rows_inv_tc_tiles(const void* vtiles, int count, int ny, int nx, const void* consts, float* out,
+                                void* stream);
 OI_API int oi_band_spectrum_tc(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c,
                                int bc, const void* wconsts, const void* wn_y, float scale, void* scratch,
                                void* band, void* stream);

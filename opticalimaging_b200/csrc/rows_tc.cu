@@ -764,6 +764,17 @@ int rows_inv_from_tiles(const void* vtiles, int count, int ny, int nx, const voi
 
 }  // namespace oi
 
+extern "C" int oi_rows_inv_tc_tiles(const void* vtiles, int count, int ny, int nx, const void* consts, float* out,
+                                    void* stream) {
+  using namespace oi;
+  if (!vtiles || !consts || !out || count <= 0) return fail(OI_EINVAL, "oi_rows_inv_tc_tiles: bad arguments");
+  if (ny % 128 != 0 || nx % 128 != 0 || nx > 4096)
+    return fail(OI_ERANGE, "oi_rows_inv_tc_tiles: grid %dx%d unsupported", ny, nx);
+  if ((uintptr_t)consts % 16 || (uintptr_t)vtiles % 16)
+    return fail(OI_EINVAL, "oi_rows_inv_tc_tiles: constants and V tiles must be 16-byte aligned");
+  return rows_inv_from_tiles(vtiles, count, ny, nx, consts, out, (cudaStream_t)stream);
+}
+
 extern "C" int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, const void* consts, void* vtiles,
                               float* out, void* stream) {
   using namespace oi;
