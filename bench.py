@@ -7,7 +7,8 @@ the vector TCC of an annular 0.7/0.95 source (PntNum 41).  Kernels are built onc
 eigendecomposition, reported as `setup_s`) and stay resident, as they do in serving.
 
   value  images/s with the masks already in HBM (256 MB of float32 masks per step: larger than L2)
-  e2e    images/s through the public batched API from pinned host uint8 masks to host float32 images,
+  e2e    images/s through the public host-buffer API (SocsKernels.image_host) from pinned host uint8 masks to
+         pinned host float32 images,
          host<->device copies inside the timed region
   serving  the same clips as requests through the continuous-batching server, against the plain FP32 path
          (one request at a time), with p50/p99 latency
@@ -552,10 +553,8 @@ def run_engine(args, world, rank, local):
     host_in = torch.from_numpy(masks_np.astype(np.uint8)).pin_memory()
     host_out = torch.empty((BATCH, N_PIX, N_PIX), dtype=torch.float32).pin_memory()
 
-    def e2e_step():
-        d_in = host_in.to(dev, non_blocking=True)
-        img = sk.image(d_in, out=out, form=args.form)
-        host_out.copy_(img, non_blocking=True)
+    def e2e_step():   # host masks in, host images out: copies of neighbouring chunks overlap the compute
+        sk.image_host(host_in, host_out, form=args.form)
 
     for _ in range(max(args.warmup, 3)):
         e2e_step()

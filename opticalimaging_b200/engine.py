@@ -423,6 +423,56 @@ class CoherentModel:
         return coherent_image(band, self.pupils, self.weights, self.plan, out=out, marks=marks, form=form)
 
 
+    def image_host(self, masks: torch.Tensor, out: torch.Tensor, chunk: int = 16, **kw) -> torch.Tensor:
+        """image() of a batch held in pinned host memory, written into the pinned host tensor `out` (shaped as
+        image() returns it).  The batch is cut into chunks of `chunk` masks; each chunk's copy to the device,
+        its images and the copy of its result back run on three streams (copy-in, the current stream, copy-out)
+        with events between them, over three rotating device buffer sets kept by the model, so the copies of
+        neighbouring chunks -- also across consecutive calls -- overlap each other and the compute; the host
+        link then bounds the path.  The current stream waits for the last copy-out before the call returns, so
+        synchronising it (or an event recorded on it) covers the results.  Keyword arguments go to image()."""
+        if masks.is_cuda or out.is_cuda:
+            raise ValueError('image_host takes host tensors (image() takes device tensors)')
+        if not masks.is_pinned() or not out.is_pinned():
+            raise ValueError('image_host needs pinned host memory for masks and out')
+        if out.shape[0] != masks.shape[0] or out.dtype != torch.float32 or not out.is_contiguous():
+            raise ValueError('out must be a contiguous float32 host tensor with one image (set) per mask')
+        if chunk <= 0:
+            raise ValueError('chunk must be positive')
+        dev = self.device
+        key = (chunk, masks.dtype, tuple(masks.shape[1:]), tuple(out.shape[1:]))
+        pipe = getattr(self, '_host_pipe', None)
+        if pipe is None or pipe['key'] != key:
+            pipe = {'key': key, 'h2d': torch.cuda.Stream(dev), 'd2h': torch.cuda.Stream(dev), 'next': 0,
+                    'slots': [{'d_in': torch.empty((chunk,) + tuple(masks.shape[1:]), dtype=masks.dtype, device=dev),
+                               'd_out': torch.empty((chunk,) + tuple(out.shape[1:]), dtype=torch.float32, device=dev),
+                               'in_done': torch.cuda.Event(), 'comp_done': torch.cuda.Event(),
+                               'out_done': torch.cuda.Event()} for _ in range(3)]}
+            self._host_pipe = pipe
+        cur = torch.cuda.current_stream(dev)
+        masks = masks.contiguous()
+        for s0 in range(0, masks.shape[0], chunk):
+            c = min(chunk, masks.shape[0] - s0)
+            slot = pipe['slots'][pipe['next']]
+            pipe['next'] = (pipe['next'] + 1) % 3
+            with torch.cuda.stream(pipe['h2d']):
+                pipe['h2d'].wait_event(slot['comp_done'])     # the slot's previous chunk has been read
+                slot['d_in'][:c].copy_(masks[s0:s0 + c], non_blocking=True)
+                slot['in_done'].record(pipe['h2d'])
+            cur.wait_event(slot['in_done'])
+            cur.wait_event(slot['out_done'])                  # the slot's previous result has been copied out
+            self.image(slot['d_in'][:c], out=slot['d_out'][:c], **kw)
+            slot['comp_done'].record(cur)
+            with torch.cuda.stream(pipe['d2h']):
+                pipe['d2h'].wait_event(slot['comp_done'])
+                out[s0:s0 + c].copy_(slot['d_out'][:c], non_blocking=True)
+                slot['out_done'].record(pipe['d2h'])
+        done = torch.cuda.Event()
+        done.record(pipe['d2h'])
+        cur.wait_event(done)
+        return out
+
+
 class SocsKernels(CoherentModel):
     """SOCS kernels of one focus plane resident on the device in band form: [K, br, bc] complex64.
 

@@ -219,3 +219,27 @@ def test_gram_kernels_match_tcc_kernels(oi, order, threshold):
     b = full.image(masks).cpu().numpy()
     assert rel_err(a, b) < 2e-6
     assert N.device_status() == 0
+
+
+@pytest.mark.parametrize('form,tol', [('fft', 1e-6), ('bf16x3', 5e-5)])
+def test_image_host_matches_device_image(oi, form, tol):
+    """image_host (pinned host masks in, pinned host images out, chunked over three streams) gives the images
+    of image() on device masks: bit-identical per image for the FFT form up to float rounding of the batch split,
+    within the split form's batch-composition tolerance for BF16x3; twice in a row (rotating buffer slots), with
+    a ragged last chunk."""
+    from opticalimaging_b200 import workloads as W
+    sr, po, nm = W.config3_optics(order=24)
+    T, fg = oi.CalculateTCCMatrix(sr, [512.0, 512.0], po, 0.0, nm)
+    sk = oi.socs_kernels_from_tcc(T, fg, [256, 256], nm)
+    masks = (np.random.default_rng(5).random((11, 256, 256)) > 0.6).astype(np.uint8)
+    want = sk.image(torch.from_numpy(masks).cuda(), form=form).cpu().numpy()
+    host_in = torch.from_numpy(masks).pin_memory()
+    for _ in range(2):
+        host_out = torch.full((11, 256, 256), float('nan')).pin_memory()
+        sk.image_host(host_in, host_out, chunk=4, form=form)
+        torch.cuda.current_stream().synchronize()
+        got = host_out.numpy()
+        assert np.isfinite(got).all()
+        assert rel_err(got, want) < tol
+    with pytest.raises(ValueError, match='pinned'):
+        sk.image_host(torch.from_numpy(masks), torch.empty((11, 256, 256)), form=form)
