@@ -350,9 +350,12 @@ __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
     expect_tx(bar4, L.consts);
     for (uint32_t o = 0; o < L.consts; o += 16384)
       bulk_g2s(base + o, a.consts + o, L.consts - o < 16384 ? L.consts - o : 16384, bar4);
+    pdl_wait();   // the band comes from the spectrum pass
     if (L.staged) stage_copy(a, cur, stage, L.stage_arr, bar3);
   }
   __syncthreads();  // barrier inits and the stage's unaligned end elements
+  pdl_trigger();
+  pdl_wait();
   uint32_t ph3 = 0;
   bool bad = false;
   if (L.staged) {
@@ -575,7 +578,7 @@ extern "C" int oi_coherent_coarse_tc(const void* band, int batch, int nch, int m
   const tc::Layout L = tc::make_layout(m0r == m0c, br * bc);
   int rc = ensure_smem((const void*)tc::coherent_tc_kernel, L.bytes, "oi_coherent_coarse_tc");
   if (rc) return rc;
-  tc::coherent_tc_kernel<<<(unsigned)ctas, tc::T, L.bytes, (cudaStream_t)stream>>>(a);
+  (void)launch_pdl(tc::coherent_tc_kernel, dim3((unsigned)ctas), dim3(tc::T), (size_t)L.bytes, (cudaStream_t)stream, a);
   oi::note_launch();
   return check_launch("oi_coherent_coarse_tc");
 }

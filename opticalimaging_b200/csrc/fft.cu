@@ -186,6 +186,8 @@ __global__ void __launch_bounds__(256, 3) fft_cols_fwd_kernel(const float2* __re
   float2* ys = (float2*)smem_raw;
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
   const long long col = (long long)blockIdx.x * G + g;
+  pdl_trigger();
+  pdl_wait();   // t comes from the row pass
   float2 z[32];
   if (col < ncols) {
     const float2* src = t + col * N;
@@ -303,6 +305,8 @@ __global__ void __launch_bounds__(G * N1) cols_inv_tiles_kernel(const float2* __
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
   const long long i = blockIdx.y;
   const int qc0 = blockIdx.x * G;
+  pdl_trigger();
+  pdl_wait();   // ihat comes from the coarse spectrum
   for (int e = tid; e < G * nq; e += T) {
     const int jr = e / G, gg = e % G, qc = qc0 + gg;
     cs[gg * nq + jr] = qc < bc ? ihat[(i * nq + jr) * (long long)bc + qc] : make_float2(0.f, 0.f);
@@ -361,7 +365,7 @@ static int cols_inv_tiles(const float2* ihat, int count, int br, int bc, int ny,
   int rc = set_smem(cols_inv_tiles_kernel<N1, G>, smem, "oi_coarse_to_image_tc/cols");
   if (rc) return rc;
   dim3 grid(64 / G, (unsigned)count);
-  cols_inv_tiles_kernel<N1, G><<<grid, G * N1, smem, s>>>(ihat, br, bc, ny, wn_y, tiles);
+  (void)launch_pdl(cols_inv_tiles_kernel<N1, G>, grid, dim3(G * N1), smem, s, ihat, br, bc, ny, wn_y, tiles);
   oi::note_launch();
   return check_launch("oi_coarse_to_image_tc/cols");
 }
@@ -447,6 +451,8 @@ __global__ void __launch_bounds__(512) coarse_spec_fft_kernel(const float* __res
   const int cw = (bc + gridDim.y - 1) / gridDim.y, c0 = blockIdx.y * cw, c1 = min(bc, c0 + cw);
   build_tables<N1R>(wr_g, r2, r1, tid, T);
   build_tables<N1C>(wc_g, c2, c1t, tid, T);
+  pdl_trigger();
+  pdl_wait();   // the partial coarse images come from the coherent sum
   float* cimg = (float*)area;
   const float4* src = (const float4*)(coarse + img * (long long)MR * MC);
   constexpr int PER = MR * MC / 4 / T;   // float4 per thread
@@ -522,8 +528,8 @@ static int launch_coarse_spec_fft(float* coarse, int nparts, int count, int br, 
   auto kern = coarse_spec_fft_kernel<N1R, N1C>;
   int rc = set_smem(kern, smem, "coarse spectrum fft");
   if (rc) return rc;
-  kern<<<dim3((unsigned)count, COARSE_PARTS), 512, smem, s>>>(coarse, nparts, (long long)count * MR * MC, br, bc, wr,
-                                                              wc, area_f2, ihat);
+  (void)launch_pdl(kern, dim3((unsigned)count, COARSE_PARTS), dim3(512), smem, s, (const float*)coarse, nparts,
+                   (long long)count * MR * MC, br, bc, wr, wc, area_f2, ihat);
   oi::note_launch();
   return check_launch("coarse spectrum fft");
 }
@@ -567,7 +573,8 @@ static int cols_fwd(const float2* t, int batch, int bc, const float2* wn_y, int 
   int rc = set_smem(fft_cols_fwd_kernel<N1>, smem, "oi_band_spectrum_fft/cols");
   if (rc) return rc;
   const long long ncols = (long long)batch * bc;
-  fft_cols_fwd_kernel<N1><<<(unsigned)ceil_div(ncols, G), 256, smem, s>>>(t, ncols, bc, wn_y, m0r, br, scale, band);
+  (void)launch_pdl(fft_cols_fwd_kernel<N1>, dim3((unsigned)ceil_div(ncols, G)), dim3(256), smem, s, (const float2*)t,
+                   ncols, bc, wn_y, m0r, br, scale, band);
   oi::note_launch();
   return check_launch("oi_band_spectrum_fft/cols");
 }

@@ -21,6 +21,31 @@ int check_launch(const char* what);
 // capture, make no attribute call.
 int ensure_smem(const void* kern, size_t bytes, const char* what);
 
+// Programmatic dependent launch.  The kernels of the split-form step are launched with programmatic stream
+// serialisation (launch_pdl): a kernel's CTAs may start -- allocate tensor memory, initialise barriers, load
+// constant operands -- while the previous kernel's last CTAs finish.  Before reading anything an earlier kernel
+// wrote, and before writing global memory, a thread calls pdl_wait(), which returns once the preceding grids
+// have completed and their writes are visible; pdl_trigger() lets the next such kernel launch once every CTA of
+// this one has started.  A kernel launched this way after any other work is correct too (the wait covers it).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 __host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }

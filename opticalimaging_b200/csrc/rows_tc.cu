@@ -147,6 +147,8 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   __syncthreads();
   fence_after();
   const uint32_t tmem = *tmem_slot;
+  pdl_trigger();
+  pdl_wait();   // the masks and t are ordered after the preceding kernels from here on
 
   // Loop state advances incrementally (ring slot / phase, chunk / item): no integer division per chunk.
   const int NC = (int)nchunks;
@@ -477,6 +479,9 @@ __global__ void __launch_bounds__(I_NT, 1) rows_inv_tc_kernel(InvArgs a, const _
   fence_after();
   const uint32_t tmem = *tmem_slot;
 
+  pdl_trigger();
+  if (warp != 8) pdl_wait();   // warp 8 streams only the constant C tiles; the rest read V or write the image
+
   // item i0 + n = (pair P, x tile j); counters advance per item (the pair changes exactly when j wraps)
   const long long P0 = i0 / JT;
   const int j0 = (int)(i0 - P0 * JT);
@@ -731,12 +736,13 @@ extern "C" int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, in
   if (u8) {
     rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_U8>, rt::F_SMEM, "oi_rows_fwd_tc");
     if (rc) return rc;
-    rt::rows_fwd_tc_kernel<OI_FIELD_U8><<<(unsigned)ctas, rt::F_NT, rt::F_SMEM, s>>>(a, map);
+    (void)launch_pdl(rt::rows_fwd_tc_kernel<OI_FIELD_U8>, dim3((unsigned)ctas), dim3(rt::F_NT), rt::F_SMEM, s, a, map);
     oi::note_launch();
   } else {
     rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32>, rt::F_SMEM, "oi_rows_fwd_tc");
     if (rc) return rc;
-    rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32><<<(unsigned)ctas, rt::F_NT, rt::F_SMEM, s>>>(a, map);
+    (void)launch_pdl(rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32>, dim3((unsigned)ctas), dim3(rt::F_NT), rt::F_SMEM, s, a,
+                     map);
     oi::note_launch();
   }
   return check_launch("oi_rows_fwd_tc");
@@ -757,7 +763,7 @@ int rows_inv_from_tiles(const void* vtiles, int count, int ny, int nx, const voi
   if (!rc) rc = rt::encode_2d(&v_map, CU_TENSOR_MAP_DATA_TYPE_UINT16, vtiles, 64, (unsigned long long)R * 512, 128, 64, 128);
   if (!rc) rc = ensure_smem((const void*)rt::rows_inv_tc_kernel, rt::I_SMEM, "oi_rows_inv_tc");
   if (rc) return rc;
-  rt::rows_inv_tc_kernel<<<(unsigned)ctas, rt::I_NT, rt::I_SMEM, s>>>(a, c_map, v_map);
+  (void)launch_pdl(rt::rows_inv_tc_kernel, dim3((unsigned)ctas), dim3(rt::I_NT), rt::I_SMEM, s, a, c_map, v_map);
   oi::note_launch();
   return check_launch("oi_rows_inv_tc");
 }
