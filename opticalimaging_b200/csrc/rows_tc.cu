@@ -445,11 +445,11 @@ __global__ void __launch_bounds__(I_NT, 1) rows_inv_tc_kernel(InvArgs a, const _
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* gbase = smem_raw + (base - raw);
   const uint32_t misc = base + I_MISC;
-  // barriers: cfull[6] (piece landed), cfree[6] (MMAs reading the piece finished), vfull (V tiles landed), vfree
-  // (MMAs reading the V tiles finished), accf[2] (accumulator complete), acce[2] (accumulator drained), fin (MMAs
-  // finished, failure path)
-  const uint32_t cfull = misc, cfree = misc + 48, vfull = misc + 96, vfree = misc + 104, accf = misc + 112,
-                 acce = misc + 128, fin = misc + 144;
+  // barriers: cfull[6] (piece landed), cfree[6] (MMAs reading the piece finished), vfull[4] (V block q of the
+  // pair landed), vfree[4] (MMAs reading V block q finished), accf[2] (accumulator complete), acce[2]
+  // (accumulator drained), fin (MMAs finished, failure path)
+  const uint32_t cfull = misc, cfree = misc + 48, vfull = misc + 96, vfree = misc + 128, accf = misc + 160,
+                 acce = misc + 176, fin = misc + 192;
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + I_MISC + 256);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int JT = a.nx / 128;                       // x tiles
@@ -469,8 +469,10 @@ __global__ void __launch_bounds__(I_NT, 1) rows_inv_tc_kernel(InvArgs a, const _
       mbar_init(accf + 8 * s, 1);
       mbar_init(acce + 8 * s, 8);
     }
-    mbar_init(vfull, 1);
-    mbar_init(vfree, 1);
+    for (int q = 0; q < 4; ++q) {
+      mbar_init(vfull + 8 * q, 1);
+      mbar_init(vfree + 8 * q, 1);
+    }
     mbar_init(fin, 1);
     mbar_init_fence();
   }
@@ -507,43 +509,49 @@ __global__ void __launch_bounds__(I_NT, 1) rows_inv_tc_kernel(InvArgs a, const _
       drain_ring(cfull, cs, g, I_NC);   // the copies in flight land before shared memory is released
     }
   } else if (warp == 10) {
-    // ---- V tiles of pair k of the range, once the MMAs of pair k-1 have finished
+    // ---- V tiles of pair k of the range: block q (hi kc 0, hi kc 1, lo kc 0, lo kc 1; both row blocks) once the
+    // MMAs of pair k-1 that read it have finished, in the order the MMAs first need them (0, 2, 1, 3)
     if (lane == 0) {
       const long long npairs = N > 0 ? (i1 - 1) / JT - P0 + 1 : 0;
-      int k = 0;
+      int lq[4] = {0, 0, 0, 0};   // loads issued per block
       bool ok = true;
-      for (; k < npairs; ++k) {
-        if (k >= 1 && !wait_bar(vfree, (uint32_t)((k - 1) & 1))) {
-          ok = false;
-          break;
-        }
-        expect_tx(vfull, 8 * OPER);
+      for (int k = 0; k < npairs && ok; ++k) {
         const long long rb = 2 * (P0 + k);
-        for (int q = 0; q < 4; ++q)
+        for (int i = 0; i < 4; ++i) {
+          const int q = ((i & 1) << 1) | (i >> 1);
+          if (k >= 1 && !wait_bar(vfree + 8 * q, (uint32_t)((k - 1) & 1))) {
+            ok = false;
+            break;
+          }
+          expect_tx(vfull + 8 * q, 2 * OPER);
           for (int h = 0; h < 2; ++h)   // rows past the tensor's end read as zeros
-            tma_load_2d(base + I_V + (2 * q + h) * OPER, &v_map, 0, (int)(((rb + h) * 4 + q) * 128), vfull);
+            tma_load_2d(base + I_V + (2 * q + h) * OPER, &v_map, 0, (int)(((rb + h) * 4 + q) * 128), vfull + 8 * q);
+          ++lq[q];
+        }
       }
       if (!ok) fail_status();
-      if (k > 0) wait_bar(vfull, (uint32_t)((k - 1) & 1));   // the last tiles have landed
+      for (int q = 0; q < 4; ++q)   // the last tiles have landed
+        if (lq[q] > 0) wait_bar(vfull + 8 * q, (uint32_t)((lq[q] - 1) & 1));
     }
   } else if (warp == 9) {
     if (lane == 0) {
       constexpr uint32_t ID = idesc(I_ACC, false);
       Ring cs{0, 0}, ab{0, 0};
-      uint32_t vph = 0;
+      uint32_t vph = 1;
       int j = j0;
       bool ok = true;
       int issued = 0;
       for (long long n = 0; n < N && ok; ++n) {
-        if (n == 0 || j == 0) {   // a new pair: release the previous V tiles, wait for this pair's
-          if (n > 0) commit(vfree);
-          ok = wait_bar(vfull, vph);
-          vph ^= 1u;
-        }
+        const bool first = n == 0 || j == 0, last = j == JT - 1;   // first / last item of its pair
+        if (first) vph ^= 1u;                                       // parity of this pair's V loads
         if (++j == JT) j = 0;
         if (ok && n >= 2) ok = wait_bar(acce + 8 * ab.slot, ab.phase ^ 1u);
         const uint32_t d = tmem + ab.slot * I_ACC;
         for (int p = 0; p < 4 && ok; ++p) {
+          if (first && (p & 1) == 0) {   // V hi and lo of this kc for the new pair
+            ok = wait_bar(vfull + 8 * (p >> 1), vph) && wait_bar(vfull + 8 * ((p >> 1) + 2), vph);
+            if (!ok) break;
+          }
           ok = wait_bar(cfull + 8 * cs.slot, cs.phase);
           if (!ok) break;
           fence_after();
@@ -562,6 +570,10 @@ __global__ void __launch_bounds__(I_NT, 1) rows_inv_tc_kernel(InvArgs a, const _
           issued = 1;
           commit(cfree + 8 * cs.slot);
           cs.next(I_NC);
+          if (last && (p & 1)) {   // the pair's last MMAs on V hi / lo of this kc have been issued
+            commit(vfree + 8 * (p >> 1));
+            commit(vfree + 8 * ((p >> 1) + 2));
+          }
         }
         if (!ok) break;
         commit(accf + 8 * ab.slot);
