@@ -213,12 +213,16 @@ __device__ __forceinline__ uint32_t stage_array(uint32_t s, const float2* p, int
 }
 
 // Stage copy of task t's pupil and band (issued by one thread; completes on `bar`).
-__device__ __forceinline__ void stage_copy(const Args& a, const FieldSrc& f, uint32_t stage, uint32_t arr, uint32_t bar) {
+// The band is copied only when it differs from the one the stage holds (consecutive fields of one image and
+// channel share it: the SOCS kernels of a clip).
+__device__ __forceinline__ void stage_copy(const Args& a, const FieldSrc& f, uint32_t stage, uint32_t arr, uint32_t bar,
+                                           bool with_band) {
   const int plane = a.br * a.bc;
-  const uint32_t bytes = 8u * ((plane - stage_shift(f.pupil)) & ~1) + 8u * ((plane - stage_shift(f.band)) & ~1);
+  const uint32_t bytes = 8u * ((plane - stage_shift(f.pupil)) & ~1) +
+                         (with_band ? 8u * ((plane - stage_shift(f.band)) & ~1) : 0u);
   expect_tx(bar, bytes);
   stage_array(stage, f.pupil, plane, bar);
-  stage_array(stage + arr, f.band, plane, bar);
+  if (with_band) stage_array(stage + arr, f.band, plane, bar);
 }
 
 // The stage-1 B operand of a field, A = P .* band zero-padded to 64 x 64: rows [0,64) = -Ai, [64,128) = Ar,
@@ -351,7 +355,7 @@ __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
     for (uint32_t o = 0; o < L.consts; o += 16384)
       bulk_g2s(base + o, a.consts + o, L.consts - o < 16384 ? L.consts - o : 16384, bar4);
     pdl_wait();   // the band comes from the spectrum pass
-    if (L.staged) stage_copy(a, cur, stage, L.stage_arr, bar3);
+    if (L.staged) stage_copy(a, cur, stage, L.stage_arr, bar3, true);
   }
   __syncthreads();  // barrier inits and the stage's unaligned end elements
   pdl_trigger();
@@ -389,7 +393,7 @@ __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
     p1.next(a);
     if (t0 + 1 < t1) nxt = field_src(a, p1);
     if (L.staged && t0 + 1 < t1) {
-      if (tid == 32) stage_copy(a, nxt, stage, L.stage_arr, bar3);
+      if (tid == 32) stage_copy(a, nxt, stage, L.stage_arr, bar3, nxt.band != cur.band);
       pending3 = 1;
     }
   }
@@ -479,7 +483,10 @@ __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
       }
       pending1 = 1;
       if (L.staged && t + 2 < t1) {
-        if (tid == 32) stage_copy(a, field_src(a, p2), stage, L.stage_arr, bar3);
+        if (tid == 32) {
+          const FieldSrc f2 = field_src(a, p2);
+          stage_copy(a, f2, stage, L.stage_arr, bar3, f2.band != cur.band);   // cur: field t+1, in the stage
+        }
         pending3 = 1;
       }
     }
