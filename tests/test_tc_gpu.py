@@ -193,3 +193,23 @@ def test_rows_inv_tc_direct(oi, count, ny, nx, bc):
     print(f'inverse rows {count}x{ny}x{nx} bc {bc}: max {err:.2e} rms {rms:.2e}')
     assert err < BF16X3_VS_FP64
     assert N.device_status() == 0
+
+
+def test_kernels_wait_for_the_preceding_torch_kernel(oi):
+    """The split form's kernels may start before the previous kernel on the stream has finished (programmatic
+    dependent launch) but wait for it before reading: masks written by a torch kernel right before the call give
+    bit-identical images to masks that were synchronised first, and a torch kernel right after sees the images."""
+    from opticalimaging_b200 import workloads as W
+    sr, po, nm = W.config3_optics(order=24)
+    T, fg = oi.CalculateTCCMatrix(sr, [512.0, 512.0], po, 0.0, nm)
+    sk = oi.socs_kernels_from_tcc(T, fg, [256, 256], nm)
+    torch.manual_seed(7)
+    base = torch.rand((8, 256, 256), device='cuda')
+    want = sk.image((base > 0.5).float(), form='bf16x3').clone()
+    torch.cuda.synchronize()
+    for _ in range(3):
+        masks = (base > 0.5).float()                  # a torch kernel, not synchronised
+        got = sk.image(masks, form='bf16x3')
+        total = got.sum()                             # a torch kernel reading the images right away
+        assert torch.equal(got, want)
+        assert torch.isclose(total, want.sum(), rtol=1e-6)
