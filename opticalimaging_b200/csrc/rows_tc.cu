@@ -46,7 +46,6 @@ using namespace tc;
 
 constexpr int NT = 320;                    // threads: 8 converter warps, producer warp, MMA warp
 constexpr uint32_t OPER = 128 * 128;       // one [128 rows][64 bf16] swizzled operand block (16 KB)
-constexpr uint32_t ACC_COLS = 128;         // one accumulator: 128 lanes x 128 fp32 columns
 
 __device__ __forceinline__ void fail_status() { atomicExch(&g_rows_status, 1); }
 
@@ -81,18 +80,26 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
 }
 
 // ------------------------------------------------------------------------------------------ forward
-// Shared memory: a ring of 3 staging slots (a 64-column chunk of 128 mask rows, as two 128-byte-swizzled
-// [128][32] float boxes, or one 64-byte-swizzled [128][64] uint8 box) and a ring of 3 W chunks (hi, lo).  The A
-// operand (the chunk as bf16 hi / lo) goes to tensor memory, two slots of 64 columns, and the MMA reads it there.
-constexpr int F_NS = 3;                              // staging slots
+// Items are pairs of 128-row blocks (rows 256 P .. 256 P + 255): one W chunk feeds both blocks' MMAs, so each
+// 64-column chunk of mask costs 32 KB of mask plus 16 KB of W over the SM-to-L2 path instead of 32 + 32 (that
+// path, about 30 bytes per cycle per SM, bounds this pass).  Shared memory: a ring of 2 staging slots (the chunk
+// of both blocks: per block two 128-byte-swizzled [128][32] float boxes, or one 64-byte-swizzled [128][64]
+// uint8 box) and a ring of 3 W chunks (hi, lo).  Tensor memory: the two blocks' accumulators (columns 0 and
+// 128, 128 each) and two A slots at 256 + 128 s (block h: hi at 64 h, lo at 64 h + 32), the chunk as bf16 hi /
+// lo written by the converters, read by the MMA.  A pair past the last row block (odd count) reads zeros and
+// stores nothing for its second block.
+constexpr int F_NS = 2;                              // staging slots (pairs)
 constexpr int F_NWS = 3;                             // W slots
-constexpr uint32_t F_STG = 128 * 64 * 4;             // one staging slot (float)
+constexpr uint32_t F_STG = 128 * 64 * 4;             // one row block's chunk (float)
+constexpr uint32_t F_PSTG = 2 * F_STG;               // one staging slot: both blocks
 constexpr uint32_t F_W = 2 * OPER;                   // one W chunk (hi, lo)
-constexpr uint32_t F_WOFF = F_NS * F_STG;
+constexpr uint32_t F_WOFF = F_NS * F_PSTG;
 constexpr uint32_t F_MISC = F_WOFF + F_NWS * F_W;
 constexpr uint32_t F_SMEM = F_MISC + 384 + 1024;
-constexpr uint32_t F_COL_A = 2 * ACC_COLS;           // A slot s at columns 256 + 64 s: hi [0,32), lo [32,64)
+constexpr uint32_t F_ACC = 128;                      // accumulator columns per block
+constexpr uint32_t F_COL_A = 2 * F_ACC;
 constexpr uint32_t F_TMEM_COLS = 512;
+static_assert(F_SMEM <= SMEM_LIMIT, "forward row pass: shared memory");
 
 struct FwdArgs {
   long long rows;           // batch * ny (a multiple of 128)
@@ -110,37 +117,41 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* gbase = smem_raw + (base - raw);
   const uint32_t misc = base + F_MISC;
-  // barriers: sfull[3] (staging landed), sfree[3] (staging read), wfull[3] (W landed), wdone[3] (MMAs reading
-  // the W slot finished), conv[2] (A slot written), adone[2] (MMAs reading the A slot finished), accf[2]
-  // (accumulator complete), acce[2] (accumulator drained)
-  const uint32_t sfull = misc, sfree = misc + 24, wfull = misc + 48, wdone = misc + 72, conv = misc + 96,
-                 adone = misc + 112, accf = misc + 128, acce = misc + 144;
+  // barriers: sfull[2] (staging landed), sfree[2] (staging read), wfull[3] (W landed), wdone[3] (MMAs reading
+  // the W slot finished), conv[2] (A slot written), adone[2] (MMAs reading the A slot finished), accf
+  // (accumulators complete), acce (accumulators drained)
+  const uint32_t sfull = misc, sfree = misc + 16, wfull = misc + 32, wdone = misc + 56, conv = misc + 80,
+                 adone = misc + 96, accf = misc + 112, acce = misc + 120;
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + F_MISC + 192);
   // per A slot and converter warp: 1 when the warp's part of the chunk has a non-zero bf16 lo half (a mask value
   // not exact in bf16); when no warp sets it the lo x hi products are exactly zero and are not issued
   volatile uint32_t* lo_flags = (volatile uint32_t*)(gbase + F_MISC + 256);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int KC = a.nx / 64;
-  const long long items = a.rows / 128;
+  const long long R = a.rows / 128;                  // row blocks
+  const long long items = (R + 1) / 2;               // pairs
   const long long G = gridDim.x;
   const long long i0 = (long long)blockIdx.x * items / G, i1 = ((long long)blockIdx.x + 1) * items / G;
   const long long nchunks = (i1 - i0) * KC;
   constexpr bool U8 = KIND == OI_FIELD_U8;
+  constexpr uint32_t BLK = U8 ? 128 * 64 : F_STG;    // bytes of one block's chunk
 
   if (warp == 0) tmem_alloc(misc + 192, F_TMEM_COLS);
   if (tid == 0) {
-    for (int s = 0; s < 3; ++s) {
+    for (int s = 0; s < F_NS; ++s) {
       mbar_init(sfull + 8 * s, 1);
       mbar_init(sfree + 8 * s, 8);
+    }
+    for (int s = 0; s < F_NWS; ++s) {
       mbar_init(wfull + 8 * s, 1);
       mbar_init(wdone + 8 * s, 1);
     }
     for (int s = 0; s < 2; ++s) {
       mbar_init(conv + 8 * s, 8);
       mbar_init(adone + 8 * s, 1);
-      mbar_init(accf + 8 * s, 1);
-      mbar_init(acce + 8 * s, 8);
     }
+    mbar_init(accf, 1);
+    mbar_init(acce, 8);
     mbar_init_fence();
   }
   fence_before();
@@ -153,23 +164,26 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   // Loop state advances incrementally (ring slot / phase, chunk / item): no integer division per chunk.
   const int NC = (int)nchunks;
   if (warp == 8) {
-    // ---- mask producer: chunk g into staging slot g % 3 as soon as the slot has been read
+    // ---- mask producer: chunk g of both blocks into staging slot g % 2 as soon as the slot has been read
     if (lane == 0) {
       Ring st{0, 0};
-      int c = 0, y = (int)(i0 * 128);
+      int c = 0, y = (int)(i0 * 256);
       for (int g = 0; g < NC; ++g) {
         if (g >= F_NS && !wait_bar(sfree + 8 * st.slot, st.phase ^ 1u)) {
           fail_status();
           break;
         }
-        const uint32_t dst = base + st.slot * F_STG;
-        expect_tx(sfull + 8 * st.slot, U8 ? 128 * 64 : F_STG);
-        tma_load_2d(dst, &mask_map, 64 * c, y, sfull + 8 * st.slot);
-        if (!U8) tma_load_2d(dst + F_STG / 2, &mask_map, 64 * c + 32, y, sfull + 8 * st.slot);
+        const uint32_t dst = base + st.slot * F_PSTG;
+        expect_tx(sfull + 8 * st.slot, 2 * BLK);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {   // rows past the tensor's end read as zeros
+          tma_load_2d(dst + h * F_STG, &mask_map, 64 * c, y + 128 * h, sfull + 8 * st.slot);
+          if (!U8) tma_load_2d(dst + h * F_STG + F_STG / 2, &mask_map, 64 * c + 32, y + 128 * h, sfull + 8 * st.slot);
+        }
         st.next(F_NS);
         if (++c == KC) {
           c = 0;
-          y += 128;
+          y += 256;
         }
       }
     }
@@ -190,38 +204,40 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
       }
     }
   } else if (warp == 9) {
-    // ---- MMA issue: D[buf] += A(tmem slot) x W^T over the chunk (K steps of 16), split BF16x3
+    // ---- MMA issue: D[h] += A[h](tmem slot) x W^T over the chunk (K steps of 16), split BF16x3, h = both blocks
     if (lane == 0) {
       constexpr uint32_t ID = idesc(128, false);
       Ring as{0, 0}, ws{0, 0};
       int c = 0, n = 0;
       for (int g = 0; g < NC; ++g) {
-        const int buf = n & 1;
         bool ok = wait_bar(conv + 8 * as.slot, as.phase);
         if (ok) ok = wait_bar(wfull + 8 * ws.slot, ws.phase);
-        if (ok && c == 0 && n >= 2) ok = wait_bar(acce + 8 * buf, (uint32_t)(((n - 2) >> 1) & 1));
+        if (ok && c == 0 && n >= 1) ok = wait_bar(acce, (uint32_t)((n - 1) & 1));   // previous pair drained
         if (!ok) {
           fail_status();
           break;
         }
         fence_after();
-        const uint32_t wch = base + F_WOFF + ws.slot * F_W, at = tmem + F_COL_A + 64 * as.slot;
-        const uint32_t d = tmem + buf * ACC_COLS;
+        const uint32_t wch = base + F_WOFF + ws.slot * F_W;
         uint32_t lo_any = 0;
         if (!U8) {
 #pragma unroll
           for (int w = 0; w < 8; ++w) lo_any |= lo_flags[8 * as.slot + w];
         }
 #pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
-          const uint32_t ko = 32 * ks;
-          mma_ts(d, at + 8 * ks, sdesc(wch + ko), ID, (c | ks) ? 1u : 0u);            // hi hi
-          mma_ts(d, at + 8 * ks, sdesc(wch + OPER + ko), ID, 1);                     // hi lo
-          if (lo_any) mma_ts(d, at + 32 + 8 * ks, sdesc(wch + ko), ID, 1);           // lo hi
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t d = tmem + h * F_ACC, at = tmem + F_COL_A + 128 * as.slot + 64 * h;
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks) {
+            const uint32_t ko = 32 * ks;
+            mma_ts(d, at + 8 * ks, sdesc(wch + ko), ID, (c | ks) ? 1u : 0u);            // hi hi
+            mma_ts(d, at + 8 * ks, sdesc(wch + OPER + ko), ID, 1);                     // hi lo
+            if (lo_any) mma_ts(d, at + 32 + 8 * ks, sdesc(wch + ko), ID, 1);           // lo hi
+          }
         }
         commit(adone + 8 * as.slot);
         commit(wdone + 8 * ws.slot);
-        if (c == KC - 1) commit(accf + 8 * buf);
+        if (c == KC - 1) commit(accf);
         as.next(2);
         ws.next(F_NWS);
         if (++c == KC) {
@@ -230,29 +246,37 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
         }
       }
     }
-  } else {
+  } else if (warp < 8) {
     // ---- converters (warps 0-7): staging -> A slot in tensor memory; drain finished accumulators.
-    // Warp w converts rows 32 (w & 3) .. +31 (its tensor-memory lane quarter), columns 32 (w >> 2) .. +31.
+    // Warp w converts rows 32 (w & 3) .. +31 of both blocks (its tensor-memory lane quarter), columns
+    // 32 (w >> 2) .. +31.
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
     const int half = warp >> 2, r = 32 * (warp & 3) + lane;
     bool ok = true;
     auto drain = [&](int n) {
-      // accumulator of item n: lanes = rows, columns re [0,64) / im [64,128) of band column ic
-      const int buf = n & 1;
-      if (!warp_wait(accf + 8 * buf, (uint32_t)((n >> 1) & 1))) return false;
+      // accumulators of pair n: lanes = rows, columns re [0,64) / im [64,128) of band column ic; block by
+      // block, released (acce) once the second block is in registers
+      if (!warp_wait(accf, (uint32_t)(n & 1))) return false;
       fence_after();
-      float re[32], im[32];
-      tmem_ld32x2(tmem + lane_base + buf * ACC_COLS + 32 * half, tmem + lane_base + buf * ACC_COLS + 64 + 32 * half,
-                  re, im);
-      fence_before();
-      __syncwarp();
-      if (lane == 0) arrive(acce + 8 * buf);
-      const int row = (int)((i0 + n) * 128) + r;
-      const int b = row / a.ny, y = row - b * a.ny;
-      float2* dst = a.t + ((long long)b * a.bc + 32 * half) * a.ny + y;
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        float re[32], im[32];
+        tmem_ld32x2(tmem + lane_base + h * F_ACC + 32 * half, tmem + lane_base + h * F_ACC + 64 + 32 * half, re, im);
+        if (h == 1) {
+          fence_before();
+          __syncwarp();
+          if (lane == 0) arrive(acce);
+        }
+        const long long rb = 2 * (i0 + n) + h;
+        if (rb < R) {
+          const int row = (int)(rb * 128) + r;
+          const int b = row / a.ny, y = row - b * a.ny;
+          float2* dst = a.t + ((long long)b * a.bc + 32 * half) * a.ny + y;
 #pragma unroll
-      for (int j = 0; j < 32; ++j)
-        if (32 * half + j < a.bc) dst[(long long)j * a.ny] = make_float2(re[j], im[j]);
+          for (int j = 0; j < 32; ++j)
+            if (32 * half + j < a.bc) dst[(long long)j * a.ny] = make_float2(re[j], im[j]);
+        }
+      }
       return true;
     };
     Ring st{0, 0}, as{0, 0};
@@ -261,38 +285,42 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
       ok = warp_wait(sfull + 8 * st.slot, st.phase);
       if (ok && g >= 2) ok = warp_wait(adone + 8 * as.slot, as.phase ^ 1u);   // A slot free (chunk g-2 done)
       if (!ok) break;
-      float v[32];
-      if (U8) {
-        const unsigned char* row = gbase + st.slot * F_STG + r * 64;   // 64-byte swizzle: chunk j at j ^ ((r >> 1) & 3)
+      bool lo_nz = false;
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        float v[32];
+        const unsigned char* blk = gbase + st.slot * F_PSTG + h * F_STG;
+        if (U8) {
+          const unsigned char* row = blk + r * 64;   // 64-byte swizzle: chunk j at j ^ ((r >> 1) & 3)
 #pragma unroll
-        for (int jj = 0; jj < 2; ++jj) {
-          const uint4 u = *(const uint4*)(row + (((2 * half + jj) ^ ((r >> 1) & 3)) << 4));
-          const uint32_t w4[4] = {u.x, u.y, u.z, u.w};
+          for (int jj = 0; jj < 2; ++jj) {
+            const uint4 u = *(const uint4*)(row + (((2 * half + jj) ^ ((r >> 1) & 3)) << 4));
+            const uint32_t w4[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-          for (int e = 0; e < 16; ++e) v[16 * jj + e] = (float)((w4[e >> 2] >> (8 * (e & 3))) & 0xFF);
+            for (int e = 0; e < 16; ++e) v[16 * jj + e] = (float)((w4[e >> 2] >> (8 * (e & 3))) & 0xFF);
+          }
+        } else {
+          const unsigned char* row = blk + half * (F_STG / 2) + r * 128;   // 128-byte swizzle
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const float4 x = *(const float4*)(row + ((j ^ (r & 7)) << 4));
+            v[4 * j] = x.x, v[4 * j + 1] = x.y, v[4 * j + 2] = x.z, v[4 * j + 3] = x.w;
+          }
         }
-      } else {
-        const unsigned char* row = gbase + st.slot * F_STG + half * (F_STG / 2) + r * 128;   // 128-byte swizzle
+        uint32_t hi[16], lo[16];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const float4 x = *(const float4*)(row + ((j ^ (r & 7)) << 4));
-          v[4 * j] = x.x, v[4 * j + 1] = x.y, v[4 * j + 2] = x.z, v[4 * j + 3] = x.w;
+        for (int e = 0; e < 16; ++e) split2(v[2 * e], v[2 * e + 1], hi[e], lo[e]);
+        const uint32_t at = tmem + lane_base + F_COL_A + 128 * as.slot + 64 * h + 16 * half;
+        tmem_st16(at, hi);
+        if (!U8) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) lo_nz |= lo[e] != 0u;
+          tmem_st16(at + 32, lo);          // always written: another warp's flag may make the MMAs read it
         }
       }
       __syncwarp();
       if (lane == 0) arrive(sfree + 8 * st.slot);          // the staging slot may be refilled
-      uint32_t hi[16], lo[16];
-#pragma unroll
-      for (int e = 0; e < 16; ++e) split2(v[2 * e], v[2 * e + 1], hi[e], lo[e]);
-      const uint32_t at = tmem + lane_base + F_COL_A + 64 * as.slot + 16 * half;
-      tmem_st16(at, hi);
-      bool lo_nz = false;
-      if (!U8) {
-#pragma unroll
-        for (int e = 0; e < 16; ++e) lo_nz |= lo[e] != 0u;
-        lo_nz = __any_sync(0xffffffffu, lo_nz);
-        tmem_st16(at + 32, lo);          // always written: another warp's flag may make the MMAs read it
-      }
+      if (!U8) lo_nz = __any_sync(0xffffffffu, lo_nz);
       wait_st();
       fence_before();
       __syncwarp();
@@ -300,7 +328,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
         if (!U8) lo_flags[8 * as.slot + warp] = lo_nz ? 1u : 0u;   // read by the MMA thread after `conv`
         arrive(conv + 8 * as.slot);
       }
-      // the previous item's accumulator is complete once this item's first chunk is converted
+      // the previous pair's accumulators are complete once this pair's first chunk is converted
       if (c == 0 && n >= 1) ok = drain(n - 1);
       st.next(F_NS);
       as.next(2);
@@ -733,9 +761,10 @@ extern "C" int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, in
     return fail(OI_ERANGE, "oi_rows_fwd_tc: grid %dx%d / band width %d unsupported", ny, nx, bc);
   if ((uintptr_t)field % 16 || (uintptr_t)consts % 16)
     return fail(OI_EINVAL, "oi_rows_fwd_tc: field and constants must be 16-byte aligned");
-  const long long rows = (long long)batch * ny, items = rows / 128;
+  const long long rows = (long long)batch * ny, items = (rows / 128 + 1) / 2;   // pairs of row blocks
   const int sms = rt::sm_count();
   if (!sms) return fail(OI_ECUDA, "oi_rows_fwd_tc: no CUDA device");
+  if (rows + 256 > 0x7fffffffLL) return fail(OI_ERANGE, "oi_rows_fwd_tc: %lld rows exceed the tensor-map range", rows);
   const long long ctas = items < sms ? items : sms;
   rt::FwdArgs a{rows, ny, nx, bc, (const unsigned char*)consts, (float2*)t};
   cudaStream_t s = (cudaStream_t)stream;

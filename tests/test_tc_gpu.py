@@ -213,3 +213,33 @@ def test_kernels_wait_for_the_preceding_torch_kernel(oi):
         total = got.sum()                             # a torch kernel reading the images right away
         assert torch.equal(got, want)
         assert torch.isclose(total, want.sum(), rtol=1e-6)
+
+
+@pytest.mark.parametrize('count,ny,nx,m0c,bc,u8', [(1, 384, 256, -7, 15, False), (3, 640, 512, -29, 59, False),
+                                                   (2, 256, 1024, 0, 64, True), (5, 1024, 1024, -29, 59, False)])
+def test_rows_fwd_tc_direct(oi, count, ny, nx, m0c, bc, u8):
+    """The forward tensor-core row pass through the C ABI against an FP64 evaluation of
+    t[b][ic][y] = sum_x mask[b][y][x] exp(+2 pi i (m0c+ic) x / nx): an odd number of 128-row blocks (the last
+    pair of blocks half empty), grey float32 masks and uint8 masks, more pairs than CTAs."""
+    from opticalimaging_b200 import _native as N
+    dev = torch.device('cuda')
+    rng = np.random.default_rng(count * ny + nx)
+    if u8:
+        m = (rng.random((count, ny, nx)) > 0.5).astype(np.uint8) * rng.integers(1, 255, (count, ny, nx)).astype(np.uint8)
+    else:
+        m = (rng.random((count, ny, nx)) > 0.6).astype(np.float32) * rng.random((count, ny, nx)).astype(np.float32)
+    s = N.stream_handle(dev)
+    nbytes = (nx // 64) * 32768
+    consts = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    N.call('oi_rows_tc_constants', 0, nx, m0c, bc, N.ptr(consts), nbytes, s)
+    md = torch.from_numpy(m).to(dev)
+    t = torch.full((count, bc, ny), complex(float('nan'), 0.0), dtype=torch.complex64, device=dev)
+    N.call('oi_rows_fwd_tc', N.ptr(md), N.FIELD_U8 if u8 else N.FIELD_REAL_F32, count, ny, nx, m0c, bc,
+           N.ptr(consts), N.ptr(t), s)
+    got = t.cpu().numpy()
+    E = np.exp(2j * np.pi * np.outer(np.arange(nx), m0c + np.arange(bc)) / nx)     # [nx][bc]
+    want = np.stack([(m[i].astype(np.float64) @ E).T for i in range(count)])       # [count][bc][ny]
+    err = rel_err(got, want)
+    print(f'forward rows {count}x{ny}x{nx} bc {bc} u8={u8}: max {err:.2e}')
+    assert err < 2e-5
+    assert N.device_status() == 0
