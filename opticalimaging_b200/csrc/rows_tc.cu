@@ -220,9 +220,13 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
         fence_after();
         const uint32_t wch = base + F_WOFF + ws.slot * F_W;
         uint32_t lo_any = 0;
-        if (!U8) {
-#pragma unroll
-          for (int w = 0; w < 8; ++w) lo_any |= lo_flags[8 * as.slot + w];
+        if (!U8) {   // the eight warps' flags of this A slot, as two 16-byte reads
+          uint32_t f0, f1, f2, f3, f4, f5, f6, f7;
+          const uint32_t fa = smem_u32((const void*)(lo_flags + 8 * as.slot));
+          asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(f0), "=r"(f1), "=r"(f2), "=r"(f3) : "r"(fa));
+          asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(f4), "=r"(f5), "=r"(f6), "=r"(f7)
+                       : "r"(fa + 16u));
+          lo_any = f0 | f1 | f2 | f3 | f4 | f5 | f6 | f7;
         }
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
