@@ -131,6 +131,19 @@ __device__ __forceinline__ void tmem_ld32x2(uint32_t addr_a, uint32_t addr_b, fl
     vb[i] = __uint_as_float(b[i]);
   }
 }
+// One 32-lane x 32-column load and its completion wait in one asm statement (see tmem_ld16x2).
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, float (&v)[32]) {
+  uint32_t a[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : OI_R8(a), OI_R8((a + 8)), OI_R8((a + 16)), OI_R8((a + 24))
+      : "r"(addr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(a[i]);
+}
 __device__ __forceinline__ void tmem_st32(uint32_t addr, const uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"

@@ -110,7 +110,8 @@ class Plan:
             self.wn_x = fft_tables(nx, device)
             self.wn_y = fft_tables(ny, device)
         self.coarse_fft = self.mr in (64, 128) and self.mc in (64, 128)
-        if self.coarse_fft:                                   # the coarse-grid FFT tables
+        self.coarse256 = (self.mr, self.mc) == (256, 256)     # the tensor-memory accumulator kernel
+        if self.coarse_fft or self.coarse256:                 # the coarse-grid FFT tables
             self.wm_r = t(1, self.mr, 1, 0, self.mr, +1)
             self.wm_c = t(1, self.mc, 1, 0, self.mc, +1)
 
@@ -165,6 +166,9 @@ class Plan:
     def use_coarse_fft(self, form):
         return self.coarse_fft and form != 'dft'
 
+    def use_coarse256(self, form):
+        return self.coarse256 and form != 'dft'
+
 
     @classmethod
     def get(cls, ny, nx, band: Band, device, coarse=None) -> 'Plan':
@@ -193,6 +197,18 @@ def field_split(nfields: int, blocks: int) -> int:
         if nfields % d == 0 and blocks * d >= target:
             return d
     return nfields
+
+
+def field_split_sm(nfields: int, blocks: int) -> int:
+    """Field split for a kernel of one block per SM (the 256 x 256 coarse grid): the d minimising
+    waves(d) * (fields per block + 1/2), the half standing for a block's fixed start and partial-sum write;
+    ties go to the smaller d (fewer partial sums)."""
+    best, best_cost = 1, None
+    for d in range(1, nfields + 1):
+        cost = -(-blocks * d // SM_COUNT) * (-(-nfields // d) + 0.5)
+        if best_cost is None or cost < best_cost:
+            best, best_cost = d, cost
+    return best
 
 
 # --------------------------------------------------------------------------------------------- stages
@@ -254,8 +270,8 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
         N.call('oi_coherent_coarse_tc', N.ptr(band), batch, nch, b.m0r, b.br, b.m0c, b.bc, N.ptr(pupils),
                int(pupil_batch_stride), N.ptr(weights), nz, nk, N.ptr(plan.tc_constants()), ctas, nsplit,
                N.ptr(coarse), s)
-    elif plan.use_coarse_fft(form):
-        nsplit = field_split(nk * nch, batch * nz)
+    elif plan.use_coarse_fft(form) or plan.use_coarse256(form):
+        nsplit = (field_split_sm(nk * nch, batch * nz) if plan.coarse256 else field_split(nk * nch, batch * nz))
         coarse = torch.empty((nsplit, batch, nz, plan.mr, plan.mc), dtype=torch.float32, device=dev)
         N.call('oi_coherent_coarse_fft', N.ptr(band), batch, nch, b.m0r, b.br, b.m0c, b.bc, N.ptr(pupils),
                int(pupil_batch_stride), N.ptr(weights), nz, nk, plan.mr, plan.mc, N.ptr(plan.wm_r),
@@ -389,6 +405,7 @@ class CoherentModel:
         nz = self.planes
         form = self.form if form is None else form
         split = (field_split(self.count * nch, batch * nz) if p.use_coarse_fft(None)
+                 else field_split_sm(self.count * nch, batch * nz) if p.use_coarse256(form)
                  else field_split(self.count * nch, batch * nz * ((p.mr + 15) // 16)))
         if form == 'bf16x3':
             split = tc_parts_bound(batch * nz, self.count * nch)

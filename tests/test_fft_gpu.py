@@ -100,3 +100,41 @@ def test_large_band_coarse_256_fft_vs_dft_and_oracle(eng):
     sc.ScatterField = W.thin_field(masks[0])
     assert rel_err(fft[0], O.socs(sc, K, sr, po)) < 1e-5
     assert N.device_status() == 0
+
+
+@pytest.mark.parametrize('batch,nch,nz,nk,br,bc,m0r,m0c,nsplit,per_image', [
+    (2, 2, 2, 3, 70, 66, -35, -30, 4, False),     # 12 fields over 4 splits, two planes, two channels
+    (2, 1, 1, 5, 128, 128, -64, -64, 2, True),    # the largest band; pupils per image
+    (1, 1, 1, 2, 117, 65, -58, 5, 1, False),      # asymmetric band, offset column band
+])
+def test_coherent_coarse_fft_256(eng, batch, nch, nz, nk, br, bc, m0r, m0c, nsplit, per_image):
+    """The 256 x 256 coarse grid (tensor-memory accumulator) against an FP64 numpy evaluation of
+    sum_{k,c} w |sum A[ir][ic] exp(-2 pi i ((m0r+ir) sr + (m0c+ic) sc) / 256)|^2, A = P[z][k] .* band[b][c]."""
+    from opticalimaging_b200 import _native as N
+    rng = np.random.default_rng(br * 1000 + bc)
+    cplx = lambda *s: (rng.standard_normal(s) + 1j * rng.standard_normal(s))  # noqa: E731
+    band = cplx(batch, nch, br, bc)
+    pup = cplx(batch if per_image else 1, nz, nk, br, bc)
+    w = rng.random((nz, nk)) + 0.1
+    j = np.arange(256)
+    cr = np.exp(-2j * np.pi * np.outer(j, m0r + np.arange(br)) / 256)     # [sr][ir]
+    cc = np.exp(-2j * np.pi * np.outer(m0c + np.arange(bc), j) / 256)     # [ic][sc]
+    want = np.zeros((batch, nz, 256, 256))
+    for b in range(batch):
+        for z in range(nz):
+            for k in range(nk):
+                for c in range(nch):
+                    e = cr @ (pup[b if per_image else 0, z, k] * band[b, c]) @ cc
+                    want[b, z] += w[z, k] * np.abs(e) ** 2
+    dev = torch.device('cuda')
+    tb = torch.from_numpy(band.astype(np.complex64)).to(dev)
+    tp = torch.from_numpy(pup.astype(np.complex64)).to(dev)
+    tw = torch.from_numpy(w.astype(np.float32)).to(dev)
+    tab = torch.from_numpy(np.exp(2j * np.pi * j / 256).astype(np.complex64)).to(dev)
+    coarse = torch.full((nsplit, batch, nz, 256, 256), float('nan'), device=dev)
+    stride = nz * nk * br * bc if per_image else 0
+    N.call('oi_coherent_coarse_fft', N.ptr(tb), batch, nch, m0r, br, m0c, bc, N.ptr(tp), stride, N.ptr(tw), nz, nk,
+           256, 256, N.ptr(tab), N.ptr(tab), nsplit, N.ptr(coarse), N.stream_handle(dev))
+    got = coarse.sum(dim=0).cpu().numpy()
+    assert rel_err(got, want) < 5e-6
+    assert N.device_status() == 0
