@@ -162,14 +162,42 @@ def stage_times(sk, masks, out, form, reps=5):
     return acc
 
 
+def wait_until(t):
+    """Wait for perf_counter() to reach t without holding the GIL (the server's scheduler thread shares it):
+    sleeps while more than 0.2 ms remain, then yields with sleep(0)."""
+    while True:
+        d = t - time.perf_counter()
+        if d <= 0:
+            return
+        time.sleep(d - 1e-4 if d > 2e-4 else 0)
+
+
+def poisson_run(srv, stream, rate, seed, submit):
+    """Open-loop arrivals: request i of `stream` is submitted at the i-th arrival of a Poisson process of
+    `rate` per second (the schedule runs from the start time, so late submissions do not lower the rate).
+    Returns (requests per second achieved, latency statistics)."""
+    import random
+    srv.completed.clear()
+    rng = random.Random(seed)
+    futs = []
+    t_next = t0 = time.perf_counter()
+    for item in stream:
+        t_next += rng.expovariate(rate)
+        wait_until(t_next)
+        futs.append(submit(item))
+    for f in futs:
+        f.result()
+    return len(stream) / (time.perf_counter() - t0), srv.latency_ms()
+
+
 def serve_measure(sk, info, masks_np, dev, args):
     """Served throughput and latency of config-3 requests, against the plain path on the same requests.
 
     The client keeps a ring of pinned result buffers and passes one with each request (the server copies the
     image into it).  Saturated: a closed loop keeping `window` requests outstanding (throughput).  Poisson:
-    open-loop arrivals at 70 % of the saturated rate (latency under load).  Plain: one request at a time."""
+    open-loop arrivals at 70 % of the saturated rate (latency under load), result buffers recycled as each
+    request completes.  Plain: one request at a time."""
     import collections
-    import random
     from opticalimaging_b200 import serve
     spec = serve.ModelSpec(('socs24', N_PIX, PERIOD, args.form), N_PIX, N_PIX, 1,
                            build=lambda: serve_model_from(sk, args.form))
@@ -199,20 +227,27 @@ def serve_measure(sk, info, masks_np, dev, args):
     dt = time.perf_counter() - t0
     sat = srv.latency_ms()
     served = nreq / dt
-    srv.completed.clear()
-    rng = random.Random(5)
     rate = 0.7 * served
-    futs = []
-    t_next = time.perf_counter()
-    for i in range(nreq):
-        t_next += rng.expovariate(rate)
-        while time.perf_counter() < t_next:
-            pass
-        futs.append(srv.submit(spec, pinned[i % len(pinned)], out=ring[i]))
-    for f in futs:
-        f.result()
-    poisson = srv.latency_ms()
-    batches = srv.batches
+    free = collections.deque(ring)
+    lock = threading.Lock()
+
+    def submit(i):
+        with lock:
+            buf = free.popleft() if free else None
+        if buf is None:
+            buf = torch.empty((1, N_PIX, N_PIX), dtype=torch.float32).pin_memory()
+        f = srv.submit(spec, pinned[i % len(pinned)], out=buf)
+
+        def recycle(_f, buf=buf):
+            with lock:
+                free.append(buf)
+        f.add_done_callback(recycle)
+        return f
+
+    batches0 = srv.batches
+    npois = max(nreq, args.poisson_requests)
+    _, poisson = poisson_run(srv, range(npois), rate, 5, submit)
+    batches = srv.batches - batches0
     srv.close()
     nplain = min(32, nreq)
     serve.plain_run([(plain_spec, pinned[0])], device=dev)       # build the plain model outside the timing
@@ -221,7 +256,8 @@ def serve_measure(sk, info, masks_np, dev, args):
     return {"images_per_s": served, "p50_ms": poisson.get("p50_ms"), "p99_ms": poisson.get("p99_ms"),
             "latency_at": f"Poisson arrivals at {rate:.0f} requests/s (70 % of the saturated rate)",
             "saturated_p50_ms": sat.get("p50_ms"), "saturated_p99_ms": sat.get("p99_ms"),
-            "requests": nreq, "window": window, "batches": batches, "form": args.form, "plain_images_per_s": plain,
+            "requests": nreq, "poisson_requests": npois, "window": window, "poisson_batches": batches,
+            "form": args.form, "plain_images_per_s": plain,
             "served_over_plain": served / plain,
             "plain": "one request at a time: H2D, image (batch 1, FP32 FFT form, no graph), D2H, synchronise",
             "h2d_bytes_per_image": N_PIX * N_PIX, "d2h_bytes_per_image": 4 * N_PIX * N_PIX}
@@ -232,7 +268,6 @@ def serve_mix(dev, args, state):
     three-plane SOCS) through the server with a 150 GB HBM budget, against the plain FP32 path on a sample of the
     same requests, with the served form's error against the FP32 form (every model) and the FP64 oracle."""
     import collections
-    import random
     from opticalimaging_b200 import serve, workloads as W
     from tests.fixtures import rel_err
     t_setup = time.perf_counter()
@@ -284,22 +319,10 @@ def serve_mix(dev, args, state):
         q.popleft().result()
     sat_rate = len(stream) / (time.perf_counter() - t0)
     # Poisson arrivals at 70 % of the saturated rate: latency under load
-    srv.completed.clear()
-    rng = random.Random(11)
     rate = 0.7 * sat_rate
-    futs = []
-    t_next = t0 = time.perf_counter()
-    for k, n, i in stream:
-        t_next += rng.expovariate(rate)
-        while time.perf_counter() < t_next:
-            pass
-        futs.append(submit(k, n, i))
-    for f in futs:
-        f.result()
-    del futs
-    served_rate = len(stream) / (time.perf_counter() - t0)
-    lat = srv.latency_ms()
-    batches = srv.batches
+    batches0 = srv.batches
+    served_rate, lat = poisson_run(srv, stream, rate, 11, lambda item: submit(*item))
+    batches = srv.batches - batches0
     resident = ex.resident_bytes()
     srv.close()
     # plain FP32 path, one request at a time, on a sample with the same mix (models built outside the timing)
@@ -635,7 +658,9 @@ def main():
     ap.add_argument('--mix-requests', type=int, default=2000,
                     help='requests of the mixed serving stream (configuration 5); 0 skips it')
     ap.add_argument('--batch', type=int, default=64, help='clips per step (64 in the benchmark configuration)')
-    ap.add_argument('--serve-requests', type=int, default=512, help='requests in the served measurement')
+    ap.add_argument('--serve-requests', type=int, default=512, help='requests in the saturated served measurement')
+    ap.add_argument('--poisson-requests', type=int, default=2048,
+                    help='requests of the served measurement under Poisson arrivals')
     ap.add_argument('--form', default='bf16x3', choices=['fft', 'dft', 'bf16x3'],
                     help='transform form of the timed path (bf16x3: split-BF16x3 contraction on tensor cores)')
     args = ap.parse_args()
