@@ -430,9 +430,15 @@ def kernel_rooflines(sk, masks, reps=10):
     v = torch.zeros(B * b.bc * sk.ny, dtype=torch.complex64, device=dev)
     tiles = torch.empty(B * sk.ny * 512, dtype=torch.uint8, device=dev)
     out = torch.empty((B, sk.ny, sk.nx), device=dev)
+    # the forward row pass as the image path runs it: the Hermitian half for a symmetric band
+    if plan.symmetric_band():
+        fwd = lambda: N.call('oi_rows_fwd_tc_half', N.ptr(masks), N.FIELD_REAL_F32, B, sk.ny, sk.nx,  # noqa: E731
+                             (b.bc + 1) // 2, N.ptr(plan.rows_consts(2)), N.ptr(t), s)
+    else:
+        fwd = lambda: N.call('oi_rows_fwd_tc', N.ptr(masks), N.FIELD_REAL_F32, B, sk.ny, sk.nx, b.m0c,  # noqa: E731
+                             b.bc, N.ptr(plan.rows_consts(0)), N.ptr(t), s)
     calls = {
-        "rows_fwd_tc": lambda: N.call('oi_rows_fwd_tc', N.ptr(masks), N.FIELD_REAL_F32, B, sk.ny, sk.nx, b.m0c, b.bc,
-                                      N.ptr(plan.rows_consts(0)), N.ptr(t), s),
+        "rows_fwd_tc": fwd,
         "coherent_tc": lambda: N.call('oi_coherent_coarse_tc', N.ptr(band), B, 1, b.m0r, b.br, b.m0c, b.bc,
                                       N.ptr(sk.pupils), 0, N.ptr(sk.weights), 1, sk.count,
                                       N.ptr(tplan.tc_constants()), ctas, nparts, N.ptr(coarse), s),

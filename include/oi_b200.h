@@ -17,7 +17,7 @@
  *                         <- the same three stages in FFT form (power-of-two grids)
  *   oi_spectrum_to_image(_fft) <- the synthesis half of the two above
  *   oi_coherent_coarse_tc <- the |fft2(.)|^2 accumulation again, split-BF16x3 on tensor cores (tcgen05)
- *   oi_band_spectrum_tc / oi_coarse_to_image_tc / oi_rows_fwd_tc / oi_rows_inv_tc
+ *   oi_band_spectrum_tc(_sym) / oi_coarse_to_image_tc / oi_rows_fwd_tc(_half) / oi_rows_inv_tc
  *                         <- the N-point stages with their row passes on the tensor cores (split-BF16x3 form)
  *   oi_coherent_adjoint   <- (no counterpart: the reference differentiates through torch autograd)
  *   oi_twiddle            <- (no counterpart: fills the phase tables the transforms read)
@@ -204,9 +204,12 @@ OI_API int oi_tc_constants(int m0r, int m0c, const void* wr, const void* wc, voi
  *                   t as the scratch of oi_band_spectrum_fft, float2 [batch][bc][ny])
  *   oi_rows_inv_tc  out[i][y][x] = sum_{qc<bc} Re(v[i][qc][y] exp(-2 pi i qc x / nx))  (v float2 [count][bc][ny];
  *                   vtiles: scratch of count * ny * 512 bytes that receives v as bf16 operand tiles)
+ *   oi_rows_fwd_tc_half  the same for ic = 0 .. bch-1 at m0c = 0 (bch <= 32): the non-negative columns of a
+ *                   real mask's row transform (t[-ic] = conj(t[ic])), t float2 [batch][bch][ny]
  * `consts` is the constant operand image from oi_rows_tc_constants: which = 0 (forward; depends on nx, m0c, bc;
- * nx/64 * 32768 bytes) or 1 (inverse; depends on nx, bc; nx/128 * 65536 bytes).  A wait that exceeds 2 s ends
- * the kernel early and sets the device status.
+ * nx/64 * 32768 bytes), 1 (inverse; depends on nx, bc; nx/128 * 65536 bytes) or 2 (forward half for
+ * oi_rows_fwd_tc_half, given the symmetric band m0c = -(bc-1)/2, bc odd <= 63, it covers bch = (bc+1)/2 columns;
+ * nx/64 * 16384 bytes).  A wait that exceeds 2 s ends the kernel early and sets the device status.
  * oi_band_spectrum_tc and oi_coarse_to_image_tc are oi_band_spectrum_fft and oi_coarse_to_image_fft (coarse grid
  * 128 x 128) with these row passes; oi_coarse_to_image_tc writes the column pass straight into the V operand tiles
  * (scratch_tiles, count * ny * 512 bytes; scratch_v is unused and may be NULL).
@@ -214,6 +217,8 @@ OI_API int oi_tc_constants(int m0r, int m0c, const void* wr, const void* wc, voi
 OI_API int oi_rows_tc_constants(int which, int nx, int m0c, int bc, void* image, long long bytes, void* stream);
 OI_API int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, int nx, int m0c, int bc,
                           const void* consts, void* t, void* stream);
+OI_API int oi_rows_fwd_tc_half(const void* field, int kind, int batch, int ny, int nx, int bch, const void* consts,
+                               void* t, void* stream);
 OI_API int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, const void* consts, void* vtiles,
                           float* out, void* stream);
 /* The synthesis row pass alone, from V operand tiles already written (by oi_rows_inv_tc's conversion or by the
@@ -223,6 +228,14 @@ OI_API int oi_rows_inv_tc_tiles(const void* vtiles, int count, int ny, int nx, c
 OI_API int oi_band_spectrum_tc(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c,
                                int bc, const void* wconsts, const void* wn_y, float scale, void* scratch,
                                void* band, void* stream);
+/* oi_band_spectrum_tc for a real mask and an odd symmetric band (m0r = -(br-1)/2, m0c = -(bc-1)/2, bc <= 63):
+ * the row pass computes the band's (bc+1)/2 non-negative columns only (oi_rows_fwd_tc_half, hconsts from
+ * oi_rows_tc_constants(2, nx, m0c, bc, ...)) and the column pass writes each column and its mirror
+ * band[-ky][-kx] = conj(band[ky][kx]).  scratch: batch * ny * (bc+1)/2 complex.  Same band as
+ * oi_band_spectrum_tc (Scatter.CalculateSpectrum, Scatter.py:10-35, restricted to the band). */
+OI_API int oi_band_spectrum_tc_sym(const void* field, int kind, int batch, int ny, int nx, int br, int bc,
+                                   const void* hconsts, const void* wn_y, float scale, void* scratch, void* band,
+                                   void* stream);
 OI_API int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int br, int bc, const void* wm_r,
                                  const void* wm_c, const void* wn_y, const void* cconsts, int ny, int nx,
                                  void* scratch_ihat, void* scratch_v, void* scratch_tiles, float* out, void* stream);

@@ -174,11 +174,14 @@ __global__ void __launch_bounds__(256, 3) fft_rows_fwd_kernel(const void* __rest
 }
 
 // ------------------------------------------------------------------------------ forward, columns
-// t[b][ic][y] (N = ny) -> band[b][ir][ic] = scale * sum_y t exp(+2 pi i (m0r+ir) y / ny)
-template <int N1>
+// t[b][ic][y] (N = ny) -> band[b][ir][ic] = scale * sum_y t exp(+2 pi i (m0r+ir) y / ny).
+// SYM: t holds the non-negative columns kx = 0 .. bc-1 of a real mask's row transform and the band is the
+// symmetric bco x br band (m0c = -(bco-1)/2, m0r = -(br-1)/2): column kx lands at ic = kx + (bco-1)/2 and, for
+// kx > 0, its mirror band[-ky][-kx] = conj(band[ky][kx]) at row br-1-ir, column (bco-1)/2 - kx.
+template <int N1, bool SYM>
 __global__ void __launch_bounds__(256, 3) fft_cols_fwd_kernel(const float2* __restrict__ t, long long ncols, int bc,
                                                            const float2* __restrict__ wn_g, int m0r, int br,
-                                                           float scale, float2* __restrict__ band) {
+                                                           float scale, float2* __restrict__ band, int bco) {
   constexpr int N = 32 * N1, G = 256 / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const float2* t2 = wn_g;
@@ -205,9 +208,18 @@ __global__ void __launch_bounds__(256, 3) fft_cols_fwd_kernel(const float2* __re
   if (col >= ncols) return;
   const long long b = col / bc;
   const int ic = (int)(col - b * bc);
-  for (int ir = n1; ir < br; ir += N1) {
-    float2 v = outer_bin<+1, N1>(yg, t1, (m0r + ir) & (N - 1));
-    band[(b * br + ir) * (long long)bc + ic] = make_float2(v.x * scale, v.y * scale);
+  if (!SYM) {
+    for (int ir = n1; ir < br; ir += N1) {
+      float2 v = outer_bin<+1, N1>(yg, t1, (m0r + ir) & (N - 1));
+      band[(b * br + ir) * (long long)bc + ic] = make_float2(v.x * scale, v.y * scale);
+    }
+  } else {
+    const int h = (bco - 1) / 2;
+    for (int ir = n1; ir < br; ir += N1) {
+      float2 v = outer_bin<+1, N1>(yg, t1, (m0r + ir) & (N - 1));
+      band[(b * br + ir) * (long long)bco + h + ic] = make_float2(v.x * scale, v.y * scale);
+      if (ic > 0) band[(b * br + br - 1 - ir) * (long long)bco + h - ic] = make_float2(v.x * scale, -v.y * scale);
+    }
   }
 }
 
@@ -565,16 +577,17 @@ static int band_fft(const void* field, int kind, int batch, int ny, int nx, int 
   return check_launch("oi_band_spectrum_fft/rows");
 }
 
-template <int N1>
+// bco: the output band width (SYM: bc = (bco + 1) / 2 input columns; else bco = bc)
+template <int N1, bool SYM = false>
 static int cols_fwd(const float2* t, int batch, int bc, const float2* wn_y, int m0r, int br, float scale,
-                    float2* band, cudaStream_t s) {
+                    float2* band, cudaStream_t s, int bco = 0) {
   constexpr int G = 256 / N1;
   size_t smem = smem_cols_fwd<N1>();
-  int rc = set_smem(fft_cols_fwd_kernel<N1>, smem, "oi_band_spectrum_fft/cols");
+  int rc = set_smem(fft_cols_fwd_kernel<N1, SYM>, smem, "oi_band_spectrum_fft/cols");
   if (rc) return rc;
   const long long ncols = (long long)batch * bc;
-  (void)launch_pdl(fft_cols_fwd_kernel<N1>, dim3((unsigned)ceil_div(ncols, G)), dim3(256), smem, s, (const float2*)t,
-                   ncols, bc, wn_y, m0r, br, scale, band);
+  (void)launch_pdl(fft_cols_fwd_kernel<N1, SYM>, dim3((unsigned)ceil_div(ncols, G)), dim3(256), smem, s,
+                   (const float2*)t, ncols, bc, wn_y, m0r, br, scale, band, SYM ? bco : bc);
   oi::note_launch();
   return check_launch("oi_band_spectrum_fft/cols");
 }
@@ -741,6 +754,34 @@ extern "C" int oi_band_spectrum_tc(const void* field, int kind, int batch, int n
     case 16: return cols_fwd<16>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
     case 32: return cols_fwd<32>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
     default: return cols_fwd<64>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+  }
+}
+
+// oi_band_spectrum_tc for a symmetric band (m0r = -(br-1)/2, m0c = -(bc-1)/2, br and bc odd, bc <= 63): the row
+// pass computes only the band's non-negative columns (oi_rows_fwd_tc_half against `hconsts` of
+// oi_rows_tc_constants(2, nx, m0c, bc, ...)) and the column pass fills the negative ones from
+// band[-ky][-kx] = conj(band[ky][kx]) (a real mask).  scratch: batch * ny * (bc+1)/2 complex.
+extern "C" int oi_band_spectrum_tc_sym(const void* field, int kind, int batch, int ny, int nx, int br, int bc,
+                                       const void* hconsts, const void* wn_y, float scale, void* scratch, void* band,
+                                       void* stream) {
+  using namespace oi;
+  if (!field || !hconsts || !wn_y || !scratch || !band || batch <= 0 || br <= 0 || bc <= 0)
+    return fail(OI_EINVAL, "oi_band_spectrum_tc_sym: bad arguments");
+  const int ny1 = n1_of(ny);
+  if (!ny1 || nx % 128 != 0 || nx > 4096)
+    return fail(OI_ERANGE, "oi_band_spectrum_tc_sym: grid %dx%d unsupported", ny, nx);
+  if (bc % 2 == 0 || br % 2 == 0 || bc > 63 || br > ny)
+    return fail(OI_ERANGE, "oi_band_spectrum_tc_sym: band %dx%d is not an odd symmetric band of width <= 63", br, bc);
+  const int bch = (bc + 1) / 2, m0r = -(br - 1) / 2;
+  int rc = oi_rows_fwd_tc_half(field, kind, batch, ny, nx, bch, hconsts, scratch, stream);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const float2* t = (const float2*)scratch;
+  switch (ny1) {
+    case 8: return cols_fwd<8, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc);
+    case 16: return cols_fwd<16, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc);
+    case 32: return cols_fwd<32, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc);
+    default: return cols_fwd<64, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc);
   }
 }
 

@@ -3,6 +3,8 @@
 //
 //   forward   (oi_rows_fwd_tc)  t[b][ic][y] = sum_x mask[b][y][x] exp(+2 pi i (m0c+ic) x / nx)
 //             -- the row half of the band spectrum (Scatter.CalculateSpectrum, Scatter.py:10-35, on the band);
+//             (oi_rows_fwd_tc_half) the same for ic = 0 .. bch-1 at m0c = 0 only: for a real mask
+//             t[-ic] = conj(t[ic]), so a symmetric band needs only its non-negative columns;
 //   inverse   (oi_rows_inv_tc)  out[i][y][x] = sum_qc Re(v[i][qc][y] exp(-2 pi i qc x / nx))
 //             -- the last pass of the synthesis (qc > 0 terms already doubled by the caller).
 //
@@ -88,11 +90,14 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
 // 128, 128 each) and two A slots at 256 + 128 s (block h: hi at 64 h, lo at 64 h + 32), the chunk as bf16 hi /
 // lo written by the converters, read by the MMA.  A pair past the last row block (odd count) reads zeros and
 // stores nothing for its second block.
+// NB = band columns per real / imaginary part of W: 64 (a band of up to 64 columns, N = 128), or 32 for the
+// Hermitian half of a real mask's symmetric band (columns 0 .. bch-1 only, N = 64, a 16 KB W chunk: half the
+// W bytes per mask byte over the SM-to-L2 path and half the MMA width).
 constexpr int F_NS = 2;                              // staging slots (pairs)
 constexpr int F_NWS = 3;                             // W slots
 constexpr uint32_t F_STG = 128 * 64 * 4;             // one row block's chunk (float)
 constexpr uint32_t F_PSTG = 2 * F_STG;               // one staging slot: both blocks
-constexpr uint32_t F_W = 2 * OPER;                   // one W chunk (hi, lo)
+constexpr uint32_t F_W = 2 * OPER;                   // one W slot (a chunk's hi and lo at NB = 64)
 constexpr uint32_t F_WOFF = F_NS * F_PSTG;
 constexpr uint32_t F_MISC = F_WOFF + F_NWS * F_W;
 constexpr uint32_t F_SMEM = F_MISC + 384 + 1024;
@@ -104,14 +109,17 @@ static_assert(F_SMEM <= SMEM_LIMIT, "forward row pass: shared memory");
 struct FwdArgs {
   long long rows;           // batch * ny (a multiple of 128)
   int ny, nx, bc;
-  const unsigned char* w;   // constant image: per 64-column chunk, [hi | lo] x [128 rows][64]
+  const unsigned char* w;   // constant image: per 64-column chunk, [hi | lo] x [2 NB rows][64]
   float2* t;                // [batch][bc][ny]
 };
 
 constexpr int F_NT = NT + 32;   // + a warp issuing the W loads
 
-template <int KIND>
+template <int KIND, int NB>
 __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const __grid_constant__ CUtensorMap mask_map) {
+  static_assert(NB == 64 || NB == 32, "forward row pass: NB");
+  constexpr uint32_t WOP = 2 * NB * 128;             // one precision of a W chunk: [2 NB rows][64 bf16]
+  constexpr uint32_t FW = 2 * WOP;                   // one W chunk (hi, lo)
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -197,8 +205,8 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
           fail_status();
           break;
         }
-        expect_tx(wfull + 8 * ws.slot, F_W);
-        bulk_g2s(base + F_WOFF + ws.slot * F_W, a.w + (long long)c * F_W, F_W, wfull + 8 * ws.slot);
+        expect_tx(wfull + 8 * ws.slot, FW);
+        bulk_g2s(base + F_WOFF + ws.slot * F_W, a.w + (long long)c * FW, FW, wfull + 8 * ws.slot);
         ws.next(F_NWS);
         if (++c == KC) c = 0;
       }
@@ -206,7 +214,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   } else if (warp == 9) {
     // ---- MMA issue: D[h] += A[h](tmem slot) x W^T over the chunk (K steps of 16), split BF16x3, h = both blocks
     if (lane == 0) {
-      constexpr uint32_t ID = idesc(128, false);
+      constexpr uint32_t ID = idesc(2 * NB, false);
       Ring as{0, 0}, ws{0, 0};
       int c = 0, n = 0;
       for (int g = 0; g < NC; ++g) {
@@ -235,7 +243,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
           for (int ks = 0; ks < 4; ++ks) {
             const uint32_t ko = 32 * ks;
             mma_ts(d, at + 8 * ks, sdesc(wch + ko), ID, (c | ks) ? 1u : 0u);            // hi hi
-            mma_ts(d, at + 8 * ks, sdesc(wch + OPER + ko), ID, 1);                     // hi lo
+            mma_ts(d, at + 8 * ks, sdesc(wch + WOP + ko), ID, 1);                      // hi lo
             if (lo_any) mma_ts(d, at + 32 + 8 * ks, sdesc(wch + ko), ID, 1);           // lo hi
           }
         }
@@ -258,14 +266,17 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
     const int half = warp >> 2, r = 32 * (warp & 3) + lane;
     bool ok = true;
     auto drain = [&](int n) {
-      // accumulators of pair n: lanes = rows, columns re [0,64) / im [64,128) of band column ic; block by
-      // block, released (acce) once the second block is in registers
+      // accumulators of pair n: lanes = rows, columns re [0,NB) / im [NB,2NB) of band column ic (this warp:
+      // DC columns from DC half); block by block, released (acce) once the second block is in registers
+      constexpr int DC = NB / 2;
       if (!warp_wait(accf, (uint32_t)(n & 1))) return false;
       fence_after();
 #pragma unroll 1
       for (int h = 0; h < 2; ++h) {
-        float re[32], im[32];
-        tmem_ld32x2(tmem + lane_base + h * F_ACC + 32 * half, tmem + lane_base + h * F_ACC + 64 + 32 * half, re, im);
+        float re[DC], im[DC];
+        const uint32_t ta = tmem + lane_base + h * F_ACC + DC * half;
+        if constexpr (DC == 32) tmem_ld32x2(ta, ta + NB, re, im);
+        else tmem_ld16x2(ta, ta + NB, re, im);
         if (h == 1) {
           fence_before();
           __syncwarp();
@@ -275,10 +286,10 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
         if (rb < R) {
           const int row = (int)(rb * 128) + r;
           const int b = row / a.ny, y = row - b * a.ny;
-          float2* dst = a.t + ((long long)b * a.bc + 32 * half) * a.ny + y;
+          float2* dst = a.t + ((long long)b * a.bc + DC * half) * a.ny + y;
 #pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (32 * half + j < a.bc) dst[(long long)j * a.ny] = make_float2(re[j], im[j]);
+          for (int j = 0; j < DC; ++j)
+            if (DC * half + j < a.bc) dst[(long long)j * a.ny] = make_float2(re[j], im[j]);
         }
       }
       return true;
@@ -649,14 +660,16 @@ __global__ void __launch_bounds__(I_NT, 1) rows_inv_tc_kernel(InvArgs a, const _
 }
 
 // --------------------------------------------------------------------------------- constant images
-// Forward: for each 64-column chunk c, W rows n < 64: cos(2 pi (m0c+n) x / nx), rows 64+n: sin(...) (n < bc;
-// zero rows above), K = x = 64c .. 64c+63; [hi | lo].  One thread per (chunk, row, 8 columns).
-__global__ void rows_fwd_consts_kernel(int nx, int m0c, int bc, unsigned char* img) {
+// Forward: for each 64-column chunk c, W rows n < nb: cos(2 pi (m0c+n) x / nx), rows nb+n: sin(...) (n < bc;
+// zero rows above), K = x = 64c .. 64c+63; [hi | lo], 2 (2 nb) 128 bytes per chunk.  nb = 64, or 32 for the
+// Hermitian half (m0c = 0).  One thread per (chunk, row, 8 columns).
+__global__ void rows_fwd_consts_kernel(int nx, int m0c, int bc, int nb, unsigned char* img) {
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int kc = nx / 64;
-  if (id >= (long long)kc * 128 * 8) return;
-  const int c = (int)(id / 1024), row = (int)((id / 8) % 128), q = (int)(id % 8);
-  const int n = row & 63;
+  const uint32_t wop = 2u * nb * 128u;
+  if (id >= (long long)kc * 2 * nb * 8) return;
+  const int c = (int)(id / (16 * nb)), row = (int)((id / 8) % (2 * nb)), q = (int)(id % 8);
+  const int n = row & (nb - 1);
   float v[8];
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
@@ -668,13 +681,13 @@ __global__ void rows_fwd_consts_kernel(int nx, int m0c, int bc, unsigned char* i
       if (p < 0) p += nx;
       sincospi(2.0 * (double)p / (double)nx, &s, &co);
     }
-    v[e] = (float)(row < 64 ? co : s);
+    v[e] = (float)(row < nb ? co : s);
   }
   uint32_t hi[4], lo[4];
   split8(v, hi, lo);
-  unsigned char* o = img + (long long)c * 2 * OPER + swz(row, q);
+  unsigned char* o = img + (long long)c * 2 * wop + swz(row, q);
   *(uint4*)o = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-  *(uint4*)(o + OPER) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  *(uint4*)(o + wop) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
 }
 
 // Inverse: for each 128-column x tile j, rows x (128), K kc = 0: cos(2 pi qc x / nx), kc = 1: sin(...),
@@ -739,36 +752,47 @@ static int sm_count() {
 
 extern "C" int oi_rows_tc_constants(int which, int nx, int m0c, int bc, void* image, long long bytes, void* stream) {
   using namespace oi;
-  if (!image || nx <= 0 || bc <= 0 || bc > 64 || (which != 0 && which != 1))
+  if (!image || nx <= 0 || bc <= 0 || bc > 64 || which < 0 || which > 2)
     return fail(OI_EINVAL, "oi_rows_tc_constants: bad arguments");
   if (nx % 128 != 0 || nx > 4096) return fail(OI_ERANGE, "oi_rows_tc_constants: nx=%d is not a multiple of 128", nx);
-  const long long need = which == 0 ? (long long)(nx / 64) * 2 * rt::OPER : (long long)(nx / 128) * 4 * rt::OPER;
+  // which 2: the Hermitian half of the symmetric band of width bc (m0c = -(bc-1)/2): columns 0 .. (bc-1)/2
+  if (which == 2 && (bc % 2 == 0 || m0c != -(bc - 1) / 2 || (bc + 1) / 2 > 32))
+    return fail(OI_ERANGE, "oi_rows_tc_constants: band %d at %d is not symmetric of width <= 63", bc, m0c);
+  const long long need = which == 0 ? (long long)(nx / 64) * 2 * rt::OPER
+                         : which == 2 ? (long long)(nx / 64) * rt::OPER : (long long)(nx / 128) * 4 * rt::OPER;
   if (bytes < need) return fail(OI_ERANGE, "oi_rows_tc_constants: %lld bytes given, %lld needed", bytes, need);
   if ((uintptr_t)image % 16) return fail(OI_EINVAL, "oi_rows_tc_constants: image not 16-byte aligned");
   const long long threads = need / 16 / 2;
   cudaStream_t s = (cudaStream_t)stream;
   if (which == 0)
-    rt::rows_fwd_consts_kernel<<<(unsigned)ceil_div(threads, 256), 256, 0, s>>>(nx, m0c, bc, (unsigned char*)image);
+    rt::rows_fwd_consts_kernel<<<(unsigned)ceil_div(threads, 256), 256, 0, s>>>(nx, m0c, bc, 64, (unsigned char*)image);
+  else if (which == 2)
+    rt::rows_fwd_consts_kernel<<<(unsigned)ceil_div(threads, 256), 256, 0, s>>>(nx, 0, (bc + 1) / 2, 32,
+                                                                               (unsigned char*)image);
   else
     rt::rows_inv_consts_kernel<<<(unsigned)ceil_div(threads, 256), 256, 0, s>>>(nx, bc, (unsigned char*)image);
   oi::note_launch();
   return check_launch("oi_rows_tc_constants");
 }
 
-extern "C" int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, int nx, int m0c, int bc,
-                              const void* consts, void* t, void* stream) {
-  using namespace oi;
-  if (!field || !consts || !t || batch <= 0 || bc <= 0) return fail(OI_EINVAL, "oi_rows_fwd_tc: bad arguments");
+namespace oi {
+
+// The forward row pass at NB band columns per part (64: oi_rows_fwd_tc; 32: oi_rows_fwd_tc_half); `what` names
+// the entry point in errors.
+template <int NB>
+static int rows_fwd_launch(const void* field, int kind, int batch, int ny, int nx, int bc, const void* consts, void* t,
+                           void* stream, const char* what) {
+  if (!field || !consts || !t || batch <= 0 || bc <= 0) return fail(OI_EINVAL, "%s: bad arguments", what);
   if (kind != OI_FIELD_REAL_F32 && kind != OI_FIELD_U8)
-    return fail(OI_EINVAL, "oi_rows_fwd_tc: real float32 or uint8 masks only (kind=%d)", kind);
-  if (ny % 128 != 0 || nx % 128 != 0 || nx > 4096 || bc > 64)
-    return fail(OI_ERANGE, "oi_rows_fwd_tc: grid %dx%d / band width %d unsupported", ny, nx, bc);
+    return fail(OI_EINVAL, "%s: real float32 or uint8 masks only (kind=%d)", what, kind);
+  if (ny % 128 != 0 || nx % 128 != 0 || nx > 4096 || bc > NB)
+    return fail(OI_ERANGE, "%s: grid %dx%d / band width %d unsupported", what, ny, nx, bc);
   if ((uintptr_t)field % 16 || (uintptr_t)consts % 16)
-    return fail(OI_EINVAL, "oi_rows_fwd_tc: field and constants must be 16-byte aligned");
+    return fail(OI_EINVAL, "%s: field and constants must be 16-byte aligned", what);
   const long long rows = (long long)batch * ny, items = (rows / 128 + 1) / 2;   // pairs of row blocks
   const int sms = rt::sm_count();
-  if (!sms) return fail(OI_ECUDA, "oi_rows_fwd_tc: no CUDA device");
-  if (rows + 256 > 0x7fffffffLL) return fail(OI_ERANGE, "oi_rows_fwd_tc: %lld rows exceed the tensor-map range", rows);
+  if (!sms) return fail(OI_ECUDA, "%s: no CUDA device", what);
+  if (rows + 256 > 0x7fffffffLL) return fail(OI_ERANGE, "%s: %lld rows exceed the tensor-map range", what, rows);
   const long long ctas = items < sms ? items : sms;
   rt::FwdArgs a{rows, ny, nx, bc, (const unsigned char*)consts, (float2*)t};
   cudaStream_t s = (cudaStream_t)stream;
@@ -779,18 +803,32 @@ extern "C" int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, in
                          u8 ? 64 : 32, 128, u8 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B);
   if (rc) return rc;
   if (u8) {
-    rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_U8>, rt::F_SMEM, "oi_rows_fwd_tc");
+    rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_U8, NB>, rt::F_SMEM, what);
     if (rc) return rc;
-    (void)launch_pdl(rt::rows_fwd_tc_kernel<OI_FIELD_U8>, dim3((unsigned)ctas), dim3(rt::F_NT), rt::F_SMEM, s, a, map);
-    oi::note_launch();
-  } else {
-    rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32>, rt::F_SMEM, "oi_rows_fwd_tc");
-    if (rc) return rc;
-    (void)launch_pdl(rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32>, dim3((unsigned)ctas), dim3(rt::F_NT), rt::F_SMEM, s, a,
+    (void)launch_pdl(rt::rows_fwd_tc_kernel<OI_FIELD_U8, NB>, dim3((unsigned)ctas), dim3(rt::F_NT), rt::F_SMEM, s, a,
                      map);
     oi::note_launch();
+  } else {
+    rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32, NB>, rt::F_SMEM, what);
+    if (rc) return rc;
+    (void)launch_pdl(rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32, NB>, dim3((unsigned)ctas), dim3(rt::F_NT), rt::F_SMEM,
+                     s, a, map);
+    oi::note_launch();
   }
-  return check_launch("oi_rows_fwd_tc");
+  return check_launch(what);
+}
+
+}  // namespace oi
+
+extern "C" int oi_rows_fwd_tc(const void* field, int kind, int batch, int ny, int nx, int m0c, int bc,
+                              const void* consts, void* t, void* stream) {
+  (void)m0c;   // carried by the constant image
+  return oi::rows_fwd_launch<64>(field, kind, batch, ny, nx, bc, consts, t, stream, "oi_rows_fwd_tc");
+}
+
+extern "C" int oi_rows_fwd_tc_half(const void* field, int kind, int batch, int ny, int nx, int bch, const void* consts,
+                                   void* t, void* stream) {
+  return oi::rows_fwd_launch<32>(field, kind, batch, ny, nx, bch, consts, t, stream, "oi_rows_fwd_tc_half");
 }
 
 namespace oi {

@@ -133,13 +133,20 @@ class Plan:
         return (form == 'bf16x3' and self.fft and self.ny % 128 == 0 and self.nx % 128 == 0 and b.bc <= 64
                 and b.br <= 64)
 
+    def symmetric_band(self) -> bool:
+        """Odd band centred on frequency 0 in both axes (m0 = -(b-1)/2): a real mask's band spectrum then follows
+        from its non-negative columns, band[-ky][-kx] = conj(band[ky][kx])."""
+        b = self.band
+        return b.br % 2 == 1 and b.bc % 2 == 1 and b.m0r == -(b.br - 1) // 2 and b.m0c == -(b.bc - 1) // 2
+
     def rows_consts(self, which: int) -> torch.Tensor:
-        """Constant operand image of the tensor-core row pass: 0 forward (band columns), 1 inverse (synthesis)."""
+        """Constant operand image of the tensor-core row pass: 0 forward (band columns), 1 inverse (synthesis),
+        2 forward over the non-negative half of a symmetric band."""
         attr = '_rows_consts_%d' % which
         c = getattr(self, attr, None)
         if c is None:
             b = self.band
-            nbytes = (self.nx // 64) * 32768 if which == 0 else (self.nx // 128) * 65536
+            nbytes = {0: (self.nx // 64) * 32768, 1: (self.nx // 128) * 65536, 2: (self.nx // 64) * 16384}[which]
             c = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
             N.call('oi_rows_tc_constants', which, self.nx, b.m0c, b.bc, N.ptr(c), nbytes, N.stream_handle(self.device))
             setattr(self, attr, c)
@@ -228,7 +235,10 @@ def band_spectrum(field: torch.Tensor, kind: int, plan: Plan, nch: int = 1, scal
     band = torch.empty((batch, nch, b.br, b.bc), dtype=torch.complex64, device=plan.device)
     s = N.stream_handle(plan.device)
     sc = float(scale / (plan.ny * plan.nx))
-    if plan.tc_rows(form) and kind != N.FIELD_COMPLEX_C64 and nch == 1:
+    if plan.tc_rows(form) and kind != N.FIELD_COMPLEX_C64 and nch == 1 and plan.symmetric_band():
+        N.call('oi_band_spectrum_tc_sym', N.ptr(field), kind, batch, plan.ny, plan.nx, b.br, b.bc,
+               N.ptr(plan.rows_consts(2)), N.ptr(plan.wn_y), sc, N.ptr(scratch), N.ptr(band), s)
+    elif plan.tc_rows(form) and kind != N.FIELD_COMPLEX_C64 and nch == 1:
         N.call('oi_band_spectrum_tc', N.ptr(field), kind, batch, plan.ny, plan.nx, b.m0r, b.br, b.m0c, b.bc,
                N.ptr(plan.rows_consts(0)), N.ptr(plan.wn_y), sc, N.ptr(scratch), N.ptr(band), s)
     elif plan.use_fft(form) and kind != N.FIELD_COMPLEX_C64 and nch == 1:

@@ -243,3 +243,75 @@ def test_rows_fwd_tc_direct(oi, count, ny, nx, m0c, bc, u8):
     print(f'forward rows {count}x{ny}x{nx} bc {bc} u8={u8}: max {err:.2e}')
     assert err < 2e-5
     assert N.device_status() == 0
+
+
+@pytest.mark.parametrize('count,ny,nx,bc,u8', [(1, 384, 256, 15, False), (3, 640, 512, 59, False),
+                                               (2, 256, 1024, 63, True), (5, 1024, 1024, 59, False)])
+def test_rows_fwd_tc_half_direct(oi, count, ny, nx, bc, u8):
+    """The Hermitian-half forward row pass (oi_rows_fwd_tc_half, constants of oi_rows_tc_constants(2, ...)) against
+    FP64 t[b][kx][y] = sum_x mask[b][y][x] exp(+2 pi i kx x / nx), kx = 0 .. (bc-1)/2: odd block counts, the widest
+    half (32 columns), uint8 masks."""
+    from opticalimaging_b200 import _native as N
+    dev = torch.device('cuda')
+    rng = np.random.default_rng(count * ny + nx + 1)
+    if u8:
+        m = (rng.random((count, ny, nx)) > 0.5).astype(np.uint8) * rng.integers(1, 255, (count, ny, nx)).astype(np.uint8)
+    else:
+        m = (rng.random((count, ny, nx)) > 0.6).astype(np.float32) * rng.random((count, ny, nx)).astype(np.float32)
+    s = N.stream_handle(dev)
+    bch = (bc + 1) // 2
+    nbytes = (nx // 64) * 16384
+    consts = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    N.call('oi_rows_tc_constants', 2, nx, -(bc - 1) // 2, bc, N.ptr(consts), nbytes, s)
+    md = torch.from_numpy(m).to(dev)
+    t = torch.full((count, bch + 1, ny), complex(float('nan'), 0.0), dtype=torch.complex64, device=dev)
+    N.call('oi_rows_fwd_tc_half', N.ptr(md), N.FIELD_U8 if u8 else N.FIELD_REAL_F32, count, ny, nx, bch,
+           N.ptr(consts), N.ptr(t), s)
+    got = t.cpu().numpy().reshape(-1)[:count * bch * ny].reshape(count, bch, ny)
+    assert np.isnan(t.cpu().numpy().reshape(-1)[count * bch * ny:]).all()     # nothing written past the output
+    E = np.exp(2j * np.pi * np.outer(np.arange(nx), np.arange(bch)) / nx)        # [nx][bch]
+    want = np.stack([(m[i].astype(np.float64) @ E).T for i in range(count)])    # [count][bch][ny]
+    err = rel_err(got, want)
+    print(f'forward half rows {count}x{ny}x{nx} bch {bch} u8={u8}: max {err:.2e}')
+    assert err < 2e-5
+    assert N.device_status() == 0
+
+
+def test_rows_tc_constants_half_rejects_asymmetric_band(oi):
+    from opticalimaging_b200 import _native as N
+    dev = torch.device('cuda')
+    c = torch.empty(4 * 16384, dtype=torch.uint8, device=dev)
+    for m0c, bc in ((-6, 15), (-7, 16), (-32, 65)):
+        with pytest.raises(N.NativeError):
+            N.call('oi_rows_tc_constants', 2, 256, m0c, bc, N.ptr(c), c.numel(), N.stream_handle(dev))
+
+
+@pytest.mark.parametrize('batch,n,b', [(3, 256, 15), (2, 1024, 59), (1, 512, 63)])
+def test_band_spectrum_tc_sym_matches_full(oi, batch, n, b):
+    """The symmetric-band spectrum (half row pass + mirrored column pass) against the full tensor-core row pass
+    and against FP64, float32 masks."""
+    from opticalimaging_b200 import engine as E, _native as N
+    dev = torch.device('cuda')
+    band = E.Band(-(b - 1) // 2, b, -(b - 1) // 2, b)
+    plan = E.Plan.get(n, n, band, dev)
+    assert plan.symmetric_band()
+    rng = np.random.default_rng(n + b)
+    m = ((rng.random((batch, n, n)) > 0.6) * rng.random((batch, n, n))).astype(np.float32)
+    md = torch.from_numpy(m).to(dev)
+    s = N.stream_handle(dev)
+    scratch = torch.empty(batch * n * b, dtype=torch.complex64, device=dev)
+    full = torch.empty((batch, 1, b, b), dtype=torch.complex64, device=dev)
+    half = torch.full((batch, 1, b, b), complex(float('nan'), 0.0), dtype=torch.complex64, device=dev)
+    N.call('oi_band_spectrum_tc', N.ptr(md), N.FIELD_REAL_F32, batch, n, n, band.m0r, b, band.m0c, b,
+           N.ptr(plan.rows_consts(0)), N.ptr(plan.wn_y), 1.0 / (n * n), N.ptr(scratch), N.ptr(full), s)
+    N.call('oi_band_spectrum_tc_sym', N.ptr(md), N.FIELD_REAL_F32, batch, n, n, b, b, N.ptr(plan.rows_consts(2)),
+           N.ptr(plan.wn_y), 1.0 / (n * n), N.ptr(scratch), N.ptr(half), s)
+    h, f = half.cpu().numpy(), full.cpu().numpy()
+    assert not np.isnan(h).any()
+    k = np.arange(b) - (b - 1) // 2
+    Ey = np.exp(2j * np.pi * np.outer(k, np.arange(n)) / n)       # [ky][y]
+    Ex = np.exp(2j * np.pi * np.outer(np.arange(n), k) / n)       # [x][kx]
+    want = np.stack([Ey @ m[i].astype(np.float64) @ Ex for i in range(batch)])[:, None] / (n * n)
+    assert rel_err(h, want) < 2e-5
+    assert rel_err(h, f) < 2e-5
+    assert N.device_status() == 0
