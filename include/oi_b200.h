@@ -162,8 +162,9 @@ OI_API int oi_coarse_to_image_fft(float* coarse, int nparts, int count, int mr, 
                                   void* scratch_v, float* out, void* stream);
 
 /*
- * FFT form of oi_coherent_coarse for coarse grids of 64 or 128 per axis: the fields of each (image, plane) are
- * split over `nsplit` blocks that write partial sums coarse[s][b][z][mr][mc] (s < nsplit), which
+ * FFT form of oi_coherent_coarse for coarse grids of 64 or 128 per axis, or of 256 x 256 (bands up to 128 x 128;
+ * one block of 512 threads per SM holding its 256 x 256 partial sum in tensor memory): the fields of each
+ * (image, plane) are split over `nsplit` blocks that write partial sums coarse[s][b][z][mr][mc] (s < nsplit), which
  * oi_coarse_to_image_fft adds (nparts = nsplit).  wr / wc: oi_twiddle(1, m, 1, 0, m, +1) for m = mr / mc.
  * The band starts at frequency (m0r, m0c).
  */
