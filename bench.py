@@ -409,7 +409,7 @@ def cpu_reference_sample(sk_info, masks_np, budget_s, threads):
 
 # DRAM bytes per launch (read + write) of the three largest kernels at this workload, from the ncu capture
 # summarised in profiles/socs24-1024-bf16x3-step.md
-NCU_TRAFFIC = {"rows_fwd_tc": 289.7e6, "rows_inv_tc": 247.9e6, "coherent_tc": 2.6e6}
+NCU_TRAFFIC = {"rows_fwd_tc": 275.9e6, "rows_inv_tc": 243.9e6, "coherent_tc": 2.6e6}
 
 
 def kernel_rooflines(sk, masks, reps=10):
