@@ -203,10 +203,12 @@ def serve_measure(sk, info, masks_np, dev, args):
                            build=lambda: serve_model_from(sk, args.form))
     plain_spec = serve.ModelSpec(('socs24', N_PIX, PERIOD, 'fft'), N_PIX, N_PIX, 1,
                                  build=lambda: serve_model_from(sk, 'fft'))
-    pinned = [torch.from_numpy(m.astype(np.uint8)).pin_memory() for m in masks_np]
+    # masks and result buffers as views of one pinned slab each: consecutive requests' buffers are adjacent, so
+    # the executor moves a batch's runs with one copy each
+    pinned = list(torch.from_numpy(np.stack([m.astype(np.uint8) for m in masks_np])).pin_memory())
     nreq = max(4 * BATCH, args.serve_requests)
     window = 4 * BATCH
-    ring = [torch.empty((1, N_PIX, N_PIX), dtype=torch.float32).pin_memory() for _ in range(nreq)]
+    ring = list(torch.empty((nreq, 1, N_PIX, N_PIX), dtype=torch.float32).pin_memory())
     ex = serve.CudaExecutor(device=dev, nslots=3)
     srv = serve.Server(ex, hbm_budget=150e9, max_batch=BATCH)
 

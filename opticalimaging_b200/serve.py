@@ -12,7 +12,8 @@ under the kernels of another, and requests that arrive while batches are in flig
 
 The scheduler only talks to an executor interface (``launch`` / ``poll`` / ``collect`` / memory accounting), so
 its batching, admission and failure handling are exercised on the CPU with a fake executor in the tests; the
-device executor is ``CudaExecutor``.
+device executor is ``CudaExecutor``.  Masks and caller-provided result buffers that are consecutive views of one
+(pinned) slab are moved with one copy per run rather than one per request (``adjacent_runs``).
 
 Failure behaviour: a malformed request (wrong shape or dtype) fails at submit; a request whose batch can never
 fit the budget fails with MemoryError; a cancelled future is dropped before launch; an executor error fails
@@ -54,6 +55,36 @@ class Request:
     t_done: float = 0.0
     rid: int = 0
     out: torch.Tensor | None = None   # caller-provided result storage [planes, ny, nx] float32
+
+
+def adjacent_runs(tensors) -> list:
+    """Split a batch's host tensors into runs [i, j) that lie back to back in one storage: same shape, dtype and
+    device, contiguous, tensors[k + 1] starting where tensors[k] ends (views of one slab, in order).  A run moves
+    between host and device as one copy instead of j - i."""
+    runs, i, n = [], 0, len(tensors)
+    while i < n:
+        j, t0 = i + 1, tensors[i]
+        if t0.is_contiguous():
+            base = t0.untyped_storage().data_ptr()
+            while j < n:
+                a, b = tensors[j - 1], tensors[j]
+                if not (b.is_contiguous() and b.shape == t0.shape and b.dtype == t0.dtype and b.device == t0.device
+                        and b.untyped_storage().data_ptr() == base
+                        and b.storage_offset() == a.storage_offset() + a.numel()):
+                    break
+                j += 1
+        runs.append((i, j))
+        i = j
+    return runs
+
+
+def run_view(tensors, i: int, j: int) -> torch.Tensor:
+    """The run [i, j) of adjacent_runs as one tensor [j - i, *shape] over the same memory."""
+    t0 = tensors[i]
+    if j - i == 1:
+        return t0.unsqueeze(0)
+    return torch.empty(0, dtype=t0.dtype, device=t0.device).set_(t0.untyped_storage(), t0.storage_offset(),
+                                                                  (j - i,) + tuple(t0.shape))
 
 
 def bucket(n: int) -> int:
@@ -372,16 +403,18 @@ class CudaExecutor:
         graph = self._graph(spec, model, slot, dtype, b, d_in, d_out) if self.use_graphs else None
         s = self.streams[slot]
         with torch.cuda.device(self.device), torch.cuda.stream(s):
-            for i, r in enumerate(reqs):
-                d_in[i].copy_(r.mask, non_blocking=True)
+            masks = [r.mask for r in reqs]
+            for i, j in adjacent_runs(masks):             # masks that are adjacent views of one slab: one copy
+                d_in[i:j].copy_(run_view(masks, i, j), non_blocking=True)
             if graph is not None:
                 graph.replay()
             else:
                 model.image(d_in[:n], out=d_out[:n])
             if all(r.out is not None for r in reqs):      # caller-provided storage: copy each image there
-                for i, r in enumerate(reqs):
-                    r.out.copy_(d_out[i], non_blocking=True)
-                out = [r.out for r in reqs]
+                outs = [r.out for r in reqs]
+                for i, j in adjacent_runs(outs):
+                    run_view(outs, i, j).copy_(d_out[i:j], non_blocking=True)
+                out = outs
             elif self.result_device == 'cpu':
                 # bucket-sized pinned buffer: sizes repeat, so the host caching allocator recycles them
                 host = torch.empty((b, spec.planes, spec.ny, spec.nx), dtype=torch.float32, pin_memory=True)

@@ -90,3 +90,30 @@ def test_prepare_captures_every_bucket():
         f.result(timeout=120)
     srv.close()
     assert len(ex.graphs) == n0
+
+
+@pytest.mark.parametrize('shuffle', [False, True])
+def test_slab_buffers_coalesced_match_alone(shuffle):
+    """Masks and caller-provided result buffers that are views of one pinned slab: in slab order the executor
+    moves each batch's runs with one copy each, shuffled the runs break up; every result equals the request alone
+    and lands in its own buffer."""
+    from opticalimaging_b200 import serve, workloads as W
+    sp = _specs()[0]
+    n = 24
+    rng = np.random.default_rng(3)
+    masks = torch.from_numpy(np.stack([(W.rect_mask(sp.ny, sp.nx, 2.0 * sp.ny, 2.0 * sp.nx, 20, 30, 300, rng) > 0)
+                                       .astype(np.uint8) for _ in range(n)])).pin_memory()
+    outs = torch.full((n, sp.planes, sp.ny, sp.nx), float('nan')).pin_memory()
+    order = list(range(n))
+    if shuffle:
+        rng.shuffle(order)
+    ex = serve.CudaExecutor(nslots=3)
+    srv = serve.Server(ex, hbm_budget=40e9, max_batch=8)
+    futs = {i: srv.submit(sp, masks[i], out=outs[i]) for i in order}
+    got = {i: f.result(timeout=300) for i, f in futs.items()}
+    srv.close()
+    model = ex.models[sp.key]
+    alone = model.image(masks.cuda()).cpu()
+    for i in range(n):
+        assert got[i].data_ptr() == outs[i].data_ptr()
+        assert rel_err(outs[i].numpy(), alone[i].numpy()) < TOL

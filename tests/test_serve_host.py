@@ -135,3 +135,22 @@ def test_submit_after_close_is_refused():
     srv.close()
     with pytest.raises(RuntimeError):
         srv.submit(spec('a'), torch.ones(4, 4)).result(timeout=1)
+
+
+def test_adjacent_runs_groups_slab_views_only():
+    from opticalimaging_b200.serve import adjacent_runs, run_view
+    slab = torch.arange(6 * 2 * 3, dtype=torch.float32).reshape(6, 2, 3)
+    views = list(slab)
+    assert adjacent_runs(views) == [(0, 6)]
+    r = run_view(views, 1, 4)
+    assert r.shape == (3, 2, 3) and r.data_ptr() == views[1].data_ptr() and torch.equal(r, slab[1:4])
+    r.fill_(-1.0)                                  # the view writes the slab itself
+    assert torch.equal(slab[2], torch.full((2, 3), -1.0))
+    # out of order, a gap, another storage, another dtype or shape, a non-contiguous view: runs break there
+    other = torch.zeros(2, 3)
+    mixed = [views[0], views[1], views[3], other, views[4], views[5].to(torch.float64), slab[:, 0][0:2].t()[0]]
+    assert adjacent_runs(mixed) == [(0, 2), (2, 3), (3, 4), (4, 5), (5, 6), (6, 7)]
+    assert adjacent_runs([views[2], views[1]]) == [(0, 1), (1, 2)]
+    assert adjacent_runs([]) == []
+    single = run_view([other], 0, 1)
+    assert single.shape == (1, 2, 3) and single.data_ptr() == other.data_ptr()
