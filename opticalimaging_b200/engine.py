@@ -35,7 +35,7 @@ def require_cuda(device=None) -> torch.device:
     if not torch.cuda.is_available():
         raise N.NativeError('opticalimaging_b200 needs a CUDA device; there is no CPU path')
     d = torch.device(device) if device is not None else torch.device('cuda', torch.cuda.current_device())
-    if d.type != 'cuda':
+    if d.type != 'cuda' or d.index is None:   # 'cuda' alone means the current device
         d = torch.device('cuda', torch.cuda.current_device())
     N.load()
     return d

@@ -17,7 +17,9 @@ device executor is ``CudaExecutor``.  Masks and caller-provided result buffers t
 
 Failure behaviour: a malformed request (wrong shape or dtype) fails at submit; a request whose batch can never
 fit the budget fails with MemoryError; a cancelled future is dropped before launch; an executor error fails
-the futures of its batch and the server keeps serving.
+the futures of its batch and the server keeps serving.  An error that escapes the scheduler thread itself (for
+instance the executor's thread set-up) closes the server and fails every request it holds; later submits fail
+at once.
 """
 from __future__ import annotations
 
@@ -109,6 +111,7 @@ class Server:
         self._slots = [None] * executor.nslots            # slot -> (spec, [requests])
         self._last_used: dict = {}
         self._closed = False
+        self.error = None            # the exception that ended the scheduler thread, if one did
         self._rid = 0
         self.completed = []          # (submit, done) times of finished requests, for latency statistics
         self.batches = 0
@@ -136,7 +139,8 @@ class Server:
             return fut
         with self._cv:
             if self._closed:
-                fut.set_exception(RuntimeError('server is closed'))
+                fut.set_exception(RuntimeError('server is closed' if self.error is None else
+                                               f'server is closed: its scheduler thread failed ({self.error!r})'))
                 return fut
             self._rid += 1
             self._inbox.append(Request(spec, mask, fut, time.perf_counter(), rid=self._rid, out=out))
@@ -180,6 +184,36 @@ class Server:
         return self._max_batch(spec)
 
     def _run(self):
+        try:
+            self._loop()
+        except BaseException as e:  # noqa: BLE001 -- the scheduler must not die silently with requests waiting
+            self._fail_all(e)
+
+    def _fail_all(self, err: BaseException):
+        """The scheduler thread is ending on an unexpected error: close the server and fail every request it
+        holds -- queued, pending and in flight -- with that error, so no caller waits forever."""
+        with self._cv:
+            self._closed = True
+            self.error = err
+            reqs = list(self._inbox)
+            self._inbox.clear()
+            for q in self._pending.values():
+                reqs.extend(q)
+            self._pending.clear()
+            for i, s in enumerate(self._slots):
+                if s is not None:
+                    reqs.extend(s[1])
+                    self._slots[i] = None
+        failure = RuntimeError(f'the server\'s scheduler thread failed: {type(err).__name__}: {err}')
+        failure.__cause__ = err
+        for r in reqs:
+            if not r.future.done():
+                try:
+                    r.future.set_exception(failure)
+                except cf.InvalidStateError:   # completed or cancelled meanwhile
+                    pass
+
+    def _loop(self):
         init = getattr(self.ex, 'thread_init', None)
         if init is not None:
             init()

@@ -61,3 +61,17 @@ def test_abbe_band_covers_every_shifted_pupil():
     # clipped to the grid's frequencies
     b = E.abbe_band(16, 16, 20.0, 20.0, sx, sy)
     assert b.m0r >= -8 and b.m0r + b.br - 1 <= 7
+
+
+def test_require_cuda_resolves_a_bare_cuda_device(monkeypatch):
+    """'cuda' without an index means the current device (a scheduler thread calls torch.cuda.set_device with
+    it, which needs an index); no GPU needed: CUDA availability is faked."""
+    import torch
+    from opticalimaging_b200 import engine as E, _native as N
+    monkeypatch.setattr(torch.cuda, 'is_available', lambda: True)
+    monkeypatch.setattr(torch.cuda, 'current_device', lambda: 3)
+    monkeypatch.setattr(N, 'load', lambda *a, **k: None)
+    assert E.require_cuda(torch.device('cuda')) == torch.device('cuda', 3)
+    assert E.require_cuda('cuda') == torch.device('cuda', 3)
+    assert E.require_cuda(None) == torch.device('cuda', 3)
+    assert E.require_cuda('cuda:1') == torch.device('cuda', 1)

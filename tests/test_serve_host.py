@@ -154,3 +154,43 @@ def test_adjacent_runs_groups_slab_views_only():
     assert adjacent_runs([]) == []
     single = run_view([other], 0, 1)
     assert single.shape == (1, 2, 3) and single.data_ptr() == other.data_ptr()
+
+
+class SetupFailsExecutor(FakeExecutor):
+    def thread_init(self):
+        raise ValueError('thread set-up failed (injected on the host)')
+
+
+class PollFailsExecutor(FakeExecutor):
+    """Fails inside the scheduler loop once a batch is in flight (an error outside launch/collect)."""
+
+    def poll(self, slot):
+        if self.slot[slot] is not None:
+            raise KeyError('poll failed (injected on the host)')
+        return False
+
+
+def test_scheduler_setup_failure_fails_requests_instead_of_hanging():
+    srv = Server(SetupFailsExecutor(), hbm_budget=1e9)
+    srv._thread.join(timeout=10)
+    assert not srv._thread.is_alive()
+    f = srv.submit(spec('a'), torch.ones(4, 4))
+    with pytest.raises(RuntimeError, match='scheduler thread failed'):
+        f.result(timeout=5)
+    assert isinstance(srv.error, ValueError)
+    srv.close()
+
+
+def test_scheduler_failure_in_flight_fails_queued_and_running_requests():
+    ex = PollFailsExecutor(nslots=1, delay=0.5)
+    srv = Server(ex, hbm_budget=1e9)
+    futs = [srv.submit(spec('a'), torch.full((4, 4), float(i))) for i in range(20)]   # more than one batch
+    for f in futs:
+        with pytest.raises(RuntimeError, match='scheduler thread failed'):
+            f.result(timeout=10)
+    assert isinstance(srv.error, KeyError)
+    late = srv.submit(spec('a'), torch.ones(4, 4))
+    with pytest.raises(RuntimeError, match='scheduler thread failed'):
+        late.result(timeout=1)
+    srv.drain(timeout=5)
+    srv.close()
