@@ -75,3 +75,23 @@ def test_require_cuda_resolves_a_bare_cuda_device(monkeypatch):
     assert E.require_cuda('cuda') == torch.device('cuda', 3)
     assert E.require_cuda(None) == torch.device('cuda', 3)
     assert E.require_cuda('cuda:1') == torch.device('cuda', 1)
+
+
+def test_field_split_sm_minimises_waves_times_fields():
+    """The field split of the one-block-per-SM coherent kernel (256 x 256 coarse grid): the d in [1, nfields]
+    minimising ceil(blocks d / SMs) * (ceil(nfields / d) + 1/2), the smallest d on ties."""
+    from opticalimaging_b200.engine import SM_COUNT, field_split_sm
+
+    def cost(nf, b, d):
+        return -(-b * d // SM_COUNT) * (-(-nf // d) + 0.5)
+
+    assert field_split_sm(324, 8) == 18      # vector Abbe 2048^2 at batch 8: 144 blocks of 18 fields, one wave
+    assert field_split_sm(24, 8) == 12       # SOCS-24: 96 blocks of 2 fields (18 ties, more partial sums)
+    assert field_split_sm(1, 1) == 1
+    for nf in (1, 5, 24, 72, 324):
+        for b in (1, 2, 8, 64, 200):
+            d = field_split_sm(nf, b)
+            assert 1 <= d <= nf
+            best = min(cost(nf, b, e) for e in range(1, nf + 1))
+            assert cost(nf, b, d) == best
+            assert all(cost(nf, b, e) > best for e in range(1, d))
