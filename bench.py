@@ -129,11 +129,20 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The largest x over the ranks (NCCL reduces a device tensor, gloo a host one)."""
     if world == 1:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dev = 'cuda' if torch.distributed.get_backend() == 'nccl' else 'cpu'
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(units_per_rank, ms, world):
+    """Whole-job throughput of `world` replicas that each processed `units_per_rank` units, `ms` being this
+    rank's device time: every rank's units over the slowest rank's time.  Returns (units per second, max ms)."""
+    m = max_over_ranks(ms, world)
+    return world * units_per_rank / (m / 1000.0), m
 
 
 def build_kernels():
@@ -578,8 +587,7 @@ def run_engine(args, world, rank, local):
         torch.cuda.synchronize()
         barrier(world)
         clk.wait_samples(len(clk.lines) + 1, timeout=0.5)
-    ms = max_over_ranks(start.elapsed_time(end), world)
-    value = world * BATCH * args.steps / (ms / 1000.0)
+    value, ms = job_rate(BATCH * args.steps, start.elapsed_time(end), world)
     # ---- end to end through the public API: pinned uint8 masks in, float32 images out
     host_in = torch.from_numpy(masks_np.astype(np.uint8)).pin_memory()
     host_out = torch.empty((BATCH, N_PIX, N_PIX), dtype=torch.float32).pin_memory()
@@ -598,8 +606,7 @@ def run_engine(args, world, rank, local):
     e2.record()
     torch.cuda.synchronize()
     barrier(world)
-    ms_e2e = max_over_ranks(s2.elapsed_time(e2), world)
-    e2e_value = world * BATCH * args.steps / (ms_e2e / 1000.0)
+    e2e_value, _ = job_rate(BATCH * args.steps, s2.elapsed_time(e2), world)
     # ---- served: the same clips as requests through the continuous-batching server (pinned uint8 in,
     # host float32 images out), saturated arrival; and the plain one-request-at-a-time path
     serving = serve_measure(sk, info, masks_np, dev, args) if not args.no_serve else None
