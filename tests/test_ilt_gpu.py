@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 import torch
 
-from tests.fixtures import load, make_source, rel_err
+from tests.fixtures import load, rel_err
 
 pytestmark = pytest.mark.gpu
 
