@@ -607,6 +607,8 @@ def run_engine(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     e2e_value, _ = job_rate(BATCH * args.steps, s2.elapsed_time(e2), world)
+    if rank != 0:   # the last collective is behind us; what follows is reported by rank 0 alone
+        return
     # ---- served: the same clips as requests through the continuous-batching server (pinned uint8 in,
     # host float32 images out), saturated arrival; and the plain one-request-at-a-time path
     serving = serve_measure(sk, info, masks_np, dev, args) if not args.no_serve else None
