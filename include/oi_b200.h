@@ -87,8 +87,9 @@ OI_API int oi_band_spectrum(const void* field, int kind, int batch, int ny, int 
  *   - Same inputs, output and result as oi_band_spectrum; the row-transform scratch is an array built into the
  *     library, OI_NOALLOC_SCRATCH_COMPLEX complex values (16 MiB) on every GPU that loads it, held until the
  *     process exits.  batch * nch * ny * bc above that capacity is rejected with OI_ERANGE.
- *   - Calls no cudaMalloc / cudaFree.  The first call on each device looks up the array's device address
- *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - Calls no cudaMalloc / cudaFree.  A call looks up the array's device address (cudaGetSymbolAddress) on
+ *     the current device unless its stream is capturing, when it uses the address the previous call found; so
+ *     make the first call on each device before any stream capture.
  *   - All calls on a device share the one array: calls that can overlap on the GPU (different streams without
  *     ordering between them) race.  Nothing in the array needs clearing between calls.
  */

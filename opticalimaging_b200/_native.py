@@ -126,6 +126,22 @@ def device_status(reset: bool = False) -> int:
     return st.value
 
 
+class DeviceWaitError(NativeError):
+    """A kernel's bounded wait expired (the device status word was set): the results it wrote are invalid."""
+
+
+def check_device_status(what: str, reader=None) -> None:
+    """Raise DeviceWaitError if a kernel's bounded wait has expired since the last check (the status word is
+    then cleared, so the next work starts clean).  Call it after synchronising with the work it covers.
+    `reader(reset)` replaces device_status (tests)."""
+    read = device_status if reader is None else reader
+    st = read(False)
+    if st:
+        read(True)
+        raise DeviceWaitError(f'{what}: a kernel ended early on an expired wait (device status {st}); its results '
+                              'are invalid')
+
+
 def launch_count() -> int:
     """Kernel launches the library has enqueued so far (graph replays are not counted)."""
     n = ctypes.c_longlong(0)

@@ -25,7 +25,9 @@
 // MMAs and commits them to mbarriers.  Accumulators are double-buffered so that draining
 // overlaps the MMAs of the next blocks.
 // Every mbarrier wait is bounded (2 s); on expiry the role records the status (oi_device_status) and stops,
-// the others then expire in turn, and the CTA frees tensor memory and exits.
+// the others then expire in turn.  Before the CTA frees tensor memory and exits, each producer waits (bounded)
+// for the copies it issued to land and the MMA thread commits its issued MMAs to a barrier and waits for them,
+// so nothing writes shared or tensor memory after it is released.
 #include <cuda.h>
 #include "tc_common.cuh"
 
@@ -66,6 +68,17 @@ struct Ring {
     }
   }
 };
+
+// Wait (bounded) for the last copies of a ring of n slots whose cursor is `c` after `g` issued copies (copy g-k
+// went to slot (g-k) mod n, in the cursor's round when that slot is below the cursor, else the round before).
+// Returns immediately for copies already consumed: their slot's barrier is then one phase further.
+__device__ __forceinline__ void drain_ring(uint32_t full, const Ring& c, int g, int n) {
+  const int last = g < n ? g : n;
+  for (int k = 1; k <= last; ++k) {
+    const int s = (c.slot - k + n) % n;
+    wait_bar(full + 8 * s, s < c.slot ? c.phase : c.phase ^ 1u);
+  }
+}
 
 // 8 floats -> 4 packed bf16 hi words and 4 lo words
 __device__ __forceinline__ void split8(const float (&v)[8], uint32_t (&hi)[4], uint32_t (&lo)[4]) {
@@ -127,9 +140,9 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   const uint32_t misc = base + F_MISC;
   // barriers: sfull[2] (staging landed), sfree[2] (staging read), wfull[3] (W landed), wdone[3] (MMAs reading
   // the W slot finished), conv[2] (A slot written), adone[2] (MMAs reading the A slot finished), accf
-  // (accumulators complete), acce (accumulators drained)
+  // (accumulators complete), acce (accumulators drained), fin (every issued MMA finished, at the end)
   const uint32_t sfull = misc, sfree = misc + 16, wfull = misc + 32, wdone = misc + 56, conv = misc + 80,
-                 adone = misc + 96, accf = misc + 112, acce = misc + 120;
+                 adone = misc + 96, accf = misc + 112, acce = misc + 120, fin = misc + 128;
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + F_MISC + 192);
   // per A slot and converter warp: 1 when the warp's part of the chunk has a non-zero bf16 lo half (a mask value
   // not exact in bf16); when no warp sets it the lo x hi products are exactly zero and are not issued
@@ -160,6 +173,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
     }
     mbar_init(accf, 1);
     mbar_init(acce, 8);
+    mbar_init(fin, 1);
     mbar_init_fence();
   }
   fence_before();
@@ -175,8 +189,8 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
     // ---- mask producer: chunk g of both blocks into staging slot g % 2 as soon as the slot has been read
     if (lane == 0) {
       Ring st{0, 0};
-      int c = 0, y = (int)(i0 * 256);
-      for (int g = 0; g < NC; ++g) {
+      int c = 0, y = (int)(i0 * 256), g = 0;
+      for (; g < NC; ++g) {
         if (g >= F_NS && !wait_bar(sfree + 8 * st.slot, st.phase ^ 1u)) {
           fail_status();
           break;
@@ -194,13 +208,14 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
           y += 256;
         }
       }
+      drain_ring(sfull, st, g, F_NS);   // the copies in flight land before shared memory is released
     }
   } else if (warp == 10) {
     // ---- W producer: chunk g's W into slot g % 3 once the MMAs of chunk g-3 have finished
     if (lane == 0) {
       Ring ws{0, 0};
-      int c = 0;
-      for (int g = 0; g < NC; ++g) {
+      int c = 0, g = 0;
+      for (; g < NC; ++g) {
         if (g >= F_NWS && !wait_bar(wdone + 8 * ws.slot, ws.phase ^ 1u)) {
           fail_status();
           break;
@@ -210,6 +225,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
         ws.next(F_NWS);
         if (++c == KC) c = 0;
       }
+      drain_ring(wfull, ws, g, F_NWS);
     }
   } else if (warp == 9) {
     // ---- MMA issue: D[h] += A[h](tmem slot) x W^T over the chunk (K steps of 16), split BF16x3, h = both blocks
@@ -217,6 +233,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
       constexpr uint32_t ID = idesc(2 * NB, false);
       Ring as{0, 0}, ws{0, 0};
       int c = 0, n = 0;
+      bool issued = false;
       for (int g = 0; g < NC; ++g) {
         bool ok = wait_bar(conv + 8 * as.slot, as.phase);
         if (ok) ok = wait_bar(wfull + 8 * ws.slot, ws.phase);
@@ -225,6 +242,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
           fail_status();
           break;
         }
+        issued = true;
         fence_after();
         const uint32_t wch = base + F_WOFF + ws.slot * F_W;
         uint32_t lo_any = 0;
@@ -256,6 +274,10 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
           c = 0;
           ++n;
         }
+      }
+      if (issued) {   // every MMA issued has finished before tensor and shared memory are released
+        commit(fin);
+        wait_bar(fin, 0);
       }
     }
   } else if (warp < 8) {
@@ -466,15 +488,6 @@ __device__ __forceinline__ void inv_drain(const InvArgs& a, uint32_t taddr, uint
   if (lane == 0) arrive(acce + 8 * buf);
 }
 
-// Wait (bounded) for the last copies of a ring of n slots whose cursor is `c` after `g` issued copies.
-__device__ __forceinline__ void drain_ring(uint32_t full, const Ring& c, int g, int n) {
-  const int last = g < n ? g : n;
-  for (int k = 1; k <= last; ++k) {
-    const int s = (c.slot - k + n) % n;
-    wait_bar(full + 8 * s, s < c.slot ? c.phase : c.phase ^ 1u);
-  }
-}
-
 // Producers: warp 8 the C pieces of every item, warp 10 the V tiles of every pair (after the MMAs of the previous
 // pair have finished).  MMA (warp 9): D[acc] = C x V^T, per C piece the MMAs that read it (C hi: hi x V hi and
 // hi x V lo; C lo: lo x V hi), 24 of 128 x 256 x 16 per item, both operands from shared memory.  Warps 0-7 drain.
@@ -622,12 +635,10 @@ __global__ void __launch_bounds__(I_NT, 1) rows_inv_tc_kernel(InvArgs a, const _
         commit(accf + 8 * ab.slot);
         ab.next(2);
       }
-      if (!ok) {
-        fail_status();
-        if (issued) {   // every MMA issued has finished before tensor memory is released
-          commit(fin);
-          wait_bar(fin, 0);
-        }
+      if (!ok) fail_status();
+      if (issued) {   // every MMA issued has finished before tensor and shared memory are released
+        commit(fin);
+        wait_bar(fin, 0);
       }
     }
   } else if (warp < 8) {

@@ -223,23 +223,33 @@ namespace oi {
 constexpr long long kStaticScratchF2 = OI_NOALLOC_SCRATCH_COMPLEX;  // complex values: 16 MiB per device
 static __device__ __align__(256) float2 g_static_scratch[kStaticScratchF2];
 
-// Device address of g_static_scratch on each device, looked up once per device.  In host code the symbol
-// itself is only a host-side handle, so the address must come from cudaGetSymbolAddress.
+// Device address of g_static_scratch on each device.  In host code the symbol itself is only a host-side handle,
+// so the address comes from cudaGetSymbolAddress.  It is looked up again on every call whose stream is not
+// capturing (a context torn down and created again -- cudaDeviceReset -- loads the module anew, possibly
+// elsewhere, so an address kept from before would be stale); a call on a capturing stream makes no lookup and
+// uses the address the last call on that device found.
 static float2* g_static_scratch_ptr[64] = {nullptr};
 static std::mutex g_static_scratch_mu;
 
-static int static_scratch(float2** out) {
+static int static_scratch(cudaStream_t stream, float2** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(OI_ECUDA, "oi_band_spectrum_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
   if (dev < 0 || dev >= 64) return fail(OI_ERANGE, "oi_band_spectrum_noalloc: device %d out of range", dev);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(stream, &cap);
+  if (e != cudaSuccess)
+    return fail(OI_ECUDA, "oi_band_spectrum_noalloc: cudaStreamIsCapturing: %s", cudaGetErrorString(e));
   std::lock_guard<std::mutex> lock(g_static_scratch_mu);
-  if (!g_static_scratch_ptr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess || !p)
       return fail(OI_ECUDA, "oi_band_spectrum_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
     g_static_scratch_ptr[dev] = (float2*)p;
+  } else if (!g_static_scratch_ptr[dev]) {
+    return fail(OI_EINVAL, "oi_band_spectrum_noalloc: the first call on device %d is being captured into a "
+                           "graph; make one call on that device before any stream capture", dev);
   }
   *out = g_static_scratch_ptr[dev];
   return OI_OK;
@@ -261,7 +271,7 @@ extern "C" int oi_band_spectrum_noalloc(const void* field, int kind, int batch, 
                 "scratch holds %lld; use oi_band_spectrum with a caller buffer or split the batch",
                 need, kStaticScratchF2);
   float2* scratch = nullptr;
-  int rc = static_scratch(&scratch);
+  int rc = static_scratch((cudaStream_t)stream, &scratch);
   if (rc) return rc;
   // every scratch entry the y pass reads is written by the x pass first: nothing needs clearing
   return oi_band_spectrum(field, kind, batch, ny, nx, nch, br, bc, wx, wy, scale, scratch, band, stream);

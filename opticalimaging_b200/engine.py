@@ -15,6 +15,7 @@ grid FFT evaluation index for index.
 """
 from __future__ import annotations
 
+import collections
 import math
 import threading
 from dataclasses import dataclass
@@ -84,9 +85,11 @@ def fft_supported(ny: int, nx: int, band: Band) -> bool:
 
 
 class Plan:
-    """Phase tables for one (output grid, band); cached and shared by every call with the same key."""
+    """Phase tables for one (output grid, band); cached and shared by every call with the same key.  The cache
+    keeps the CACHE_SIZE most recently used plans (a model holds on to its own plan regardless)."""
 
-    _cache: dict = {}
+    CACHE_SIZE = 64
+    _cache: collections.OrderedDict = collections.OrderedDict()
     _lock = threading.Lock()
 
     def __init__(self, ny, nx, band: Band, device, coarse=None):
@@ -183,36 +186,54 @@ class Plan:
         with cls._lock:
             p = cls._cache.get(key)
             if p is None:
-                p = cls._cache[key] = Plan(ny, nx, band, device, coarse)
+                p = cls._cache[key] = cls(ny, nx, band, device, coarse)
+                while len(cls._cache) > cls.CACHE_SIZE:
+                    cls._cache.popitem(last=False)
+            else:
+                cls._cache.move_to_end(key)
             return p
 
 
-SM_COUNT = 148
+B200_SMS = 148          # the SM count assumed for host-side layout arithmetic when no device is visible
+_SM_COUNTS: dict = {}
 
 
-def tc_parts_bound(images: int, fields: int, ctas: int = SM_COUNT) -> int:
+def sm_count() -> int:
+    """Streaming multiprocessors of the current device (148 on a B200): the grids of the one-block-per-SM
+    kernels and the field splits below are sized by it, as the native layouts are."""
+    if not torch.cuda.is_available():
+        return B200_SMS
+    d = torch.cuda.current_device()
+    n = _SM_COUNTS.get(d)
+    if n is None:
+        n = _SM_COUNTS[d] = torch.cuda.get_device_properties(d).multi_processor_count
+    return n
+
+
+def tc_parts_bound(images: int, fields: int, ctas: int | None = None) -> int:
     """Upper bound of the partial-sum slots oi_coherent_coarse_tc needs (for workspace estimates)."""
     tasks = images * fields
-    g = min(ctas, tasks)
+    g = min(sm_count() if ctas is None else ctas, tasks)
     return min(fields, -(-fields * g // tasks) + 1)
 
 
-def field_split(nfields: int, blocks: int) -> int:
+def field_split(nfields: int, blocks: int, sms: int | None = None) -> int:
     """Smallest divisor d of nfields with blocks * d >= 3 waves of one block per SM (nfields if none)."""
-    target = 3 * SM_COUNT
+    target = 3 * (sm_count() if sms is None else sms)
     for d in range(1, nfields + 1):
         if nfields % d == 0 and blocks * d >= target:
             return d
     return nfields
 
 
-def field_split_sm(nfields: int, blocks: int) -> int:
+def field_split_sm(nfields: int, blocks: int, sms: int | None = None) -> int:
     """Field split for a kernel of one block per SM (the 256 x 256 coarse grid): the d minimising
     waves(d) * (fields per block + 1/2), the half standing for a block's fixed start and partial-sum write;
     ties go to the smaller d (fewer partial sums)."""
+    sms = sm_count() if sms is None else sms
     best, best_cost = 1, None
     for d in range(1, nfields + 1):
-        cost = -(-blocks * d // SM_COUNT) * (-(-nfields // d) + 0.5)
+        cost = -(-blocks * d // sms) * (-(-nfields // d) + 0.5)
         if best_cost is None or cost < best_cost:
             best, best_cost = d, cost
     return best
@@ -450,14 +471,17 @@ class CoherentModel:
         return coherent_image(band, self.pupils, self.weights, self.plan, out=out, marks=marks, form=form)
 
 
-    def image_host(self, masks: torch.Tensor, out: torch.Tensor, chunk: int = 16, **kw) -> torch.Tensor:
+    def image_host(self, masks: torch.Tensor, out: torch.Tensor, chunk: int = 16, check: bool = False,
+                   **kw) -> torch.Tensor:
         """image() of a batch held in pinned host memory, written into the pinned host tensor `out` (shaped as
         image() returns it).  The batch is cut into chunks of `chunk` masks; each chunk's copy to the device,
         its images and the copy of its result back run on three streams (copy-in, the current stream, copy-out)
         with events between them, over three rotating device buffer sets kept by the model, so the copies of
         neighbouring chunks -- also across consecutive calls -- overlap each other and the compute; the host
         link then bounds the path.  The current stream waits for the last copy-out before the call returns, so
-        synchronising it (or an event recorded on it) covers the results.  Keyword arguments go to image()."""
+        synchronising it (or an event recorded on it) covers the results.  With check=True the call waits for
+        the batch and raises DeviceWaitError if a kernel's bounded wait expired (the results are then invalid);
+        without it, call N.check_device_status after synchronising.  Keyword arguments go to image()."""
         if masks.is_cuda or out.is_cuda:
             raise ValueError('image_host takes host tensors (image() takes device tensors)')
         if not masks.is_pinned() or not out.is_pinned():
@@ -497,6 +521,9 @@ class CoherentModel:
         done = torch.cuda.Event()
         done.record(pipe['d2h'])
         cur.wait_event(done)
+        if check:
+            done.synchronize()
+            N.check_device_status('image_host')
         return out
 
 

@@ -89,6 +89,13 @@ def _field_on_device(scatter, dev):
     return h.contiguous()
 
 
+def _check(what):
+    """Raise if a kernel of this call ended early on an expired bounded wait: the caller's stream is synchronised
+    first (the results are about to be returned anyway), so the status word covers the kernels the call launched."""
+    torch.cuda.current_stream().synchronize()
+    N.check_device_status(what)
+
+
 def _result_device(scatter):
     h = scatter.ScatterField
     return h.device if isinstance(h, torch.Tensor) else torch.device('cpu')
@@ -211,6 +218,7 @@ def CalculateAbbeImage(source, scatter, projector, numerics):
     hfull = torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
     pim = _pupil_image(scatter, projector, source, hfull, dev)
     rd = _result_device(scatter)
+    _check('CalculateAbbeImage')
     return _image_data(inten.to(rd), scatter, projector), pim.to(rd)
 
 
@@ -351,6 +359,7 @@ def CalculateAerialImage_SOCS(scatter, TCCMatrix_SOCS, source, projector):
     hfull = torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
     pim = _pupil_image(scatter, projector, source, hfull, dev)
     rd = _result_device(scatter)
+    _check('CalculateAerialImage_SOCS')
     return img.to(rd), pim.to(rd)
 
 
@@ -389,6 +398,7 @@ def CalculateHopkinsImage(source, scatter, projector, numerics):
     hfull = torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
     pim = _pupil_image(scatter, projector, source, hfull, dev)
     rd = _result_device(scatter)
+    _check('CalculateHopkinsImage')
     return _image_data(inten.to(rd), scatter, projector), pim.to(rd)
 
 
@@ -422,6 +432,7 @@ def CalculateSOCS(FloquetMode, TCCMatrix_SOCS, numerics):
     ones = torch.ones((1, 1, nox, noy), dtype=torch.complex64, device=dev)
     w = torch.ones((1, 1), dtype=torch.float32, device=dev)
     img = coherent_image(fields, ones, w, plan)[0, 0]
+    _check('CalculateSOCS')
     return img.to(_tensor_device(FloquetMode))
 
 

@@ -17,7 +17,9 @@ device executor is ``CudaExecutor``.  Masks and caller-provided result buffers t
 
 Failure behaviour: a malformed request (wrong shape or dtype) fails at submit; a request whose batch can never
 fit the budget fails with MemoryError; a cancelled future is dropped before launch; an executor error fails
-the futures of its batch and the server keeps serving.  An error that escapes the scheduler thread itself (for
+the futures of its batch and the server keeps serving; a batch collected while the device status word shows an
+expired kernel wait fails with DeviceWaitError, and so do the batches in flight beside it (``StatusGuard``).
+An error that escapes the scheduler thread itself (for
 instance the executor's thread set-up) closes the server and fails every request it holds; later submits fail
 at once.
 """
@@ -323,6 +325,32 @@ class Server:
 
 
 # ------------------------------------------------------------------------------------------- executor
+class StatusGuard:
+    """Attributes expired kernel waits to batches.  A tensor-core kernel whose bounded wait runs out sets the
+    device's status word and returns early with a partial result; the word is one per device, so when it is
+    found set at the collection of one batch it may come from any batch that ran alongside: the collected batch
+    fails, and so does every batch in flight at that moment (each when it is collected).  `reader(reset)` reads
+    the word (default: the library's oi_device_status)."""
+
+    def __init__(self, reader=None):
+        self.reader = reader
+        self.suspect = set()
+
+    def check(self, slot: int, in_flight) -> None:
+        """Raise DeviceWaitError if the batch just collected from `slot` cannot be trusted."""
+        from . import _native as N
+        suspect = slot in self.suspect
+        self.suspect.discard(slot)
+        try:
+            N.check_device_status(f'batch on slot {slot}', self.reader)
+        except N.DeviceWaitError:
+            self.suspect.update(s for s in in_flight if s != slot)
+            raise
+        if suspect:
+            raise N.DeviceWaitError(f'batch on slot {slot} ran alongside a batch whose kernel wait expired; its '
+                                    'results are invalid')
+
+
 class CudaExecutor:
     """Runs batches on `nslots` CUDA streams of one device, with CUDA graphs per (model, batch bucket, slot).
 
@@ -332,9 +360,10 @@ class CudaExecutor:
     """
 
     def __init__(self, device=None, nslots: int = 3, use_graphs: bool = True, result_device: str = 'cpu',
-                 max_batch: int = 256):
+                 max_batch: int = 256, status_reader=None):
         from .engine import require_cuda
         self.device = require_cuda(device)
+        self.guard = StatusGuard(status_reader)   # every collected batch is checked against expired kernel waits
         self.nslots = nslots
         self.use_graphs = use_graphs
         self.result_device = result_device
@@ -474,6 +503,7 @@ class CudaExecutor:
         self.events[slot] = None
         self.pending[slot] = None
         self.batch[slot] = None
+        self.guard.check(slot, [i for i, e in enumerate(self.events) if e is not None])
         if isinstance(out, list):
             return out
         return [r.out if r.out is not None else out[i] for i, r in enumerate(reqs)]

@@ -62,3 +62,18 @@ def test_every_literal_call_matches_its_signature():
                 assert len(node.args) - 1 == len(N._SIGS[name]), f'{f}:{node.lineno} {name}'
                 seen += 1
     assert seen > 10
+
+
+def test_noalloc_path_names_no_allocator():
+    """oi_band_spectrum_noalloc and the scratch lookup it calls name no device allocator (checked in the source,
+    so a later change that adds one fails here on the CPU, not only on the GPU)."""
+    src = open(os.path.join(ROOT, 'opticalimaging_b200', 'csrc', 'spectrum.cu')).read()
+    start = src.index('static __device__ __align__(256) float2 g_static_scratch')
+    end = src.index('return oi_band_spectrum(', start)
+    section = src[start:end]
+    assert 'cudaGetSymbolAddress' in section
+    for name in ('cudaMalloc', 'cudaFree', 'cudaMallocAsync', 'cudaFreeAsync', 'cuMemAlloc', 'malloc(', 'new '):
+        assert name not in section, name
+    # the scratch-form entry point it forwards to takes the caller's scratch and allocates nothing either
+    body = src[src.index('extern "C" int oi_band_spectrum('):src.index('// Band spectrum for callers that cannot')]
+    assert 'cudaMalloc' not in body and 'cudaFree' not in body

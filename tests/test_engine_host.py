@@ -19,9 +19,10 @@ def test_coarse_size_holds_intensity_band():
 
 
 def test_field_split_divides_and_fills():
-    assert E.field_split(24, 64) == 8            # 64 images x 8 splits >= 3 waves of 148 SMs
-    assert E.field_split(24, 1) == 24
-    assert E.field_split(324, 5) == 108
+    assert E.field_split(24, 64, sms=148) == 8   # 64 images x 8 splits >= 3 waves of 148 SMs
+    assert E.field_split(24, 1, sms=148) == 24
+    assert E.field_split(324, 5, sms=148) == 108
+    assert E.field_split(24, 64, sms=132) == 8 and E.field_split(24, 32, sms=132) == 24
     for n, b in ((24, 64), (7, 3), (324, 5), (1, 1)):
         d = E.field_split(n, b)
         assert n % d == 0
@@ -80,18 +81,44 @@ def test_require_cuda_resolves_a_bare_cuda_device(monkeypatch):
 def test_field_split_sm_minimises_waves_times_fields():
     """The field split of the one-block-per-SM coherent kernel (256 x 256 coarse grid): the d in [1, nfields]
     minimising ceil(blocks d / SMs) * (ceil(nfields / d) + 1/2), the smallest d on ties."""
-    from opticalimaging_b200.engine import SM_COUNT, field_split_sm
+    from opticalimaging_b200.engine import field_split_sm
+    SMS = 148
 
     def cost(nf, b, d):
-        return -(-b * d // SM_COUNT) * (-(-nf // d) + 0.5)
+        return -(-b * d // SMS) * (-(-nf // d) + 0.5)
 
-    assert field_split_sm(324, 8) == 18      # vector Abbe 2048^2 at batch 8: 144 blocks of 18 fields, one wave
-    assert field_split_sm(24, 8) == 12       # SOCS-24: 96 blocks of 2 fields (18 ties, more partial sums)
-    assert field_split_sm(1, 1) == 1
+    assert field_split_sm(324, 8, SMS) == 18   # vector Abbe 2048^2 at batch 8: 144 blocks of 18 fields, one wave
+    assert field_split_sm(24, 8, SMS) == 12    # SOCS-24: 96 blocks of 2 fields (18 ties, more partial sums)
+    assert field_split_sm(1, 1, SMS) == 1
     for nf in (1, 5, 24, 72, 324):
         for b in (1, 2, 8, 64, 200):
-            d = field_split_sm(nf, b)
+            d = field_split_sm(nf, b, SMS)
             assert 1 <= d <= nf
             best = min(cost(nf, b, e) for e in range(1, nf + 1))
             assert cost(nf, b, d) == best
             assert all(cost(nf, b, e) > best for e in range(1, d))
+
+
+def test_sm_count_without_a_device_is_the_b200s():
+    if not torch.cuda.is_available():
+        assert E.sm_count() == E.B200_SMS == 148
+
+
+def test_plan_cache_is_bounded_lru(monkeypatch):
+    made = []
+
+    class FakePlan(E.Plan):
+        def __init__(self, ny, nx, band, device, coarse=None):   # no device work: record the key only
+            made.append((ny, nx))
+
+    monkeypatch.setattr(E.Plan, '_cache', E.collections.OrderedDict())
+    monkeypatch.setattr(E.Plan, 'CACHE_SIZE', 4)
+    band = E.Band(-2, 5, -2, 5)
+    first = FakePlan.get(8, 8, band, 'cpu')
+    for n in range(9, 14):
+        FakePlan.get(n, n, band, 'cpu')
+        FakePlan.get(8, 8, band, 'cpu')             # kept in use: stays cached
+    assert len(E.Plan._cache) == 4
+    assert FakePlan.get(8, 8, band, 'cpu') is first
+    FakePlan.get(9, 9, band, 'cpu')                 # evicted earlier: built again
+    assert made.count((9, 9)) == 2 and made.count((8, 8)) == 1

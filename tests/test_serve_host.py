@@ -194,3 +194,59 @@ def test_scheduler_failure_in_flight_fails_queued_and_running_requests():
         late.result(timeout=1)
     srv.drain(timeout=5)
     srv.close()
+
+
+class StatusExecutor(FakeExecutor):
+    """FakeExecutor whose collect() checks a fake device status word through serve.StatusGuard, as
+    CudaExecutor checks the library's: the word is set by the test, as a kernel whose wait expired would."""
+
+    def __init__(self, **kw):
+        super().__init__(**kw)
+        from opticalimaging_b200.serve import StatusGuard
+        self.word = 0
+        self.guard = StatusGuard(self.read)
+
+    def read(self, reset):
+        v = self.word
+        if reset:
+            self.word = 0
+        return v
+
+    def collect(self, slot):
+        out = super().collect(slot)
+        self.guard.check(slot, [i for i, s in enumerate(self.slot) if s is not None])
+        return out
+
+
+def test_expired_device_wait_fails_the_batch_and_its_neighbours():
+    from opticalimaging_b200._native import DeviceWaitError
+    ex = StatusExecutor(nslots=2, delay=0.05)
+    srv = Server(ex, hbm_budget=1e9)
+    a, b = spec('a'), spec('b')
+    fa = srv.submit(a, torch.ones(4, 4))
+    time.sleep(0.01)
+    fb = srv.submit(b, torch.ones(4, 4))          # in flight beside the first batch
+    time.sleep(0.01)
+    ex.word = 1                                   # a kernel's bounded wait ran out
+    with pytest.raises(DeviceWaitError):
+        fa.result(timeout=10)
+    with pytest.raises(DeviceWaitError):          # it ran alongside: suspect too
+        fb.result(timeout=10)
+    assert ex.word == 0                           # the word was cleared after the failure was reported
+    ok = srv.submit(a, torch.ones(4, 4))          # later batches are served normally
+    torch.testing.assert_close(ok.result(timeout=10), 2 * torch.ones(1, 4, 4))
+    srv.close()
+
+
+def test_check_device_status_raises_and_clears():
+    from opticalimaging_b200._native import DeviceWaitError, check_device_status
+    word = [3]
+
+    def read(reset):
+        v = word[0]
+        if reset:
+            word[0] = 0
+        return v
+    with pytest.raises(DeviceWaitError, match='device status 3'):
+        check_device_status('test', read)
+    check_device_status('test', read)             # cleared: no error the second time

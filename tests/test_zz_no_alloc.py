@@ -64,3 +64,23 @@ def test_noalloc_rejects_oversize_before_launching():
                                       N.stream_handle(dev))
     assert rc == -3
     assert b'built-in scratch' in lib.oi_last_error()
+
+
+def test_noalloc_calls_allocate_no_device_memory():
+    """The property the entry point exists for: after a first call, further calls leave the device's free
+    memory and torch's reserved pool exactly as they were."""
+    from opticalimaging_b200 import _native as N, engine as E
+    lib = N.load()
+    dev = torch.device('cuda')
+    stream = N.stream_handle(dev)
+    plan = E.Plan.get(256, 256, E.Band(-20, 41, -20, 41), dev)
+    field = torch.from_numpy(np.random.default_rng(7).random((4, 256, 256), dtype=np.float32)).to(dev)
+    out = torch.empty((4, 1, 41, 41), dtype=torch.complex64, device=dev)
+    assert _call_noalloc(lib, field, N.FIELD_REAL_F32, 1, plan, out, stream) == 0, lib.oi_last_error()
+    torch.cuda.synchronize()
+    free0, reserved0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved()
+    for _ in range(50):
+        assert _call_noalloc(lib, field, N.FIELD_REAL_F32, 1, plan, out, stream) == 0, lib.oi_last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.memory_reserved() == reserved0
