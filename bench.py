@@ -393,6 +393,167 @@ def mix_fp64_check(specs, ex, pool, dev):
     return out
 
 
+def compact(x, digits=4):
+    """Floats rounded to `digits` significant digits, recursively (keeps the one JSON line short)."""
+    if isinstance(x, float):
+        return float(f'{x:.{digits}g}')
+    if isinstance(x, dict):
+        return {k: compact(v, digits) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [compact(v, digits) for v in x]
+    return x
+
+
+def reference_torch_socs(h, kernels, npx, npy):
+    """The reference's SOCS image as its own torch code, on whatever device its tensors live on: the spectrum of
+    Scatter.CalculateSpectrum (Scatter.py:10-21) and CalculateAerialImage_SOCS.py:3-11 -- a full-grid ifft2 per
+    channel, a full-grid fft2 per (kernel, channel), |.|^2 summed and fftshifted.  With CUDA tensors this is the
+    reference run with torch's default device set to the GPU: the plain GPU path it would give a user."""
+    hk = (npx * npy) * torch.fft.fftshift(torch.fft.ifft2(torch.fft.ifftshift(h, dim=(0, 1)), dim=(0, 1)),
+                                          dim=(0, 1))
+    sp = hk.unsqueeze(3).permute(0, 1, 3, 2)
+    es = kernels.unsqueeze(3) * torch.fft.ifftshift(sp, dim=(0, 1))
+    e = ((1.0 / npx) * (1.0 / npy)) * torch.fft.fft2(es, dim=(0, 1))
+    return torch.fft.fftshift(torch.sum(torch.abs(e) ** 2, dim=(2, 3)), dim=(0, 1))
+
+
+def plain_reference_cuda(sk_info, masks_np, dev, count=16):
+    """The reference's torch code on the GPU, one request at a time: the host [N, N, 3] complex64 field copied
+    in, the image computed by reference_torch_socs with the reference-layout kernels resident on the device,
+    the image copied back.  Returns images/s over `count` clips (after one warm-up clip)."""
+    from opticalimaging_b200 import imaging
+    sr, po, nm, T, fg = sk_info
+    kern = imaging.DecomposeTCC_SOCS(T, fg, [N_PIX, N_PIX], nm)            # [N, N, K] complex64 on the device
+    npx = PERIOD / (sr.Wavelength / po.NA)
+    fields = []
+    for m in masks_np[:count + 1]:
+        f = np.zeros((N_PIX, N_PIX, 3), np.complex64)
+        f[:, :, 0] = m
+        fields.append(torch.from_numpy(f))
+    reference_torch_socs(fields[0].to(dev), kern, npx, npx).cpu()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for f in fields[1:]:
+        reference_torch_socs(f.to(dev), kern, npx, npx).cpu()
+    return count / (time.perf_counter() - t0)
+
+
+def e2e_dropin(sk_info, masks_np, dev, count=16):
+    """Images/s of the drop-in call as a reference user makes it: CalculateAerialImage_SOCS per clip with a host
+    complex64 [N, N, 3] ScatterField and the reference-layout kernels DecomposeTCC_SOCS returned; the image comes
+    back on the host.  Host-to-device bytes per clip: the 24 MiB field (the reference's format)."""
+    from opticalimaging_b200 import imaging
+    from opticalimaging_b200.params import Scatter
+    sr, po, nm, T, fg = sk_info
+    kern = imaging.DecomposeTCC_SOCS(T, fg, [N_PIX, N_PIX], nm)
+    scs = []
+    for m in masks_np[:count + 1]:
+        f = np.zeros((N_PIX, N_PIX, 3), np.complex64)
+        f[:, :, 0] = m
+        sc = Scatter()
+        sc.Period_X = sc.Period_Y = PERIOD
+        sc.ScatterField = torch.from_numpy(f)
+        scs.append(sc)
+    imaging.CalculateAerialImage_SOCS(scs[0], kern, sr, po)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for sc in scs[1:]:
+        img, _ = imaging.CalculateAerialImage_SOCS(sc, kern, sr, po)
+    dt = time.perf_counter() - t0
+    return {"images_per_s": count / dt, "h2d_bytes_per_image": N_PIX * N_PIX * 3 * 8,
+            "d2h_bytes_per_image": N_PIX * N_PIX * 4,
+            "call": "CalculateAerialImage_SOCS(scatter, kernels, source, projector) per clip, host complex64 "
+                    "[1024, 1024, 3] ScatterField in, host float32 image out"}
+
+
+def time_device(fn, steps):
+    """Average device time (ms) of fn() over `steps` calls, CUDA events on the current stream, after two warm-up
+    calls."""
+    fn()
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def configs_measure(dev, steps=5):
+    """Configurations 1, 2 and 4 at their own sizes: images/s through the resident models (masks in HBM) per form,
+    error of one image against the FP64 oracle (max and RMS, relative to the FP64 peak; every plane for
+    configuration 2), and the configuration-4 adjoint step (forward + resist loss + backward) in ms."""
+    from oracle import optics64 as O
+    from opticalimaging_b200 import imaging, workloads as W
+    from opticalimaging_b200.autograd import aerial_image
+    from opticalimaging_b200.params import Scatter
+    out = {}
+
+    def errs(got, ref):
+        d = np.asarray(got, np.float64) - ref
+        pk = float(np.max(np.abs(ref)))
+        return float(np.max(np.abs(d)) / pk), float(np.sqrt(np.mean(d * d)) / pk)
+
+    # configuration 1: scalar Abbe 256^2, annular 0.6/0.9 PntNum 21, 12 rectangles; batches of 64 masks
+    sr, sc, po, nm = W.config1()
+    model = imaging.abbe_model(sr, po, nm, 1024.0, 1024.0, 256, 256)
+    masks = np.stack([W.rect_mask(256, 256, 1024, 1024, 12, 40.0, 300.0, np.random.default_rng(100 + i))
+                      for i in range(64)])
+    md = torch.from_numpy(masks).to(dev)
+    sc.ScatterField = W.thin_field(masks[0])
+    ref = O.abbe(sr, sc, po, nm)[0]
+    c1 = {"fields": model.count, "band": [model.band.br, model.band.bc], "batch": 64}
+    for form in ('fft', 'bf16x3'):
+        o = torch.empty((64, 1, 256, 256), device=dev)
+        ms = time_device(lambda: model.image(md, out=o, form=form), steps)
+        mx, rms = errs(o[0, 0].cpu().numpy(), ref)
+        c1[form] = {"images_per_s": 64 / (ms / 1e3), "max": mx, "rms": rms}
+    out["config1"] = c1
+    # configuration 2: vector Abbe 512^2, quasar PntNum 31, 5 planes, Zernike; batches of 16 line/space clips
+    sr, sc, po, nm = W.config2()
+    model = imaging.abbe_model(sr, po, nm, 2048.0, 2048.0, 512, 512)
+    masks = np.stack([W.line_space_mask(512, 2048, np.random.default_rng(2 if i == 0 else 200 + i))
+                      for i in range(16)])
+    md = torch.from_numpy(masks).to(dev)
+    ref = O.abbe(sr, sc, po, nm)                   # clip 0 is the configuration's own (seed 2)
+    c2 = {"fields": model.count, "planes": model.planes, "band": [model.band.br, model.band.bc], "batch": 16}
+    for form in ('fft', 'bf16x3'):
+        o = torch.empty((16, 5, 512, 512), device=dev)
+        ms = time_device(lambda: model.image(md, out=o, form=form), steps)
+        got = o[0].cpu().numpy()
+        per = [errs(got[z], ref[z]) for z in range(5)]
+        c2[form] = {"images_per_s": 16 / (ms / 1e3), "max_per_plane": [p[0] for p in per],
+                    "rms_per_plane": [p[1] for p in per]}
+    out["config2"] = c2
+    # configuration 4: the adjoint step at 1024^2 with the engine's SOCS-16 kernels
+    sr, po, nm, logits, target = W.config4()
+    T, fg = imaging.CalculateTCCMatrix(sr, [2048.0, 2048.0], po, 0.0, nm)
+    sk = imaging.socs_kernels_from_tcc(T, fg, [1024, 1024], nm)
+    lt = torch.from_numpy(logits).to(dev)
+    tg = torch.from_numpy(target).to(dev)
+    box = {}
+
+    def step(batch=1):
+        x = lt.expand(batch, -1, -1).clone().requires_grad_(True)
+        I = aerial_image(sk, torch.sigmoid(x))
+        loss = torch.sum((torch.sigmoid(50.0 * (I - 0.25)) - tg) ** 2)
+        loss.backward()
+        box['grad'], box['I'], box['loss'] = x.grad, I, loss
+    ms1 = time_device(lambda: step(1), steps)
+    g1 = box['grad'][0].cpu().numpy()
+    ms8 = time_device(lambda: step(8), steps)
+    K = imaging.DecomposeTCC_SOCS(T, fg, [1024, 1024], nm).cpu().numpy().astype(np.complex128)
+    I64, L64, G64 = O.socs_resist(logits, target, K, 50.0, 0.25)
+    mx, rms = errs(g1, G64)
+    out["config4"] = {"kernels": sk.count, "adjoint_ms_per_step": ms1, "adjoint_ms_per_step_batch8": ms8,
+                      "adjoint_clips_per_s_batch8": 8 / (ms8 / 1e3), "grad_max_vs_fp64": mx, "grad_rms_vs_fp64": rms,
+                      "step": "forward (recomputed in the backward), sigmoid resist loss, backward through the "
+                              "adjoint kernel; 1024^2 continuous mask"}
+    return out
+
+
 def serve_model_from(sk, form):
     from opticalimaging_b200.engine import CoherentModel
     return CoherentModel(sk.pupils, sk.weights, sk.band, sk.ny, sk.nx, form=form)
@@ -418,9 +579,12 @@ def cpu_reference_sample(sk_info, masks_np, budget_s, threads):
     return 1.0 / med, n
 
 
-# DRAM bytes per launch (read + write) of the three largest kernels at this workload, from the ncu capture
-# summarised in profiles/socs24-1024-bf16x3-step.md
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the three largest kernels at this
+# workload, measured by ncu on a B200 for the kernels as they are built now; a constant, re-measured whenever
+# those kernels change (the date and the capture command travel with the numbers: NCU_TRAFFIC_SOURCE).
 NCU_TRAFFIC = {"rows_fwd_tc": 275.9e6, "rows_inv_tc": 243.9e6, "coherent_tc": 2.6e6}
+NCU_TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none, one launch "
+                      "of each kernel at the 64-clip 1024^2 SOCS-24 step, measured 2026-12-03")
 
 
 def kernel_rooflines(sk, masks, reps=10):
@@ -484,7 +648,7 @@ def kernel_rooflines(sk, masks, reps=10):
                          "traffic": NCU_TRAFFIC[name], "us": sec * 1e6, "peak_source": src,
                          "algorithmic": "4 bytes per pixel: the float32 mask read" if name == "rows_fwd_tc"
                          else "4 bytes per pixel: the float32 image written"}
-    res["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch (profiles/)"
+    res["traffic_source"] = NCU_TRAFFIC_SOURCE
     return res
 
 
@@ -587,6 +751,7 @@ def run_engine(args, world, rank, local):
         torch.cuda.synchronize()
         barrier(world)
         clk.wait_samples(len(clk.lines) + 1, timeout=0.5)
+    status = N.device_status(reset=True)      # a kernel whose bounded wait expired invalidates the run
     value, ms = job_rate(BATCH * args.steps, start.elapsed_time(end), world)
     # ---- end to end through the public API: pinned uint8 masks in, float32 images out
     host_in = torch.from_numpy(masks_np.astype(np.uint8)).pin_memory()
@@ -606,6 +771,7 @@ def run_engine(args, world, rank, local):
     e2.record()
     torch.cuda.synchronize()
     barrier(world)
+    status |= N.device_status(reset=True)
     e2e_value, _ = job_rate(BATCH * args.steps, s2.elapsed_time(e2), world)
     if rank != 0:   # the last collective is behind us; what follows is reported by rank 0 alone
         return
@@ -633,6 +799,13 @@ def run_engine(args, world, rank, local):
         roof = {"kernel": dominant, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
                 "frac": ach / hbm, "traffic": None, "peak_source": src,
                 "algorithmic": "4 bytes per pixel (float32 mask read / image written), per stage"}
+    # ---- the drop-in call as a reference user makes it, and the reference's own torch code on the GPU
+    dropin = e2e_dropin(info, masks_np, dev) if not args.no_serve else None
+    plain_ref = plain_reference_cuda(info, masks_np, dev) if not args.no_serve else None
+    if serving is not None and plain_ref:
+        serving["plain_reference_torch_cuda_images_per_s"] = plain_ref
+        serving["served_over_plain_reference_torch_cuda"] = serving["images_per_s"] / plain_ref
+    status |= N.device_status(reset=True)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16x3" if args.form == 'bf16x3' else "fp32", "data": "synthetic",
@@ -643,9 +816,16 @@ def run_engine(args, world, rank, local):
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_in.numel()),
                     "d2h_bytes_per_step": int(host_out.numel() * 4)},
-            "gpu_launches": launches, "setup_s": setup_s, "serving": serving, "serving_mix": mix,
+            "gpu_launches": launches, "setup_s": setup_s, "device_status": status,
             "stage_ms": {k: round(v, 4) for k, v in st.items()}, "roofline": roof, "roofline_kernels": kern,
-            "clocks": clk.summary()}
+            "clocks": clk.summary(), "e2e_dropin": dropin}
+    if status:
+        line["invalid"] = "a kernel's bounded wait expired during the run (device status %d)" % status
+    if rank == 0 and not args.no_cpu and not args.no_configs:
+        try:
+            line["configs"] = configs_measure(dev)
+        except Exception as e:  # the configuration-3 line must still print
+            line["configs"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
         torch.set_num_threads(threads)
@@ -659,8 +839,10 @@ def run_engine(args, world, rank, local):
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{n} clips of 1024x1024 through the reference's SOCS algorithm "
                                           "(72 full-grid complex64 FFTs per clip, torch CPU FFT)"}
+    line["serving_mix"] = mix
+    line["serving"] = serving            # last: the end of the line is what a log tail keeps
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        print(json.dumps(compact(line)), flush=True)
 
 
 def main():
@@ -672,6 +854,7 @@ def main():
     ap.add_argument('--cpu-budget', type=float, default=15.0)
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline and the precision study')
     ap.add_argument('--no-serve', action='store_true', help='skip the served measurements (profiling runs)')
+    ap.add_argument('--no-configs', action='store_true', help='skip configurations 1, 2 and 4')
     ap.add_argument('--mix-requests', type=int, default=2000,
                     help='requests of the mixed serving stream (configuration 5); 0 skips it')
     ap.add_argument('--batch', type=int, default=64, help='clips per step (64 in the benchmark configuration)')

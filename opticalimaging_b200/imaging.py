@@ -24,6 +24,7 @@ from __future__ import annotations
 import warnings
 
 import torch
+from torch.utils.weak import WeakIdKeyDictionary
 
 from . import _native as N
 from .engine import (Band, CoherentModel, Plan, SocsKernels, abbe_band, band_spectrum, coherent_image,
@@ -77,16 +78,43 @@ def _axes(scatter, projector, source):
     return f, g, npx, npy
 
 
+def _device_field(scatter, dev):
+    """ScatterField [Ny, Nx, C] as a contiguous complex64 device tensor (one host-to-device copy)."""
+    return torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
+
+
+def _live_channels(hfull):
+    """The channels of a device field [Ny, Nx, C] that are not all zero, as one contiguous tensor (the
+    reference transforms every channel, CalculateAerialImage.py:76-86; a zero channel adds nothing).  One
+    reduction and one host read decide all channels."""
+    live = torch.nonzero((hfull != 0).flatten(0, 1).any(dim=0)).flatten().tolist() or [0]
+    h = hfull if len(live) == hfull.shape[2] else hfull[:, :, live]
+    return h.contiguous()
+
+
 def _field_on_device(scatter, dev):
     """ScatterField [Ny, Nx, C] as complex64 on the device, with all-zero channels dropped."""
-    h = torch.as_tensor(scatter.ScatterField)
-    h = h.to(dev, non_blocking=True).to(torch.complex64)
-    live = [c for c in range(h.shape[2]) if bool((h[:, :, c] != 0).any())]
-    if not live:
-        live = [0]
-    if len(live) != h.shape[2]:
-        h = h[:, :, live]
-    return h.contiguous()
+    return _live_channels(_device_field(scatter, dev))
+
+
+_SOCS_CACHE = WeakIdKeyDictionary()   # reference-layout kernel tensor -> (its version, SocsKernels)
+
+
+def _socs_kernels_of(kernels, dev) -> SocsKernels:
+    """The band form of a reference-layout kernel array [Ny, Nx, K] (what DecomposeTCC_SOCS returns), found once
+    per tensor: later calls with the same, unmodified tensor object reuse it (the scan and any host-to-device
+    copy of the full-grid array happen once).  Kernels from this module's DecomposeTCC_SOCS are registered at
+    creation."""
+    if isinstance(kernels, SocsKernels):
+        return kernels
+    t = torch.as_tensor(kernels)
+    hit = _SOCS_CACHE.get(t) if isinstance(kernels, torch.Tensor) else None
+    if hit is not None and hit[0] == t._version and hit[1].device == dev:
+        return hit[1]
+    sk = SocsKernels.from_full_grid(t.to(dev))
+    if isinstance(kernels, torch.Tensor):
+        _SOCS_CACHE[kernels] = (kernels._version, sk)
+    return sk
 
 
 def _check(what):
@@ -213,9 +241,8 @@ def abbe_intensity(source, scatter, projector, numerics, h=None):
 def CalculateAbbeImage(source, scatter, projector, numerics):
     """Abbe aerial image -> (ImageData, pupilImage) (CalculateAerialImage.py:18-103)."""
     dev = require_cuda()
-    h = _field_on_device(scatter, dev)
-    inten = abbe_intensity(source, scatter, projector, numerics, h=h)
-    hfull = torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
+    hfull = _device_field(scatter, dev)
+    inten = abbe_intensity(source, scatter, projector, numerics, h=_live_channels(hfull))
     pim = _pupil_image(scatter, projector, source, hfull, dev)
     rd = _result_device(scatter)
     _check('CalculateAbbeImage')
@@ -346,17 +373,18 @@ def DecomposeTCC_SOCS(TCCMatrix_Stacked, FG_ValidSize, Nfg, numerics):
     full = torch.zeros((ng, nf, sk.count), dtype=torch.complex64, device=dev)
     b = sk.band
     full[:b.br, :b.bc, :] = sk.kernels.permute(1, 2, 0)
-    return torch.roll(full, shifts=(b.m0r, b.m0c), dims=(0, 1))
+    full = torch.roll(full, shifts=(b.m0r, b.m0c), dims=(0, 1))
+    _SOCS_CACHE[full] = (full._version, sk)    # CalculateAerialImage_SOCS reuses the band form
+    return full
 
 
 def CalculateAerialImage_SOCS(scatter, TCCMatrix_SOCS, source, projector):
     """SOCS aerial image [Ny, Nx] and pupilImage (CalculateAerialImage_SOCS.py:3-11)."""
     dev = require_cuda()
-    sk = TCCMatrix_SOCS if isinstance(TCCMatrix_SOCS, SocsKernels) else \
-        SocsKernels.from_full_grid(torch.as_tensor(TCCMatrix_SOCS).to(dev))
-    h = _field_on_device(scatter, dev)
+    sk = _socs_kernels_of(TCCMatrix_SOCS, dev)
+    hfull = _device_field(scatter, dev)
+    h = _live_channels(hfull)
     img = sk.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
-    hfull = torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
     pim = _pupil_image(scatter, projector, source, hfull, dev)
     rd = _result_device(scatter)
     _check('CalculateAerialImage_SOCS')
@@ -393,9 +421,8 @@ def hopkins_intensity(source, scatter, projector, numerics, h=None):
 def CalculateHopkinsImage(source, scatter, projector, numerics):
     """Hopkins aerial image -> (ImageData, pupilImage) (CalculateAerialImage.py:105-130)."""
     dev = require_cuda()
-    h = _field_on_device(scatter, dev)
-    inten = hopkins_intensity(source, scatter, projector, numerics, h=h)
-    hfull = torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
+    hfull = _device_field(scatter, dev)
+    inten = hopkins_intensity(source, scatter, projector, numerics, h=_live_channels(hfull))
     pim = _pupil_image(scatter, projector, source, hfull, dev)
     rd = _result_device(scatter)
     _check('CalculateHopkinsImage')

@@ -14,6 +14,8 @@ point / kernel / channel / field component), citing the reference file:line each
 * ``tcc``             -- CalculateTCCMatrix.py:9-75
 * ``decompose``       -- DecomposeTCC_SOCS.py:3-37 (Hermitian ``eigh`` in place of ``svd``)
 * ``socs``            -- CalculateAerialImage_SOCS.py:3-11
+* ``socs_resist``     -- the resist loss on that image and its gradient (the chain rule torch autograd applies
+                         through CalculateAerialImage_SOCS.py:3-11)
 * ``hopkins``         -- CalculateAerialImage.py:105-130
 * ``socs_floquet``    -- CalculateAerialImage_SOCS.py:13-32
 
@@ -30,10 +32,29 @@ Pinned against fixtures produced by running the reference itself (``tests/golden
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 
 F32 = np.float32
+
+try:   # the same pocketfft transforms as numpy.fft, on every host core
+    import scipy.fft as _sfft
+except ImportError:   # pragma: no cover
+    _sfft = None
+
+
+def _fft2(a, axes=(-2, -1)):
+    """Forward 2-D DFT (numpy.fft.fft2 convention), threaded over the host cores when scipy is present."""
+    if _sfft is not None:
+        return _sfft.fft2(a, axes=axes, workers=os.cpu_count() or 1)
+    return np.fft.fft2(a, axes=axes)
+
+
+def _ifft2(a, axes=(-2, -1)):
+    if _sfft is not None:
+        return _sfft.ifft2(a, axes=axes, workers=os.cpu_count() or 1)
+    return np.fft.ifft2(a, axes=axes)
 
 
 # ----------------------------------------------------------------------------------------------- source
@@ -122,7 +143,7 @@ def spectrum(sc, po, sr):
     """Hk = npx*npy * fftshift(ifft2(ifftshift(h))), complex128 [Ny, Nx, C]; plus f, g (Scatter.py:10-35)."""
     h = np.asarray(sc.ScatterField).astype(np.complex128)
     f, g, npx, npy = freq_axes(sc, po, sr)
-    hk = np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(h, axes=(0, 1)), axes=(0, 1)), axes=(0, 1)) * (npx * npy)
+    hk = np.fft.fftshift(_ifft2(np.fft.ifftshift(h, axes=(0, 1)), axes=(0, 1)), axes=(0, 1)) * (npx * npy)
     return hk, f, g
 
 
@@ -202,11 +223,18 @@ def _pupil(po, sr, rho2, focus):
 
 
 # ------------------------------------------------------------------------------------------------- Abbe
-def abbe(sr, sc, po, nm, chunk=64):
-    """Abbe aerial image [nFocus, Ny, Nx], float64 (CalculateAerialImage.py:18-103)."""
+def abbe(sr, sc, po, nm, chunk=None, points=None):
+    """Abbe aerial image [nFocus, Ny, Nx], float64 (CalculateAerialImage.py:18-103).  Source points are
+    transformed `chunk` at a time (default: about 1 GB of fields per stack).
+
+    With `points` (source-point indices) it also returns {j: A_j}, A_j [nFocus, Ny, Nx] the unweighted intensity
+    of point j, dfdg^2 fftshift(sum over channels and field components |E|^2), so that the image is
+    n / sum(v) * sum_j v_j A_j (CalculateAerialImage.py:86-92) -- what a source-weight derivative needs."""
     X, Y, V = source_points(sr)
     hk, f, g = spectrum(sc, po, sr)
     ny, nx, nch = hk.shape
+    if chunk is None:
+        chunk = max(1, min(64, (1 << 30) // (16 * ny * nx * 3 * max(1, nch))))
     W = float(np.sum(V.astype(np.float64)))
     vector = nm.ImageCalculationMode.lower() == 'vector'
     ne = 3 if vector else 1
@@ -219,12 +247,14 @@ def abbe(sr, sc, po, nm, chunk=64):
     focus_range = np.atleast_1d(np.asarray(po.FocusRange, dtype=np.float64))
     px, py = (complex(v) for v in sr.PolarizationVector)
     out = np.zeros((len(focus_range), ny, nx))
+    keep = {int(j): np.zeros((len(focus_range), ny, nx)) for j in (points if points is not None else ())}
     for iz, z in enumerate(focus_range):
         acc = np.zeros((ny, nx))
         for j0 in range(0, len(V), chunk):
             js = range(j0, min(j0 + chunk, len(V)))
             fields = []
             wts = []
+            owner = []
             for j in js:
                 rho2_32 = (fg2 + F32(2) * (X[j] * fm32 + Y[j] * gm32)) + (X[j] * X[j] + Y[j] * Y[j])
                 valid = rho2_32 <= 1
@@ -246,11 +276,15 @@ def abbe(sr, sc, po, nm, chunk=64):
                         fld[valid] = base * comps[e]
                         fields.append(fld)
                         wts.append(float(V[j]))
+                        owner.append(j)
             if fields:
-                E = np.fft.fft2(np.stack(fields), axes=(1, 2))
-                acc += np.tensordot(np.asarray(wts), np.abs(E) ** 2, axes=(0, 0))
+                E2 = np.abs(_fft2(np.stack(fields), axes=(1, 2))) ** 2
+                acc += np.tensordot(np.asarray(wts), E2, axes=(0, 0))
+                for i, j in enumerate(owner):
+                    if j in keep:
+                        keep[j][iz] += dfdg ** 2 * np.fft.fftshift(E2[i])
         out[iz] = po.IndexImage / W * dfdg ** 2 * np.fft.fftshift(acc)
-    return out
+    return (out, keep) if points is not None else out
 
 
 # ------------------------------------------------------------------------------------------------- TCC
@@ -345,9 +379,47 @@ def socs(sc, kernels, sr, po):
         if not np.any(sp[:, :, c] != 0):
             continue
         for k in range(kernels.shape[2]):
-            E = dfdg * np.fft.fft2(kernels[:, :, k] * sp[:, :, c])
+            E = dfdg * _fft2(kernels[:, :, k] * sp[:, :, c])
             acc += np.abs(E) ** 2
     return np.fft.fftshift(acc)
+
+
+def socs_resist(logits, target, kernels, a, thr):
+    """SOCS image of the mask sigmoid(logits) (CalculateAerialImage_SOCS.py:3-11, one live channel), the resist
+    loss L = sum (sigmoid(a (I - thr)) - target)^2 and its exact gradient dL/dlogits, all float64.
+
+    The gradient is the chain rule through the reference's own operations -- what torch autograd computes
+    through them -- restated: with u = ifftshift(t), E_k = fft2(K_k .* ifft2(u)) (the npx npy and df dg factors
+    of Scatter.py:20 and CalculateAerialImage_SOCS.py:7 cancel), I = fftshift(sum_k |E_k|^2) and
+    gA = ifftshift(dL/dI), the adjoint of fft2 being N^2 ifft2 gives
+        dL/du = 2 sum_k Re fft2(conj(K_k) .* ifft2(gA .* E_k)),   dL/dt = fftshift(dL/du),
+    and dL/dlogits = dL/dt * t (1 - t).  Returns (I, L, grad)."""
+    l = np.asarray(logits, dtype=np.float64)
+    t = 1.0 / (1.0 + np.exp(-l))
+    d = _ifft2(np.fft.ifftshift(t))
+    K = np.asarray(kernels)
+    E = [_fft2(K[:, :, k] * d) for k in range(K.shape[2])]
+    acc = np.zeros(t.shape)
+    for e in E:
+        acc += e.real ** 2 + e.imag ** 2
+    I = np.fft.fftshift(acc)
+    s = 1.0 / (1.0 + np.exp(-a * (I - thr)))
+    r = s - np.asarray(target, dtype=np.float64)
+    loss = float(np.sum(r * r))
+    gA = np.fft.ifftshift(2.0 * r * a * s * (1.0 - s))
+    du = np.zeros(t.shape)
+    for k, e in enumerate(E):
+        du += 2.0 * _fft2(np.conj(K[:, :, k]) * _ifft2(gA * e)).real
+    return I, loss, np.fft.fftshift(du) * t * (1.0 - t)
+
+
+def socs_pixel_fields(kernels):
+    """F_k = fft2(K_k) / N^2: changing the mask t at pixel p by delta changes E_k by delta * roll(F_k, q), with
+    q = ifftshift's image of p (so E_k(x) + delta F_k(x - q)) -- the exact single-pixel update of the SOCS
+    fields, for finite differences without recomputing every transform."""
+    K = np.asarray(kernels)
+    n = K.shape[0] * K.shape[1]
+    return [_fft2(K[:, :, k]) / n for k in range(K.shape[2])]
 
 
 def hopkins(sr, sc, po, nm):

@@ -50,3 +50,13 @@ def rel_err(a, b):
     dt = np.complex128 if (np.iscomplexobj(a) or np.iscomplexobj(b)) else np.float64
     a, b = a.astype(dt), b.astype(dt)
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def cfg4_kernels(meta, arrays, dtype=np.complex128):
+    """The reference's SOCS-16 kernels of the configuration-4 fixture on the full [n, n, 16] grid (the fixture keeps
+    only their band rows and columns)."""
+    n = meta['n']
+    k = arrays['kernels_band']
+    out = np.zeros((n, n, k.shape[2]), dtype=dtype)
+    out[np.ix_(arrays['kernel_rows'], arrays['kernel_cols'])] = k
+    return out

@@ -2,9 +2,9 @@
 
 Run in a container that holds the reference sources (it imports them from ``REFERENCE_DIR``):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [REFERENCE_DIR]
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [REFERENCE_DIR [CASE ...]]
 
-Writes ``tests/golden/ref_<case>.npz`` plus ``manifest.json``.  Each fixture stores the inputs and the
+Writes ``tests/golden/ref_<case>.npz`` (every case, or only the CASEs named) plus ``manifest.json``.  Each fixture stores the inputs and the
 reference's outputs, so the tests replay the same inputs through the oracle and the engine without needing
 the reference at run time.  The reference's matplotlib-importing drivers are not imported, and its RCWA
 solver is not constructed.
@@ -252,9 +252,101 @@ def case_cfg3_tcc_spectrum():
          sv=S[:64].numpy(), diag=torch.real(torch.diagonal(T)).numpy())
 
 
-def main():
+def line_space_mask(n, period, seed, line=45.0, pitch=90.0, ncuts=3):
+    """Vertical lines (`line` nm at `pitch` nm) with `ncuts` seeded rectangular cuts of 40-200 nm."""
+    g = np.random.default_rng(seed)
+    xx = (np.arange(n) + 0.5) * period / n
+    t = np.repeat(((xx % pitch) < line).astype(np.float32)[None, :], n, axis=0)
+    yy = (np.arange(n) + 0.5) * period / n
+    for _ in range(ncuts):
+        w, h = g.uniform(40.0, 200.0, 2)
+        x0, y0 = g.uniform(0, period, 2)
+        t[np.ix_((yy >= y0) & (yy < y0 + h), (xx >= x0) & (xx < x0 + w))] = 0
+    return t
+
+
+def case_cfg2_small():
+    """Configuration 2 at a quarter of its period (512 nm at its 4 nm/pixel, 128 x 128): vector Abbe, x_pol,
+    quasar 0.5/0.85/30 deg PntNum 31, five focus planes -60..60 nm, Zernike Z5-Z37 ~ N(0, 0.01) waves, 45/90 nm
+    lines with seeded cuts."""
+    sr, po, nm, sc = Source(), Projection(), Numerics(), Scatter()
+    sr.Shape, sr.PntNum, sr.SigmaIn, sr.SigmaOut, sr.OpenAngle = 'quasar', 31, 0.5, 0.85, math.pi / 6
+    sr.PolarizationVector = [1.0, 0.0]
+    mapped(po, sr)
+    nm.ImageCalculationMode = 'vector'
+    focus = [-60.0, -30.0, 0.0, 30.0, 60.0]
+    po.FocusRange = torch.tensor(focus)
+    z = torch.zeros(37)
+    z[4:] = 0.01 * torch.randn(33, generator=torch.Generator().manual_seed(1202))
+    po.Aberration_Zernike = z
+    n, period = 128, 512
+    field = np.zeros((n, n, 3), dtype=np.complex64)
+    field[:, :, 0] = line_space_mask(n, period, 202)
+    sc.Period_X = sc.Period_Y = period
+    sc.ScatterField = torch.from_numpy(field)
+    t0 = time.time()
+    img, pim = CalculateAbbeImage(sr, sc, po, nm)
+    meta = dict(src=src_params(sr), Period_X=period, Period_Y=period, vector=True, focus=focus, NA=po.NA,
+                IndexImage=po.IndexImage, Magnification=po.Magnification, raw=False, seconds=time.time() - t0)
+    save('cfg2_small', meta, field=field, zernike=z.numpy(), abbe=img.Intensity.numpy(), abbe_pupil=pim.numpy())
+
+
+def case_autograd_cfg4():
+    """Configuration 4 at its own size through the reference, by torch autograd: SOCS-16 kernels of the vector
+    annular 0.7/0.95 (PntNum 41) system at 2048 nm, a 1024 x 1024 mask sigmoid(logits) with seeded N(0, 1)
+    logits, loss ||sigmoid(50 (I - 0.25)) - target||^2 against a seeded rectangle target.  Inputs come from
+    opticalimaging_b200.workloads.config4 (regenerated by the tests from the seed); the fixture keeps the
+    reference's kernels on their band, its loss, and its image and gradient at 4096 seeded pixels."""
+    sys.path.insert(0, os.path.dirname(os.path.dirname(OUT)))
+    from opticalimaging_b200 import workloads as Wl
+    _, _, _, logits_np, target_np = Wl.config4()
+    sr, po, nm, sc = Source(), Projection(), Numerics(), Scatter()
+    sr.Shape, sr.PntNum, sr.SigmaIn, sr.SigmaOut = 'annular', 41, 0.7, 0.95
+    mapped(po, sr)
+    nm.ImageCalculationMode = 'vector'
+    nm.Hopkins_SettingType, nm.Hopkins_Order = 'order', 16
+    n, period = 1024, 2048
+    t0 = time.time()
+    T, fg = CalculateTCCMatrix(sr, [period, period], po, 0.0, nm)
+    K = DecomposeTCC_SOCS(T, fg, [n, n], nm)
+    logits = torch.from_numpy(logits_np).requires_grad_(True)
+    target = torch.from_numpy(target_np)
+    mask = torch.sigmoid(logits)
+    zz = torch.zeros_like(mask)
+    sc.Period_X = sc.Period_Y = period
+    sc.ScatterField = torch.stack((mask, zz, zz), 2)
+    I, _ = CalculateAerialImage_SOCS(sc, K, sr, po)
+    loss = torch.sum((torch.sigmoid(50.0 * (I - 0.25)) - target) ** 2)
+    loss.backward()
+    nz = (K != 0).any(dim=2)
+    rows = torch.nonzero(nz.any(dim=1)).flatten().numpy()
+    cols = torch.nonzero(nz.any(dim=0)).flatten().numpy()
+    kb = K.detach()[rows][:, cols]                          # [len rows, len cols, 16] (cyclic index lists kept)
+    pix = np.random.default_rng(404).integers(0, n, size=(4096, 2))
+    img = I.detach().numpy()
+    grad = logits.grad.numpy()
+    save('autograd_cfg4', dict(src=src_params(sr), Period_X=period, Period_Y=period, a=50.0, thr=0.25, order=16,
+                               n=n, seed=4, seconds=time.time() - t0),
+         kernel_rows=rows, kernel_cols=cols, kernels_band=kb.numpy(), loss=np.array(loss.item()),
+         pixels=pix, image_at=img[pix[:, 0], pix[:, 1]], grad_at=grad[pix[:, 0], pix[:, 1]],
+         image_peak=np.array(float(img.max())), grad_maxabs=np.array(float(np.abs(grad).max())))
+
+
+CASES = ('sources', 'zernike_char', 'spectrum', 'cfg1', 'vec_small', 'odd_scalar', 'cfg3_small', 'raw_nan',
+         'autograd', 'floquet', 'cfg3_tcc', 'cfg2_small', 'autograd_cfg4')
+
+
+def main(only=None):
     t0 = time.time()
     print('reference fixtures ->', OUT)
+    want = set(CASES if not only else only)
+    if 'cfg2_small' in want:
+        case_cfg2_small()
+    if 'autograd_cfg4' in want:
+        case_autograd_cfg4()
+    if want <= {'cfg2_small', 'autograd_cfg4'}:
+        print('done in %.1f s' % (time.time() - t0))
+        return
     case_sources()
     case_zernike_char()
     case_spectrum()
@@ -289,4 +381,4 @@ def main():
 
 
 if __name__ == '__main__':
-    main()
+    main([a for a in sys.argv[2:]])

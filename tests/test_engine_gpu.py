@@ -1,7 +1,9 @@
 """Parity of the CUDA engine with the FP64 oracle and with the reference's own outputs (golden fixtures).
 
 Tolerances are relative to the peak of the reference image: the FP32 engine form must agree with the FP64
-oracle to 1e-5 of peak, and with the complex64 reference to 2e-5 of peak (the reference's own rounding).
+oracle and with the complex64 reference to 1e-5 of peak.  (The reference's own rounding on these fixtures is
+1.2e-6 to 2.5e-6 of peak against FP64, pinned in tests/test_oracle_golden.py; the engine's is of the same size,
+so the two stay well inside 1e-5 of each other.  Each test records its measured errors.)
 """
 import warnings
 
@@ -15,7 +17,7 @@ from tests.fixtures import build, load, rel_err
 pytestmark = pytest.mark.gpu
 
 FP32_VS_FP64 = 1e-5
-FP32_VS_REF = 2e-5
+FP32_VS_REF = 1e-5
 
 
 @pytest.fixture(scope='module')
@@ -50,33 +52,40 @@ def test_band_spectrum_matches_numpy(oi):
         assert rel_err(got_u[:, 0].cpu().numpy(), want_r) < 2e-6
 
 
-@pytest.mark.parametrize('name', ['cfg1', 'vec_small', 'odd_scalar'])
-def test_abbe_parity(oi, name):
+@pytest.mark.parametrize('name', ['cfg1', 'vec_small', 'odd_scalar', 'cfg2_small'])
+def test_abbe_parity(oi, name, report):
     meta, a = load(name)
     sr, sc, po, nm = build(meta, a)
     img, pim = oi.CalculateAbbeImage(sr, sc, po, nm)
     got = img.Intensity.numpy()
     assert got.shape == a['abbe'].shape
-    assert rel_err(got, O.abbe(sr, sc, po, nm)) < FP32_VS_FP64
+    o = O.abbe(sr, sc, po, nm)
+    report(f'abbe_{name}', engine_vs_fp64=rel_err(got, o), engine_vs_reference=rel_err(got, a['abbe']),
+           reference_vs_fp64=rel_err(a['abbe'], o))
+    assert rel_err(got, o) < FP32_VS_FP64
     assert rel_err(got, a['abbe']) < FP32_VS_REF
     np.testing.assert_array_equal(np.isnan(pim.numpy()), np.isnan(a['abbe_pupil']))
     ok = ~np.isnan(a['abbe_pupil'])
     assert rel_err(pim.numpy()[ok], a['abbe_pupil'][ok]) < 1e-5
 
 
-def test_socs_with_reference_kernels(oi):
+def test_socs_with_reference_kernels(oi, report):
     meta, a = load('vec_small')
     sr, sc, po, nm = build(meta, a)
     got, _ = oi.CalculateAerialImage_SOCS(sc, torch.from_numpy(a['kernels']), sr, po)
+    o = O.socs(sc, a['kernels'].astype(np.complex128), sr, po)
+    report('socs_vec_small', engine_vs_fp64=rel_err(got.numpy(), o), engine_vs_reference=rel_err(got.numpy(), a['socs']),
+           reference_vs_fp64=rel_err(a['socs'], o))
     assert rel_err(got.numpy(), a['socs']) < FP32_VS_REF
-    assert rel_err(got.numpy(), O.socs(sc, a['kernels'].astype(np.complex128), sr, po)) < FP32_VS_FP64
+    assert rel_err(got.numpy(), o) < FP32_VS_FP64
 
 
 @pytest.mark.parametrize('name', ['vec_small', 'odd_scalar', 'cfg3_small'])
-def test_hopkins_parity(oi, name):
+def test_hopkins_parity(oi, name, report):
     meta, a = load(name)
     sr, sc, po, nm = build(meta, a)
     img, _ = oi.CalculateHopkinsImage(sr, sc, po, nm)
+    report(f'hopkins_{name}', engine_vs_reference=rel_err(img.Intensity.numpy(), a['hopkins']))
     assert rel_err(img.Intensity.numpy(), a['hopkins']) < FP32_VS_REF
 
 
@@ -106,7 +115,7 @@ def test_tcc_cfg3_spectrum(oi):
     assert abs(float(torch.real(torch.trace(T))) - meta['trace']) < 1e-5 * meta['trace']
 
 
-def test_floquet_optimized_form(oi):
+def test_floquet_optimized_form(oi, report):
     meta, a = load('floquet')
 
     class Nm:
@@ -115,6 +124,7 @@ def test_floquet_optimized_form(oi):
     for k in ('ScatterOrder_X', 'ScatterOrder_Y', 'ScatterGrid_X', 'ScatterGrid_Y'):
         setattr(nm, k, meta[k])
     got = oi.CalculateSOCS(torch.from_numpy(a['floquet']), torch.from_numpy(a['kernels']), nm)
+    report('floquet', engine_vs_reference=rel_err(got.numpy(), a['image']))
     assert rel_err(got.numpy(), a['image']) < FP32_VS_REF
 
 
@@ -243,3 +253,25 @@ def test_image_host_matches_device_image(oi, form, tol):
         assert rel_err(got, want) < tol
     with pytest.raises(ValueError, match='pinned'):
         sk.image_host(torch.from_numpy(masks), torch.empty((11, 256, 256)), form=form)
+
+
+def test_dropin_socs_reuses_band_form_of_reference_layout_kernels(oi):
+    """CalculateAerialImage_SOCS with the [Ny, Nx, K] kernels DecomposeTCC_SOCS returned finds their band form
+    once per tensor (no full-grid scan per call); an in-place change of the tensor is seen; the image is the
+    same as through the band-form kernels."""
+    meta, a = load('vec_small')
+    sr, sc, po, nm = build(meta, a)
+    T, fg = oi.CalculateTCCMatrix(sr, [meta['Period_Y'], meta['Period_X']], po, meta['focus'][0], nm)
+    K = oi.DecomposeTCC_SOCS(T, fg, [sc.ScatterField.shape[1], sc.ScatterField.shape[0]], nm)
+    sk0 = oi._SOCS_CACHE[K][1]
+    img1, _ = oi.CalculateAerialImage_SOCS(sc, K, sr, po)
+    assert oi._SOCS_CACHE[K][1] is sk0
+    img2, _ = oi.CalculateAerialImage_SOCS(sc, sk0, sr, po)
+    np.testing.assert_array_equal(img1.numpy(), img2.numpy())
+    K.mul_(2.0)                                   # the kernels change in place: the band form is found again
+    img3, _ = oi.CalculateAerialImage_SOCS(sc, K, sr, po)
+    assert oi._SOCS_CACHE[K][1] is not sk0
+    assert rel_err(img3.numpy(), 4.0 * img1.numpy()) < 1e-6
+    host = K.cpu()                                # a host copy: its own entry, scanned once
+    img4, _ = oi.CalculateAerialImage_SOCS(sc, host, sr, po)
+    assert host in oi._SOCS_CACHE and rel_err(img4.numpy(), img3.numpy()) < 1e-6

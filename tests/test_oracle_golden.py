@@ -92,13 +92,15 @@ def test_spectrum():
     assert np.max(np.abs(pim[ok] - a['pupil'][ok])) < 2e-6 * np.max(np.abs(a['pupil'][ok]))
 
 
-@pytest.mark.parametrize('name', ['cfg1', 'vec_small', 'odd_scalar'])
+@pytest.mark.parametrize('name', ['cfg1', 'vec_small', 'odd_scalar', 'cfg2_small'])
 def test_abbe(name):
     meta, a = load(name)
     sr, sc, po, nm = build(meta, a)
     img = O.abbe(sr, sc, po, nm)
     assert img.shape == a['abbe'].shape
     assert rel_err(img, a['abbe']) < 1e-5
+    for z in range(img.shape[0]):   # every focus plane on its own
+        assert rel_err(img[z], a['abbe'][z]) < 1e-5
 
 
 def test_raw_optics_are_nan_in_reference_and_oracle():
@@ -185,3 +187,76 @@ def test_threshold_mode_counts_energy():
     with pytest.raises(ValueError):
         O.socs_count(N, lam, 5)
     assert math.isclose(float(np.sum(lam)), 10.0)
+
+
+def test_cfg4_resist_gradient_matches_reference_autograd():
+    """Configuration 4 at its own size (1024^2, the reference's SOCS-16 kernels, sigmoid(N(0,1)) mask, a = 50
+    resist loss): the FP64 image, loss and exact gradient against the reference's complex64 forward and its
+    torch-autograd gradient at 4096 seeded pixels.  The bounds are the reference's own complex64 rounding at
+    this size (measured: image 5.7e-5 of peak, loss 1.8e-4 relative, gradient 4.4e-4 of its maximum)."""
+    from opticalimaging_b200 import workloads as W
+    from tests.fixtures import cfg4_kernels
+    meta, a = load('autograd_cfg4')
+    _, _, _, logits, target = W.config4(seed=meta['seed'], n=meta['n'], order=meta['order'])
+    I, L, G = O.socs_resist(logits, target, cfg4_kernels(meta, a), meta['a'], meta['thr'])
+    px = a['pixels']
+    assert np.max(np.abs(I[px[:, 0], px[:, 1]] - a['image_at'])) < 1e-4 * float(a['image_peak'])
+    assert abs(L - float(a['loss'])) < 5e-4 * float(a['loss'])
+    assert np.max(np.abs(G[px[:, 0], px[:, 1]] - a['grad_at'])) < 1e-3 * float(a['grad_maxabs'])
+
+
+def test_cfg4_gradient_matches_central_differences():
+    """The FP64 gradient against central finite differences (h = 1e-3) of the FP64 loss on 8 pixels, each
+    difference from the exact single-pixel update of the SOCS fields (socs_pixel_fields)."""
+    from opticalimaging_b200 import workloads as W
+    from tests.fixtures import cfg4_kernels
+    meta, a = load('autograd_cfg4')
+    n, A, thr = meta['n'], meta['a'], meta['thr']
+    _, _, _, logits, target = W.config4(seed=meta['seed'], n=n, order=meta['order'])
+    K = cfg4_kernels(meta, a)
+    _, _, G = O.socs_resist(logits, target, K, A, thr)
+    fd = cfg4_central_differences(logits, target, K, A, thr, [tuple(p) for p in a['pixels'][:8]])
+    got = np.array([G[tuple(p)] for p in a['pixels'][:8]])
+    assert np.max(np.abs(got - fd)) < 1e-6 * np.max(np.abs(G))
+
+
+def cfg4_central_differences(logits, target, K, A, thr, pixels, h=1e-3):
+    """Central differences (h in the logits) of the FP64 resist loss at `pixels`, from the single-pixel field
+    update E_k + delta roll(F_k, q), q the ifftshift image of the pixel."""
+    n = logits.shape[0]
+    lg = logits.astype(np.float64)
+    t = 1.0 / (1.0 + np.exp(-lg))
+    d = O._ifft2(np.fft.ifftshift(t))
+    E = [O._fft2(K[:, :, k] * d) for k in range(K.shape[2])]
+    F = O.socs_pixel_fields(K)
+
+    def loss(p, dl):
+        dt = 1.0 / (1.0 + np.exp(-(lg[p] + dl))) - t[p]
+        q = ((p[0] + n // 2) % n, (p[1] + n // 2) % n)
+        acc = np.zeros((n, n))
+        for e, f in zip(E, F):
+            x = e + dt * np.roll(f, q, axis=(0, 1))
+            acc += x.real ** 2 + x.imag ** 2
+        s = 1.0 / (1.0 + np.exp(-A * (np.fft.fftshift(acc) - thr)))
+        return float(np.sum((s - target) ** 2))
+    return np.array([(loss(p, h) - loss(p, -h)) / (2 * h) for p in pixels])
+
+
+def test_cpu_reference_arm_matches_the_reference():
+    """The reference arm of the benchmark (oracle/cpu_reference.socs_clip: the reference's SOCS algorithm with
+    torch's CPU FFTs on complex64) reproduces the reference's own SOCS image from the reference's kernels, and
+    its host-built kernels (socs_kernels) give the reference's configuration-3 image at 256^2."""
+    from oracle import cpu_reference as R
+    meta, a = load('vec_small')
+    sr, sc, po, nm = build(meta, a)
+    npx = meta['Period_X'] / (sr.Wavelength / po.NA)
+    npy = meta['Period_Y'] / (sr.Wavelength / po.NA)
+    img = R.socs_clip(a['field'], a['kernels'], npx, npy, 2)
+    assert rel_err(img, a['socs']) < 2e-6
+    meta, a = load('cfg3_small')
+    sr, sc, po, nm = build(meta, a)
+    K = R.socs_kernels(sr, po, nm, [meta['Period_Y'], meta['Period_X']], [256, 256])
+    assert K.shape == (256, 256, 24) and K.dtype == np.complex64
+    npx = meta['Period_X'] / (sr.Wavelength / po.NA)
+    img = R.socs_clip(a['field'], K, npx, npx, 2)
+    assert rel_err(img, a['socs']) < 2e-5
