@@ -12,6 +12,9 @@
  *   oi_coarse_to_image    <- the final fftshift + normalisation of both     (CalculateAerialImage.py:89-92,
  *                                                                             CalculateAerialImage_SOCS.py:10)
  *   oi_tcc_pupils64       <- the shifted-pupil matrix of CalculateTCCMatrix  (CalculateTCCMatrix.py:17-51)
+ *   oi_abbe_pupils_pol / oi_tcc_pupils64_pol
+ *                         <- the same with a Jones vector per source point: Calc_PolarizationMap's typed maps
+ *                            (Source.py:183-221) and the states of a CoherencyMatrix (README.md:45)
  *   oi_tcc_assemble64     <- GetTCCMatrix                                    (CalculateTCCMatrix.py:58-75)
  *   oi_band_spectrum_fft / oi_coherent_coarse_fft / oi_coarse_to_image_fft
  *                         <- the same three stages in FFT form (power-of-two grids)
@@ -111,6 +114,16 @@ OI_API int oi_abbe_pupils(const float* fr, const float* fc, int br, int bc, cons
                           int vector,
                           const double* jones, double na, double mag, double index_image, double wavelength,
                           void* pupil, float* weight, void* stream);
+
+/*
+ * oi_abbe_pupils with a Jones vector per source point: jones_pts is a DEVICE array [nsrc][4] of doubles (Px.re,
+ * Px.im, Py.re, Py.im of point j), in place of the constant host `jones` -- a polarisation map (Source.py:183-221)
+ * or one eigen-polarisation of a coherency matrix.  Scalar mode (vector = 0) does not read it.
+ */
+OI_API int oi_abbe_pupils_pol(const float* fr, const float* fc, int br, int bc, const float* sx, const float* sy,
+                              const float* sv, int nsrc, double weight_sum, const double* focus, int nz,
+                              const double* zern, int vector, const double* jones_pts, double na, double mag,
+                              double index_image, double wavelength, void* pupil, float* weight, void* stream);
 
 /*
  * Coherent sum on the coarse grid (the |.|^2 accumulation of both imaging paths):
@@ -289,6 +302,13 @@ OI_API int oi_tcc_pupils64(const float* ff, int lf, const float* gg, int lg, con
                            const float* sv, int nsrc, double weight_sum, double focus, const double* zern, int vector,
                            const double* jones, double na, double mag, double index_image, double wavelength,
                            void* h, void* stream);
+
+/* oi_tcc_pupils64 with a Jones vector per source point (jones_pts: DEVICE [nsrc][4] doubles, as for
+ * oi_abbe_pupils_pol; CalculateTCCMatrix.py:40-46 with Calc_PolarizationMap, Source.py:183-221). */
+OI_API int oi_tcc_pupils64_pol(const float* ff, int lf, const float* gg, int lg, const float* sx, const float* sy,
+                               const float* sv, int nsrc, double weight_sum, double focus, const double* zern,
+                               int vector, const double* jones_pts, double na, double mag, double index_image,
+                               double wavelength, void* h, void* stream);
 
 /*
  * TCC = sum_e h_e h_e^H (GetTCCMatrix, CalculateTCCMatrix.py:58-75), complex128 [fg][fg], full Hermitian.

@@ -22,6 +22,9 @@ _SIGS = {
     'oi_coherent_coarse': [_vp, _i, _i, _i, _i, _vp, _ll, _vp, _i, _i, _i, _i, _vp, _vp, _i, _vp, _vp],
     'oi_coarse_to_image': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp],
     'oi_tcc_pupils64': [_vp, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _d, _vp, _i, _vp, _d, _d, _d, _d, _vp, _vp],
+    'oi_tcc_pupils64_pol': [_vp, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _d, _vp, _i, _vp, _d, _d, _d, _d, _vp, _vp],
+    'oi_abbe_pupils_pol': [_vp, _vp, _i, _i, _vp, _vp, _vp, _i, _d, _vp, _i, _vp, _i, _vp, _d, _d, _d, _d, _vp,
+                           _vp, _vp],
     'oi_tcc_assemble64': [_vp, _i, _i, _i, _vp, _vp],
     'oi_fft_supported': [_i, _i],
     'oi_band_spectrum_fft': [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],

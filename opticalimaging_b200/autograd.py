@@ -127,10 +127,11 @@ def source_weight_gradient(model: CoherentModel, mask: torch.Tensor, g: torch.Te
     with torch.no_grad():
         band = band_spectrum(mask.contiguous(), N.FIELD_REAL_F32, model.plan)
         gc = coarse_gradient(model, g.to(torch.float32).contiguous())
-        _, dots = coherent_adjoint(model, band, gc, field_dots=True)    # [B, Z, S*E]
+        _, dots = coherent_adjoint(model, band, gc, field_dots=True)    # [B, Z, P*S*E]
         S = values.numel()
-        E = model.count // S
-        d = dots.view(dots.shape[0], dots.shape[1], S, E).sum(dim=(1, 3)).double()   # <g, I_j> summed over planes
+        P = getattr(model, 'pol_states', 1)                              # incoherent polarisation states
+        E = model.count // (S * P)
+        d = dots.view(dots.shape[0], dots.shape[1], P, S, E).sum(dim=(1, 2, 4)).double()   # <g, I_j>
         v = values.to(d.device, torch.float64).reshape(1, -1)
         W = v.sum()
         gI = (d * v).sum(dim=1, keepdim=True) * index_image / W               # <g, I>

@@ -79,9 +79,24 @@ __device__ __forceinline__ double2 cdiv_real_den(double2 num, double2 den) {
   return make_double2((num.x * den.x + num.y * den.y) / d, (num.y * den.x - num.x * den.y) / d);
 }
 
-// Polarisation transfer (CalculateCharacteristicMatrix.py:3-17 applied to the Jones vector,
+// The Jones vector of source point j: per point from `jones_pts` (device, [nsrc][4] doubles: Px.re, Px.im,
+// Py.re, Py.im -- a polarisation map, Source.py:183-221) when given, else the constant one of the optics
+// (PolarizationVector, Source.py:222-226).
+__device__ __forceinline__ void jones_of(const Optics& o, const double* __restrict__ jones_pts, int j, double2& px,
+                                         double2& py) {
+  if (jones_pts) {
+    const double* q = jones_pts + 4 * (long long)j;
+    px = make_double2(q[0], q[1]);
+    py = make_double2(q[2], q[3]);
+  } else {
+    px = make_double2(o.pxr, o.pxi);
+    py = make_double2(o.pyr, o.pyi);
+  }
+}
+
+// Polarisation transfer (CalculateCharacteristicMatrix.py:3-17 applied to the Jones vector (px, py),
 // CalculateAerialImage.py:72-74): component e of (Px M0x? + Py M0y?).
-__device__ void transfer(const Optics& o, double f, double g, double2 out[3]) {
+__device__ void transfer(const Optics& o, double f, double g, double2 px, double2 py, double2 out[3]) {
   double al = o.na / o.index_image * f, be = o.na / o.index_image * g;
   double d = 1.0 - al * al - be * be;
   double2 gam = d >= 0 ? make_double2(sqrt(d), 0.0) : make_double2(0.0, sqrt(-d));
@@ -91,7 +106,6 @@ __device__ void transfer(const Optics& o, double f, double g, double2 out[3]) {
   double2 myx = cdiv_real_den(make_double2(-al * be, 0.0), onepg);
   double2 myy = cdiv_real_den(make_double2(be * be, 0.0), onepg);
   myy = make_double2(1.0 - myy.x, -myy.y);
-  double2 px = make_double2(o.pxr, o.pxi), py = make_double2(o.pyr, o.pyi);
   double2 t0 = cmul(px, mxx), t1 = cmul(py, myx);
   out[0] = make_double2(t0.x + t1.x, t0.y + t1.y);
   t0 = cmul(px, myx);
@@ -104,7 +118,8 @@ __device__ void transfer(const Optics& o, double f, double g, double2 out[3]) {
 __global__ void abbe_pupil_kernel(Optics o, const float* __restrict__ fr, const float* __restrict__ fc, int br, int bc,
                                   const float* __restrict__ sx, const float* __restrict__ sy,
                                   const float* __restrict__ sv, int nsrc, const double* __restrict__ focus,
-                                  double wnorm, float2* __restrict__ pupil, float* __restrict__ weight) {
+                                  double wnorm, const double* __restrict__ jones_pts, float2* __restrict__ pupil,
+                                  float* __restrict__ weight) {
   const int ne = o.vector ? 3 : 1;
   long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y, z = blockIdx.z;
@@ -130,8 +145,9 @@ __global__ void abbe_pupil_kernel(Optics o, const float* __restrict__ fr, const 
     out[0] = make_float2((float)p.x, (float)p.y);
     return;
   }
-  double2 tr[3];
-  transfer(o, f, g, tr);
+  double2 tr[3], px, py;
+  jones_of(o, jones_pts, j, px, py);
+  transfer(o, f, g, px, py, tr);
   for (int e = 0; e < 3; ++e) {
     double2 v = cmul(p, tr[e]);
     out[e * plane] = make_float2((float)v.x, (float)v.y);
@@ -142,7 +158,7 @@ __global__ void abbe_pupil_kernel(Optics o, const float* __restrict__ fr, const 
 __global__ void tcc_pupil_kernel(Optics o, const float* __restrict__ ff, int lf, const float* __restrict__ gg, int lg,
                                  const float* __restrict__ sx, const float* __restrict__ sy,
                                  const float* __restrict__ sv, int nsrc, double focus, double wnorm,
-                                 double2* __restrict__ h) {
+                                 const double* __restrict__ jones_pts, double2* __restrict__ h) {
   const int ne = o.vector ? 3 : 1;
   const long long fg = (long long)lf * lg;
   long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -168,8 +184,9 @@ __global__ void tcc_pupil_kernel(Optics o, const float* __restrict__ ff, int lf,
     out[0] = pu;
     return;
   }
-  double2 tr[3];
-  transfer(o, f, g, tr);
+  double2 tr[3], px, py;
+  jones_of(o, jones_pts, j, px, py);
+  transfer(o, f, g, px, py, tr);
   for (int e = 0; e < 3; ++e) out[e * plane] = cmul(pu, tr[e]);
 }
 
@@ -193,39 +210,80 @@ static void set_optics(Optics& o, const double* zern, int vector, const double* 
 
 }  // namespace oi
 
+namespace oi {
+
+static int abbe_pupils(const float* fr, const float* fc, int br, int bc, const float* sx, const float* sy,
+                       const float* sv, int nsrc, double weight_sum, const double* focus, int nz, const double* zern,
+                       int vector, const double* jones, const double* jones_pts, double na, double mag,
+                       double index_image, double wavelength, void* pupil, float* weight, void* stream,
+                       const char* what) {
+  if (!fr || !fc || !sx || !sy || !sv || !focus || (!jones && !jones_pts) || !pupil || !weight || br <= 0 ||
+      bc <= 0 || nsrc <= 0 || nz <= 0)
+    return fail(OI_EINVAL, "%s: bad arguments", what);
+  if (nsrc > 65535 || nz > 65535) return fail(OI_ERANGE, "%s: too many source points or planes", what);
+  cudaStream_t s = (cudaStream_t)stream;
+  Optics o;
+  const double none[4] = {1.0, 0.0, 0.0, 0.0};
+  set_optics(o, zern, vector, jones ? jones : none, na, mag, index_image, wavelength);
+  long long plane = (long long)br * bc;
+  dim3 grid((unsigned)ceil_div(plane, 128), (unsigned)nsrc, (unsigned)nz);
+  abbe_pupil_kernel<<<grid, 128, 0, s>>>(o, fr, fc, br, bc, sx, sy, sv, nsrc, focus, index_image / weight_sum,
+                                         jones_pts, (float2*)pupil, weight);
+  oi::note_launch();
+  return check_launch(what);
+}
+
+static int tcc_pupils64(const float* ff, int lf, const float* gg, int lg, const float* sx, const float* sy,
+                        const float* sv, int nsrc, double weight_sum, double focus, const double* zern, int vector,
+                        const double* jones, const double* jones_pts, double na, double mag, double index_image,
+                        double wavelength, void* h, void* stream, const char* what) {
+  if (!ff || !gg || !sx || !sy || !sv || (!jones && !jones_pts) || !h || lf <= 0 || lg <= 0 || nsrc <= 0)
+    return fail(OI_EINVAL, "%s: bad arguments", what);
+  cudaStream_t s = (cudaStream_t)stream;
+  Optics o;
+  const double none[4] = {1.0, 0.0, 0.0, 0.0};
+  set_optics(o, zern, vector, jones ? jones : none, na, mag, index_image, wavelength);
+  long long total = (long long)lf * lg * nsrc;
+  tcc_pupil_kernel<<<(unsigned)ceil_div(total, 128), 128, 0, s>>>(o, ff, lf, gg, lg, sx, sy, sv, nsrc, focus,
+                                                                   index_image / weight_sum, jones_pts, (double2*)h);
+  oi::note_launch();
+  return check_launch(what);
+}
+
+}  // namespace oi
+
 extern "C" int oi_abbe_pupils(const float* fr, const float* fc, int br, int bc, const float* sx, const float* sy,
                               const float* sv, int nsrc, double weight_sum, const double* focus, int nz,
                               const double* zern, int vector, const double* jones, double na, double mag,
                               double index_image, double wavelength, void* pupil, float* weight, void* stream) {
-  using namespace oi;
-  if (!fr || !fc || !sx || !sy || !sv || !focus || !jones || !pupil || !weight || br <= 0 || bc <= 0 || nsrc <= 0 ||
-      nz <= 0)
-    return fail(OI_EINVAL, "oi_abbe_pupils: bad arguments");
-  if (nsrc > 65535 || nz > 65535) return fail(OI_ERANGE, "oi_abbe_pupils: too many source points or planes");
-  cudaStream_t s = (cudaStream_t)stream;
-  Optics o;
-  set_optics(o, zern, vector, jones, na, mag, index_image, wavelength);
-  long long plane = (long long)br * bc;
-  dim3 grid((unsigned)ceil_div(plane, 128), (unsigned)nsrc, (unsigned)nz);
-  abbe_pupil_kernel<<<grid, 128, 0, s>>>(o, fr, fc, br, bc, sx, sy, sv, nsrc, focus, index_image / weight_sum,
-                                         (float2*)pupil, weight);
-  oi::note_launch();
-  return check_launch("oi_abbe_pupils");
+  if (!jones) return oi::fail(OI_EINVAL, "oi_abbe_pupils: bad arguments");
+  return oi::abbe_pupils(fr, fc, br, bc, sx, sy, sv, nsrc, weight_sum, focus, nz, zern, vector, jones, nullptr, na,
+                         mag, index_image, wavelength, pupil, weight, stream, "oi_abbe_pupils");
+}
+
+extern "C" int oi_abbe_pupils_pol(const float* fr, const float* fc, int br, int bc, const float* sx, const float* sy,
+                                  const float* sv, int nsrc, double weight_sum, const double* focus, int nz,
+                                  const double* zern, int vector, const double* jones_pts, double na, double mag,
+                                  double index_image, double wavelength, void* pupil, float* weight, void* stream) {
+  if (!jones_pts) return oi::fail(OI_EINVAL, "oi_abbe_pupils_pol: bad arguments");
+  return oi::abbe_pupils(fr, fc, br, bc, sx, sy, sv, nsrc, weight_sum, focus, nz, zern, vector, nullptr, jones_pts,
+                         na, mag, index_image, wavelength, pupil, weight, stream, "oi_abbe_pupils_pol");
 }
 
 extern "C" int oi_tcc_pupils64(const float* ff, int lf, const float* gg, int lg, const float* sx, const float* sy,
                                const float* sv, int nsrc, double weight_sum, double focus, const double* zern,
                                int vector, const double* jones, double na, double mag, double index_image,
                                double wavelength, void* h, void* stream) {
-  using namespace oi;
-  if (!ff || !gg || !sx || !sy || !sv || !jones || !h || lf <= 0 || lg <= 0 || nsrc <= 0)
-    return fail(OI_EINVAL, "oi_tcc_pupils64: bad arguments");
-  cudaStream_t s = (cudaStream_t)stream;
-  Optics o;
-  set_optics(o, zern, vector, jones, na, mag, index_image, wavelength);
-  long long total = (long long)lf * lg * nsrc;
-  tcc_pupil_kernel<<<(unsigned)ceil_div(total, 128), 128, 0, s>>>(o, ff, lf, gg, lg, sx, sy, sv, nsrc, focus,
-                                                                   index_image / weight_sum, (double2*)h);
-  oi::note_launch();
-  return check_launch("oi_tcc_pupils64");
+  if (!jones) return oi::fail(OI_EINVAL, "oi_tcc_pupils64: bad arguments");
+  return oi::tcc_pupils64(ff, lf, gg, lg, sx, sy, sv, nsrc, weight_sum, focus, zern, vector, jones, nullptr, na, mag,
+                          index_image, wavelength, h, stream, "oi_tcc_pupils64");
+}
+
+extern "C" int oi_tcc_pupils64_pol(const float* ff, int lf, const float* gg, int lg, const float* sx, const float* sy,
+                                   const float* sv, int nsrc, double weight_sum, double focus, const double* zern,
+                                   int vector, const double* jones_pts, double na, double mag, double index_image,
+                                   double wavelength, void* h, void* stream) {
+  if (!jones_pts) return oi::fail(OI_EINVAL, "oi_tcc_pupils64_pol: bad arguments");
+  return oi::tcc_pupils64(ff, lf, gg, lg, sx, sy, sv, nsrc, weight_sum, focus, zern, vector, nullptr, jones_pts, na,
+                          mag, index_image, wavelength, h, stream, "oi_tcc_pupils64_pol");
 }

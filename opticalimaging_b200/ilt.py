@@ -76,7 +76,9 @@ def set_source_weights(model: CoherentModel, values: torch.Tensor, index_image: 
     if K % v.numel():
         raise ValueError(f'{v.numel()} source weights do not divide the model\'s {K} fields')
     w = (index_image / v.sum()) * v
-    model.weights.copy_(w.repeat_interleave(K // v.numel()).to(torch.float32)[None].expand(Z, K))
+    P = getattr(model, 'pol_states', 1)          # fields are [polarisation state][point][component]
+    per = w.repeat_interleave(K // (P * v.numel())).repeat(P)
+    model.weights.copy_(per.to(torch.float32)[None].expand(Z, K))
 
 
 def optimize_source_mask(model: CoherentModel, values: torch.Tensor, index_image: float, target: torch.Tensor,

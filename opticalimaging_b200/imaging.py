@@ -212,13 +212,38 @@ def abbe_model(source, projector, numerics, period_y, period_x, ny, nx, focus=No
     fc = f[band.m0c + nx // 2: band.m0c + nx // 2 + band.bc].to(dev)
     Xd, Yd, Vd = X.to(dev), Y.to(dev), V.to(dev)
     fz = torch.tensor(zs, dtype=torch.float64, device=dev)
-    pupils = torch.empty((len(zs), nsrc * ne, band.br, band.bc), dtype=torch.complex64, device=dev)
-    weights = torch.empty((len(zs), nsrc * ne), dtype=torch.float32, device=dev)
-    N.call('oi_abbe_pupils', N.ptr(fr), N.ptr(fc), band.br, band.bc, N.ptr(Xd), N.ptr(Yd), N.ptr(Vd), nsrc,
-           float(torch.sum(V)), N.ptr(fz), len(zs), _zernike(projector), int(vector), _jones(source),
-           float(projector.NA), float(projector.Magnification), float(projector.IndexImage),
-           float(source.Wavelength), N.ptr(pupils), N.ptr(weights), N.stream_handle(dev))
-    return CoherentModel(pupils, weights, band, ny, nx, kind='abbe')
+    states = _pol_states(source, X, Y, vector, dev)
+    sets = []
+    for st in states:   # one field set per incoherent polarisation state, [Z, S*E] each
+        pupils = torch.empty((len(zs), nsrc * ne, band.br, band.bc), dtype=torch.complex64, device=dev)
+        weights = torch.empty((len(zs), nsrc * ne), dtype=torch.float32, device=dev)
+        args = (N.ptr(fr), N.ptr(fc), band.br, band.bc, N.ptr(Xd), N.ptr(Yd), N.ptr(Vd), nsrc, float(torch.sum(V)),
+                N.ptr(fz), len(zs), _zernike(projector), int(vector))
+        tail = (float(projector.NA), float(projector.Magnification), float(projector.IndexImage),
+                float(source.Wavelength), N.ptr(pupils), N.ptr(weights), N.stream_handle(dev))
+        if st is None:
+            N.call('oi_abbe_pupils', *args, _jones(source), *tail)
+        else:
+            N.call('oi_abbe_pupils_pol', *args, N.ptr(st), *tail)
+        sets.append((pupils, weights))
+    if len(sets) == 1:
+        pupils, weights = sets[0]
+    else:
+        pupils = torch.cat([p for p, _ in sets], dim=1)
+        weights = torch.cat([w for _, w in sets], dim=1)
+    model = CoherentModel(pupils, weights, band, ny, nx, kind='abbe')
+    model.pol_states = len(sets)
+    return model
+
+
+def _pol_states(source, X, Y, vector, dev):
+    """The polarisation states of a vector image as device Jones arrays [S, 4] float64 (Px.re, Px.im, Py.re,
+    Py.im per point), or [None] for the source's constant PolarizationVector.  Scalar images carry no
+    polarisation (as in the reference): one state."""
+    states = source.polarization_states(X, Y) if vector and hasattr(source, 'polarization_states') else None
+    if states is None:
+        return [None]
+    return [torch.view_as_real(st.to(torch.complex128)).reshape(-1, 4).contiguous().to(dev) for st in states]
 
 
 def abbe_intensity(source, scatter, projector, numerics, h=None):
@@ -262,7 +287,8 @@ def _tcc_axes(source, xypitch, projector):
 
 
 def tcc_pupil_matrix(source, xypitch, projector, focus, numerics):
-    """h [ne, FG, S] complex128 with TCC = sum_e h_e h_e^H, and FG_ValidSize [len g, len f]."""
+    """h [ne, FG, S] complex128 with TCC = sum_e h_e h_e^H, and FG_ValidSize [len g, len f].  With several
+    polarisation states (a CoherencyMatrix) their component sets are stacked: ne = 3 x states."""
     vector = _mode(numerics)
     _check_domain(projector)
     dev = require_cuda()
@@ -271,16 +297,23 @@ def tcc_pupil_matrix(source, xypitch, projector, focus, numerics):
     f, g = _tcc_axes(source, xypitch, projector)
     ne = 3 if vector else 1
     nsrc = X.numel()
-    h = torch.empty((ne, f.numel() * g.numel(), max(nsrc, 1)), dtype=torch.complex128, device=dev)
     if nsrc == 0:
-        h.fill_(float('nan'))
+        h = torch.full((ne, f.numel() * g.numel(), 1), float('nan'), dtype=torch.complex128, device=dev)
         return h, [g.numel(), f.numel()]
     fd, gd, Xd, Yd, Vd = (t.to(dev) for t in (f, g, X, Y, V))   # held until the launch is enqueued
-    N.call('oi_tcc_pupils64', N.ptr(fd), f.numel(), N.ptr(gd), g.numel(), N.ptr(Xd), N.ptr(Yd), N.ptr(Vd), nsrc,
-           float(torch.sum(V)), float(focus), _zernike(projector), int(vector), _jones(source),
-           float(projector.NA), float(projector.Magnification), float(projector.IndexImage),
-           float(source.Wavelength), N.ptr(h), N.stream_handle(dev))
-    return h, [g.numel(), f.numel()]
+    hs = []
+    for st in _pol_states(source, X, Y, vector, dev):   # TCC = sum over states and components of h h^H
+        h = torch.empty((ne, f.numel() * g.numel(), nsrc), dtype=torch.complex128, device=dev)
+        args = (N.ptr(fd), f.numel(), N.ptr(gd), g.numel(), N.ptr(Xd), N.ptr(Yd), N.ptr(Vd), nsrc,
+                float(torch.sum(V)), float(focus), _zernike(projector), int(vector))
+        tail = (float(projector.NA), float(projector.Magnification), float(projector.IndexImage),
+                float(source.Wavelength), N.ptr(h), N.stream_handle(dev))
+        if st is None:
+            N.call('oi_tcc_pupils64', *args, _jones(source), *tail)
+        else:
+            N.call('oi_tcc_pupils64_pol', *args, N.ptr(st), *tail)
+        hs.append(h)
+    return (hs[0] if len(hs) == 1 else torch.cat(hs, dim=0)), [g.numel(), f.numel()]
 
 
 def CalculateTCCMatrix(source, xypitch, projector, focus, numerics):

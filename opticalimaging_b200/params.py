@@ -74,11 +74,68 @@ class SourceData:
 
 
 class PolarizationParameters:
-    """Polarisation parameters (Source.py:305-308)."""
+    """Polarisation parameters (Source.py:305-308), plus the CoherencyMatrix the reference documents (README.md:45)
+    but does not implement: a 2 x 2 Hermitian positive semi-definite matrix J = <E E^H> of the illumination's
+    (Ex, Ey).  None (the default) keeps the Jones-vector polarisation."""
 
     def __init__(self):
         self.Degree = 1
         self.Angle = torch.tensor(0)
+        self.CoherencyMatrix = None
+
+
+POLARIZATION_TYPES = ('x_pol', 'y_pol', 'c_pol', 'd_pol', 'r_pol', 't_pol', 'line_pol', 'custom')
+
+
+def polarization_map(kind, theta, rho, vector=(1.0, 0.0), angle=0.0):
+    """Jones vector (Px, Py) per source point, complex128, for a polarisation type (README.md:41; the formulas of
+    Source.py:185-217, which the reference keeps as an unused string): x_pol (1, 0), y_pol (0, 1), c_pol
+    (1, i)/sqrt 2, d_pol (1, 1)/sqrt 2, r_pol (cos theta, sin theta), t_pol (sin theta, -cos theta), line_pol
+    (sin Angle, cos Angle); 'custom' is the constant PolarizationVector.  Points with rho below the float64
+    epsilon get (0, 0), as there."""
+    theta = torch.as_tensor(theta, dtype=torch.float64)
+    rho = torch.as_tensor(rho, dtype=torch.float64)
+    one = torch.ones_like(theta, dtype=torch.complex128)
+    h = math.sqrt(0.5)
+    if kind == 'x_pol':
+        px, py = one, 0 * one
+    elif kind == 'y_pol':
+        px, py = 0 * one, one
+    elif kind == 'c_pol':
+        px, py = h * one, 1j * h * one
+    elif kind == 'd_pol':
+        px, py = h * one, h * one
+    elif kind == 'r_pol':
+        px, py = torch.cos(theta).to(torch.complex128), torch.sin(theta).to(torch.complex128)
+    elif kind == 't_pol':
+        px, py = torch.sin(theta).to(torch.complex128), -torch.cos(theta).to(torch.complex128)
+    elif kind == 'line_pol':
+        a = float(angle)
+        px, py = math.sin(a) * one, math.cos(a) * one
+    elif kind == 'custom':
+        px, py = complex(vector[0]) * one, complex(vector[1]) * one
+    else:
+        raise ValueError("unsupported polarization type")
+    if kind != 'custom':
+        small = rho < sys.float_info.epsilon
+        px, py = px.clone(), py.clone()
+        px[small] = 0
+        py[small] = 0
+    return px, py
+
+
+def coherency_states(J):
+    """The coherency matrix as <= 2 Jones vectors whose intensities add: J = sum_i lambda_i e_i e_i^H, state i =
+    sqrt(lambda_i) e_i (eigenvalues below 1e-12 of the largest dropped).  A rank-1 J = j j^H gives j back (up to a
+    phase, which no intensity sees); J = I / 2 (unpolarised) gives two orthogonal states of weight 1/2."""
+    m = torch.as_tensor(J, dtype=torch.complex128).reshape(2, 2)
+    if not torch.allclose(m, m.conj().T, rtol=1e-9, atol=1e-12):
+        raise ValueError('CoherencyMatrix must be Hermitian')
+    lam, U = torch.linalg.eigh(m)
+    if float(lam.min()) < -1e-9 * max(1.0, float(lam.max())):
+        raise ValueError('CoherencyMatrix must be positive semi-definite')
+    top = float(lam.max())
+    return [(math.sqrt(float(lam[i])) * U[:, i]) for i in range(2) if float(lam[i]) > 1e-12 * top]
 
 
 def _grid(coord):
@@ -155,8 +212,11 @@ class Source:
     """Illumination source (Source.py:15-226).
 
     Shapes: 'annular', 'quasar', 'dipolecirc', 'multipole', 'pixel'.  The polarisation is the constant Jones
-    vector ``PolarizationVector`` (Source.py:222-226); the typed maps of README.md are not live code in the
-    reference either.
+    vector ``PolarizationVector`` (Source.py:222-226), as in the reference, unless one of two engine extensions is
+    set: ``PolarizationType`` (None by default) selects a typed polarisation map per source point
+    (``polarization_map``: the types README.md lists, whose formulas the reference keeps unused in
+    Source.py:185-217), and ``PolarizationParameters.CoherencyMatrix`` (README.md:45) describes partially
+    polarised light, imaged as the sum of its eigen-polarisations' intensities (``polarization_states``).
     """
 
     def __init__(self):
@@ -179,6 +239,7 @@ class Source:
         self.PolarizationParameters = PolarizationParameters()
         self.source_data = SourceData(self.PntNum, self.PntNum)
         self.PolarizationVector = [1.0, 0.0]
+        self.PolarizationType = None
 
     def Calc_SourceSimple(self):
         """Source samples with weight >= 1e-5, as 1-D float32 X, Y, Value (Source.py:47-54)."""
@@ -255,10 +316,32 @@ class Source:
         return d
 
     def Calc_PolarizationMap(self, theta, rho):
-        """Constant Jones vector per source point, complex64 (Source.py:222-226)."""
-        px = (self.PolarizationVector[0] * torch.ones(theta.size())).to(torch.complex64)
-        py = (self.PolarizationVector[1] * torch.ones(theta.size())).to(torch.complex64)
-        return px, py
+        """Jones vector per source point, complex64: the constant PolarizationVector (Source.py:222-226), or the
+        typed map of PolarizationType when one is set (``polarization_map``)."""
+        if self.PolarizationType is None:
+            px = (self.PolarizationVector[0] * torch.ones(theta.size())).to(torch.complex64)
+            py = (self.PolarizationVector[1] * torch.ones(theta.size())).to(torch.complex64)
+            return px, py
+        px, py = polarization_map(self.PolarizationType, theta, rho, self.PolarizationVector,
+                                  self.PolarizationParameters.Angle)
+        return px.to(torch.complex64), py.to(torch.complex64)
+
+    def polarization_states(self, X, Y):
+        """The incoherent polarisation states the image sums over, each a per-point Jones array [S, 2]
+        complex128, or None for 'the constant PolarizationVector' (one state, the reference's behaviour).  With a
+        CoherencyMatrix: one constant state per eigen-polarisation (``coherency_states``); with a PolarizationType:
+        one state from the typed map at the points' (theta, rho)."""
+        J = self.PolarizationParameters.CoherencyMatrix
+        n = torch.as_tensor(X).numel()
+        if J is not None:
+            return [torch.stack((st[0] * torch.ones(n, dtype=torch.complex128),
+                                 st[1] * torch.ones(n, dtype=torch.complex128)), 1) for st in coherency_states(J)]
+        if self.PolarizationType is None:
+            return None
+        rho, theta = cartesian_to_polar(torch.as_tensor(X).reshape(-1).double(), torch.as_tensor(Y).reshape(-1).double())
+        px, py = polarization_map(self.PolarizationType, theta, rho, self.PolarizationVector,
+                                  self.PolarizationParameters.Angle)
+        return [torch.stack((px, py), 1)]
 
 
 # Fringe Zernike Z1..Z37 as (m, trig, radial) -- Projection.py:356-434.  Each radial part is a

@@ -213,6 +213,43 @@ def char_matrix(f, g, NA, n):
     return mxx, myx, myx, myy, -a, -b
 
 
+def polarization_states(sr, X, Y):
+    """Jones vectors per source point, one (Px[S], Py[S]) complex128 pair per incoherent polarisation state.
+
+    * The reference: the constant PolarizationVector (Source.py:222-226), one state.
+    * PolarizationType set: the typed map whose formulas Source.py:185-217 keeps unused -- x (1, 0), y (0, 1),
+      c (1, i)/sqrt 2, d (1, 1)/sqrt 2, r (cos t, sin t), t (sin t, -cos t), line (sin a, cos a) with
+      (rho, t) = polar(X, Y) in float64 and points with rho below the float64 epsilon set to (0, 0); 'custom' is
+      the PolarizationVector.
+    * PolarizationParameters.CoherencyMatrix J set (README.md:45): J = sum_i l_i e_i e_i^H, states sqrt(l_i) e_i
+      (l_i above 1e-12 of the largest), whose intensities add.
+    """
+    S = len(X)
+    J = getattr(getattr(sr, 'PolarizationParameters', None), 'CoherencyMatrix', None)
+    if J is not None:
+        m = np.asarray(J, dtype=np.complex128).reshape(2, 2)
+        lam, U = np.linalg.eigh(m)
+        top = float(np.max(lam))
+        return [(np.full(S, math.sqrt(lam[i]) * U[0, i]), np.full(S, math.sqrt(lam[i]) * U[1, i]))
+                for i in range(2) if lam[i] > 1e-12 * top]
+    kind = getattr(sr, 'PolarizationType', None)
+    if kind is None or kind == 'custom':
+        px, py = (complex(v) for v in sr.PolarizationVector)
+        return [(np.full(S, px), np.full(S, py))]
+    x, y = np.asarray(X, np.float64), np.asarray(Y, np.float64)
+    rho, t = np.sqrt(x * x + y * y), np.arctan2(y, x)
+    one, h = np.ones(S, np.complex128), math.sqrt(0.5)
+    a = float(np.asarray(sr.PolarizationParameters.Angle))
+    px, py = {'x_pol': (one, 0 * one), 'y_pol': (0 * one, one), 'c_pol': (h * one, 1j * h * one),
+              'd_pol': (h * one, h * one), 'r_pol': (np.cos(t) + 0j, np.sin(t) + 0j),
+              't_pol': (np.sin(t) + 0j, -np.cos(t) + 0j), 'line_pol': (math.sin(a) * one, math.cos(a) * one)}[kind]
+    small = rho < np.finfo(np.float64).eps
+    px, py = px.copy(), py.copy()
+    px[small] = 0
+    py[small] = 0
+    return [(px, py)]
+
+
 def _pupil(po, sr, rho2, focus):
     """obliquity * exp(2 pi i W) * defocus at squared radius rho2 (CalculateAerialImage.py:64-67)."""
     NA, M, n, lam = po.NA, po.Magnification, po.IndexImage, sr.Wavelength
@@ -245,7 +282,7 @@ def abbe(sr, sc, po, nm, chunk=None, points=None):
     fm64, gm64 = fm32.astype(np.float64), gm32.astype(np.float64)
     live = [c for c in range(nch) if np.any(hk[:, :, c] != 0)]
     focus_range = np.atleast_1d(np.asarray(po.FocusRange, dtype=np.float64))
-    px, py = (complex(v) for v in sr.PolarizationVector)
+    states = polarization_states(sr, X, Y) if vector else [None]
     out = np.zeros((len(focus_range), ny, nx))
     keep = {int(j): np.zeros((len(focus_range), ny, nx)) for j in (points if points is not None else ())}
     for iz, z in enumerate(focus_range):
@@ -264,16 +301,19 @@ def abbe(sr, sc, po, nm, chunk=None, points=None):
                 obl, dz = _pupil(po, sr, r2, z)
                 ab = aberration(po.Aberration_Zernike, np.sqrt(r2), np.arctan2(gc, fc))
                 P = obl * np.exp(1j * 2 * np.pi * ab) * dz
+                comps = []
                 if vector:
                     mxx, myx, mxy, myy, mxz, myz = char_matrix(fc, gc, po.NA, po.IndexImage)
-                    comps = (px * mxx + py * myx, px * mxy + py * myy, px * mxz + py * myz)
+                    for pxs, pys in states:   # one field set per polarisation state; intensities add
+                        px, py = pxs[j], pys[j]
+                        comps += [px * mxx + py * myx, px * mxy + py * myy, px * mxz + py * myz]
                 else:
-                    comps = (1.0,)
+                    comps = [1.0]
                 for c in live:
                     base = hk[:, :, c][valid] * P
-                    for e in range(ne):
+                    for comp in comps:
                         fld = np.zeros((ny, nx), dtype=np.complex128)
-                        fld[valid] = base * comps[e]
+                        fld[valid] = base * comp
                         fields.append(fld)
                         wts.append(float(V[j]))
                         owner.append(j)
@@ -315,9 +355,12 @@ def pupil_matrix(sr, xypitch, po, focus, nm):
     ab = aberration(po.Aberration_Zernike, np.sqrt(r2[valid]), np.arctan2(ng64[valid], nf64[valid]))
     P[valid] = obl * np.exp(1j * 2 * np.pi * ab) * dz
     if nm.ImageCalculationMode == 'vector':
-        px, py = (complex(v) for v in sr.PolarizationVector)
         mxx, myx, mxy, myy, mxz, myz = char_matrix(nf64, ng64, po.NA, po.IndexImage)
-        G = np.stack(((px * mxx + py * myx) * P, (px * mxy + py * myy) * P, (px * mxz + py * myz) * P))
+        G = []
+        for pxs, pys in polarization_states(sr, X, Y):   # per point (columns j); states stack as components
+            px, py = pxs.reshape(1, -1), pys.reshape(1, -1)
+            G += [(px * mxx + py * myx) * P, (px * mxy + py * myy) * P, (px * mxz + py * myz) * P]
+        G = np.stack(G)
     else:
         G = P[None]
     return G, V.astype(np.float64), [len(g), len(f)]

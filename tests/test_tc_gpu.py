@@ -169,11 +169,14 @@ def test_tc_row_passes_vs_fft(oi, ny, nx, band):
     assert N.device_status() == 0
 
 
-@pytest.mark.parametrize('count,ny,nx,bc', [(1, 128, 256, 40), (7, 640, 2048, 33), (5, 1024, 1024, 59)])
+@pytest.mark.parametrize('count,ny,nx,bc', [(1, 128, 256, 40), (7, 640, 2048, 33), (5, 1024, 1024, 59),
+                                            (3, 384, 384, 21), (64, 1024, 1024, 59), (2, 256, 512, 64)])
 def test_rows_inv_tc_direct(oi, count, ny, nx, bc):
     """The inverse tensor-core row pass through the C ABI against an FP64 evaluation of
-    out[i][y][x] = sum_qc Re(v[i][qc][y] exp(-2 pi i qc x / nx)): an odd number of 128-row blocks (the last pair of
-    row blocks half empty), more items than CTAs with ranges crossing pairs, and one item per CTA."""
+    out[i][y][x] = sum_qc Re(v[i][qc][y] exp(-2 pi i qc x / nx)).  For nx a multiple of 256 the mirror-symmetric
+    pass runs (one item, ranges crossing x tiles, the 64-clip benchmark shape, a full 64-column band); nx = 384
+    takes the direct pass (an odd number of 128-row blocks, the last pair half empty).  Columns 0 and nx/2 are
+    checked on their own: the symmetric pass writes them from its edge lane."""
     from opticalimaging_b200 import _native as N
     dev = torch.device('cuda')
     g = torch.Generator().manual_seed(count * ny + nx)
@@ -191,7 +194,11 @@ def test_rows_inv_tc_direct(oi, count, ny, nx, bc):
     want = np.stack([np.real(vv[i].T @ E) for i in range(count)])
     err, rms = rel_err(got, want), rms_rel(got, want)
     print(f'inverse rows {count}x{ny}x{nx} bc {bc}: max {err:.2e} rms {rms:.2e}')
+    assert not np.isnan(got).any()
     assert err < BF16X3_VS_FP64
+    peak = np.max(np.abs(want))
+    for col in (0, nx // 2, nx - 1):
+        assert np.max(np.abs(got[:, :, col] - want[:, :, col])) < BF16X3_VS_FP64 * peak, col
     assert N.device_status() == 0
 
 
