@@ -199,13 +199,14 @@ def poisson_run(srv, stream, rate, seed, submit):
     return len(stream) / (time.perf_counter() - t0), srv.latency_ms()
 
 
-def serve_measure(sk, info, masks_np, dev, args):
+def serve_measure(sk, info, masks_np, dev, args, latency_budget_ms=None):
     """Served throughput and latency of config-3 requests, against the plain path on the same requests.
 
     The client keeps a ring of pinned result buffers and passes one with each request (the server copies the
     image into it).  Saturated: a closed loop keeping `window` requests outstanding (throughput).  Poisson:
     open-loop arrivals at 70 % of the saturated rate (latency under load), result buffers recycled as each
-    request completes.  Plain: one request at a time."""
+    request completes.  Plain: one request at a time.  `latency_budget_ms` turns on the server's latency-aware
+    batch cap (both the saturated and the Poisson measurements run under it)."""
     import collections
     from opticalimaging_b200 import serve
     spec = serve.ModelSpec(('socs24', N_PIX, PERIOD, args.form), N_PIX, N_PIX, 1,
@@ -219,7 +220,7 @@ def serve_measure(sk, info, masks_np, dev, args):
     window = 4 * BATCH
     ring = list(torch.empty((nreq, 1, N_PIX, N_PIX), dtype=torch.float32).pin_memory())
     ex = serve.CudaExecutor(device=dev, nslots=3)
-    srv = serve.Server(ex, hbm_budget=150e9, max_batch=BATCH)
+    srv = serve.Server(ex, hbm_budget=150e9, max_batch=BATCH, latency_budget_ms=latency_budget_ms)
 
     def closed_loop(n):
         q = collections.deque()
@@ -266,6 +267,7 @@ def serve_measure(sk, info, masks_np, dev, args):
     plain = nplain / tp
     return {"images_per_s": served, "p50_ms": poisson.get("p50_ms"), "p99_ms": poisson.get("p99_ms"),
             "latency_at": f"Poisson arrivals at {rate:.0f} requests/s (70 % of the saturated rate)",
+            "latency_budget_ms": latency_budget_ms, "batch_limit": srv.batch_limit(spec),
             "saturated_p50_ms": sat.get("p50_ms"), "saturated_p99_ms": sat.get("p99_ms"),
             "requests": nreq, "poisson_requests": npois, "window": window, "poisson_batches": batches,
             "form": args.form, "plain_images_per_s": plain,
@@ -777,7 +779,11 @@ def run_engine(args, world, rank, local):
         return
     # ---- served: the same clips as requests through the continuous-batching server (pinned uint8 in,
     # host float32 images out), saturated arrival; and the plain one-request-at-a-time path
-    serving = serve_measure(sk, info, masks_np, dev, args) if not args.no_serve else None
+    serving, unbounded = None, None
+    if not args.no_serve:   # latency-aware batching (the reported figures), and unbounded batches beside it
+        serving = serve_measure(sk, info, masks_np, dev, args, latency_budget_ms=args.latency_budget_ms)
+        unbounded = serve_measure(sk, info, masks_np, dev, args, latency_budget_ms=None)
+        serving["unbounded_batches"] = {k: unbounded[k] for k in ("images_per_s", "p50_ms", "p99_ms", "batch_limit")}
     mix, mix_state = None, {}
     if not args.no_serve and args.mix_requests > 0:
         try:
@@ -855,6 +861,8 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline and the precision study')
     ap.add_argument('--no-serve', action='store_true', help='skip the served measurements (profiling runs)')
     ap.add_argument('--no-configs', action='store_true', help='skip configurations 1, 2 and 4')
+    ap.add_argument('--latency-budget-ms', type=float, default=4.0,
+                    help='latency budget of the served measurement\'s batch cap (see serve.Server)')
     ap.add_argument('--mix-requests', type=int, default=2000,
                     help='requests of the mixed serving stream (configuration 5); 0 skips it')
     ap.add_argument('--batch', type=int, default=64, help='clips per step (64 in the benchmark configuration)')

@@ -22,6 +22,9 @@
  *   oi_coherent_coarse_tc <- the |fft2(.)|^2 accumulation again, split-BF16x3 on tensor cores (tcgen05)
  *   oi_band_spectrum_tc(_sym) / oi_coarse_to_image_tc / oi_rows_fwd_tc(_half) / oi_rows_inv_tc
  *                         <- the N-point stages with their row passes on the tensor cores (split-BF16x3 form)
+ *   oi_synth_tc_constants / oi_synth_tiles_tc / oi_coarse_to_image_tcs
+ *                         <- the final transform of CalculateAerialImage_SOCS.py:7-10 on the intensity's band,
+ *                            coarse spectrum and column synthesis as tensor-core GEMMs
  *   oi_coherent_adjoint   <- (no counterpart: the reference differentiates through torch autograd)
  *   oi_twiddle            <- (no counterpart: fills the phase tables the transforms read)
  *
@@ -254,6 +257,27 @@ OI_API int oi_band_spectrum_tc_sym(const void* field, int kind, int batch, int n
 OI_API int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int br, int bc, const void* wm_r,
                                  const void* wm_c, const void* wn_y, const void* cconsts, int ny, int nx,
                                  void* scratch_ihat, void* scratch_v, void* scratch_tiles, float* out, void* stream);
+
+/*
+ * The coarse-to-image stage of the split-BF16x3 form with the coarse spectrum and the column synthesis on the
+ * tensor cores as well (the final transform of CalculateAerialImage_SOCS.py:7-10 restricted to the intensity's
+ * band): per image two real GEMMs,
+ *   U[sr][n] = sum_sc c[sr][sc] G[sc][n]   G = ((qc ? 2 : 1)/128) (cos | sin)(2 pi qc sc / 128)  (n = re|im x qc < bc)
+ *   v[y][n]  = sum_sr A[y][sr] U[sr][n]   A = (1/128) sum_{|qr| < br} cos(2 pi qr (sr/128 - y/ny))
+ * c the coarse intensity (128 x 128, the sum of its nparts partial sums), v the band rows of the image spectrum
+ * written as the V operand tiles of the row pass (oi_rows_inv_tc_tiles layout).  ny a multiple of 128 up to 4096,
+ * bc <= 64, 2br-1 <= 128.
+ *   oi_synth_tc_constants  the constant image of G and A for (ny, br, bc): (1 + ny/128) * 65536 bytes
+ *   oi_synth_tiles_tc      V tiles [count * ny / 128][64 KB] from coarse [nparts][count][128][128]
+ *   oi_coarse_to_image_tcs oi_synth_tiles_tc then oi_rows_inv_tc_tiles (cconsts from oi_rows_tc_constants(1, ...)):
+ *                          the same result as oi_coarse_to_image_tc
+ * A wait that exceeds 2 s ends the kernel early and sets the device status.
+ */
+OI_API int oi_synth_tc_constants(int ny, int br, int bc, void* image, long long bytes, void* stream);
+OI_API int oi_synth_tiles_tc(const float* coarse, int nparts, int count, int br, int bc, const void* sconsts, int ny,
+                             void* tiles, void* stream);
+OI_API int oi_coarse_to_image_tcs(const float* coarse, int nparts, int count, int br, int bc, const void* sconsts,
+                                  const void* cconsts, int ny, int nx, void* scratch_tiles, float* out, void* stream);
 
 /* The device status word (0 = no error) set by kernels whose bounded waits expired; optionally cleared.
  * Synchronous (reads device memory). */

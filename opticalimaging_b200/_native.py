@@ -49,6 +49,9 @@ _SIGS = {
     'oi_band_spectrum_tc': [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],
     'oi_band_spectrum_tc_sym': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],
     'oi_coarse_to_image_tc': [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp],
+    'oi_synth_tc_constants': [_i, _i, _i, _vp, _ll, _vp],
+    'oi_synth_tiles_tc': [_vp, _i, _i, _i, _i, _vp, _i, _vp, _vp],
+    'oi_coarse_to_image_tcs': [_vp, _i, _i, _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp],
 }
 
 FIELD_REAL_F32, FIELD_COMPLEX_C64, FIELD_U8 = 0, 1, 2

@@ -593,10 +593,11 @@ extern "C" int oi_coherent_coarse_tc(const void* band, int batch, int nch, int m
 extern "C" int oi_device_status(int* status, int reset) {
   using namespace oi;
   if (!status) return fail(OI_EINVAL, "oi_device_status: null status");
-  int rows = 0;
-  if (cudaMemcpyFromSymbol(status, g_device_status, sizeof(int)) != cudaSuccess || rows_tc_status(&rows, reset))
+  int rows = 0, synth = 0;
+  if (cudaMemcpyFromSymbol(status, g_device_status, sizeof(int)) != cudaSuccess || rows_tc_status(&rows, reset) ||
+      synth_tc_status(&synth, reset))
     return fail(OI_ECUDA, "oi_device_status: %s", cudaGetErrorString(cudaGetLastError()));
-  *status |= rows;
+  *status |= rows | synth;
   if (reset) {
     const int zero = 0;
     if (cudaMemcpyToSymbol(g_device_status, &zero, sizeof(int)) != cudaSuccess)

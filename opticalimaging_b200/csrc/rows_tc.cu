@@ -53,45 +53,10 @@ constexpr uint32_t OPER = 128 * 128;       // one [128 rows][64 bf16] swizzled o
 
 __device__ __forceinline__ void fail_status() { atomicExch(&g_rows_status, 1); }
 
-__device__ __forceinline__ void arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-// Cursor over a ring of mbarrier-guarded slots: slot index and the parity of its current round.
-struct Ring {
-  int slot;
-  uint32_t phase;
-  __device__ __forceinline__ void next(int n) {
-    if (++slot == n) {
-      slot = 0;
-      phase ^= 1u;
-    }
-  }
-};
-
-// Wait (bounded) for the last copies of a ring of n slots whose cursor is `c` after `g` issued copies (copy g-k
-// went to slot (g-k) mod n, in the cursor's round when that slot is below the cursor, else the round before).
-// Returns immediately for copies already consumed: their slot's barrier is then one phase further.
-__device__ __forceinline__ void drain_ring(uint32_t full, const Ring& c, int g, int n) {
-  const int last = g < n ? g : n;
-  for (int k = 1; k <= last; ++k) {
-    const int s = (c.slot - k + n) % n;
-    wait_bar(full + 8 * s, s < c.slot ? c.phase : c.phase ^ 1u);
-  }
-}
-
 // 8 floats -> 4 packed bf16 hi words and 4 lo words
 __device__ __forceinline__ void split8(const float (&v)[8], uint32_t (&hi)[4], uint32_t (&lo)[4]) {
 #pragma unroll
   for (int e = 0; e < 4; ++e) split2(v[2 * e], v[2 * e + 1], hi[e], lo[e]);
-}
-
-// 2-D tiled bulk-tensor load of the box at element coordinates (x, y) of `map` (no multicast), completing on bar.
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-      "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar)
-      : "memory");
 }
 
 // ------------------------------------------------------------------------------------------ forward
@@ -999,37 +964,6 @@ __global__ void rows_inv_sym_consts_kernel(int nx, int bc, unsigned char* img) {
   unsigned char* o = img + (long long)j * 4 * OPER + 2 * t * OPER + swz(row, q);
   *(uint4*)o = make_uint4(hi[0], hi[1], hi[2], hi[3]);
   *(uint4*)(o + OPER) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-}
-
-typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-// A 2-D tensor map (dim0 contiguous, rows `stride1` bytes apart) with a box0 x box1 box, no swizzle.
-static int encode_2d(CUtensorMap* map, CUtensorMapDataType type, const void* base, unsigned long long dim0,
-                     unsigned long long dim1, unsigned long long stride1, unsigned box0, unsigned box1,
-                     CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE) {
-  static EncodeTiled encode = nullptr;
-  if (!encode) {
-    void* fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
-      return fail(OI_ECUDA, "cuTensorMapEncodeTiled is not available");
-    encode = (EncodeTiled)fn;
-  }
-  const cuuint64_t dims[2] = {dim0, dim1}, strides[1] = {stride1};
-  const cuuint32_t box[2] = {box0, box1}, estr[2] = {1, 1};
-  const CUresult r = encode(map, type, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                            swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return fail(OI_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
-  return OI_OK;
-}
-
-static int sm_count() {
-  int dev = 0, sms = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-    return 0;
-  return sms;
 }
 
 }  // namespace rt

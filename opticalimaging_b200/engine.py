@@ -155,6 +155,18 @@ class Plan:
             setattr(self, attr, c)
         return c
 
+    def synth_consts(self) -> torch.Tensor:
+        """Constant operands of the tensor-core synthesis preparation (oi_synth_tc_constants: the coarse spectrum's
+        column DFT and the row Dirichlet kernels of this grid and band), built once per plan."""
+        c = getattr(self, '_synth_consts', None)
+        if c is None:
+            b = self.band
+            nbytes = (1 + self.ny // 128) * 65536
+            c = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            N.call('oi_synth_tc_constants', self.ny, b.br, b.bc, N.ptr(c), nbytes, N.stream_handle(self.device))
+            self._synth_consts = c
+        return c
+
     def coarse_fft_tables(self):
         """Four-step FFT tables of the coarse grid (for coarse grids of 256..2048 points per axis)."""
         t = getattr(self, '_coarse_fft_tables', None)
@@ -318,10 +330,10 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
         out = torch.empty((batch, nz, plan.ny, plan.nx), dtype=torch.float32, device=dev)
     ihat = torch.empty(batch * nz * (2 * b.br - 1) * b.bc, dtype=torch.complex64, device=dev)
     if form == 'bf16x3' and plan.tc_rows(form):
+        # coarse spectrum and column synthesis as two tensor-core GEMMs straight into the row pass's operand tiles
         tiles = torch.empty(batch * nz * plan.ny * 512, dtype=torch.uint8, device=dev)
-        N.call('oi_coarse_to_image_tc', N.ptr(coarse), nsplit, batch * nz, b.br, b.bc, N.ptr(plan.wm_r),
-               N.ptr(plan.wm_c), N.ptr(plan.wn_y), N.ptr(plan.rows_consts(1)), plan.ny, plan.nx, N.ptr(ihat),
-               None, N.ptr(tiles), N.ptr(out), s)
+        N.call('oi_coarse_to_image_tcs', N.ptr(coarse), nsplit, batch * nz, b.br, b.bc, N.ptr(plan.synth_consts()),
+               N.ptr(plan.rows_consts(1)), plan.ny, plan.nx, N.ptr(tiles), N.ptr(out), s)
     elif plan.big_coarse_fft(form):
         # the coarse intensity's Hermitian half-spectrum by the FFT band pass, then the FFT synthesis
         count, nq = batch * nz, 2 * b.br - 1

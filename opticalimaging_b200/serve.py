@@ -101,12 +101,16 @@ class Server:
     """Continuous-batching scheduler over an executor (see module docstring)."""
 
     def __init__(self, executor, hbm_budget: float = 150e9, max_batch_pixels: int = 64 * 1024 * 1024,
-                 max_batch: int = 256, idle_wait: float = 0.0002):
+                 max_batch: int = 256, idle_wait: float = 0.0002, latency_budget_ms: float | None = None):
         self.ex = executor
         self.budget = float(hbm_budget)
         self.max_batch_pixels = max_batch_pixels
         self.max_batch = max_batch
         self.idle_wait = idle_wait
+        # Latency-aware batching: a request's batch waits behind at most (slots - 1) other batches on the slowest
+        # pipeline stage (for the CUDA executor the device-to-host copy of the images), then takes its own turn;
+        # batches are capped so that slots x batch x (time per image on that stage) stays within the budget.
+        self.latency_budget = None if latency_budget_ms is None else latency_budget_ms / 1e3
         self._inbox = collections.deque()
         self._cv = threading.Condition()
         self._pending: dict = collections.OrderedDict()   # group key -> deque of requests
@@ -179,7 +183,13 @@ class Server:
         return (r.spec.key, r.mask.dtype)
 
     def _max_batch(self, spec: ModelSpec) -> int:
-        return max(1, min(self.max_batch, self.max_batch_pixels // spec.pixels, self.ex.max_batch(spec)))
+        b = max(1, min(self.max_batch, self.max_batch_pixels // spec.pixels, self.ex.max_batch(spec)))
+        if self.latency_budget is not None:
+            per = getattr(self.ex, 'time_per_image', None)
+            t = per(spec) if per is not None else None
+            if t:
+                b = max(1, min(b, int(self.latency_budget / (self.ex.nslots * t))))
+        return b
 
     def batch_limit(self, spec: ModelSpec) -> int:
         """The largest batch this server forms for `spec` (by max_batch and max_batch_pixels)."""
@@ -376,12 +386,24 @@ class CudaExecutor:
         self.buffers: dict = {}       # (key, slot, dtype) -> (d_in, d_out)
         self.graphs: dict = {}        # (key, slot, dtype, bucket) -> (graph, bytes)
         self._bytes: dict = {}        # key -> device bytes attributed to it
+        self._link = None             # measured (h2d, d2h) bytes per second
+        self._device_tpi: dict = {}   # key -> device seconds per image (timed graph replay)
 
     def thread_init(self):
         torch.cuda.set_device(self.device)
 
     def max_batch(self, spec):
         return self._max_batch
+
+    def time_per_image(self, spec) -> float:
+        """Seconds per image on the slowest stage of a batch: the host<->device copies at the link rates measured
+        once (pinned memory; float32 images out, masks in at up to 4 bytes per pixel) or the device time of the
+        image itself when a graph of the spec has been timed (``prepare``)."""
+        if self._link is None:
+            self._link = measure_link(self.device)
+        h2d, d2h = self._link
+        t = max(4.0 * spec.pixels / h2d, 4.0 * spec.planes * spec.pixels / d2h)
+        return max(t, self._device_tpi.get(spec.key, 0.0))
 
     def resident_bytes(self):
         return sum(self._bytes.values())
@@ -442,6 +464,13 @@ class CudaExecutor:
             used = max(0, free0 - torch.cuda.mem_get_info(self.device)[0])
             g = self.graphs[gk] = (graph, used)
             self._bytes[spec.key] = self._bytes.get(spec.key, 0) + used
+            if b >= 8:   # device time per image of this spec, from one replay (the copies are timed apart)
+                a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(s)
+                graph.replay()
+                z.record(s)
+                z.synchronize()
+                self._device_tpi[spec.key] = max(self._device_tpi.get(spec.key, 0.0), a.elapsed_time(z) / 1e3 / b)
         return g[0]
 
     def prepare(self, spec, dtype=torch.uint8, max_batch: int | None = None):
@@ -519,6 +548,28 @@ class CudaExecutor:
     def shutdown(self):
         for s in self.streams:
             s.synchronize()
+
+
+def measure_link(device, nbytes: int = 32 << 20, reps: int = 3):
+    """(host-to-device, device-to-host) bytes per second of pinned copies of `nbytes`, best of `reps`."""
+    dev = torch.device(device)
+    host = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    s = torch.cuda.Stream(dev)
+    rates = []
+    for src, dst in ((host, d), (d, host)):
+        best = None
+        for _ in range(reps):
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(s):
+                a.record(s)
+                dst.copy_(src, non_blocking=True)
+                z.record(s)
+            z.synchronize()
+            t = a.elapsed_time(z) / 1e3
+            best = t if best is None else min(best, t)
+        rates.append(nbytes / best)
+    return rates[0], rates[1]
 
 
 def plain_run(spec_masks, device=None):

@@ -250,3 +250,38 @@ def test_check_device_status_raises_and_clears():
     with pytest.raises(DeviceWaitError, match='device status 3'):
         check_device_status('test', read)
     check_device_status('test', read)             # cleared: no error the second time
+
+
+class TimedExecutor(FakeExecutor):
+    """FakeExecutor that reports a time per image on its slowest stage."""
+
+    def __init__(self, tpi, **kw):
+        super().__init__(**kw)
+        self.tpi = tpi
+
+    def time_per_image(self, spec):
+        return self.tpi
+
+    def max_batch(self, spec):
+        return 64
+
+
+def test_latency_budget_caps_batches():
+    """With a latency budget, batches are capped at budget / (slots x time per image); without one they fill."""
+    a = spec('a')
+    ex = TimedExecutor(tpi=1e-4, nslots=2, delay=0.02)
+    srv = Server(ex, hbm_budget=1e9, max_batch=64, latency_budget_ms=2.0)
+    assert srv.batch_limit(a) == 10                       # 2 ms / (2 slots x 0.1 ms)
+    futs = [srv.submit(a, torch.ones(4, 4)) for _ in range(60)]
+    for f in futs:
+        f.result(timeout=10)
+    srv.close()
+    assert max(n for _, n in ex.launched) <= 10
+    ex2 = TimedExecutor(tpi=1e-4, nslots=2, delay=0.02)
+    srv2 = Server(ex2, hbm_budget=1e9, max_batch=64)
+    assert srv2.batch_limit(a) == 64
+    srv2.close()
+    ex3 = TimedExecutor(tpi=1.0, nslots=2)                 # a budget below one image still admits one
+    srv3 = Server(ex3, hbm_budget=1e9, latency_budget_ms=1.0)
+    assert srv3.batch_limit(a) == 1
+    srv3.close()

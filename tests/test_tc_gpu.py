@@ -322,3 +322,51 @@ def test_band_spectrum_tc_sym_matches_full(oi, batch, n, b):
     assert rel_err(h, want) < 2e-5
     assert rel_err(h, f) < 2e-5
     assert N.device_status() == 0
+
+
+def decode_v_tiles(tiles: np.ndarray, count: int, ny: int) -> np.ndarray:
+    """v [count, 64, ny] complex from V operand tiles ([count*ny/128][hi re | hi im | lo re | lo im][128 y][64 qc] bf16,
+    128-byte swizzled): hi + lo of each part."""
+    t = tiles.reshape(count * ny // 128, 4, 128, 128)                     # bytes: [tile][block][row][128 B]
+    r = np.arange(128)[:, None]
+    k = np.arange(64)[None, :]
+    off = ((k // 8) ^ (r % 8)) * 16 + (k % 8) * 2
+    lo_b = np.take_along_axis(t, np.broadcast_to(off, (t.shape[0], 4, 128, 64)), axis=3).astype(np.uint32)
+    hi_b = np.take_along_axis(t, np.broadcast_to(off + 1, (t.shape[0], 4, 128, 64)), axis=3).astype(np.uint32)
+    f = ((hi_b << 24) | (lo_b << 16)).view(np.float32).astype(np.float64)   # bf16 -> float32 bits
+    re, im = f[:, 0] + f[:, 2], f[:, 1] + f[:, 3]                          # [tile][y][qc]
+    v = (re + 1j * im).reshape(count, ny, 64)
+    return v.transpose(0, 2, 1)
+
+
+@pytest.mark.parametrize('count,nparts,ny,br,bc', [(3, 3, 256, 59, 59), (64, 2, 1024, 59, 59), (5, 1, 512, 30, 17)])
+def test_synth_tiles_tc_direct(oi, count, nparts, ny, br, bc):
+    """The tensor-core synthesis preparation through the C ABI against FP64: the V tiles (hi + lo) of
+    v[qc][y] = sum_|qr|<br Ihat[qr][qc] exp(-2 pi i qr y / ny), Ihat the (qc > 0 doubled) coarse spectrum of the
+    sum of the partial coarse images; zero beyond bc."""
+    from opticalimaging_b200 import _native as N
+    dev = torch.device('cuda')
+    g = np.random.default_rng(count * ny + br)
+    coarse = g.random((nparts, count, 128, 128)).astype(np.float32)
+    c = coarse.astype(np.float64).sum(axis=0)
+    consts = torch.empty((1 + ny // 128) * 65536, dtype=torch.uint8, device=dev)
+    s = N.stream_handle(dev)
+    N.call('oi_synth_tc_constants', ny, br, bc, N.ptr(consts), consts.numel(), s)
+    cd = torch.from_numpy(coarse).to(dev)
+    tiles = torch.zeros(count * ny * 512, dtype=torch.uint8, device=dev)
+    N.call('oi_synth_tiles_tc', N.ptr(cd), nparts, count, br, bc, N.ptr(consts), ny, N.ptr(tiles), s)
+    got = decode_v_tiles(tiles.cpu().numpy(), count, ny)
+    qr = np.arange(-(br - 1), br)
+    qc = np.arange(bc)
+    s128 = np.arange(128)
+    Er = np.exp(2j * np.pi * np.outer(qr, s128) / 128)
+    Ec = np.exp(2j * np.pi * np.outer(s128, qc) / 128)
+    ih = np.einsum('ra,iab,bc->irc', Er, c, Ec) / 128 ** 2
+    ih[:, :, 1:] *= 2
+    Sy = np.exp(-2j * np.pi * np.outer(qr, np.arange(ny)) / ny)            # [nq, ny]
+    want = np.einsum('irc,ry->icy', ih, Sy)
+    err = np.max(np.abs(got[:, :bc] - want)) / np.max(np.abs(want))
+    print(f'synth tiles {count}x{ny} br {br} bc {bc} parts {nparts}: max {err:.2e}')
+    assert err < BF16X3_VS_FP64
+    assert np.all(got[:, bc:] == 0)
+    assert N.device_status() == 0
