@@ -462,7 +462,12 @@ def e2e_dropin(sk_info, masks_np, dev, count=16):
     for sc in scs[1:]:
         img, _ = imaging.CalculateAerialImage_SOCS(sc, kern, sr, po)
     dt = time.perf_counter() - t0
-    return {"images_per_s": count / dt, "h2d_bytes_per_image": N_PIX * N_PIX * 3 * 8,
+    t1 = time.perf_counter()   # the field's copy alone (pageable host memory, as the caller holds it)
+    for sc in scs[1:]:
+        sc.ScatterField.to(dev)
+    torch.cuda.synchronize(dev)
+    h2d = (time.perf_counter() - t1) / count
+    return {"images_per_s": count / dt, "h2d_ms_per_image": 1e3 * h2d, "h2d_bytes_per_image": N_PIX * N_PIX * 3 * 8,
             "d2h_bytes_per_image": N_PIX * N_PIX * 4,
             "call": "CalculateAerialImage_SOCS(scatter, kernels, source, projector) per clip, host complex64 "
                     "[1024, 1024, 3] ScatterField in, host float32 image out"}
@@ -602,7 +607,7 @@ def kernel_rooflines(sk, masks, reps=10):
     s = N.stream_handle(dev)
     t = torch.empty(B * sk.ny * b.bc, dtype=torch.complex64, device=dev)
     band = band_spectrum(masks, N.FIELD_REAL_F32, plan, form='bf16x3')
-    ctas, nparts = N.tc_layout(B, sk.count)
+    ctas, nparts = N.tc_layout(B, sk.count)   # nparts also sizes the synthesis kernel's partial sums
     coarse = torch.empty((nparts, B, 1, 128, 128), device=dev)
     v = torch.zeros(B * b.bc * sk.ny, dtype=torch.complex64, device=dev)
     tiles = torch.empty(B * sk.ny * 512, dtype=torch.uint8, device=dev)
@@ -614,8 +619,12 @@ def kernel_rooflines(sk, masks, reps=10):
     else:
         fwd = lambda: N.call('oi_rows_fwd_tc', N.ptr(masks), N.FIELD_REAL_F32, B, sk.ny, sk.nx, b.m0c,  # noqa: E731
                              b.bc, N.ptr(plan.rows_consts(0)), N.ptr(t), s)
+    scoarse = torch.rand((nparts, B, 128, 128), device=dev)
+    stiles = torch.empty(B * sk.ny * 512, dtype=torch.uint8, device=dev)
     calls = {
         "rows_fwd_tc": fwd,
+        "synth_tc": lambda: N.call('oi_synth_tiles_tc', N.ptr(scoarse), nparts, B, b.br, b.bc,    # noqa: E731
+                                   N.ptr(tplan.synth_consts()), sk.ny, N.ptr(stiles), s),
         "coherent_tc": lambda: N.call('oi_coherent_coarse_tc', N.ptr(band), B, 1, b.m0r, b.br, b.m0c, b.bc,
                                       N.ptr(sk.pupils), 0, N.ptr(sk.weights), 1, sk.count,
                                       N.ptr(tplan.tc_constants()), ctas, nparts, N.ptr(coarse), s),
@@ -641,13 +650,20 @@ def kernel_rooflines(sk, masks, reps=10):
             flops = 8.0 * B * sk.count * (128 * b.br * b.bc + 128 * 128 * b.br)
             ach = flops / sec / 1e12
             res[name] = {"bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16,
-                         "traffic": NCU_TRAFFIC[name], "us": sec * 1e6, "peak_source": src,
+                         "traffic": NCU_TRAFFIC.get(name), "us": sec * 1e6, "peak_source": src,
                          "algorithmic": "8 (M B^2 + M^2 B) flops per field, M = 128, B = 59, 24 fields per image",
                          "executed_tflops": 3 * 8.0 * B * sk.count * (128 * 64 * 64 + 128 * 128 * 64) / sec / 1e12}
+        elif name == "synth_tc":   # two real GEMMs per image: U = c G (128 x 2bc x 128), v = A U (ny x 2bc x 128)
+            flops = 2.0 * B * (128 * 2 * b.bc * 128 + sk.ny * 2 * b.bc * 128)
+            ach = flops / sec / 1e12
+            res[name] = {"bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16,
+                         "traffic": NCU_TRAFFIC.get(name), "us": sec * 1e6, "peak_source": src,
+                         "algorithmic": "2 (M 2bc M + ny 2bc M) flops per image, M = 128, bc = 59",
+                         "executed_tflops": 3 * 2.0 * B * (128 * 128 * 128 + sk.ny * 128 * 128) / sec / 1e12}
         else:
             ach = 4.0 * px / sec / 1e9
             res[name] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                         "traffic": NCU_TRAFFIC[name], "us": sec * 1e6, "peak_source": src,
+                         "traffic": NCU_TRAFFIC.get(name), "us": sec * 1e6, "peak_source": src,
                          "algorithmic": "4 bytes per pixel: the float32 mask read" if name == "rows_fwd_tc"
                          else "4 bytes per pixel: the float32 image written"}
     res["traffic_source"] = NCU_TRAFFIC_SOURCE

@@ -283,6 +283,12 @@ OI_API int oi_coarse_to_image_tcs(const float* coarse, int nparts, int count, in
  * Synchronous (reads device memory). */
 OI_API int oi_device_status(int* status, int reset);
 
+/* The failure path of the tensor-core kernels' bounded waits, on its own (no counterpart in the reference): one
+ * CTA allocates tmem_cols columns of tensor memory (a power of two, 32..512), waits with the kernels' bounded wait
+ * -- limit_ns, at most 100 ms -- on a barrier that nothing completes, sets the device status to 1, releases the
+ * tensor memory and returns.  For tests of the status reporting and of the context staying usable. */
+OI_API int oi_wait_probe(long long limit_ns, int tmem_cols, void* stream);
+
 /* Kernel launches this library has enqueued since it was loaded (launches captured into a CUDA graph are
  * counted once, at capture). */
 OI_API int oi_launch_count(long long* count);

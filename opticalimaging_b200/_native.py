@@ -41,6 +41,7 @@ _SIGS = {
     'oi_tc_constants': [_i, _i, _vp, _vp, _vp, _ll, _vp],
     'oi_device_status': [_vp, _i],
     'oi_launch_count': [_vp],
+    'oi_wait_probe': [_ll, _i, _vp],
     'oi_rows_tc_constants': [_i, _i, _i, _i, _vp, _ll, _vp],
     'oi_rows_fwd_tc': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp],
     'oi_rows_fwd_tc_half': [_vp, _i, _i, _i, _i, _i, _vp, _vp, _vp],

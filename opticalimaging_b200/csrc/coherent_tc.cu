@@ -590,6 +590,50 @@ extern "C" int oi_coherent_coarse_tc(const void* band, int batch, int nch, int m
   return check_launch("oi_coherent_coarse_tc");
 }
 
+namespace oi {
+namespace tc {
+
+// The failure path every tensor-core kernel takes when a wait runs out, on its own: a CTA allocates tensor
+// memory, waits with the bounded wait of the kernels (limit `limit_ns`) on a barrier phase that nothing
+// completes, records the expiry in the device status, releases tensor memory and returns.  Nothing is in
+// flight while it waits.
+__global__ void wait_probe_kernel(unsigned long long limit_ns, unsigned cols) {
+  __shared__ __align__(16) uint64_t bar;
+  __shared__ uint32_t slot;
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) tmem_alloc(smem_u32(&slot), cols);
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&bar), 1);
+    mbar_init_fence();
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = slot;
+  const bool ok = warp_wait_for(smem_u32(&bar), 0, limit_ns);   // no thread arrives: the phase never completes
+  if (!ok && threadIdx.x == 0) atomicExch(&g_device_status, 1);
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after();
+    tmem_dealloc(tmem, cols);
+  }
+}
+
+}  // namespace tc
+}  // namespace oi
+
+extern "C" int oi_wait_probe(long long limit_ns, int tmem_cols, void* stream) {
+  using namespace oi;
+  if (limit_ns <= 0 || limit_ns > 100000000LL)
+    return fail(OI_ERANGE, "oi_wait_probe: limit %lld ns outside (0, 100 ms]", limit_ns);
+  if (tmem_cols < 32 || tmem_cols > 512 || (tmem_cols & (tmem_cols - 1)))
+    return fail(OI_EINVAL, "oi_wait_probe: tensor-memory columns must be a power of two in [32, 512]");
+  tc::wait_probe_kernel<<<1, 64, 0, (cudaStream_t)stream>>>((unsigned long long)limit_ns, (unsigned)tmem_cols);
+  oi::note_launch();
+  return check_launch("oi_wait_probe");
+}
+
 extern "C" int oi_device_status(int* status, int reset) {
   using namespace oi;
   if (!status) return fail(OI_EINVAL, "oi_device_status: null status");

@@ -77,14 +77,16 @@ __device__ __forceinline__ bool try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for the barrier phase of the given parity; false on expiry.
-__device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity) {
+// Bounded wait for the barrier phase of the given parity; false once `limit_ns` has passed without it.
+__device__ __forceinline__ bool wait_bar_for(uint32_t bar, uint32_t parity, unsigned long long limit_ns) {
   if (try_wait(bar, parity)) return true;
   const unsigned long long t0 = globaltimer();
   while (!try_wait(bar, parity))
-    if (globaltimer() - t0 > WAIT_NS) return false;
+    if (globaltimer() - t0 > limit_ns) return false;
   return true;
 }
+// The bound every kernel uses.
+__device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity) { return wait_bar_for(bar, parity, WAIT_NS); }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -193,6 +195,9 @@ __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t
 // Warp-uniform bounded wait: true when every lane saw the phase complete.
 __device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity) {
   return __all_sync(0xffffffffu, wait_bar(bar, parity));
+}
+__device__ __forceinline__ bool warp_wait_for(uint32_t bar, uint32_t parity, unsigned long long limit_ns) {
+  return __all_sync(0xffffffffu, wait_bar_for(bar, parity, limit_ns));
 }
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");

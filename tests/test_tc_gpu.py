@@ -370,3 +370,30 @@ def test_synth_tiles_tc_direct(oi, count, nparts, ny, br, bc):
     assert err < BF16X3_VS_FP64
     assert np.all(got[:, bc:] == 0)
     assert N.device_status() == 0
+
+
+def test_bounded_wait_expiry_reports_and_recovers(oi):
+    """The tensor-core kernels' failure path, made to happen without a fault: a bounded wait (10 ms here) on a
+    barrier that nothing completes sets the device status and releases tensor memory (all 512 columns), the
+    status is read and cleared on the host, and the next calls -- which allocate all 512 columns again -- run
+    normally with bit-identical results."""
+    from opticalimaging_b200 import _native as N, workloads as W
+    sr, po, nm = W.config3_optics(order=8)
+    T, fg = oi.CalculateTCCMatrix(sr, [512.0, 512.0], po, 0.0, nm)
+    sk = oi.socs_kernels_from_tcc(T, fg, [256, 256], nm)
+    g = torch.Generator(device='cuda').manual_seed(3)
+    masks = (torch.rand((4, 256, 256), device='cuda', generator=g) > 0.5).float()
+    before = sk.image(masks, form='bf16x3').clone()
+    N.device_status(reset=True)
+    N.call('oi_wait_probe', 10_000_000, 512, N.stream_handle())
+    torch.cuda.synchronize()
+    assert N.device_status() == 1
+    with pytest.raises(N.DeviceWaitError):
+        N.check_device_status('wait probe')
+    assert N.device_status() == 0
+    after = sk.image(masks, form='bf16x3')
+    torch.cuda.synchronize()
+    assert torch.equal(before, after)
+    assert N.device_status() == 0
+    with pytest.raises(N.NativeError, match='outside'):
+        N.call('oi_wait_probe', 10 ** 9, 512, N.stream_handle())      # limits above 100 ms are refused
