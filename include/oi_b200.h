@@ -16,6 +16,7 @@
  *                         <- the same with a Jones vector per source point: Calc_PolarizationMap's typed maps
  *                            (Source.py:183-221) and the states of a CoherencyMatrix (README.md:45)
  *   oi_tcc_assemble64     <- GetTCCMatrix                                    (CalculateTCCMatrix.py:58-75)
+ *   oi_eig_topk64         <- the SVD and truncation of DecomposeTCC_SOCS     (DecomposeTCC_SOCS.py:7-9)
  *   oi_band_spectrum_fft / oi_coherent_coarse_fft / oi_coarse_to_image_fft
  *                         <- the same three stages in FFT form (power-of-two grids)
  *   oi_spectrum_to_image(_fft) <- the synthesis half of the two above
@@ -32,7 +33,8 @@
  *   - Every function returns 0 on success or a negative OI_E* status; oi_last_error() describes the last
  *     failure on the calling thread.  Nothing aborts the process.
  *   - All pointers are device pointers owned by the caller; nothing here allocates device memory.
- *   - `stream` is a cudaStream_t passed as void*; all work is enqueued on it and nothing synchronises.
+ *   - `stream` is a cudaStream_t passed as void*; all work is enqueued on it and nothing synchronises, except
+ *     where an entry point says so (oi_eig_topk64, oi_device_status).
  *   - float2 / double2 are interleaved (re, im) pairs, the layout of torch complex64 / complex128.
  *   - Frequencies are centred integers: band row i means frequency m0r + i (cycles per period).
  *   - Image convention: out[y][x] = sum_fields w * |sum_m P(m) c(m) exp(-2 pi i (m_r y/Ny + m_c x/Nx))|^2
@@ -339,6 +341,21 @@ OI_API int oi_tcc_pupils64_pol(const float* ff, int lf, const float* gg, int lg,
                                const float* sv, int nsrc, double weight_sum, double focus, const double* zern,
                                int vector, const double* jones_pts, double na, double mag, double index_image,
                                double wavelength, void* h, void* stream);
+
+/*
+ * The k leading eigenpairs of the TCC in FP64 (DecomposeTCC_SOCS.py:7-9, where the reference runs a full
+ * torch.svd of its complex64 TCC): block subspace iteration on p vectors with Cholesky-QR orthonormalisation and
+ * Rayleigh-Ritz every 4 iterations (one-CTA Jacobi on the p x p projection), until the leading k residuals
+ * ||T u - lambda u|| are below tol * lambda_0 or max_iter iterations have run.  The TCC is given densely (tcc:
+ * complex128 [n][n], h NULL) or as its pupil factor (h: complex128 [ne][n][s] with TCC = sum_e h_e h_e^H,
+ * tcc NULL; the TCC is not formed).  k <= p <= min(n, 64), p even.  Output: vecs complex128 [n][k] (row-major,
+ * column i the eigenvector of vals[i]), vals double [k] descending, clamped at zero (device pointers); *iters
+ * (host) the iterations run, negative when tol was not reached.  work: oi_eig_topk64_workspace bytes.  Unlike
+ * the imaging entry points this one synchronises its stream (it reads the residuals to decide when to stop).
+ */
+OI_API int oi_eig_topk64_workspace(int n, int p, int ne, int s, long long* bytes);
+OI_API int oi_eig_topk64(const void* tcc, const void* h, int ne, int n, int s, int k, int p, int max_iter, double tol,
+                         void* vecs, double* vals, void* work, long long work_bytes, int* iters, void* stream);
 
 /*
  * TCC = sum_e h_e h_e^H (GetTCCMatrix, CalculateTCCMatrix.py:58-75), complex128 [fg][fg], full Hermitian.

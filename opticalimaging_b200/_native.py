@@ -42,6 +42,8 @@ _SIGS = {
     'oi_device_status': [_vp, _i],
     'oi_launch_count': [_vp],
     'oi_wait_probe': [_ll, _i, _vp],
+    'oi_eig_topk64_workspace': [_i, _i, _i, _i, _vp],
+    'oi_eig_topk64': [_vp, _vp, _i, _i, _i, _i, _i, _i, _d, _vp, _vp, _vp, _ll, _vp, _vp],
     'oi_rows_tc_constants': [_i, _i, _i, _i, _vp, _ll, _vp],
     'oi_rows_fwd_tc': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp],
     'oi_rows_fwd_tc_half': [_vp, _i, _i, _i, _i, _i, _vp, _vp, _vp],

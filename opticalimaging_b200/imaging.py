@@ -21,6 +21,7 @@ Divergences from the reference, all deliberate and documented:
 """
 from __future__ import annotations
 
+import ctypes
 import warnings
 
 import torch
@@ -349,9 +350,44 @@ def _socs_count(numerics, evals, size):
 
 
 def _eig_desc(tcc):
-    """Eigenpairs of the Hermitian TCC, eigenvalues descending and clamped at zero (FP64, on the device)."""
+    """Every eigenpair of the Hermitian TCC, eigenvalues descending and clamped at zero (FP64, on the device;
+    the library's dense solver, for decompositions that keep more kernels than eig_topk covers)."""
     lam, U = torch.linalg.eigh(tcc)
     return torch.clamp(lam.flip(0), min=0), U.flip(1)
+
+
+TOPK_MAX = 48          # kernels the hand-written solver keeps (its block holds 64 vectors)
+
+
+def eig_topk(k: int, tcc: torch.Tensor | None = None, h: torch.Tensor | None = None, tol: float = 1e-13,
+             max_iter: int = 300):
+    """The k leading eigenpairs (eigenvalues descending, clamped at zero; eigenvectors [n, k]) of the Hermitian
+    TCC, given densely (`tcc` [n, n] complex128) or as its pupil factor (`h` [ne, n, s] complex128 with
+    TCC = sum_e h_e h_e^H, never formed), by the library's FP64 block subspace iteration (oi_eig_topk64):
+    Rayleigh-Ritz residuals below tol x the largest eigenvalue.  Returns None when k is out of its range
+    (k > TOPK_MAX or a TCC of fewer than 64 rows)."""
+    A = tcc if tcc is not None else h
+    n = A.shape[0] if tcc is not None else A.shape[1]
+    p = 64
+    if k > TOPK_MAX or k <= 0 or n < p:
+        return None
+    dev = A.device
+    ne, s_ = (0, 0) if tcc is not None else (A.shape[0], A.shape[2])
+    nbytes = ctypes.c_longlong(0)
+    N.call('oi_eig_topk64_workspace', n, p, ne, s_, ctypes.byref(nbytes))
+    work = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
+    vecs = torch.empty((n, k), dtype=torch.complex128, device=dev)
+    vals = torch.empty(k, dtype=torch.float64, device=dev)
+    iters = ctypes.c_int(0)
+    A = A.to(torch.complex128).contiguous()
+    N.call('oi_eig_topk64', N.ptr(A) if tcc is not None else None, N.ptr(A) if tcc is None else None, ne, n, s_,
+           k, p, max_iter, float(tol), N.ptr(vecs), N.ptr(vals), N.ptr(work), nbytes.value, ctypes.byref(iters),
+           N.stream_handle(dev))
+    if iters.value < 0:
+        warnings.warn(f'oi_eig_topk64 did not reach tol={tol} in {max_iter} iterations; using the dense solver',
+                      RuntimeWarning, stacklevel=2)
+        return None
+    return vals, vecs
 
 
 def _placement(n, length):
@@ -367,8 +403,15 @@ def socs_kernels_from_tcc(tcc, FG_ValidSize, Nfg, numerics) -> SocsKernels:
     lg, lf = FG_ValidSize
     if lf > ng or lg > nf:
         raise ValueError(f'TCC grid {lf}x{lg} does not fit the {ng}x{nf} image grid')
-    lam, U = _eig_desc(tcc)
-    k = _socs_count(numerics, lam, U.shape[1])
+    top = None
+    if numerics.Hopkins_SettingType.lower() == 'order':
+        top = eig_topk(min(numerics.Hopkins_Order, tcc.shape[0] - 1), tcc=tcc)
+    if top is not None:
+        lam, U = top
+        k = lam.numel()
+    else:
+        lam, U = _eig_desc(tcc)
+        k = _socs_count(numerics, lam, U.shape[1])
     kb = (U[:, :k] * torch.sqrt(lam[:k])).T.reshape(k, lf, lg)
     band = Band(_placement(ng, lf), lf, _placement(nf, lg), lg)
     return SocsKernels(kb.to(torch.complex64), band, ng, nf)
@@ -388,6 +431,15 @@ def socs_kernels_from_pupils(h, FG_ValidSize, Nfg, numerics) -> SocsKernels:
     lg, lf = FG_ValidSize
     if lf > ng or lg > nf:
         raise ValueError(f'TCC grid {lf}x{lg} does not fit the {ng}x{nf} image grid')
+    top = None
+    if numerics.Hopkins_SettingType.lower() == 'order':   # leading kernels of h h^H, the TCC never formed
+        top = eig_topk(min(numerics.Hopkins_Order, fg - 1, ne * s), h=h)
+    if top is not None:
+        lam, U = top
+        k = lam.numel()
+        kb = (U * torch.sqrt(lam)).T.reshape(k, lf, lg)
+        band = Band(_placement(ng, lf), lf, _placement(nf, lg), lg)
+        return SocsKernels(kb.to(torch.complex64).contiguous(), band, ng, nf)
     H = h.permute(1, 0, 2).reshape(fg, ne * s)
     lam, V = torch.linalg.eigh(H.conj().T @ H)
     lam, V = torch.clamp(lam.flip(0), min=0), V.flip(1)

@@ -275,3 +275,41 @@ def test_dropin_socs_reuses_band_form_of_reference_layout_kernels(oi):
     host = K.cpu()                                # a host copy: its own entry, scanned once
     img4, _ = oi.CalculateAerialImage_SOCS(sc, host, sr, po)
     assert host in oi._SOCS_CACHE and rel_err(img4.numpy(), img3.numpy()) < 1e-6
+
+
+@pytest.mark.parametrize('form', ['dense', 'factored'])
+def test_eig_topk_matches_dense_eigh(oi, form, report):
+    """The library's FP64 top-K solver (oi_eig_topk64) on the configuration-3 TCC (3481 x 3481, K = 24): the
+    rank-24 projector and eigenvalues against torch.linalg.eigh of the same FP64 matrix -- from the dense TCC
+    and from its pupil factor h (the TCC never formed)."""
+    from opticalimaging_b200 import workloads as W
+    sr, po, nm = W.config3_optics(order=24)
+    h, fg = oi.tcc_pupil_matrix(sr, [2048.0, 2048.0], po, 0.0, nm)
+    T = torch.einsum('eps,eqs->pq', h, h.conj())
+    lam, U = torch.linalg.eigh(T)
+    lam, U = lam.flip(0)[:24], U.flip(1)[:, :24]
+    got = oi.eig_topk(24, tcc=T) if form == 'dense' else oi.eig_topk(24, h=h)
+    assert got is not None
+    gl, gU = got
+    P = (U @ U.conj().T).cpu().numpy()
+    Pg = (gU @ gU.conj().T).cpu().numpy()
+    perr = float(np.max(np.abs(Pg - P)) / np.max(np.abs(P)))
+    lerr = float(torch.max(torch.abs(gl - lam)) / lam[0])
+    orth = float(torch.max(torch.abs(gU.conj().T @ gU - torch.eye(24, dtype=gU.dtype, device=gU.device))))
+    report(f'eig_topk_{form}', projector=perr, eigenvalues=lerr, orthonormality=orth)
+    assert perr < 1e-10 and lerr < 1e-12 and orth < 1e-12
+
+
+def test_eig_topk_small_and_edge_cases(oi):
+    """A small TCC (vec_small, three live channels' optics), K = 12: kernels from the solver give the reference's
+    SOCS image; k above the solver's range returns None (the caller takes the dense solver)."""
+    meta, a = load('vec_small')
+    sr, sc, po, nm = build(meta, a)
+    T, fg = oi.CalculateTCCMatrix(sr, [meta['Period_Y'], meta['Period_X']], po, meta['focus'][0], nm)
+    if T.shape[0] >= 64:
+        vals, vecs = oi.eig_topk(12, tcc=T)
+        lam = torch.linalg.eigvalsh(T).flip(0)[:12]
+        assert float(torch.max(torch.abs(vals - lam)) / lam[0]) < 1e-12
+    assert oi.eig_topk(oi.TOPK_MAX + 1, tcc=T) is None
+    img, _ = oi.CalculateHopkinsImage(sr, sc, po, nm)
+    assert rel_err(img.Intensity.numpy(), a['hopkins']) < FP32_VS_REF
