@@ -115,6 +115,7 @@ class Server:
         self._cv = threading.Condition()
         self._pending: dict = collections.OrderedDict()   # group key -> deque of requests
         self._slots = [None] * executor.nslots            # slot -> (spec, [requests])
+        self._delivered = [0] * executor.nslots           # slot -> requests of its batch already completed
         self._last_used: dict = {}
         self._closed = False
         self.error = None            # the exception that ended the scheduler thread, if one did
@@ -244,7 +245,21 @@ class Server:
                 if not progressed and not self._inbox:
                     self._cv.wait(self.idle_wait)
 
+    def _deliver(self, reqs, results, err, now):
+        for j, r in enumerate(reqs):
+            r.t_done = now
+            if err is not None:
+                r.future.set_exception(err)
+            else:
+                r.future.set_result(results[j])
+                self.completed.append((r.t_submit, now))   # not the request: it holds the result
+
     def _complete(self) -> bool:
+        """Hand finished results to their futures.  An executor with ``ready`` / ``collect_range`` / ``release``
+        reports results in order as their copies land (requests of a batch complete progressively); the slot is
+        freed once the whole batch has finished.  Otherwise a batch completes as one (``poll`` / ``collect``)."""
+        if getattr(self.ex, 'ready', None) is not None:
+            return self._complete_progressive()
         done = False
         for i, s in enumerate(self._slots):
             if s is None or not self.ex.poll(i):
@@ -255,16 +270,38 @@ class Server:
                 err = None
             except Exception as e:  # noqa: BLE001 -- an executor failure fails this batch only
                 results, err = None, e
-            now = time.perf_counter()
-            for j, r in enumerate(reqs):
-                r.t_done = now
-                if err is not None:
-                    r.future.set_exception(err)
-                else:
-                    r.future.set_result(results[j])
-                    self.completed.append((r.t_submit, now))   # not the request: it holds the result
+            self._deliver(reqs, results, err, time.perf_counter())
             self._slots[i] = None
             done = True
+        return done
+
+    def _complete_progressive(self) -> bool:
+        done = False
+        for i, s in enumerate(self._slots):
+            if s is None:
+                continue
+            spec, reqs = s
+            d = self._delivered[i]
+            if d < len(reqs):
+                k = self.ex.ready(i)
+                if k > d:
+                    try:
+                        results = self.ex.collect_range(i, d, k)
+                        err = None
+                    except Exception as e:  # noqa: BLE001 -- an executor failure fails this batch only
+                        results, err = None, e
+                    if err is not None:   # the rest of the batch cannot be trusted either
+                        self._deliver(reqs[d:], None, err, time.perf_counter())
+                        self._delivered[i] = len(reqs)
+                    else:
+                        self._deliver(reqs[d:k], results, None, time.perf_counter())
+                        self._delivered[i] = k
+                    done = True
+            if self._delivered[i] == len(reqs) and self.ex.poll(i):   # every copy of the batch is done
+                self.ex.release(i)
+                self._slots[i] = None
+                self._delivered[i] = 0
+                done = True
         return done
 
     def _take(self, key, spec):
@@ -370,7 +407,7 @@ class CudaExecutor:
     """
 
     def __init__(self, device=None, nslots: int = 3, use_graphs: bool = True, result_device: str = 'cpu',
-                 max_batch: int = 256, status_reader=None):
+                 max_batch: int = 256, status_reader=None, result_chunk: int = 8):
         from .engine import require_cuda
         self.device = require_cuda(device)
         self.guard = StatusGuard(status_reader)   # every collected batch is checked against expired kernel waits
@@ -379,6 +416,8 @@ class CudaExecutor:
         self.result_device = result_device
         self._max_batch = max_batch
         self.streams = [torch.cuda.Stream(self.device) for _ in range(nslots)]
+        self.result_chunk = max(1, int(result_chunk))     # requests per device-to-host copy (and completion mark)
+        self.marks = [[] for _ in range(nslots)]          # slot -> [(requests complete, event)], in order
         self.events = [None] * nslots
         self.pending = [None] * nslots
         self.batch = [None] * nslots
@@ -502,23 +541,39 @@ class CudaExecutor:
                 graph.replay()
             else:
                 model.image(d_in[:n], out=d_out[:n])
+            marks, c = [], self.result_chunk
+
+            def mark(end):   # requests [0, end) have their images where they are going once this event completes
+                ev = torch.cuda.Event()
+                ev.record(s)
+                marks.append((end, ev))
             if all(r.out is not None for r in reqs):      # caller-provided storage: copy each image there
                 outs = [r.out for r in reqs]
-                for i, j in adjacent_runs(outs):
-                    run_view(outs, i, j).copy_(d_out[i:j], non_blocking=True)
+                for i, j in adjacent_runs(outs):          # runs of adjacent views, cut into chunks of c requests
+                    for a in range(i, j, c):
+                        e = min(j, a + c)
+                        run_view(outs, a, e).copy_(d_out[a:e], non_blocking=True)
+                        mark(e)
                 out = outs
             elif self.result_device == 'cpu':
                 # bucket-sized pinned buffer: sizes repeat, so the host caching allocator recycles them
                 host = torch.empty((b, spec.planes, spec.ny, spec.nx), dtype=torch.float32, pin_memory=True)
-                host[:n].copy_(d_out[:n], non_blocking=True)
+                mixed = any(r.out is not None for r in reqs)
+                for a in range(0, n, c):
+                    e = min(n, a + c)
+                    host[a:e].copy_(d_out[a:e], non_blocking=True)
+                    if not mixed:
+                        mark(e)
                 out = host
             else:
                 out = d_out[:n].clone()
             for i, r in enumerate(reqs):
                 if r.out is not None and not isinstance(out, list):
                     r.out.copy_(d_out[i], non_blocking=True)
-            ev = torch.cuda.Event()
-            ev.record(s)
+            if not marks or marks[-1][0] != n:
+                mark(n)
+            ev = marks[-1][1]
+        self.marks[slot] = marks
         self.events[slot] = ev
         self.pending[slot] = out
         self.batch[slot] = reqs
@@ -526,6 +581,34 @@ class CudaExecutor:
     def poll(self, slot):
         ev = self.events[slot]
         return ev is not None and ev.query()
+
+    def ready(self, slot) -> int:
+        """How many leading requests of the slot's batch have their images in place (their copy has finished)."""
+        n = 0
+        for end, ev in self.marks[slot]:
+            if not ev.query():
+                break
+            n = end
+        return n
+
+    def collect_range(self, slot, a: int, b: int):
+        """Results of requests [a, b) of the slot's batch (b <= ready(slot)).  The first call of a batch checks the
+        device status: its kernels have all finished once its first copy has."""
+        out, reqs = self.pending[slot], self.batch[slot]
+        if a == 0:
+            self.guard.check(slot, [i for i, e in enumerate(self.events) if e is not None and i != slot])
+        if isinstance(out, list):
+            return out[a:b]
+        return [r.out if r.out is not None else out[i] for i, r in enumerate(reqs) if a <= i < b]
+
+    def release(self, slot):
+        """The slot's batch has finished (poll): its buffers may take the next batch.  A suspicion the status
+        guard attached to the slot belonged to this batch (it was checked, or found clean before)."""
+        self.guard.suspect.discard(slot)
+        self.events[slot] = None
+        self.pending[slot] = None
+        self.batch[slot] = None
+        self.marks[slot] = []
 
     def collect(self, slot):
         out, reqs = self.pending[slot], self.batch[slot]

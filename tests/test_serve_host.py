@@ -285,3 +285,63 @@ def test_latency_budget_caps_batches():
     srv3 = Server(ex3, hbm_budget=1e9, latency_budget_ms=1.0)
     assert srv3.batch_limit(a) == 1
     srv3.close()
+
+
+class ProgressiveExecutor(FakeExecutor):
+    """FakeExecutor whose batch results land one request every `step` seconds after `delay` (as chunked
+    device-to-host copies do), reported through ready / collect_range / release."""
+
+    def __init__(self, step=0.004, fail_at=None, **kw):
+        super().__init__(**kw)
+        self.step, self.fail_at, self.released = step, fail_at, 0
+
+    def ready(self, slot):
+        t0, out = self.slot[slot]
+        return max(0, min(len(out), int((time.perf_counter() - t0) / self.step) + 1))
+
+    def poll(self, slot):
+        t0, out = self.slot[slot]
+        return time.perf_counter() >= t0 + self.step * len(out)
+
+    def collect_range(self, slot, a, b):
+        if self.fail_at is not None and a <= self.fail_at < b:
+            raise RuntimeError('copy failure injected on the host')
+        return self.slot[slot][1][a:b]
+
+    def release(self, slot):
+        self.released += 1
+        self.slot[slot] = None
+
+
+def test_results_of_a_batch_complete_progressively():
+    ex = ProgressiveExecutor(nslots=1, delay=0.0, step=0.01)
+    srv = Server(ex, hbm_budget=1e9)
+    a = spec('a')
+    futs = [srv.submit(a, torch.full((4, 4), float(i))) for i in range(6)]
+    for i, f in enumerate(futs):
+        torch.testing.assert_close(f.result(timeout=10), torch.full((1, 4, 4), 2.0 * i))
+    srv.drain()
+    done = sorted(t for _, t in srv.completed)
+    assert done[-1] - done[0] > 0.02                  # the batch's requests did not all complete at once
+    assert ex.released == srv.batches
+    srv.close()
+
+
+def test_progressive_failure_fails_the_rest_and_frees_the_slot():
+    ex = ProgressiveExecutor(nslots=1, delay=0.0, step=0.005, fail_at=3)
+    srv = Server(ex, hbm_budget=1e9)
+    a = spec('a')
+    futs = [srv.submit(a, torch.ones(4, 4)) for _ in range(6)]
+    outcomes = []
+    for f in futs:
+        try:
+            f.result(timeout=10)
+            outcomes.append('ok')
+        except RuntimeError:
+            outcomes.append('failed')
+    assert 'failed' in outcomes and outcomes[0] == 'ok'
+    assert outcomes[outcomes.index('failed'):] == ['failed'] * (6 - outcomes.index('failed'))
+    ex.fail_at = None
+    later = srv.submit(a, torch.ones(4, 4))           # the slot came free: later batches are served
+    torch.testing.assert_close(later.result(timeout=10), 2 * torch.ones(1, 4, 4))
+    srv.close()
