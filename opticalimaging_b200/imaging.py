@@ -22,6 +22,7 @@ Divergences from the reference, all deliberate and documented:
 from __future__ import annotations
 
 import ctypes
+import threading
 import warnings
 
 import torch
@@ -79,9 +80,56 @@ def _axes(scatter, projector, source):
     return f, g, npx, npy
 
 
+class _HostStage:
+    """Pinned staging for host-to-device copies of pageable host tensors (what a reference caller passes): the
+    tensor moves in chunks through two pinned buffers, the host-side copy of one chunk (torch's threaded memcpy)
+    overlapping the DMA of the previous one; pageable copies go through the driver's own bounce buffer at a
+    fraction of the link rate."""
+    CHUNK = 8 << 20
+
+    def __init__(self):
+        self.bufs, self.events, self.lock = None, None, threading.Lock()
+
+    def to_device(self, host: torch.Tensor, dev) -> torch.Tensor:
+        flat = host.contiguous().view(torch.uint8).reshape(-1)
+        out = torch.empty(flat.numel(), dtype=torch.uint8, device=dev)
+        with self.lock:
+            if self.bufs is None:
+                self.bufs = [torch.empty(self.CHUNK, dtype=torch.uint8).pin_memory() for _ in range(2)]
+                self.events = [None, None]
+            stream = torch.cuda.current_stream(dev)
+            for k, a in enumerate(range(0, flat.numel(), self.CHUNK)):
+                b = min(flat.numel(), a + self.CHUNK)
+                i = k & 1
+                if self.events[i] is not None:
+                    self.events[i].synchronize()          # the buffer's previous chunk has left for the device
+                self.bufs[i][:b - a].copy_(flat[a:b])
+                out[a:b].copy_(self.bufs[i][:b - a], non_blocking=True)
+                self.events[i] = torch.cuda.Event()
+                self.events[i].record(stream)
+        return out.view(host.dtype).reshape(host.shape)
+
+
+_STAGE = _HostStage()
+
+
 def _device_field(scatter, dev):
-    """ScatterField [Ny, Nx, C] as a contiguous complex64 device tensor (one host-to-device copy)."""
-    return torch.as_tensor(scatter.ScatterField).to(dev).to(torch.complex64).contiguous()
+    """ScatterField [Ny, Nx, C] as a contiguous complex64 device tensor (one host-to-device copy; large pageable
+    host fields go through the pinned staging)."""
+    h = torch.as_tensor(scatter.ScatterField)
+    if h.device.type == 'cpu' and not h.is_pinned() and h.numel() * h.element_size() >= (4 << 20):
+        h = _STAGE.to_device(h.contiguous(), dev)
+    return h.to(dev).to(torch.complex64).contiguous()
+
+
+def _to_host(t: torch.Tensor, rd) -> torch.Tensor:
+    """`t` on the result device `rd`; a host result is copied asynchronously into pinned memory (the caller's
+    synchronisation, _check, completes it)."""
+    if rd.type != 'cpu':
+        return t.to(rd)
+    out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    out.copy_(t, non_blocking=True)
+    return out
 
 
 def _live_channels(hfull):
@@ -271,8 +319,9 @@ def CalculateAbbeImage(source, scatter, projector, numerics):
     inten = abbe_intensity(source, scatter, projector, numerics, h=_live_channels(hfull))
     pim = _pupil_image(scatter, projector, source, hfull, dev)
     rd = _result_device(scatter)
+    inten, pim = _to_host(inten, rd), _to_host(pim, rd)
     _check('CalculateAbbeImage')
-    return _image_data(inten.to(rd), scatter, projector), pim.to(rd)
+    return _image_data(inten, scatter, projector), pim
 
 
 # ------------------------------------------------------------------------------------------------ TCC
@@ -472,8 +521,9 @@ def CalculateAerialImage_SOCS(scatter, TCCMatrix_SOCS, source, projector):
     img = sk.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
     pim = _pupil_image(scatter, projector, source, hfull, dev)
     rd = _result_device(scatter)
+    img, pim = _to_host(img, rd), _to_host(pim, rd)
     _check('CalculateAerialImage_SOCS')
-    return img.to(rd), pim.to(rd)
+    return img, pim
 
 
 def socs_model(source, projector, numerics, period_y, period_x, ny, nx, focus=None) -> CoherentModel:
@@ -510,8 +560,9 @@ def CalculateHopkinsImage(source, scatter, projector, numerics):
     inten = hopkins_intensity(source, scatter, projector, numerics, h=_live_channels(hfull))
     pim = _pupil_image(scatter, projector, source, hfull, dev)
     rd = _result_device(scatter)
+    inten, pim = _to_host(inten, rd), _to_host(pim, rd)
     _check('CalculateHopkinsImage')
-    return _image_data(inten.to(rd), scatter, projector), pim.to(rd)
+    return _image_data(inten, scatter, projector), pim
 
 
 # ------------------------------------------------------------------------------ Floquet-mode ("optimized")

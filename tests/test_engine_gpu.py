@@ -313,3 +313,23 @@ def test_eig_topk_small_and_edge_cases(oi):
     assert oi.eig_topk(oi.TOPK_MAX + 1, tcc=T) is None
     img, _ = oi.CalculateHopkinsImage(sr, sc, po, nm)
     assert rel_err(img.Intensity.numpy(), a['hopkins']) < FP32_VS_REF
+
+
+def test_dropin_large_host_field_through_pinned_staging(oi):
+    """A 1024 x 1024 x 3 complex64 host ScatterField (24 MiB, pageable) takes the pinned staging to the device;
+    the drop-in image equals the resident kernels' image of the same mask, and comes back as a host tensor."""
+    from opticalimaging_b200 import workloads as W
+    from opticalimaging_b200.params import Scatter
+    sr, po, nm = W.config3_optics(order=8)
+    T, fg = oi.CalculateTCCMatrix(sr, [2048.0, 2048.0], po, 0.0, nm)
+    K = oi.DecomposeTCC_SOCS(T, fg, [1024, 1024], nm)
+    mask = W.config3_masks(count=1, n=1024, seed=77)[0]
+    sc = Scatter()
+    sc.Period_X = sc.Period_Y = 2048.0
+    sc.ScatterField = W.thin_field(mask)
+    assert not sc.ScatterField.is_pinned() and sc.ScatterField.numel() * 8 >= (4 << 20)
+    img, pim = oi.CalculateAerialImage_SOCS(sc, K, sr, po)
+    assert img.device.type == 'cpu' and img.shape == (1024, 1024)
+    sk = oi._SOCS_CACHE[K][1]
+    want = sk.image(torch.from_numpy(mask).cuda()[None])[0].cpu().numpy()
+    assert rel_err(img.numpy(), want) < 2e-6

@@ -328,10 +328,15 @@ def test_results_of_a_batch_complete_progressively():
 
 
 def test_progressive_failure_fails_the_rest_and_frees_the_slot():
-    ex = ProgressiveExecutor(nslots=1, delay=0.0, step=0.005, fail_at=3)
+    """A batch whose fourth result fails to arrive: its first three requests complete, the rest fail with the
+    error, and the slot comes free for later batches."""
+    ex = ProgressiveExecutor(nslots=1, delay=0.05, step=0.005, fail_at=3)
     srv = Server(ex, hbm_budget=1e9)
     a = spec('a')
+    first = srv.submit(a, torch.ones(4, 4))          # occupies the only slot while the six below queue up
+    time.sleep(0.01)
     futs = [srv.submit(a, torch.ones(4, 4)) for _ in range(6)]
+    first.result(timeout=10)
     outcomes = []
     for f in futs:
         try:
@@ -339,8 +344,7 @@ def test_progressive_failure_fails_the_rest_and_frees_the_slot():
             outcomes.append('ok')
         except RuntimeError:
             outcomes.append('failed')
-    assert 'failed' in outcomes and outcomes[0] == 'ok'
-    assert outcomes[outcomes.index('failed'):] == ['failed'] * (6 - outcomes.index('failed'))
+    assert outcomes == ['ok'] * 3 + ['failed'] * 3
     ex.fail_at = None
     later = srv.submit(a, torch.ones(4, 4))           # the slot came free: later batches are served
     torch.testing.assert_close(later.result(timeout=10), 2 * torch.ones(1, 4, 4))
