@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
   fence_after();
   const uint32_t tmem = *tmem_slot;
   pdl_trigger();
-  if (warp != 8) pdl_wait();   // warp 8 loads only the constant image; the rest read the coarse sums or write tiles
+  pdl_wait();   // the coarse sums come from the coherent sum (and the constant image may be fresh on the stream)
 
   if (warp == 8) {
     // ---- constant pieces: per item G (4 pieces), then the A tile of each y tile (4 pieces each)
