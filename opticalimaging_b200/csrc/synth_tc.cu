@@ -164,14 +164,15 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
       bool ok = true;
       for (long long it = i0; it < i1 && ok; ++it) {
         const int grp = (int)(it % H), t0 = grp * a.tp, t1 = min(TY, t0 + a.tp);
-        for (int t = t0 - 1; t < t1 && ok; ++t) {   // t = t0 - 1 stands for G
+        for (int t = t0 - 1; t < t1 && ok; ++t) {   // t = t0 - 1 stands for G (blocks 0-3), then A_t (4 + 4t ..)
           for (int p = 0; p < 4; ++p, ++g) {
             if (g >= NR && !wait_bar(rfree + 8 * rs.slot, rs.phase ^ 1u)) {
               ok = false;
               break;
             }
+            const int blk = t < t0 ? p : 4 * (1 + t) + p;
             expect_tx(rfull + 8 * rs.slot, OPER);
-            tma_load_2d(base + R_OFF + rs.slot * OPER, &k_map, 0, ((t + 1) * 4 + p) * 128, rfull + 8 * rs.slot);
+            tma_load_2d(base + R_OFF + rs.slot * OPER, &k_map, 0, blk * 128, rfull + 8 * rs.slot);
             rs.next(NR);
           }
         }
@@ -186,14 +187,14 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
       Ring rs{0, 0}, ab{0, 0};
       bool ok = true, issued = false;
       int m = 0;   // v tiles issued
-      // wait for the next ring piece; returns its shared address (0 on expiry)
-      auto piece = [&](int& slot) -> uint32_t {
-        if (!wait_bar(rfull + 8 * rs.slot, rs.phase)) return 0u;
+      // wait for the next ring piece: false on expiry, else its shared address in `addr`
+      auto piece = [&](int& slot, uint32_t& addr) -> bool {
+        if (!wait_bar(rfull + 8 * rs.slot, rs.phase)) return false;
         fence_after();
         slot = rs.slot;
-        const uint32_t addr = base + R_OFF + rs.slot * OPER;
+        addr = base + R_OFF + rs.slot * OPER;
         rs.next(NR);
-        return addr;
+        return true;
       };
       for (int n = 0; n < NI && ok; ++n) {
         const long long it = i0 + n;
@@ -204,8 +205,8 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
         // stage 1: D1 = c G^T; pieces G hi k0, G hi k1, G lo k0, G lo k1
         int sl[4];
         for (int p = 0; p < 4 && ok; ++p) {
-          const uint32_t gp = piece(sl[p]);
-          if (!gp) {
+          uint32_t gp = 0;
+          if (!piece(sl[p], gp)) {
             ok = false;
             break;
           }
@@ -236,8 +237,8 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
           }
           const uint32_t d2 = tmem + 128 * (1 + ab.slot);
           for (int p = 0; p < 4 && ok; ++p) {
-            const uint32_t ap = piece(sl[p]);
-            if (!ap) {
+            uint32_t ap = 0;
+            if (!piece(sl[p], ap)) {
               ok = false;
               break;
             }
