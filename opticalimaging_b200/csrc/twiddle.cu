@@ -30,9 +30,14 @@ int ensure_smem(const void* kern, size_t bytes, const char* what) {
   int optin = 0;
   e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return fail(OI_ECUDA, "%s: shared memory limit: %s", what, cudaGetErrorString(e));
-  if (bytes > (size_t)optin)
-    return fail(OI_ERANGE, "%s: needs %zu bytes of shared memory, the device allows %d", what, bytes, optin);
-  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  cudaFuncAttributes fa;   // the kernel's static shared memory counts against the same per-block limit
+  e = cudaFuncGetAttributes(&fa, kern);
+  if (e != cudaSuccess) return fail(OI_ECUDA, "%s: kernel attributes: %s", what, cudaGetErrorString(e));
+  const int room = optin - (int)fa.sharedSizeBytes;
+  if (bytes > (size_t)room)
+    return fail(OI_ERANGE, "%s: needs %zu + %zu bytes of shared memory, the device allows %d", what, bytes,
+                fa.sharedSizeBytes, optin);
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, room);
   if (e != cudaSuccess) return fail(OI_ECUDA, "%s: smem attribute: %s", what, cudaGetErrorString(e));
   done.insert({kern, dev});
   return OI_OK;
