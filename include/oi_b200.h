@@ -316,6 +316,15 @@ OI_API int oi_spectrum_to_image(const void* ihat, int count, int br, int bc, con
                                 int nx, float* out, void* stream);
 OI_API int oi_spectrum_to_image_fft(const void* ihat, int count, int br, int bc, const void* wn_y, const void* wn_x,
                                     int ny, int nx, void* scratch_v, float* out, void* stream);
+/*
+ * The input of oi_spectrum_to_image_fft from a coarse intensity held as nparts partial sums ([nparts][count][mr][mc]
+ * float32, oi_coherent_coarse_fft's output on a 256 x 256 or larger power-of-two coarse grid):
+ * ihat[i][qr+br-1][qc] = w(qc) / (mr mc) sum_{y,x} (sum_p coarse[p][i][y][x]) exp(+2 pi i (qr y/mr + qc x/mc)),
+ * |qr| < br, 0 <= qc < bc, w(0) = 1, w(qc > 0) = 2.  wn_c / wn_r: the FFT tables of mc and mr (as wn_x / wn_y of
+ * oi_band_spectrum_fft); scratch: count * mr * bc complex.  The parts are summed as the row pass loads them.
+ */
+OI_API int oi_coarse_half_spectrum_fft(const float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
+                                       const void* wn_c, const void* wn_r, void* scratch, void* ihat, void* stream);
 
 /*
  * Adjoint of the coherent sum (inverse lithography; no counterpart in the reference, whose gradients come from

@@ -51,6 +51,7 @@ _SIGS = {
     'oi_rows_inv_tc': [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp],
     'oi_rows_inv_tc_tiles': [_vp, _i, _i, _i, _vp, _vp, _vp],
     'oi_band_spectrum_tc': [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],
+    'oi_coarse_half_spectrum_fft': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp],
     'oi_band_spectrum_tc_sym': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],
     'oi_coarse_to_image_tc': [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp],
     'oi_synth_tc_constants': [_i, _i, _i, _vp, _ll, _vp],

@@ -129,7 +129,9 @@ __device__ __forceinline__ float2 outer_bin(const float2* ys, const float2* t1, 
 template <int N1, int KIND>
 __global__ void __launch_bounds__(256, 3) fft_rows_fwd_kernel(const void* __restrict__ field, long long nrows, int ny,
                                                            const float2* __restrict__ wn_g, int m0c, int bc, int u0,
-                                                           int nu, float2* __restrict__ t) {
+                                                           int nu, float2* __restrict__ t, int nparts,
+                                                           long long pstride) {
+  // nparts > 1 (float32 only): the field is the sum of nparts arrays pstride elements apart
   constexpr int N = 32 * N1, G = 256 / N1;  // G row pairs per block
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const float2* t2 = wn_g;                    // global [32][N1], read through L1 (warp-coalesced)
@@ -144,6 +146,14 @@ __global__ void __launch_bounds__(256, 3) fft_rows_fwd_kernel(const void* __rest
 #pragma unroll
     for (int n2 = 0; n2 < 32; ++n2)
       z[n2] = make_float2(load_real<KIND>(field, o0 + n1 + N1 * n2), load_real<KIND>(field, o1 + n1 + N1 * n2));
+    for (int p = 1; p < nparts; ++p) {
+      const long long op = p * pstride;
+#pragma unroll
+      for (int n2 = 0; n2 < 32; ++n2) {
+        z[n2].x += load_real<KIND>(field, op + o0 + n1 + N1 * n2);
+        z[n2].y += load_real<KIND>(field, op + o1 + n1 + N1 * n2);
+      }
+    }
   } else {
 #pragma unroll
     for (int n2 = 0; n2 < 32; ++n2) z[n2] = make_float2(0.f, 0.f);
@@ -182,7 +192,8 @@ template <int N1, bool SYM>
 __global__ void __launch_bounds__(256, 3) fft_cols_fwd_kernel(const float2* __restrict__ t, long long ncols, int bc,
                                                            const float2* __restrict__ wn_g, int m0r, int br,
                                                            float scale, float2* __restrict__ band, int bco,
-                                                           const float2* __restrict__ tpart, FwdSplit split) {
+                                                           const float2* __restrict__ tpart, FwdSplit split,
+                                                           int dbl_from) {
   constexpr int N = 32 * N1, G = 256 / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const float2* t2 = wn_g;
@@ -227,10 +238,11 @@ __global__ void __launch_bounds__(256, 3) fft_cols_fwd_kernel(const float2* __re
   if (col >= ncols) return;
   const long long b = col / bc;
   const int ic = (int)(col - b * bc);
-  if (!SYM) {
+  if (!SYM) {   // columns ic >= dbl_from are doubled (a Hermitian half-spectrum standing for both halves)
+    const float sc = ic >= dbl_from ? 2.f * scale : scale;
     for (int ir = n1; ir < br; ir += N1) {
       float2 v = outer_bin<+1, N1>(yg, t1, (m0r + ir) & (N - 1));
-      band[(b * br + ir) * (long long)bc + ic] = make_float2(v.x * scale, v.y * scale);
+      band[(b * br + ir) * (long long)bc + ic] = make_float2(v.x * sc, v.y * sc);
     }
   } else {
     const int h = (bco - 1) / 2;
@@ -573,7 +585,8 @@ static size_t smem_cols_fwd() { return sizeof(float2) * ((256 / N1) * 32 * (N1 +
 
 template <int N1>
 static int band_fft(const void* field, int kind, int batch, int ny, int nx, int m0r, int br, int m0c, int bc,
-                    const float2* wn_x, const float2* wn_y, float scale, float2* t, float2* band, cudaStream_t s) {
+                    const float2* wn_x, const float2* wn_y, float scale, float2* t, float2* band, cudaStream_t s,
+                    int nparts = 1, long long pstride = 0) {
   // row transforms have length nx = 32 * N1; the column kernel picks its own N1 for ny
   const int u0 = min(m0c, -(m0c + bc - 1)), u1 = max(m0c + bc - 1, -m0c), nu = u1 - u0 + 1;
   constexpr int G = 256 / N1;
@@ -584,13 +597,13 @@ static int band_fft(const void* field, int kind, int batch, int ny, int nx, int 
     rc = set_smem(fft_rows_fwd_kernel<N1, OI_FIELD_U8>, smem, "oi_band_spectrum_fft/rows");
     if (rc) return rc;
     fft_rows_fwd_kernel<N1, OI_FIELD_U8><<<(unsigned)ceil_div(nrows, 2 * G), 256, smem, s>>>(
-        field, nrows, ny, wn_x, m0c, bc, u0, nu, t);
+        field, nrows, ny, wn_x, m0c, bc, u0, nu, t, 1, 0LL);
     oi::note_launch();
   } else {
     rc = set_smem(fft_rows_fwd_kernel<N1, OI_FIELD_REAL_F32>, smem, "oi_band_spectrum_fft/rows");
     if (rc) return rc;
     fft_rows_fwd_kernel<N1, OI_FIELD_REAL_F32><<<(unsigned)ceil_div(nrows, 2 * G), 256, smem, s>>>(
-        field, nrows, ny, wn_x, m0c, bc, u0, nu, t);
+        field, nrows, ny, wn_x, m0c, bc, u0, nu, t, nparts, pstride);
     oi::note_launch();
   }
   return check_launch("oi_band_spectrum_fft/rows");
@@ -600,14 +613,14 @@ static int band_fft(const void* field, int kind, int batch, int ny, int nx, int 
 template <int N1, bool SYM = false>
 static int cols_fwd(const float2* t, int batch, int bc, const float2* wn_y, int m0r, int br, float scale,
                     float2* band, cudaStream_t s, int bco = 0, const float2* t2 = nullptr,
-                    FwdSplit split = FwdSplit{1, 1, 1}) {
+                    FwdSplit split = FwdSplit{1, 1, 1}, int dbl_from = 0x7fffffff) {
   constexpr int G = 256 / N1;
   size_t smem = smem_cols_fwd<N1>();
   int rc = set_smem(fft_cols_fwd_kernel<N1, SYM>, smem, "oi_band_spectrum_fft/cols");
   if (rc) return rc;
   const long long ncols = (long long)batch * bc;
   (void)launch_pdl(fft_cols_fwd_kernel<N1, SYM>, dim3((unsigned)ceil_div(ncols, G)), dim3(256), smem, s,
-                   (const float2*)t, ncols, bc, wn_y, m0r, br, scale, band, SYM ? bco : bc, t2, split);
+                   (const float2*)t, ncols, bc, wn_y, m0r, br, scale, band, SYM ? bco : bc, t2, split, dbl_from);
   oi::note_launch();
   return check_launch("oi_band_spectrum_fft/cols");
 }
@@ -683,6 +696,42 @@ extern "C" int oi_band_spectrum_fft(const void* field, int kind, int batch, int 
   }
 }
 
+// The Hermitian half-spectrum of a coarse intensity held as nparts partial sums (oi_coherent_coarse_fft's output,
+// [nparts][count][mr][mc] float32): ihat[i][qr + br-1][qc] = w(qc) / (mr mc) sum_{y,x} (sum_p coarse[p][i][y][x])
+// exp(+2 pi i (qr y / mr + qc x / mc)), |qr| < br, 0 <= qc < bc, w(0) = 1 and w(qc > 0) = 2 -- the input of
+// oi_spectrum_to_image_fft.  The parts are summed in the row pass's loads; scratch: count * mr * bc complex.
+extern "C" int oi_coarse_half_spectrum_fft(const float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
+                                           const void* wn_c, const void* wn_r, void* scratch, void* ihat,
+                                           void* stream) {
+  using namespace oi;
+  if (!coarse || !wn_c || !wn_r || !scratch || !ihat || nparts <= 0 || count <= 0 || br <= 0 || bc <= 0)
+    return fail(OI_EINVAL, "oi_coarse_half_spectrum_fft: bad arguments");
+  const int nx1 = n1_of(mc), ny1 = n1_of(mr);
+  if (!nx1 || !ny1)
+    return fail(OI_ERANGE, "oi_coarse_half_spectrum_fft: coarse grid %dx%d is not 256..2048, power of 2", mr, mc);
+  if (2 * (bc - 1) >= mc || 2 * br - 1 > mr)
+    return fail(OI_ERANGE, "oi_coarse_half_spectrum_fft: band %dx%d too wide for %dx%d", br, bc, mr, mc);
+  cudaStream_t s = (cudaStream_t)stream;
+  float2* t = (float2*)scratch;
+  float2* out = (float2*)ihat;
+  const int nq = 2 * br - 1, m0r = -(br - 1);
+  const float scale = 1.f / ((float)mr * (float)mc);
+  const long long pstride = (long long)count * mr * mc;
+  int rc;
+  switch (nx1) {
+    case 8: rc = band_fft<8>(coarse, OI_FIELD_REAL_F32, count, mr, mc, m0r, nq, 0, bc, (const float2*)wn_c, (const float2*)wn_r, scale, t, out, s, nparts, pstride); break;
+    case 16: rc = band_fft<16>(coarse, OI_FIELD_REAL_F32, count, mr, mc, m0r, nq, 0, bc, (const float2*)wn_c, (const float2*)wn_r, scale, t, out, s, nparts, pstride); break;
+    case 32: rc = band_fft<32>(coarse, OI_FIELD_REAL_F32, count, mr, mc, m0r, nq, 0, bc, (const float2*)wn_c, (const float2*)wn_r, scale, t, out, s, nparts, pstride); break;
+    default: rc = band_fft<64>(coarse, OI_FIELD_REAL_F32, count, mr, mc, m0r, nq, 0, bc, (const float2*)wn_c, (const float2*)wn_r, scale, t, out, s, nparts, pstride); break;
+  }
+  if (rc) return rc;
+  switch (ny1) {
+    case 8: return cols_fwd<8>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, nullptr, FwdSplit{1, 1, 1}, 1);
+    case 16: return cols_fwd<16>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, nullptr, FwdSplit{1, 1, 1}, 1);
+    case 32: return cols_fwd<32>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, nullptr, FwdSplit{1, 1, 1}, 1);
+    default: return cols_fwd<64>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, nullptr, FwdSplit{1, 1, 1}, 1);
+  }
+}
 
 extern "C" int oi_coarse_to_image_fft(float* coarse, int nparts, int count, int mr, int mc, int br, int bc,
                                       const void* gc, const void* gr, const void* wm_r, const void* wm_c,

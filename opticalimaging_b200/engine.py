@@ -338,17 +338,14 @@ def coherent_image(band: torch.Tensor, pupils: torch.Tensor, weights: torch.Tens
                N.ptr(plan.rows_consts(1)), plan.ny, plan.nx, N.ptr(tiles), N.ptr(out), s)
     elif plan.big_coarse_fft(form):
         # the coarse intensity's Hermitian half-spectrum by the FFT band pass, then the FFT synthesis
-        count, nq = batch * nz, 2 * b.br - 1
-        cimg = (coarse[0] if nsplit == 1 else coarse.sum(dim=0)).reshape(count, plan.mr, plan.mc)
+        count = batch * nz
         wn_r, wn_c = plan.coarse_fft_tables()
         t = torch.empty(count * plan.mr * b.bc, dtype=torch.complex64, device=dev)
-        ih = ihat.view(count, 1, nq, b.bc)
-        N.call('oi_band_spectrum_fft', N.ptr(cimg), N.FIELD_REAL_F32, count, plan.mr, plan.mc, -(b.br - 1), nq, 0,
-               b.bc, N.ptr(wn_c), N.ptr(wn_r), 1.0 / (plan.mr * plan.mc), N.ptr(t), N.ptr(ih), s)
-        ih[..., 1:] *= 2.0
+        N.call('oi_coarse_half_spectrum_fft', N.ptr(coarse), nsplit, count, plan.mr, plan.mc, b.br, b.bc, N.ptr(wn_c),
+               N.ptr(wn_r), N.ptr(t), N.ptr(ihat), s)
         v = torch.empty(count * b.bc * plan.ny, dtype=torch.complex64, device=dev)
-        N.call('oi_spectrum_to_image_fft', N.ptr(ih), count, b.br, b.bc, N.ptr(plan.wn_y), N.ptr(plan.wn_x), plan.ny,
-               plan.nx, N.ptr(v), N.ptr(out), s)
+        N.call('oi_spectrum_to_image_fft', N.ptr(ihat), count, b.br, b.bc, N.ptr(plan.wn_y), N.ptr(plan.wn_x),
+               plan.ny, plan.nx, N.ptr(v), N.ptr(out), s)
     elif plan.use_fft(form):
         v = torch.empty(batch * nz * b.bc * plan.ny, dtype=torch.complex64, device=dev)
         wm_r, wm_c = (plan.wm_r, plan.wm_c) if plan.coarse_fft else (None, None)

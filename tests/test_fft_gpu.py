@@ -102,6 +102,33 @@ def test_large_band_coarse_256_fft_vs_dft_and_oracle(eng):
     assert N.device_status() == 0
 
 
+@pytest.mark.parametrize('nparts,count,m,br,bc', [(3, 2, 256, 117, 59), (1, 3, 256, 70, 66), (2, 1, 512, 128, 128)])
+def test_coarse_half_spectrum_fft(eng, nparts, count, m, br, bc):
+    """oi_coarse_half_spectrum_fft (parts summed in the row pass, columns qc > 0 doubled) against FP64
+    ihat[qr][qc] = w(qc) / m^2 sum_{y,x} c[y][x] exp(+2 pi i (qr y + qc x) / m)."""
+    from opticalimaging_b200 import _native as N
+    dev = torch.device('cuda')
+    rng = np.random.default_rng(nparts * 100 + br)
+    coarse = rng.random((nparts, count, m, m)).astype(np.float32)
+    c = coarse.astype(np.float64).sum(axis=0)
+    tables = eng.fft_tables(m, dev)
+    cd = torch.from_numpy(coarse).to(dev)
+    t = torch.empty(count * m * bc, dtype=torch.complex64, device=dev)
+    ihat = torch.empty((count, 2 * br - 1, bc), dtype=torch.complex64, device=dev)
+    N.call('oi_coarse_half_spectrum_fft', N.ptr(cd), nparts, count, m, m, br, bc, N.ptr(tables), N.ptr(tables),
+           N.ptr(t), N.ptr(ihat), N.stream_handle(dev))
+    qr = np.arange(-(br - 1), br)
+    E = np.exp(2j * np.pi * np.arange(m) / m)
+    Er = E[np.outer(qr, np.arange(m)) % m]                  # [nq][y]
+    Ec = E[np.outer(np.arange(m), np.arange(bc)) % m]       # [x][qc]
+    want = np.einsum('ry,iyx,xc->irc', Er, c, Ec) / m ** 2
+    want[:, :, 1:] *= 2
+    err = rel_err(ihat.cpu().numpy(), want)
+    print(f'coarse half spectrum {nparts} parts {count}x{m}^2 band {br}x{bc}: {err:.2e}')
+    assert err < 2e-6
+    assert N.device_status() == 0
+
+
 @pytest.mark.parametrize('batch,nch,nz,nk,br,bc,m0r,m0c,nsplit,per_image', [
     (2, 2, 2, 3, 70, 66, -35, -30, 4, False),     # 12 fields over 4 splits, two planes, two channels
     (2, 1, 1, 5, 128, 128, -64, -64, 2, True),    # the largest band; pupils per image
