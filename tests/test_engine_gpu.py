@@ -332,4 +332,6 @@ def test_dropin_large_host_field_through_pinned_staging(oi):
     assert img.device.type == 'cpu' and img.shape == (1024, 1024)
     sk = oi._SOCS_CACHE[K][1]
     want = sk.image(torch.from_numpy(mask).cuda()[None])[0].cpu().numpy()
-    assert rel_err(img.numpy(), want) < 2e-6
+    # two FP32 paths (complex field through the DFT band pass, float mask through the FFT): rounding only (2.1e-6
+    # measured); a staging fault would show as O(1)
+    assert rel_err(img.numpy(), want) < 1e-5
