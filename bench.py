@@ -605,7 +605,7 @@ def kernel_rooflines(sk, masks, reps=10):
     plan = sk.plan
     tplan = Plan.get(sk.ny, sk.nx, b, dev, coarse=TC_COARSE)
     s = N.stream_handle(dev)
-    t = torch.empty(2 * B * sk.ny * b.bc, dtype=torch.complex64, device=dev)
+    t = torch.empty(B * sk.ny * b.bc, dtype=torch.complex64, device=dev)
     band = band_spectrum(masks, N.FIELD_REAL_F32, plan, form='bf16x3')
     ctas, nparts = N.tc_layout(B, sk.count)   # nparts also sizes the synthesis kernel's partial sums
     coarse = torch.empty((nparts, B, 1, 128, 128), device=dev)
@@ -613,11 +613,12 @@ def kernel_rooflines(sk, masks, reps=10):
     tiles = torch.empty(B * sk.ny * 512, dtype=torch.uint8, device=dev)
     out = torch.empty((B, sk.ny, sk.nx), device=dev)
     # the forward row pass as the image path runs it: the Hermitian half for a symmetric band
-    half = plan.symmetric_band()   # the Hermitian half for a symmetric band; ranges cut at chunk boundaries
-    bcols = (b.bc + 1) // 2 if half else b.bc
-    t2 = t[B * sk.ny * bcols:]
-    fwd = lambda: N.call('oi_rows_fwd_tc_split', N.ptr(masks), N.FIELD_REAL_F32, B, sk.ny, sk.nx,  # noqa: E731
-                         bcols, int(half), N.ptr(plan.rows_consts(2 if half else 0)), N.ptr(t), N.ptr(t2), s)
+    if plan.symmetric_band():
+        fwd = lambda: N.call('oi_rows_fwd_tc_half', N.ptr(masks), N.FIELD_REAL_F32, B, sk.ny, sk.nx,  # noqa: E731
+                             (b.bc + 1) // 2, N.ptr(plan.rows_consts(2)), N.ptr(t), s)
+    else:
+        fwd = lambda: N.call('oi_rows_fwd_tc', N.ptr(masks), N.FIELD_REAL_F32, B, sk.ny, sk.nx, b.m0c,  # noqa: E731
+                             b.bc, N.ptr(plan.rows_consts(0)), N.ptr(t), s)
     scoarse = torch.rand((nparts, B, 128, 128), device=dev)
     stiles = torch.empty(B * sk.ny * 512, dtype=torch.uint8, device=dev)
     calls = {

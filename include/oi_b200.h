@@ -231,8 +231,7 @@ OI_API int oi_tc_constants(int m0r, int m0c, const void* wr, const void* wc, voi
  * oi_rows_fwd_tc_half, given the symmetric band m0c = -(bc-1)/2, bc odd <= 63, it covers bch = (bc+1)/2 columns;
  * nx/64 * 16384 bytes).  A wait that exceeds 2 s ends the kernel early and sets the device status.
  * oi_band_spectrum_tc and oi_coarse_to_image_tc are oi_band_spectrum_fft and oi_coarse_to_image_fft (coarse grid
- * 128 x 128) with these row passes (oi_band_spectrum_tc's scratch: 2 * batch * bc * ny complex, the second half
- * for the row pass's shared pairs, see oi_rows_fwd_tc_split); oi_coarse_to_image_tc writes the column pass straight into the V operand tiles
+ * 128 x 128) with these row passes; oi_coarse_to_image_tc writes the column pass straight into the V operand tiles
  * (scratch_tiles, count * ny * 512 bytes; scratch_v is unused and may be NULL).
  */
 OI_API int oi_rows_tc_constants(int which, int nx, int m0c, int bc, void* image, long long bytes, void* stream);
@@ -242,14 +241,6 @@ OI_API int oi_rows_fwd_tc_half(const void* field, int kind, int batch, int ny, i
                                void* t, void* stream);
 OI_API int oi_rows_inv_tc(const void* v, int count, int ny, int nx, int bc, const void* consts, void* vtiles,
                           float* out, void* stream);
-/* oi_rows_fwd_tc (half = 0, bcols = bc) or oi_rows_fwd_tc_half (half = 1, bcols = bch) with the CTAs' work cut into
- * equal shares of the (row-block pair, 64-column chunk) sequence instead of whole pairs: a pair whose chunks two
- * CTAs share has the sum over its first chunks in t and over the rest in t2 (same layout, float2
- * [batch][bcols][ny]); t + t2 is the result for those pairs, t alone for the others.  Which pairs are shared
- * follows from the launch (pairs = (batch*ny/128 + 1)/2, ranges = min(pairs, SMs)); oi_band_spectrum_tc(_sym)
- * run this form and add the parts in their column pass. */
-OI_API int oi_rows_fwd_tc_split(const void* field, int kind, int batch, int ny, int nx, int bcols, int half,
-                                const void* consts, void* t, void* t2, void* stream);
 /* The synthesis row pass alone, from V operand tiles already written (by oi_rows_inv_tc's conversion or by the
  * column pass of oi_coarse_to_image_tc): the second half of oi_rows_inv_tc. */
 OI_API int oi_rows_inv_tc_tiles(const void* vtiles, int count, int ny, int nx, const void* consts, float* out,
@@ -260,7 +251,7 @@ OI_API int oi_band_spectrum_tc(const void* field, int kind, int batch, int ny, i
 /* oi_band_spectrum_tc for a real mask and an odd symmetric band (m0r = -(br-1)/2, m0c = -(bc-1)/2, bc <= 63):
  * the row pass computes the band's (bc+1)/2 non-negative columns only (oi_rows_fwd_tc_half, hconsts from
  * oi_rows_tc_constants(2, nx, m0c, bc, ...)) and the column pass writes each column and its mirror
- * band[-ky][-kx] = conj(band[ky][kx]).  scratch: 2 * batch * ny * (bc+1)/2 complex.  Same band as
+ * band[-ky][-kx] = conj(band[ky][kx]).  scratch: batch * ny * (bc+1)/2 complex.  Same band as
  * oi_band_spectrum_tc (Scatter.CalculateSpectrum, Scatter.py:10-35, restricted to the band). */
 OI_API int oi_band_spectrum_tc_sym(const void* field, int kind, int batch, int ny, int nx, int br, int bc,
                                    const void* hconsts, const void* wn_y, float scale, void* scratch, void* band,

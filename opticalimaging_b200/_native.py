@@ -47,7 +47,6 @@ _SIGS = {
     'oi_rows_tc_constants': [_i, _i, _i, _i, _vp, _ll, _vp],
     'oi_rows_fwd_tc': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp],
     'oi_rows_fwd_tc_half': [_vp, _i, _i, _i, _i, _i, _vp, _vp, _vp],
-    'oi_rows_fwd_tc_split': [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp],
     'oi_rows_inv_tc': [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp],
     'oi_rows_inv_tc_tiles': [_vp, _i, _i, _i, _vp, _vp, _vp],
     'oi_band_spectrum_tc': [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _f, _vp, _vp, _vp],

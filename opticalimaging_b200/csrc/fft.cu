@@ -192,7 +192,6 @@ template <int N1, bool SYM>
 __global__ void __launch_bounds__(256, 3) fft_cols_fwd_kernel(const float2* __restrict__ t, long long ncols, int bc,
                                                            const float2* __restrict__ wn_g, int m0r, int br,
                                                            float scale, float2* __restrict__ band, int bco,
-                                                           const float2* __restrict__ tpart, FwdSplit split,
                                                            int dbl_from) {
   constexpr int N = 32 * N1, G = 256 / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -208,24 +207,6 @@ __global__ void __launch_bounds__(256, 3) fft_cols_fwd_kernel(const float2* __re
     const float2* src = t + col * N;
 #pragma unroll
     for (int n2 = 0; n2 < 32; ++n2) z[n2] = src[n1 + N1 * n2];
-    if (tpart) {   // row-block pairs whose chunks two CTAs of the row pass shared: add the second CTA's sum
-      const long long row0 = (col / bc) * N;            // this column's image starts at flat row row0
-      const long long p0 = row0 >> 8;
-      uint32_t cut = 0;                                  // bit k: pair p0 + k is cut (a column spans <= 9 pairs)
-      for (long long p = p0; p <= (row0 + N - 1) >> 8; ++p)
-        if (pair_is_cut(p, split.total, split.ctas, split.kc)) cut |= 1u << (int)(p - p0);
-      if (cut) {
-        const float2* src2 = tpart + col * N;
-#pragma unroll
-        for (int n2 = 0; n2 < 32; ++n2) {
-          const int y = n1 + N1 * n2;
-          if ((cut >> (int)(((row0 + y) >> 8) - p0)) & 1u) {
-            const float2 e = src2[y];
-            z[n2] = make_float2(z[n2].x + e.x, z[n2].y + e.y);
-          }
-        }
-      }
-    }
   } else {
 #pragma unroll
     for (int n2 = 0; n2 < 32; ++n2) z[n2] = make_float2(0.f, 0.f);
@@ -612,15 +593,14 @@ static int band_fft(const void* field, int kind, int batch, int ny, int nx, int 
 // bco: the output band width (SYM: bc = (bco + 1) / 2 input columns; else bco = bc)
 template <int N1, bool SYM = false>
 static int cols_fwd(const float2* t, int batch, int bc, const float2* wn_y, int m0r, int br, float scale,
-                    float2* band, cudaStream_t s, int bco = 0, const float2* t2 = nullptr,
-                    FwdSplit split = FwdSplit{1, 1, 1}, int dbl_from = 0x7fffffff) {
+                    float2* band, cudaStream_t s, int bco = 0, int dbl_from = 0x7fffffff) {
   constexpr int G = 256 / N1;
   size_t smem = smem_cols_fwd<N1>();
   int rc = set_smem(fft_cols_fwd_kernel<N1, SYM>, smem, "oi_band_spectrum_fft/cols");
   if (rc) return rc;
   const long long ncols = (long long)batch * bc;
   (void)launch_pdl(fft_cols_fwd_kernel<N1, SYM>, dim3((unsigned)ceil_div(ncols, G)), dim3(256), smem, s,
-                   (const float2*)t, ncols, bc, wn_y, m0r, br, scale, band, SYM ? bco : bc, t2, split, dbl_from);
+                   (const float2*)t, ncols, bc, wn_y, m0r, br, scale, band, SYM ? bco : bc, dbl_from);
   oi::note_launch();
   return check_launch("oi_band_spectrum_fft/cols");
 }
@@ -726,10 +706,10 @@ extern "C" int oi_coarse_half_spectrum_fft(const float* coarse, int nparts, int 
   }
   if (rc) return rc;
   switch (ny1) {
-    case 8: return cols_fwd<8>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, nullptr, FwdSplit{1, 1, 1}, 1);
-    case 16: return cols_fwd<16>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, nullptr, FwdSplit{1, 1, 1}, 1);
-    case 32: return cols_fwd<32>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, nullptr, FwdSplit{1, 1, 1}, 1);
-    default: return cols_fwd<64>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, nullptr, FwdSplit{1, 1, 1}, 1);
+    case 8: return cols_fwd<8>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, 1);
+    case 16: return cols_fwd<16>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, 1);
+    case 32: return cols_fwd<32>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, 1);
+    default: return cols_fwd<64>(t, count, bc, (const float2*)wn_r, m0r, nq, scale, out, s, 0, 1);
   }
 }
 
@@ -814,27 +794,22 @@ extern "C" int oi_band_spectrum_tc(const void* field, int kind, int batch, int n
   if (!ny1 || nx % 128 != 0 || nx > 4096)
     return fail(OI_ERANGE, "oi_band_spectrum_tc: grid %dx%d unsupported", ny, nx);
   if (bc > 64 || br > ny) return fail(OI_ERANGE, "oi_band_spectrum_tc: band %dx%d unsupported", br, bc);
-  // row pass with its ranges cut at chunk boundaries: a shared pair's second part goes to the scratch's second half
-  const float2* t = (const float2*)scratch;
-  const float2* t2 = t + (long long)batch * bc * ny;
-  FwdSplit sp{};
-  int rc = rows_fwd_split(64, field, kind, batch, ny, nx, bc, wconsts, scratch, (void*)t2, &sp, stream,
-                          "oi_band_spectrum_tc");
+  int rc = oi_rows_fwd_tc(field, kind, batch, ny, nx, m0c, bc, wconsts, scratch, stream);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
+  const float2* t = (const float2*)scratch;
   switch (ny1) {
-    case 8: return cols_fwd<8>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, 0, t2, sp);
-    case 16: return cols_fwd<16>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, 0, t2, sp);
-    case 32: return cols_fwd<32>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, 0, t2, sp);
-    default: return cols_fwd<64>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, 0, t2, sp);
+    case 8: return cols_fwd<8>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+    case 16: return cols_fwd<16>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+    case 32: return cols_fwd<32>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
+    default: return cols_fwd<64>(t, batch, bc, (const float2*)wn_y, m0r, br, scale, (float2*)band, s);
   }
 }
 
 // oi_band_spectrum_tc for a symmetric band (m0r = -(br-1)/2, m0c = -(bc-1)/2, br and bc odd, bc <= 63): the row
 // pass computes only the band's non-negative columns (oi_rows_fwd_tc_half against `hconsts` of
 // oi_rows_tc_constants(2, nx, m0c, bc, ...)) and the column pass fills the negative ones from
-// band[-ky][-kx] = conj(band[ky][kx]) (a real mask).  scratch: 2 * batch * ny * (bc+1)/2 complex (the second
-// half for the row pass's shared row-block pairs).
+// band[-ky][-kx] = conj(band[ky][kx]) (a real mask).  scratch: batch * ny * (bc+1)/2 complex.
 extern "C" int oi_band_spectrum_tc_sym(const void* field, int kind, int batch, int ny, int nx, int br, int bc,
                                        const void* hconsts, const void* wn_y, float scale, void* scratch, void* band,
                                        void* stream) {
@@ -847,18 +822,15 @@ extern "C" int oi_band_spectrum_tc_sym(const void* field, int kind, int batch, i
   if (bc % 2 == 0 || br % 2 == 0 || bc > 63 || br > ny)
     return fail(OI_ERANGE, "oi_band_spectrum_tc_sym: band %dx%d is not an odd symmetric band of width <= 63", br, bc);
   const int bch = (bc + 1) / 2, m0r = -(br - 1) / 2;
-  const float2* t = (const float2*)scratch;
-  const float2* t2 = t + (long long)batch * bch * ny;
-  FwdSplit sp{};
-  int rc = rows_fwd_split(32, field, kind, batch, ny, nx, bch, hconsts, scratch, (void*)t2, &sp, stream,
-                          "oi_band_spectrum_tc_sym");
+  int rc = oi_rows_fwd_tc_half(field, kind, batch, ny, nx, bch, hconsts, scratch, stream);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
+  const float2* t = (const float2*)scratch;
   switch (ny1) {
-    case 8: return cols_fwd<8, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc, t2, sp);
-    case 16: return cols_fwd<16, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc, t2, sp);
-    case 32: return cols_fwd<32, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc, t2, sp);
-    default: return cols_fwd<64, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc, t2, sp);
+    case 8: return cols_fwd<8, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc);
+    case 16: return cols_fwd<16, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc);
+    case 32: return cols_fwd<32, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc);
+    default: return cols_fwd<64, true>(t, batch, bch, (const float2*)wn_y, m0r, br, scale, (float2*)band, s, bc);
   }
 }
 

@@ -89,11 +89,7 @@ struct FwdArgs {
   int ny, nx, bc;
   const unsigned char* w;   // constant image: per 64-column chunk, [hi | lo] x [2 NB rows][64]
   float2* t;                // [batch][bc][ny]
-  float2* t2;               // NULL: each CTA takes whole pairs.  Else the CTAs' ranges are cut at chunk boundaries
-                            // (equal shares of the pairs x chunks); a pair whose chunks two CTAs share gets its
-                            // first chunks' sum in t and the rest's in t2 (same layout), t + t2 being its result.
 };
-
 
 constexpr int F_NT = NT + 32;   // + a warp issuing the W loads
 
@@ -121,13 +117,8 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   const long long R = a.rows / 128;                  // row blocks
   const long long items = (R + 1) / 2;               // pairs
   const long long G = gridDim.x;
-  // this CTA's chunks [g0, g1) of the pairs x KC sequence: whole pairs, or (t2 given) an equal share cut anywhere
-  const long long total = items * KC;
-  const long long g0 = a.t2 ? (long long)blockIdx.x * total / G : ((long long)blockIdx.x * items / G) * KC;
-  const long long g1 = a.t2 ? ((long long)blockIdx.x + 1) * total / G : (((long long)blockIdx.x + 1) * items / G) * KC;
-  const long long P0 = g0 / KC;                      // pair of the first chunk
-  const int c0 = (int)(g0 - P0 * KC);                // its chunk: > 0 when the range starts inside a pair
-  const long long nchunks = g1 - g0;
+  const long long i0 = (long long)blockIdx.x * items / G, i1 = ((long long)blockIdx.x + 1) * items / G;
+  const long long nchunks = (i1 - i0) * KC;
   constexpr bool U8 = KIND == OI_FIELD_U8;
   constexpr uint32_t BLK = U8 ? 128 * 64 : F_STG;    // bytes of one block's chunk
 
@@ -163,7 +154,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
     // ---- mask producer: chunk g of both blocks into staging slot g % 2 as soon as the slot has been read
     if (lane == 0) {
       Ring st{0, 0};
-      int c = c0, y = (int)(P0 * 256), g = 0;
+      int c = 0, y = (int)(i0 * 256), g = 0;
       for (; g < NC; ++g) {
         if (g >= F_NS && !wait_bar(sfree + 8 * st.slot, st.phase ^ 1u)) {
           fail_status();
@@ -188,7 +179,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
     // ---- W producer: chunk g's W into slot g % 3 once the MMAs of chunk g-3 have finished
     if (lane == 0) {
       Ring ws{0, 0};
-      int c = c0, g = 0;
+      int c = 0, g = 0;
       for (; g < NC; ++g) {
         if (g >= F_NWS && !wait_bar(wdone + 8 * ws.slot, ws.phase ^ 1u)) {
           fail_status();
@@ -206,13 +197,12 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
     if (lane == 0) {
       constexpr uint32_t ID = idesc(2 * NB, false);
       Ring as{0, 0}, ws{0, 0};
-      int c = c0, n = 0;   // n: segments (runs of one pair's chunks) begun
+      int c = 0, n = 0;
       bool issued = false;
       for (int g = 0; g < NC; ++g) {
-        const bool seg_start = g == 0 || c == 0, seg_end = g == NC - 1 || c == KC - 1;
         bool ok = wait_bar(conv + 8 * as.slot, as.phase);
         if (ok) ok = wait_bar(wfull + 8 * ws.slot, ws.phase);
-        if (ok && seg_start && n >= 1) ok = wait_bar(acce, (uint32_t)((n - 1) & 1));   // previous segment drained
+        if (ok && c == 0 && n >= 1) ok = wait_bar(acce, (uint32_t)((n - 1) & 1));   // previous pair drained
         if (!ok) {
           fail_status();
           break;
@@ -235,18 +225,20 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
 #pragma unroll
           for (int ks = 0; ks < 4; ++ks) {
             const uint32_t ko = 32 * ks;
-            mma_ts(d, at + 8 * ks, sdesc(wch + ko), ID, (!seg_start || ks) ? 1u : 0u);   // hi hi
+            mma_ts(d, at + 8 * ks, sdesc(wch + ko), ID, (c | ks) ? 1u : 0u);            // hi hi
             mma_ts(d, at + 8 * ks, sdesc(wch + WOP + ko), ID, 1);                      // hi lo
             if (lo_any) mma_ts(d, at + 32 + 8 * ks, sdesc(wch + ko), ID, 1);           // lo hi
           }
         }
         commit(adone + 8 * as.slot);
         commit(wdone + 8 * ws.slot);
-        if (seg_end) commit(accf);
+        if (c == KC - 1) commit(accf);
         as.next(2);
         ws.next(F_NWS);
-        if (seg_start) ++n;
-        if (++c == KC) c = 0;
+        if (++c == KC) {
+          c = 0;
+          ++n;
+        }
       }
       if (issued) {   // every MMA issued has finished before tensor and shared memory are released
         commit(fin);
@@ -277,12 +269,11 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
           __syncwarp();
           if (lane == 0) arrive(acce);
         }
-        const long long rb = 2 * (P0 + n) + h;
+        const long long rb = 2 * (i0 + n) + h;
         if (rb < R) {
           const int row = (int)(rb * 128) + r;
           const int b = row / a.ny, y = row - b * a.ny;
-          float2* out = (n == 0 && c0 != 0) ? a.t2 : a.t;   // a range starting inside a pair holds its later chunks
-          float2* dst = out + ((long long)b * a.bc + DC * half) * a.ny + y;
+          float2* dst = a.t + ((long long)b * a.bc + DC * half) * a.ny + y;
 #pragma unroll
           for (int j = 0; j < DC; ++j)
             if (DC * half + j < a.bc) dst[(long long)j * a.ny] = make_float2(re[j], im[j]);
@@ -291,9 +282,8 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
       return true;
     };
     Ring st{0, 0}, as{0, 0};
-    int c = c0, n = 0;   // n: segments begun, as in the MMA role
+    int c = 0, n = 0;
     for (int g = 0; g < NC && ok; ++g) {
-      const bool seg_start = g == 0 || c == 0;
       ok = warp_wait(sfull + 8 * st.slot, st.phase);
       if (ok && g >= 2) ok = warp_wait(adone + 8 * as.slot, as.phase ^ 1u);   // A slot free (chunk g-2 done)
       if (!ok) break;
@@ -340,14 +330,16 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
         if (!U8) lo_flags[8 * as.slot + warp] = lo_nz ? 1u : 0u;   // read by the MMA thread after `conv`
         arrive(conv + 8 * as.slot);
       }
-      // the previous segment's accumulators are complete once this segment's first chunk is converted
-      if (seg_start && n >= 1) ok = drain(n - 1);
+      // the previous pair's accumulators are complete once this pair's first chunk is converted
+      if (c == 0 && n >= 1) ok = drain(n - 1);
       st.next(F_NS);
       as.next(2);
-      if (seg_start) ++n;
-      if (++c == KC) c = 0;
+      if (++c == KC) {
+        c = 0;
+        ++n;
+      }
     }
-    if (ok && NC > 0) ok = drain(n - 1);
+    if (ok && NC > 0) ok = drain((int)(i1 - i0) - 1);
     if (!ok && lane == 0) fail_status();
   }
   fence_before();
@@ -1016,7 +1008,7 @@ namespace oi {
 // the entry point in errors.
 template <int NB>
 static int rows_fwd_launch(const void* field, int kind, int batch, int ny, int nx, int bc, const void* consts, void* t,
-                           void* stream, const char* what, void* t2 = nullptr, FwdSplit* split = nullptr) {
+                           void* stream, const char* what) {
   if (!field || !consts || !t || batch <= 0 || bc <= 0) return fail(OI_EINVAL, "%s: bad arguments", what);
   if (kind != OI_FIELD_REAL_F32 && kind != OI_FIELD_U8)
     return fail(OI_EINVAL, "%s: real float32 or uint8 masks only (kind=%d)", what, kind);
@@ -1029,8 +1021,7 @@ static int rows_fwd_launch(const void* field, int kind, int batch, int ny, int n
   if (!sms) return fail(OI_ECUDA, "%s: no CUDA device", what);
   if (rows + 256 > 0x7fffffffLL) return fail(OI_ERANGE, "%s: %lld rows exceed the tensor-map range", what, rows);
   const long long ctas = items < sms ? items : sms;
-  rt::FwdArgs a{rows, ny, nx, bc, (const unsigned char*)consts, (float2*)t, (float2*)t2};
-  if (split) *split = FwdSplit{items * (nx / 64), (int)ctas, nx / 64};
+  rt::FwdArgs a{rows, ny, nx, bc, (const unsigned char*)consts, (float2*)t};
   cudaStream_t s = (cudaStream_t)stream;
   const bool u8 = kind == OI_FIELD_U8;
   CUtensorMap map;   // mask boxes: [128 rows][32 float] with the 128-byte swizzle, or [128][64 uint8], 64-byte
@@ -1066,23 +1057,6 @@ extern "C" int oi_rows_fwd_tc_half(const void* field, int kind, int batch, int n
                                    void* t, void* stream) {
   return oi::rows_fwd_launch<32>(field, kind, batch, ny, nx, bch, consts, t, stream, "oi_rows_fwd_tc_half");
 }
-
-extern "C" int oi_rows_fwd_tc_split(const void* field, int kind, int batch, int ny, int nx, int bcols, int half,
-                                    const void* consts, void* t, void* t2, void* stream) {
-  if (!t2) return oi::fail(OI_EINVAL, "oi_rows_fwd_tc_split: t2 is required");
-  return half ? oi::rows_fwd_launch<32>(field, kind, batch, ny, nx, bcols, consts, t, stream, "oi_rows_fwd_tc_split", t2)
-              : oi::rows_fwd_launch<64>(field, kind, batch, ny, nx, bcols, consts, t, stream, "oi_rows_fwd_tc_split", t2);
-}
-
-namespace oi {
-
-int rows_fwd_split(int nb, const void* field, int kind, int batch, int ny, int nx, int bc, const void* consts, void* t,
-                   void* t2, FwdSplit* split, void* stream, const char* what) {
-  return nb == 32 ? rows_fwd_launch<32>(field, kind, batch, ny, nx, bc, consts, t, stream, what, t2, split)
-                  : rows_fwd_launch<64>(field, kind, batch, ny, nx, bc, consts, t, stream, what, t2, split);
-}
-
-}  // namespace oi
 
 namespace oi {
 

@@ -19,24 +19,6 @@ int rows_tc_status(int* status, bool reset);
 // oi_rows_tc_constants(1, ...).
 int rows_inv_from_tiles(const void* vtiles, int count, int ny, int nx, const void* consts, float* out, cudaStream_t s);
 
-// The forward row pass with its CTAs' ranges cut at chunk boundaries (rows_tc.cu): equal shares of the
-// pairs x chunks sequence; a pair two CTAs share has its first chunks' sum in t and the rest's in t2 (same layout).
-// `split` receives what a consumer needs to find those pairs (pair_is_cut in rows_tc.cu, restated in fft.cu).
-struct FwdSplit {
-  long long total;   // pairs x chunks
-  int ctas, kc;      // ranges, chunks per pair
-};
-int rows_fwd_split(int nb, const void* field, int kind, int batch, int ny, int nx, int bc, const void* consts, void* t,
-                   void* t2, FwdSplit* split, void* stream, const char* what);
-
-// Whether row-block pair P has its chunks split between two CTAs when `total` = pairs x kc chunks are cut into
-// g equal contiguous ranges [floor(i total / g), floor((i+1) total / g)) (every range at least kc long, so a pair
-// holds at most one cut).
-__host__ __device__ __forceinline__ bool pair_is_cut(long long P, long long total, int g, int kc) {
-  const long long b = ((P * kc + 1) * g + total - 1) / total;   // first range starting after the pair's first chunk
-  return b < g && (b * total) / g < (P + 1) * kc;
-}
-
 // The synthesis preparation on the tensor cores (synth_tc.cu): V operand tiles from the coarse partial sums, and
 // its status word.
 int synth_tiles_tc(const float* coarse, int nparts, int count, int br, int bc, const void* sconsts, int ny,

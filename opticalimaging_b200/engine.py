@@ -263,8 +263,6 @@ def band_spectrum(field: torch.Tensor, kind: int, plan: Plan, nch: int = 1, scal
     b = plan.band
     batch = field.shape[0]
     need = batch * nch * plan.ny * b.bc
-    if plan.tc_rows(form):   # the tensor-core row pass keeps shared row-block pairs' second parts in a second half
-        need = max(need, 2 * batch * plan.ny * ((b.bc + 1) // 2 if plan.symmetric_band() else b.bc))
     if scratch is None or scratch.numel() < need:
         scratch = torch.empty(need, dtype=torch.complex64, device=plan.device)
     band = torch.empty((batch, nch, b.br, b.bc), dtype=torch.complex64, device=plan.device)

@@ -284,54 +284,6 @@ def test_rows_fwd_tc_half_direct(oi, count, ny, nx, bc, u8):
     assert N.device_status() == 0
 
 
-def _pair_is_cut(p, total, ctas, kc):
-    """Row-block pair p's chunks [p kc, (p+1) kc) hold a CTA range boundary floor(j total / ctas), 0 < j < ctas."""
-    j = -(-((p * kc + 1) * ctas) // total)
-    return j < ctas and (j * total) // ctas < (p + 1) * kc
-
-
-@pytest.mark.parametrize('count,ny,nx,bc,half,u8', [(101, 384, 512, 59, False, False), (48, 1024, 1024, 63, True, True),
-                                                    (41, 1024, 256, 15, True, False), (3, 256, 256, 15, False, False)])
-def test_rows_fwd_tc_split_direct(oi, count, ny, nx, bc, half, u8):
-    """The forward row pass with CTA ranges cut at 64-column chunk boundaries (oi_rows_fwd_tc_split): t, plus t2 on
-    the row-block pairs two CTAs share, against FP64; more pairs than SMs (shared pairs), an odd block count, both
-    widths, uint8 masks, and a launch with no shared pair (t2 untouched)."""
-    from opticalimaging_b200 import _native as N
-    dev = torch.device('cuda')
-    rng = np.random.default_rng(count * ny + nx + 7)
-    if u8:
-        m = (rng.random((count, ny, nx)) > 0.5).astype(np.uint8) * rng.integers(1, 255, (count, ny, nx)).astype(np.uint8)
-    else:
-        m = (rng.random((count, ny, nx)) > 0.6).astype(np.float32) * rng.random((count, ny, nx)).astype(np.float32)
-    s = N.stream_handle(dev)
-    m0c = -(bc - 1) // 2
-    bcols = (bc + 1) // 2 if half else bc
-    nbytes = (nx // 64) * (16384 if half else 32768)
-    consts = torch.empty(nbytes, dtype=torch.uint8, device=dev)
-    N.call('oi_rows_tc_constants', 2 if half else 0, nx, m0c, bc, N.ptr(consts), nbytes, s)
-    md = torch.from_numpy(m).to(dev)
-    t = torch.full((2, count, bcols, ny), complex(float('nan'), 0.0), dtype=torch.complex64, device=dev)
-    N.call('oi_rows_fwd_tc_split', N.ptr(md), N.FIELD_U8 if u8 else N.FIELD_REAL_F32, count, ny, nx, bcols,
-           int(half), N.ptr(consts), N.ptr(t[0]), N.ptr(t[1]), s)
-    t1, t2 = t.cpu().numpy()
-    pairs = (count * ny // 128 + 1) // 2
-    ctas = min(pairs, torch.cuda.get_device_properties(dev).multi_processor_count)
-    kc = nx // 64
-    cut = np.array([_pair_is_cut(p, pairs * kc, ctas, kc) for p in range(pairs)])
-    rows_cut = np.repeat(cut, 256)[:count * ny].reshape(count, 1, ny)         # [count][1][ny]
-    assert not np.isnan(t1).any()
-    assert not np.isnan(np.where(rows_cut, t2, 0)).any()
-    assert np.isnan(np.where(rows_cut, np.nan, t2)).all()                      # t2 written on shared pairs only
-    got = t1 + np.where(rows_cut, t2, 0)
-    E = np.exp(2j * np.pi * np.outer(np.arange(nx), (0 if half else m0c) + np.arange(bcols)) / nx)
-    want = np.stack([(m[i].astype(np.float64) @ E).T for i in range(count)])
-    err = rel_err(got, want)
-    print(f'split forward rows {count}x{ny}x{nx} bcols {bcols} u8={u8}: {int(cut.sum())} shared pairs, max {err:.2e}')
-    assert err < 2e-5
-    assert (cut.sum() > 0) == (pairs > ctas)
-    assert N.device_status() == 0
-
-
 def test_rows_tc_constants_half_rejects_asymmetric_band(oi):
     from opticalimaging_b200 import _native as N
     dev = torch.device('cuda')
@@ -354,7 +306,7 @@ def test_band_spectrum_tc_sym_matches_full(oi, batch, n, b):
     m = ((rng.random((batch, n, n)) > 0.6) * rng.random((batch, n, n))).astype(np.float32)
     md = torch.from_numpy(m).to(dev)
     s = N.stream_handle(dev)
-    scratch = torch.empty(2 * batch * n * b, dtype=torch.complex64, device=dev)
+    scratch = torch.empty(batch * n * b, dtype=torch.complex64, device=dev)
     full = torch.empty((batch, 1, b, b), dtype=torch.complex64, device=dev)
     half = torch.full((batch, 1, b, b), complex(float('nan'), 0.0), dtype=torch.complex64, device=dev)
     N.call('oi_band_spectrum_tc', N.ptr(md), N.FIELD_REAL_F32, batch, n, n, band.m0r, b, band.m0c, b,
