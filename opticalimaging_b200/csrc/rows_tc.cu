@@ -635,240 +635,6 @@ __global__ void __launch_bounds__(I_NT, 1) rows_inv_tc_kernel(InvArgs a, const _
   }
 }
 
-// --------------------------------------------------------------------------- inverse, mirror-symmetric
-// For nx a multiple of 256 the synthesis uses cos(2 pi qc (nx - x) / nx) = cos(2 pi qc x / nx) and
-// sin(2 pi qc (nx - x) / nx) = -sin(2 pi qc x / nx): with D1[x][y] = sum_qc vr cos and D2[x][y] = sum_qc vi sin,
-//   out[y][x] = D1 + D2   and   out[y][nx - x] = D1 - D2,
-// so x tiles over [0, nx/2) give whole rows with half the MMA work of the direct pass.  Column nx/2 (its own
-// mirror; sin = 0 there) is sum_qc vr (-1)^qc: tile 0 adds it to D2's row x = 0, whose sine part is zero, through
-// one more constant block E (row 0 = (-1)^qc, exact in bf16), and the drain writes D1 to column 0 and D2 to
-// column nx/2 for that row.
-// Items (x tile j, row block r) in x-tile-major order, one contiguous range per CTA: the CTA keeps C(j) --
-// [cos hi | cos lo | sin hi | sin lo] x [128 x][64 qc], 64 KB -- and E resident (C reloaded when the range crosses
-// into the next tile) and streams the V tiles of its row blocks through a ring of 16 KB pieces (two items deep),
-// in the order re hi, re lo, im hi, im lo, so D1's MMAs start after the first piece.  M = 128 (x), N = 128 (y),
-// K = 64 band columns per accumulator; tensor memory: two item buffers of D1 | D2 (2 x 128 columns each).
-constexpr int S_NV = 8;                                  // V pieces in the ring
-constexpr uint32_t S_V = 0;
-constexpr uint32_t S_C = S_NV * OPER;                    // C(j): cos hi, cos lo, sin hi, sin lo
-constexpr uint32_t S_E = S_C + 4 * OPER;                 // E hi (E lo is zero)
-constexpr uint32_t S_MISC = S_E + OPER;
-constexpr uint32_t S_SMEM = S_MISC + 512 + 1024;
-static_assert(S_SMEM <= SMEM_LIMIT, "symmetric inverse row pass: shared memory");
-
-struct SymArgs {
-  long long rows;           // count * ny (a multiple of 128)
-  int nx;
-  float* out;               // [count][ny][nx]
-};
-
-// Warps 0-7 drain, warp 8 streams the V pieces, warp 9 lane 0 issues the MMAs, warp 10 loads C(j) and E.
-__global__ void __launch_bounds__(I_NT, 1) rows_inv_sym_kernel(SymArgs a, const __grid_constant__ CUtensorMap c_map,
-                                                                const __grid_constant__ CUtensorMap v_map) {
-  extern __shared__ unsigned char smem_raw[];
-  const uint32_t raw = smem_u32(smem_raw);
-  const uint32_t base = (raw + 1023u) & ~1023u;
-  unsigned char* gbase = smem_raw + (base - raw);
-  const uint32_t misc = base + S_MISC;
-  // barriers: vfull[8] (V piece landed), vfree[8] (MMAs reading the piece finished), cfull (C(j) and E landed),
-  // cfree (MMAs of the items of the current C(j) finished), accf[2] (accumulator complete), acce[2] (accumulator
-  // drained), fin (every issued MMA finished, at the end)
-  const uint32_t vfull = misc, vfree = misc + 64, cfull = misc + 128, cfree = misc + 136, accf = misc + 144,
-                 acce = misc + 160, fin = misc + 176;
-  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + S_MISC + 256);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long long R = a.rows / 128;                // row blocks
-  const int JT = a.nx / 256;                       // x tiles of the half row
-  const long long items = R * JT;
-  const long long G = gridDim.x;
-  const long long i0 = (long long)blockIdx.x * items / G, i1 = ((long long)blockIdx.x + 1) * items / G;
-  const long long N = i1 - i0;
-  const int j0 = (int)(i0 / R);
-  const long long r0 = i0 - (long long)j0 * R;
-
-  if (warp == 0) tmem_alloc(misc + 256, 512);
-  if (tid == 0) {
-    for (int s = 0; s < S_NV; ++s) {
-      mbar_init(vfull + 8 * s, 1);
-      mbar_init(vfree + 8 * s, 1);
-    }
-    mbar_init(cfull, 1);
-    mbar_init(cfree, 1);
-    for (int s = 0; s < 2; ++s) {
-      mbar_init(accf + 8 * s, 1);
-      mbar_init(acce + 8 * s, 8);
-    }
-    mbar_init(fin, 1);
-    mbar_init_fence();
-  }
-  fence_before();
-  __syncthreads();
-  fence_after();
-  const uint32_t tmem = *tmem_slot;
-  pdl_trigger();
-  if (warp != 10) pdl_wait();   // warp 10 loads only the constant image; the rest read V or write the image
-
-  if (warp == 8) {
-    // ---- V pieces: item n's four blocks (re hi, re lo, im hi, im lo) into ring slots once their MMAs are done
-    if (lane == 0) {
-      Ring vs{0, 0};
-      long long r = r0;
-      int g = 0;
-      bool ok = true;
-      for (long long n = 0; n < N && ok; ++n) {
-        for (int k = 0; k < 4; ++k, ++g) {
-          const int q = (k & 1) * 2 + (k >> 1);   // tile block: 0 hi re, 2 lo re, 1 hi im, 3 lo im
-          if (g >= S_NV && !wait_bar(vfree + 8 * vs.slot, vs.phase ^ 1u)) {
-            ok = false;
-            break;
-          }
-          expect_tx(vfull + 8 * vs.slot, OPER);
-          tma_load_2d(base + S_V + vs.slot * OPER, &v_map, 0, (int)((r * 4 + q) * 128), vfull + 8 * vs.slot);
-          vs.next(S_NV);
-        }
-        if (++r == R) r = 0;
-      }
-      if (!ok) fail_status();
-      drain_ring(vfull, vs, g, S_NV);   // the copies in flight land before shared memory is released
-    }
-  } else if (warp == 10) {
-    // ---- C(j) of every tile the range touches (after the MMAs of the previous tile's items), E with the first
-    if (lane == 0) {
-      const int jl = N > 0 ? (int)((i1 - 1) / R) : j0 - 1;
-      int loads = 0;
-      bool ok = true;
-      for (int j = j0; j <= jl; ++j, ++loads) {
-        if (loads >= 1 && !wait_bar(cfree, (uint32_t)((loads - 1) & 1))) {
-          ok = false;
-          break;
-        }
-        expect_tx(cfull, 4 * OPER + (loads == 0 ? OPER : 0u));
-        for (int p = 0; p < 4; ++p) tma_load_2d(base + S_C + p * OPER, &c_map, 0, (j * 4 + p) * 128, cfull);
-        if (loads == 0) tma_load_2d(base + S_E, &c_map, 0, JT * 4 * 128, cfull);
-      }
-      if (!ok) fail_status();
-      if (loads > 0) wait_bar(cfull, (uint32_t)((loads - 1) & 1));   // the last copies have landed
-    }
-  } else if (warp == 9) {
-    if (lane == 0) {
-      constexpr uint32_t ID = idesc(128, false);
-      const uint32_t chi = base + S_C, clo = chi + OPER, shi = chi + 2 * OPER, slo = chi + 3 * OPER, e = base + S_E;
-      Ring vs{0, 0}, ab{0, 0};
-      long long r = r0;
-      int j = j0, cl = 0;
-      bool ok = true, issued = false;
-      for (long long n = 0; n < N && ok; ++n) {
-        if (n == 0 || r == 0) {   // the first item, or the range has crossed into tile j: C(j) must be resident
-          if (n > 0) commit(cfree);
-          ok = wait_bar(cfull, (uint32_t)(cl & 1));
-          ++cl;
-          if (!ok) break;
-        }
-        if (n >= 2) {
-          ok = wait_bar(acce + 8 * ab.slot, ab.phase ^ 1u);
-          if (!ok) break;
-        }
-        const uint32_t d1 = tmem + ab.slot * 256, d2 = d1 + 128;
-        int vslot[4];
-        uint32_t vb[4];
-        for (int k = 0; k < 4; ++k) {
-          ok = wait_bar(vfull + 8 * vs.slot, vs.phase);
-          if (!ok) break;
-          fence_after();
-          vslot[k] = vs.slot;
-          vb[k] = base + S_V + vs.slot * OPER;
-          vs.next(S_NV);
-          issued = true;
-          if (k == 0) {          // D1 = cos . Vr: hi x hi, lo x hi
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
-              mma_ss(d1, sdesc(chi + 32 * ks), sdesc(vb[0] + 32 * ks), ID, ks ? 1u : 0u);
-              mma_ss(d1, sdesc(clo + 32 * ks), sdesc(vb[0] + 32 * ks), ID, 1);
-            }
-          } else if (k == 1) {   // hi x lo
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks) mma_ss(d1, sdesc(chi + 32 * ks), sdesc(vb[1] + 32 * ks), ID, 1);
-          } else if (k == 2) {   // D2 = sin . Vi: hi x hi, lo x hi
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
-              mma_ss(d2, sdesc(shi + 32 * ks), sdesc(vb[2] + 32 * ks), ID, ks ? 1u : 0u);
-              mma_ss(d2, sdesc(slo + 32 * ks), sdesc(vb[2] + 32 * ks), ID, 1);
-            }
-          } else {               // hi x lo; tile 0 adds row 0's (-1)^qc . Vr (column nx/2)
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks) mma_ss(d2, sdesc(shi + 32 * ks), sdesc(vb[3] + 32 * ks), ID, 1);
-            if (j == 0) {
-#pragma unroll
-              for (int ks = 0; ks < 4; ++ks) {
-                mma_ss(d2, sdesc(e + 32 * ks), sdesc(vb[0] + 32 * ks), ID, 1);
-                mma_ss(d2, sdesc(e + 32 * ks), sdesc(vb[1] + 32 * ks), ID, 1);
-              }
-            }
-          }
-        }
-        if (!ok) break;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) commit(vfree + 8 * vslot[k]);
-        commit(accf + 8 * ab.slot);
-        ab.next(2);
-        if (++r == R) {
-          r = 0;
-          ++j;
-        }
-      }
-      if (!ok) fail_status();
-      if (issued) {   // every MMA issued has finished before tensor and shared memory are released
-        commit(fin);
-        wait_bar(fin, 0);
-      }
-    }
-  } else if (warp < 8) {
-    // ---- warps 0-7: lanes = x of this warp's quarter, columns = y (warps 0-3 rows 0-63, 4-7 rows 64-127)
-    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
-    const int half = warp >> 2;
-    Ring ab{0, 0};
-    long long r = r0;
-    int j = j0;
-    bool ok = true;
-    for (long long n = 0; n < N && ok; ++n) {
-      ok = warp_wait(accf + 8 * ab.slot, ab.phase);
-      if (!ok) break;
-      fence_after();
-      const int x = 128 * j + 32 * (warp & 3) + lane;
-      const bool edge = x == 0;   // columns 0 (D1) and nx/2 (D2) instead of a mirror pair
-      const int xm = edge ? a.nx / 2 : a.nx - x;
-      float* row0 = a.out + (r * 128 + 64 * half) * (long long)a.nx;
-      const uint32_t t1 = tmem + lane_base + ab.slot * 256 + 64 * half, t2 = t1 + 128;
-#pragma unroll 1
-      for (int p = 0; p < 4; ++p) {
-        float s1[16], s2[16];
-        tmem_ld16x2(t1 + 16 * p, t2 + 16 * p, s1, s2);
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          float* dst = row0 + (long long)(16 * p + k) * a.nx;
-          __stcs(dst + x, edge ? s1[k] : s1[k] + s2[k]);
-          __stcs(dst + xm, edge ? s2[k] : s1[k] - s2[k]);
-        }
-      }
-      fence_before();
-      __syncwarp();
-      if (lane == 0) arrive(acce + 8 * ab.slot);
-      ab.next(2);
-      if (++r == R) {
-        r = 0;
-        ++j;
-      }
-    }
-    if (!ok && lane == 0) fail_status();
-  }
-  fence_before();
-  __syncthreads();
-  if (warp == 0) {
-    fence_after();
-    tmem_dealloc(tmem, 512);
-  }
-}
-
 // --------------------------------------------------------------------------------- constant images
 // Forward: for each 64-column chunk c, W rows n < nb: cos(2 pi (m0c+n) x / nx), rows nb+n: sin(...) (n < bc;
 // zero rows above), K = x = 64c .. 64c+63; [hi | lo], 2 (2 nb) 128 bytes per chunk.  nb = 64, or 32 for the
@@ -926,46 +692,6 @@ __global__ void rows_inv_consts_kernel(int nx, int bc, unsigned char* img) {
   *(uint4*)(o + 2 * OPER) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
 }
 
-// Symmetric inverse (nx a multiple of 256): for each 128-column x tile j of [0, nx/2), rows x = 128 j + row,
-// K = qc = 0 .. 63: [cos hi | cos lo | sin hi | sin lo] of 2 pi qc x / nx (zero for qc >= bc); after the tiles one
-// block E: row 0 = (-1)^qc (qc < bc), every other row zero (bf16 hi; its lo part is zero).
-__global__ void rows_inv_sym_consts_kernel(int nx, int bc, unsigned char* img) {
-  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int nt = nx / 256;
-  if (id >= (long long)nt * 2048 + 1024) return;
-  if (id >= (long long)nt * 2048) {   // E
-    const int e = (int)(id - (long long)nt * 2048), row = e / 8, q = e % 8;
-    float v[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int qc = 8 * q + k;
-      v[k] = (row == 0 && qc < bc) ? ((qc & 1) ? -1.0f : 1.0f) : 0.0f;
-    }
-    uint32_t hi[4], lo[4];
-    split8(v, hi, lo);
-    *(uint4*)(img + (long long)nt * 4 * OPER + swz(row, q)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-    return;
-  }
-  const int j = (int)(id / 2048), t = (int)((id / 1024) % 2), row = (int)((id / 8) % 128), q = (int)(id % 8);
-  const long long x = 128LL * j + row;
-  float v[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int qc = 8 * q + k;
-    double sn = 0.0, co = 0.0;
-    if (qc < bc) {
-      const long long p = ((long long)qc * x) % nx;
-      sincospi(2.0 * (double)p / (double)nx, &sn, &co);
-    }
-    v[k] = (float)(t == 0 ? co : sn);
-  }
-  uint32_t hi[4], lo[4];
-  split8(v, hi, lo);
-  unsigned char* o = img + (long long)j * 4 * OPER + 2 * t * OPER + swz(row, q);
-  *(uint4*)o = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-  *(uint4*)(o + OPER) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-}
-
 }  // namespace rt
 }  // namespace oi
 
@@ -977,21 +703,13 @@ extern "C" int oi_rows_tc_constants(int which, int nx, int m0c, int bc, void* im
   // which 2: the Hermitian half of the symmetric band of width bc (m0c = -(bc-1)/2): columns 0 .. (bc-1)/2
   if (which == 2 && (bc % 2 == 0 || m0c != -(bc - 1) / 2 || (bc + 1) / 2 > 32))
     return fail(OI_ERANGE, "oi_rows_tc_constants: band %d at %d is not symmetric of width <= 63", bc, m0c);
-  // which 1 with nx a multiple of 256: the image of the mirror-symmetric synthesis (rows_inv_sym_kernel), which
-  // the synthesis uses for such nx; it is smaller than the direct pass's, so the same byte count covers both
-  const bool sym = which == 1 && nx % 256 == 0;
   const long long need = which == 0 ? (long long)(nx / 64) * 2 * rt::OPER
-                         : which == 2 ? (long long)(nx / 64) * rt::OPER
-                         : sym ? (long long)(nx / 256) * 4 * rt::OPER + rt::OPER : (long long)(nx / 128) * 4 * rt::OPER;
-  const long long room = which == 1 ? (long long)(nx / 128) * 4 * rt::OPER : need;
-  if (bytes < room) return fail(OI_ERANGE, "oi_rows_tc_constants: %lld bytes given, %lld needed", bytes, room);
+                         : which == 2 ? (long long)(nx / 64) * rt::OPER : (long long)(nx / 128) * 4 * rt::OPER;
+  if (bytes < need) return fail(OI_ERANGE, "oi_rows_tc_constants: %lld bytes given, %lld needed", bytes, need);
   if ((uintptr_t)image % 16) return fail(OI_EINVAL, "oi_rows_tc_constants: image not 16-byte aligned");
   const long long threads = need / 16 / 2;
   cudaStream_t s = (cudaStream_t)stream;
-  if (sym) {
-    const long long th = (long long)(nx / 256) * 2048 + 1024;
-    rt::rows_inv_sym_consts_kernel<<<(unsigned)ceil_div(th, 256), 256, 0, s>>>(nx, bc, (unsigned char*)image);
-  } else if (which == 0)
+  if (which == 0)
     rt::rows_fwd_consts_kernel<<<(unsigned)ceil_div(threads, 256), 256, 0, s>>>(nx, m0c, bc, 64, (unsigned char*)image);
   else if (which == 2)
     rt::rows_fwd_consts_kernel<<<(unsigned)ceil_div(threads, 256), 256, 0, s>>>(nx, 0, (bc + 1) / 2, 32,
@@ -1065,19 +783,6 @@ int rows_inv_from_tiles(const void* vtiles, int count, int ny, int nx, const voi
   const int sms = rt::sm_count();
   if (!sms) return fail(OI_ECUDA, "oi_rows_inv_tc: no CUDA device");
   if ((R + 1) * 512 > 0x7fffffffLL) return fail(OI_ERANGE, "oi_rows_inv_tc: %lld rows exceed the tensor-map range", rows);
-  if (nx % 256 == 0) {   // mirror-symmetric pass over half of each row (constants of the symmetric layout)
-    const long long sitems = R * (nx / 256), ctas = sitems < sms ? sitems : sms;
-    rt::SymArgs a{rows, nx, out};
-    CUtensorMap c_map, v_map;
-    int rc = rt::encode_2d(&c_map, CU_TENSOR_MAP_DATA_TYPE_UINT16, consts, 64,
-                           (unsigned long long)((nx / 256) * 4 + 1) * 128, 128, 64, 128);
-    if (!rc) rc = rt::encode_2d(&v_map, CU_TENSOR_MAP_DATA_TYPE_UINT16, vtiles, 64, (unsigned long long)R * 512, 128, 64, 128);
-    if (!rc) rc = ensure_smem((const void*)rt::rows_inv_sym_kernel, rt::S_SMEM, "oi_rows_inv_tc");
-    if (rc) return rc;
-    (void)launch_pdl(rt::rows_inv_sym_kernel, dim3((unsigned)ctas), dim3(rt::I_NT), rt::S_SMEM, s, a, c_map, v_map);
-    oi::note_launch();
-    return check_launch("oi_rows_inv_tc");
-  }
   const long long ctas = items < sms ? items : sms;
   rt::InvArgs a{(const unsigned char*)vtiles, rows, ny, nx, (const unsigned char*)consts, out};
   CUtensorMap c_map, v_map;   // [rows of 128 bytes] of the constant image and of the V tiles

@@ -19,7 +19,9 @@
 //
 // Roles (320 threads): warps 0-7 convert (fold, U transpose, V drain; two warps per tensor-memory lane
 // quarter), warp 8 streams the constant pieces (2-D tensor-map boxes, no multicast), warp 9 lane 0 issues the
-// MMAs.  Every mbarrier wait is bounded (2 s); on expiry the role records the device status and stops, the
+// MMAs.  A V tile is staged in shared memory in its final (swizzled operand) layout -- in the stage-1 A region,
+// free while the item's tiles drain -- and leaves as bulk copies issued by warp 0 lane 0: written straight from
+// registers, each lane's 16-byte pieces of one row would touch 32 lines per warp store.  Every mbarrier wait is bounded (2 s); on expiry the role records the device status and stops, the
 // producer waits for its copies in flight and the MMA thread for its issued MMAs before memory is released.
 #include "tc_common.cuh"
 
@@ -118,9 +120,10 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
   // memory), b2full (stage-2 B written), b2free (the item's stage-2 MMAs finished), accf[2] / acce[2] (v tile
   // complete / drained), fin (every issued MMA finished, at the end), ustage (the U staging written by all eight
   // converter warps), uread (the staging read by all of them)
+  // vstaged (a V tile is staged by all eight converter warps), vsfree (its bulk copies have read the staging)
   const uint32_t rfull = misc, rfree = misc + 32, a1full = misc + 64, d1full = misc + 72, b2full = misc + 80,
                  b2free = misc + 88, accf = misc + 96, acce = misc + 112, fin = misc + 128, ustage = misc + 136,
-                 uread = misc + 144;
+                 uread = misc + 144, vstaged = misc + 152, vsfree = misc + 160;
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + MISC + 256);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int TY = a.ny / 128;                           // y tiles per image
@@ -147,6 +150,8 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
     mbar_init(fin, 1);
     mbar_init(ustage, 8);
     mbar_init(uread, 8);
+    mbar_init(vstaged, 8);
+    mbar_init(vsfree, 1);
     mbar_init_fence();
   }
   fence_before();
@@ -277,9 +282,14 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
     const int half = warp >> 2, row = 32 * (warp & 3) + lane;
     Ring ab{0, 0};
     bool ok = true;
+    uint32_t vt = 0;   // V tiles staged
     for (int n = 0; n < NI && ok; ++n) {
       const long long it = i0 + n, img = it / H;
       const int grp = (int)(it % H), t0 = grp * a.tp, t1 = min(TY, t0 + a.tp);
+      if (vt >= 1) {   // the previous item's last V tile has left the staging (the stage-1 A region)
+        ok = warp_wait(vsfree, (vt - 1) & 1u);
+        if (!ok) break;
+      }
       fold(a, img, tid, a1);
       fence_async_smem();
       fence_before();
@@ -332,7 +342,7 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
       ok = warp_wait(uread, (uint32_t)(n & 1));      // every read of the staging is done before the next fold
       if (!ok) break;
       // V tiles: lane = y of the tile, this warp's half = re (blocks hi 0, lo 2) or im (hi 1, lo 3)
-      for (int t = t0; t < t1 && ok; ++t) {
+      for (int t = t0; t < t1 && ok; ++t, ++vt) {
         ok = warp_wait(accf + 8 * ab.slot, ab.phase);
         if (!ok) break;
         fence_after();
@@ -342,7 +352,10 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
         fence_before();
         __syncwarp();
         if (lane == 0) arrive(acce + 8 * ab.slot);
-        unsigned char* tile = a.tiles + (img * TY + t) * (long long)(4 * OPER);
+        if (vt >= 1 && t > t0) {   // the previous tile's copies have read the staging
+          ok = warp_wait(vsfree, (vt - 1) & 1u);
+          if (!ok) break;
+        }
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const float* src = q < 4 ? v0 + 8 * q : v1 + 8 * (q - 4);
@@ -350,12 +363,28 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
 #pragma unroll
           for (int e = 0; e < 4; ++e) split2(src[2 * e], src[2 * e + 1], hi[e], lo[e]);
           const uint32_t o = swz(row, q);
-          *(uint4*)(tile + half * OPER + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-          *(uint4*)(tile + (2 + half) * OPER + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+          *(uint4*)(a1 + half * OPER + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+          *(uint4*)(a1 + (2 + half) * OPER + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
         }
+        fence_async_smem();   // visible to the bulk copies
+        __syncwarp();
+        if (lane == 0) arrive(vstaged);
+        if (tid == 0) {
+          ok = wait_bar(vstaged, vt & 1u);
+          if (ok) {
+            unsigned char* tile = a.tiles + (img * TY + t) * (long long)(4 * OPER);
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bulk_s2g(tile + b * OPER, base + A1_OFF + b * OPER, OPER);
+            bulk_commit();
+            bulk_wait_read();
+            arrive(vsfree);
+          }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
         ab.next(2);
       }
     }
+    if (tid == 0) bulk_wait_all();   // the V tiles are written before the CTA exits
     if (!ok && lane == 0) fail_status();
   }
   fence_before();

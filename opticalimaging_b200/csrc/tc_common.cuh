@@ -252,6 +252,17 @@ typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, v
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+// A 1-D bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from shared to global memory, in
+// the issuing thread's bulk async-group.
+__device__ __forceinline__ void bulk_s2g(void* dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// the issuing thread's bulk groups have finished reading shared memory / have completed
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // A 2-D tensor map (dim0 contiguous, rows `stride1` bytes apart) with a box0 x box1 box, no swizzle.
 inline int encode_2d(CUtensorMap* map, CUtensorMapDataType type, const void* base, unsigned long long dim0,
                      unsigned long long dim1, unsigned long long stride1, unsigned box0, unsigned box1,

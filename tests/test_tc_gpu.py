@@ -173,10 +173,9 @@ def test_tc_row_passes_vs_fft(oi, ny, nx, band):
                                             (3, 384, 384, 21), (64, 1024, 1024, 59), (2, 256, 512, 64)])
 def test_rows_inv_tc_direct(oi, count, ny, nx, bc):
     """The inverse tensor-core row pass through the C ABI against an FP64 evaluation of
-    out[i][y][x] = sum_qc Re(v[i][qc][y] exp(-2 pi i qc x / nx)).  For nx a multiple of 256 the mirror-symmetric
-    pass runs (one item, ranges crossing x tiles, the 64-clip benchmark shape, a full 64-column band); nx = 384
-    takes the direct pass (an odd number of 128-row blocks, the last pair half empty).  Columns 0 and nx/2 are
-    checked on their own: the symmetric pass writes them from its edge lane."""
+    out[i][y][x] = sum_qc Re(v[i][qc][y] exp(-2 pi i qc x / nx)): one item, ranges crossing x tiles and images,
+    the 64-clip benchmark shape, a full 64-column band, nx = 384 and odd numbers of 128-row blocks (the last pair
+    half empty); columns 0, nx/2 and nx - 1 checked on their own."""
     from opticalimaging_b200 import _native as N
     dev = torch.device('cuda')
     g = torch.Generator().manual_seed(count * ny + nx)
