@@ -183,17 +183,24 @@ class Server:
     def _group_key(self, r: Request):
         return (r.spec.key, r.mask.dtype)
 
-    def _max_batch(self, spec: ModelSpec) -> int:
+    def _max_batch(self, spec: ModelSpec, backlog: int = 0) -> int:
         b = max(1, min(self.max_batch, self.max_batch_pixels // spec.pixels, self.ex.max_batch(spec)))
         if self.latency_budget is not None:
             per = getattr(self.ex, 'time_per_image', None)
             t = per(spec) if per is not None else None
             if t:
-                b = max(1, min(b, int(self.latency_budget / (self.ex.nslots * t))))
+                cap = max(1, min(b, int(self.latency_budget / (self.ex.nslots * t))))
+                # A backlog that the slots cannot clear at the capped size within the budget is late already:
+                # it is taken in batches that drain it (larger batches spread the per-batch costs), so that
+                # overload is absorbed at full throughput while light load keeps the capped latency.
+                if backlog > cap * self.ex.nslots:
+                    return max(cap, min(b, -(-backlog // self.ex.nslots)))
+                return cap
         return b
 
     def batch_limit(self, spec: ModelSpec) -> int:
-        """The largest batch this server forms for `spec` (by max_batch and max_batch_pixels)."""
+        """The largest batch this server forms for `spec` under light load (by max_batch, max_batch_pixels and
+        the latency budget); a backlog beyond what the slots clear within the budget is taken in larger batches."""
         return self._max_batch(spec)
 
     def _run(self):
@@ -304,10 +311,9 @@ class Server:
                 done = True
         return done
 
-    def _take(self, key, spec):
+    def _take(self, key, limit):
         q = self._pending[key]
         batch = []
-        limit = self._max_batch(spec)
         while q and len(batch) < limit:
             r = q.popleft()
             if r.future.set_running_or_notify_cancel():
@@ -342,7 +348,8 @@ class Server:
                 del self._pending[key]
                 continue
             spec = self._pending[key][0].spec
-            n = min(len(self._pending[key]), self._max_batch(spec))
+            limit = self._max_batch(spec, len(self._pending[key]))
+            n = min(len(self._pending[key]), limit)
             if not self._fits(spec, n):
                 if all(s is None for s in self._slots):     # nothing will free memory: refuse the group
                     err = MemoryError(f'model {spec.key!r} with a batch of {n} needs '
@@ -354,7 +361,7 @@ class Server:
                             self.rejected += 1
                     continue
                 break                                          # wait for an in-flight batch to free memory
-            batch = self._take(key, spec)
+            batch = self._take(key, limit)
             if not batch:
                 continue
             slot = free[0]
