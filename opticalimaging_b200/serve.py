@@ -191,10 +191,10 @@ class Server:
             if t:
                 cap = max(1, min(b, int(self.latency_budget / (self.ex.nslots * t))))
                 # A backlog that the slots cannot clear at the capped size within the budget is late already:
-                # it is taken in batches that drain it (larger batches spread the per-batch costs), so that
+                # it is taken whole (up to the executor's limit), since larger batches spread the per-batch costs;
                 # overload is absorbed at full throughput while light load keeps the capped latency.
                 if backlog > cap * self.ex.nslots:
-                    return max(cap, min(b, -(-backlog // self.ex.nslots)))
+                    return max(cap, min(b, backlog))
                 return cap
         return b
 
@@ -516,7 +516,10 @@ class CudaExecutor:
                 graph.replay()
                 z.record(s)
                 z.synchronize()
-                self._device_tpi[spec.key] = max(self._device_tpi.get(spec.key, 0.0), a.elapsed_time(z) / 1e3 / b)
+                # the steady per-image cost: the least over the timed buckets (a small batch's time is mostly
+                # the step's fixed part)
+                t = a.elapsed_time(z) / 1e3 / b
+                self._device_tpi[spec.key] = min(self._device_tpi.get(spec.key, t), t)
         return g[0]
 
     def prepare(self, spec, dtype=torch.uint8, max_batch: int | None = None):
