@@ -191,10 +191,11 @@ class Server:
             if t:
                 cap = max(1, min(b, int(self.latency_budget / (self.ex.nslots * t))))
                 # A backlog that the slots cannot clear at the capped size within the budget is late already:
-                # it is taken whole (up to the executor's limit), since larger batches spread the per-batch costs;
-                # overload is absorbed at full throughput while light load keeps the capped latency.
+                # it is shared out over the slots (larger batches spread the per-batch costs), so overload is
+                # absorbed at close to full throughput while light load keeps the capped latency.  Taking the whole
+                # backlog instead made a burst at 70 % load cascade: each long batch let a longer queue build.
                 if backlog > cap * self.ex.nslots:
-                    return max(cap, min(b, backlog))
+                    return max(cap, min(b, -(-backlog // self.ex.nslots)))
                 return cap
         return b
 

@@ -268,14 +268,14 @@ class TimedExecutor(FakeExecutor):
 
 def test_latency_budget_caps_batches():
     """With a latency budget, batches are capped at budget / (slots x time per image) while the backlog is within
-    what the slots clear at that size; a larger backlog is taken whole (up to the executor's limit); without a
-    budget batches fill."""
+    what the slots clear at that size; a larger backlog is shared out over the slots (up to the executor's limit);
+    without a budget batches fill."""
     a = spec('a')
     ex = TimedExecutor(tpi=1e-4, nslots=2, delay=0.02)
     srv = Server(ex, hbm_budget=1e9, max_batch=64, latency_budget_ms=2.0)
     assert srv.batch_limit(a) == 10                       # 2 ms / (2 slots x 0.1 ms)
     assert srv._max_batch(a, backlog=20) == 10            # the slots clear 2 x 10 within the budget
-    assert srv._max_batch(a, backlog=60) == 60            # 60 queued: late already, taken whole
+    assert srv._max_batch(a, backlog=60) == 30            # 60 queued: late already, shared over the two slots
     assert srv._max_batch(a, backlog=500) == 64           # the executor's limit
     for _ in range(12):                                   # light load: one request at a time
         srv.submit(a, torch.ones(4, 4)).result(timeout=10)
