@@ -221,6 +221,7 @@ def serve_measure(sk, info, masks_np, dev, args, latency_budget_ms=None):
     ring = list(torch.empty((nreq, 1, N_PIX, N_PIX), dtype=torch.float32).pin_memory())
     ex = serve.CudaExecutor(device=dev, nslots=3)
     srv = serve.Server(ex, hbm_budget=150e9, max_batch=BATCH, latency_budget_ms=latency_budget_ms)
+    ex.prepare(spec, torch.uint8, srv.batch_ceiling(spec))   # every bucket's graph before any timing
 
     def closed_loop(n):
         q = collections.deque()
@@ -314,7 +315,7 @@ def serve_mix(dev, args, state):
 
     # every model built and the graph of every batch bucket captured before any timing; then a short warm-up
     for sp in specs.values():
-        ex.prepare(sp, torch.uint8, srv.batch_limit(sp))
+        ex.prepare(sp, torch.uint8, srv.batch_ceiling(sp))
     futs = [submit(k, n, i) for k, n, i in stream[:min(len(stream), 300)]]
     for f in futs:
         f.result()

@@ -204,6 +204,11 @@ class Server:
         the latency budget); a backlog beyond what the slots clear within the budget is taken in larger batches."""
         return self._max_batch(spec)
 
+    def batch_ceiling(self, spec: ModelSpec) -> int:
+        """The largest batch this server ever forms for `spec` (under any backlog): the size up to which an
+        executor's graphs should be prepared."""
+        return self._max_batch(spec, backlog=1 << 30)
+
     def _run(self):
         try:
             self._loop()
@@ -506,7 +511,8 @@ class CudaExecutor:
             torch.cuda.synchronize(self.device)
             free0 = torch.cuda.mem_get_info(self.device)[0]
             graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(graph, stream=s):
+            # thread-local capture: client threads may allocate pinned memory or copy while a bucket is captured
+            with torch.cuda.graph(graph, stream=s, capture_error_mode='thread_local'):
                 model.image(d_in[:b], out=d_out[:b])
             used = max(0, free0 - torch.cuda.mem_get_info(self.device)[0])
             g = self.graphs[gk] = (graph, used)

@@ -277,6 +277,7 @@ def test_latency_budget_caps_batches():
     assert srv._max_batch(a, backlog=20) == 10            # the slots clear 2 x 10 within the budget
     assert srv._max_batch(a, backlog=60) == 30            # 60 queued: late already, shared over the two slots
     assert srv._max_batch(a, backlog=500) == 64           # the executor's limit
+    assert srv.batch_ceiling(a) == 64                     # what an executor prepares graphs up to
     for _ in range(12):                                   # light load: one request at a time
         srv.submit(a, torch.ones(4, 4)).result(timeout=10)
     assert max(n for _, n in ex.launched) == 1
