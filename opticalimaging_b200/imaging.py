@@ -93,6 +93,8 @@ class _HostStage:
     def to_device(self, host: torch.Tensor, dev) -> torch.Tensor:
         flat = host.contiguous().view(torch.uint8).reshape(-1)
         out = torch.empty(flat.numel(), dtype=torch.uint8, device=dev)
+        # the host-side copies move 8-byte words (a byte-typed copy runs element by element, at a few GB/s)
+        word = torch.int64 if flat.numel() % 8 == 0 else torch.uint8
         with self.lock:
             if self.bufs is None:
                 self.bufs = [torch.empty(self.CHUNK, dtype=torch.uint8).pin_memory() for _ in range(2)]
@@ -103,7 +105,7 @@ class _HostStage:
                 i = k & 1
                 if self.events[i] is not None:
                     self.events[i].synchronize()          # the buffer's previous chunk has left for the device
-                self.bufs[i][:b - a].copy_(flat[a:b])
+                self.bufs[i][:b - a].view(word).copy_(flat[a:b].view(word))
                 out[a:b].copy_(self.bufs[i][:b - a], non_blocking=True)
                 self.events[i] = torch.cuda.Event()
                 self.events[i].record(stream)
@@ -178,41 +180,68 @@ def _result_device(scatter):
     return h.device if isinstance(h, torch.Tensor) else torch.device('cpu')
 
 
+_PUPIL_GEOMETRY: dict = {}   # (grid, pupil radius in frequencies, device) -> what _pupil_image needs of it
+
+
+def _pupil_geometry(ny, nx, f, g, npx, npy, dev):
+    """The grid-dependent part of PupilImage, built once per grid and pupil: the crop band (or the full band and
+    the reference's slices when the crop leaves the grid), the centring phase on it and the mask of the samples
+    outside the unit disc, on the device."""
+    key = (ny, nx, float(npx), float(npy), str(dev))
+    geo = _PUPIL_GEOMETRY.get(key)
+    if geo is None:
+        ox, oy = int(npx) + 3, int(npy) + 3
+        r0, c0 = ny // 2 - oy, nx // 2 - ox
+        sl = None
+        if r0 >= 0 and c0 >= 0 and ny // 2 + oy <= ny and nx // 2 + ox <= nx:
+            band = Band(r0 - ny // 2, 2 * oy, c0 - nx // 2, 2 * ox)
+            fm, gm = torch.meshgrid(g[r0:r0 + 2 * oy], f[c0:c0 + 2 * ox], indexing='ij')
+        else:   # crop window leaves the grid: Python slicing of the full spectrum, as the reference does
+            band = Band(-(ny // 2), ny, -(nx // 2), nx)
+            fm, gm = torch.meshgrid(g, f, indexing='ij')
+            sl = (slice(ny // 2 - oy, ny // 2 + oy), slice(nx // 2 - ox, nx // 2 + ox))
+            fm, gm = fm[sl], gm[sl]
+        outside = (fm ** 2 + gm ** 2 > 1).to(dev)
+        if len(_PUPIL_GEOMETRY) >= 64:
+            _PUPIL_GEOMETRY.clear()
+        geo = _PUPIL_GEOMETRY[key] = (band, _centring_phase(ny, nx, band).to(dev), outside, sl)
+    return geo
+
+
 def _pupil_image(scatter, projector, source, h, dev):
     """PupilImage of Scatter.CalculateSpectrum (Scatter.py:22-33): the cropped centred spectrum, NaN outside
     the unit disc."""
     ny, nx = h.shape[0], h.shape[1]
     f, g, npx, npy = _axes(scatter, projector, source)
-    ox, oy = int(npx) + 3, int(npy) + 3
-    r0, c0 = ny // 2 - oy, nx // 2 - ox
-    if r0 >= 0 and c0 >= 0 and ny // 2 + oy <= ny and nx // 2 + ox <= nx:
-        band = Band(r0 - ny // 2, 2 * oy, c0 - nx // 2, 2 * ox)
-        hk = _spectrum_band(h, band, npx * npy, dev)
-        fm, gm = torch.meshgrid(g[r0:r0 + 2 * oy], f[c0:c0 + 2 * ox], indexing='ij')
-    else:   # crop window leaves the grid: Python slicing of the full spectrum, as the reference does
-        hk = _spectrum_band(h, Band(-(ny // 2), ny, -(nx // 2), nx), npx * npy, dev)
-        fm, gm = torch.meshgrid(g, f, indexing='ij')
-        sl = (slice(ny // 2 - oy, ny // 2 + oy), slice(nx // 2 - ox, nx // 2 + ox))
-        hk, fm, gm = hk[sl], fm[sl], gm[sl]
-    out = hk.clone()
-    out[(fm ** 2 + gm ** 2 > 1).to(out.device)] = float('nan')
-    return out
+    band, ph, outside, sl = _pupil_geometry(ny, nx, f, g, npx, npy, dev)
+    hk = _spectrum_band(h, band, npx * npy, dev, ph)
+    if sl is not None:
+        hk = hk[sl]
+    return hk.masked_fill(outside[:, :, None], float('nan'))
 
 
-def _spectrum_band(h, band: Band, scale, dev):
+def _centring_phase(ny, nx, band: Band) -> torch.Tensor:
+    """exp(-2 pi i m (N//2)/N) per axis on `band`: [br, bc] complex64 (host)."""
+    mr = torch.arange(band.m0r, band.m0r + band.br, dtype=torch.float64)
+    mc = torch.arange(band.m0c, band.m0c + band.bc, dtype=torch.float64)
+    ph = torch.exp(-2j * torch.pi * ((mr * (ny // 2) % ny / ny)[:, None] + (mc * (nx // 2) % nx / nx)[None, :]))
+    return ph.to(torch.complex64)
+
+
+def _spectrum_band(h, band: Band, scale, dev, ph: torch.Tensor | None = None):
     """Centred spectrum Hk on `band` of a [Ny, Nx, C] complex64 device field -> [br, bc, C].
 
     The engine's band spectrum has its origin at pixel 0; the reference's centred spectrum has it at pixel
-    N//2 (ifftshift before the transform, Scatter.py:20), i.e. an extra phase exp(-2 pi i m (N//2)/N) per axis.
-    The phase cancels in every intensity, so only the spectrum outputs apply it.
+    N//2 (ifftshift before the transform, Scatter.py:20), i.e. an extra phase exp(-2 pi i m (N//2)/N) per axis
+    (`ph`, [br, bc] on the device, when the caller holds it).  The phase cancels in every intensity, so only the
+    spectrum outputs apply it.
     """
     ny, nx, nch = h.shape
     plan = Plan.get(ny, nx, band, dev)
     c = band_spectrum(h.unsqueeze(0), N.FIELD_COMPLEX_C64, plan, nch=nch, scale=scale)
-    mr = torch.arange(band.m0r, band.m0r + band.br, dtype=torch.float64)
-    mc = torch.arange(band.m0c, band.m0c + band.bc, dtype=torch.float64)
-    ph = torch.exp(-2j * torch.pi * ((mr * (ny // 2) % ny / ny)[:, None] + (mc * (nx // 2) % nx / nx)[None, :]))
-    return c[0].permute(1, 2, 0) * ph.to(dev, torch.complex64)[:, :, None]
+    if ph is None:
+        ph = _centring_phase(ny, nx, band).to(dev)
+    return c[0].permute(1, 2, 0) * ph[:, :, None]
 
 
 def calculate_spectrum(scatter, projector, source):
