@@ -11,15 +11,18 @@
 // taken first: over a symmetric qr range it is a real Dirichlet kernel in (sr / M - y / ny).
 //
 // Items are (image, group of TP consecutive 128-row y tiles), one contiguous range per CTA.  Per item the
-// converter warps fold the partial sums into the A operand of stage 1 (bf16 hi / lo, shared memory), one lane
-// issues the 24 MMAs of U = c G^T (M = 128 sr, N = 128 n, K = 128 sc), the converters move U through shared
-// memory (fp32, padded rows) into the B operand of stage 2 (U^T, K = sr), and per y tile 24 MMAs give
+// converter warps fold the partial sums into the B operand of stage 1 (bf16 hi / lo, shared memory), one lane
+// issues the 24 MMAs of U^T = G^T c^T (M = 128 n, N = 128 sr, K = 128 sc), the converters turn each tensor-memory
+// lane (a row n of U^T) into the B operand of stage 2 (K = sr) in place, and per y tile 24 MMAs give
 // v = A U (M = 128 y, N = 128, K = 128 sr), drained from tensor memory as the V tile's bf16 hi / lo blocks.  The
-// constant operands (G, then the A tile of each y tile) stream through a ring of 16 KB pieces.
+// constant operands (G, then the A tile of each y tile) stream through a ring of 16 KB pieces, 1.5 tiles deep,
+// each piece released as soon as the MMAs reading it finish.  Per y tile a CTA moves the A tile's 64 KB in and
+// the V tile's 64 KB out over its path to L2 (about 24 bytes per cycle for both together, measured: ~2.7 us
+// per tile with the stores, ~1.5 us without them), which bounds the pass.
 //
 // Roles (320 threads): warps 0-7 convert (fold, U transpose, V drain; two warps per tensor-memory lane
 // quarter), warp 8 streams the constant pieces (2-D tensor-map boxes, no multicast), warp 9 lane 0 issues the
-// MMAs.  A V tile is staged in shared memory in its final (swizzled operand) layout -- in the stage-1 A region,
+// MMAs.  A V tile is staged in shared memory in its final (swizzled operand) layout -- in the stage-1 B region,
 // free while the item's tiles drain -- and leaves as bulk copies issued by warp 0 lane 0: written straight from
 // registers, each lane's 16-byte pieces of one row would touch 32 lines per warp store.  Every mbarrier wait is bounded (2 s); on expiry the role records the device status and stops, the
 // producer waits for its copies in flight and the MMA thread for its issued MMAs before memory is released.
@@ -44,16 +47,14 @@ using namespace tc;
 
 constexpr int M = 128;                     // coarse grid per axis
 constexpr uint32_t OPER = 128 * 128;       // one [128 rows][64 bf16] swizzled operand block (16 KB)
-constexpr int NR = 4;                      // constant pieces in the ring
+constexpr int NR = 6;                      // constant pieces in the ring (1.5 tiles: a tile's A loads overlap
+                                           // the previous tile's MMAs)
 constexpr int T = 320;                     // 8 converter warps, producer warp, MMA warp
-constexpr uint32_t UF_STRIDE = 129;        // floats per row of the fp32 U staging (conflict-free column reads)
 constexpr uint32_t R_OFF = 0;                            // ring of constant pieces
-constexpr uint32_t A1_OFF = NR * OPER;                   // stage-1 A (the folded coarse image), aliased by U staging
-constexpr uint32_t A1_BYTES = 66 * 1024;                 // >= 4 OPER and >= 128 * 129 * 4
-constexpr uint32_t B2_OFF = A1_OFF + A1_BYTES;           // stage-2 B (U^T)
+constexpr uint32_t A1_OFF = NR * OPER;                   // the folded coarse image (stage-1 B), later the V staging
+constexpr uint32_t B2_OFF = A1_OFF + 4 * OPER;           // stage-2 B (U^T)
 constexpr uint32_t MISC = B2_OFF + 4 * OPER;
 constexpr uint32_t SMEM = MISC + 512 + 1024;
-static_assert(A1_BYTES >= 4 * OPER && A1_BYTES >= M * UF_STRIDE * 4, "U staging");
 static_assert(A1_OFF % 1024 == 0 && B2_OFF % 1024 == 0, "operand alignment");
 static_assert(SMEM <= SMEM_LIMIT, "synthesis preparation: shared memory");
 
@@ -66,49 +67,8 @@ struct Args {
 
 __device__ __forceinline__ void fail_status() { atomicExch(&g_synth_status, 1); }
 
-// Converter warps' share of the fold: image `img`, 2048 tasks (row sr, 8-column chunk q16) over 256 threads,
-// partial sums added in order, written as the bf16 hi / lo stage-1 A operand (blocks [hi k0 | hi k1 | lo k0 |
-// lo k1], K = sc).
-__device__ __forceinline__ void fold(const Args& a, long long img, int tid, unsigned char* a1) {
-  const float* src = a.coarse + img * (long long)(M * M);
-  float4 acc[16];
-#pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const int task = tid + 256 * t, sr = task >> 4, q16 = task & 15;
-    const float4* p = (const float4*)(src + sr * M + 8 * q16);
-    acc[2 * t] = __ldg(p);
-    acc[2 * t + 1] = __ldg(p + 1);
-  }
-  for (int part = 1; part < a.nparts; ++part) {
-    float4 x[16];
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const int task = tid + 256 * t, sr = task >> 4, q16 = task & 15;
-      const float4* p = (const float4*)(src + part * a.part_stride + sr * M + 8 * q16);
-      x[2 * t] = __ldg(p);
-      x[2 * t + 1] = __ldg(p + 1);
-    }
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      acc[k].x += x[k].x;
-      acc[k].y += x[k].y;
-      acc[k].z += x[k].z;
-      acc[k].w += x[k].w;
-    }
-  }
-#pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const int task = tid + 256 * t, sr = task >> 4, q16 = task & 15, kb = q16 >> 3, q = q16 & 7;
-    uint32_t hi[4], lo[4];
-    split2(acc[2 * t].x, acc[2 * t].y, hi[0], lo[0]);
-    split2(acc[2 * t].z, acc[2 * t].w, hi[1], lo[1]);
-    split2(acc[2 * t + 1].x, acc[2 * t + 1].y, hi[2], lo[2]);
-    split2(acc[2 * t + 1].z, acc[2 * t + 1].w, hi[3], lo[3]);
-    const uint32_t o = swz(sr, q);
-    *(uint4*)(a1 + kb * OPER + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-    *(uint4*)(a1 + (2 + kb) * OPER + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-  }
-}
+// The k-th y tile of a CTA's group [t0, t1).
+__device__ __forceinline__ int tile_of(int t0, int, int k) { return t0 + k; }
 
 __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __grid_constant__ CUtensorMap k_map) {
   extern __shared__ unsigned char smem_raw[];
@@ -116,14 +76,14 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* gbase = smem_raw + (base - raw);
   const uint32_t misc = base + MISC;
-  // barriers: rfull[4] / rfree[4] (constant pieces), a1full (stage-1 A written), d1full (U complete in tensor
+  // barriers: rfull[6] / rfree[6] (constant pieces), a1full (stage-1 B written), d1full (U^T complete in tensor
   // memory), b2full (stage-2 B written), b2free (the item's stage-2 MMAs finished), accf[2] / acce[2] (v tile
-  // complete / drained), fin (every issued MMA finished, at the end), ustage (the U staging written by all eight
-  // converter warps), uread (the staging read by all of them)
+  // complete / drained), fin (every issued MMA finished, at the end)
   // vstaged (a V tile is staged by all eight converter warps), vsfree (its bulk copies have read the staging)
-  const uint32_t rfull = misc, rfree = misc + 32, a1full = misc + 64, d1full = misc + 72, b2full = misc + 80,
-                 b2free = misc + 88, accf = misc + 96, acce = misc + 112, fin = misc + 128, ustage = misc + 136,
-                 uread = misc + 144, vstaged = misc + 152, vsfree = misc + 160;
+  const uint32_t rfull = misc, rfree = misc + 8 * NR, a1full = misc + 16 * NR, d1full = a1full + 8, b2full = a1full + 16,
+                 b2free = a1full + 24, accf = a1full + 32, acce = a1full + 48, fin = a1full + 64, vstaged = a1full + 72,
+                 vsfree = a1full + 80;
+  static_assert(16 * NR + 88 <= 256, "synthesis preparation: barrier block");
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + MISC + 256);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int TY = a.ny / 128;                           // y tiles per image
@@ -148,8 +108,6 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
       mbar_init(acce + 8 * s, 8);
     }
     mbar_init(fin, 1);
-    mbar_init(ustage, 8);
-    mbar_init(uread, 8);
     mbar_init(vstaged, 8);
     mbar_init(vsfree, 1);
     mbar_init_fence();
@@ -169,7 +127,8 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
       bool ok = true;
       for (long long it = i0; it < i1 && ok; ++it) {
         const int grp = (int)(it % H), t0 = grp * a.tp, t1 = min(TY, t0 + a.tp);
-        for (int t = t0 - 1; t < t1 && ok; ++t) {   // t = t0 - 1 stands for G (blocks 0-3), then A_t (4 + 4t ..)
+        for (int k = -1; k < t1 - t0 && ok; ++k) {   // k = -1 stands for G (blocks 0-3), then A_t (4 + 4t ..)
+          const int t = k < 0 ? t0 - 1 : tile_of(t0, t1, k);
           for (int p = 0; p < 4; ++p, ++g) {
             if (g >= NR && !wait_bar(rfree + 8 * rs.slot, rs.phase ^ 1u)) {
               ok = false;
@@ -207,7 +166,8 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
         ok = wait_bar(a1full, (uint32_t)(n & 1));
         if (!ok) break;
         fence_after();
-        // stage 1: D1 = c G^T; pieces G hi k0, G hi k1, G lo k0, G lo k1
+        // stage 1: D1 = G^T c^T = U^T (lanes n, columns sr); pieces G hi k0, G hi k1, G lo k0, G lo k1 (A),
+        // the folded image (B)
         int sl[4];
         for (int p = 0; p < 4 && ok; ++p) {
           uint32_t gp = 0;
@@ -217,25 +177,26 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
           }
           issued = true;
           const int kb = p & 1;
-          const uint32_t ahi = a1 + kb * OPER, alo = a1 + (2 + kb) * OPER;
+          const uint32_t chi = a1 + kb * OPER, clo = a1 + (2 + kb) * OPER;
 #pragma unroll
           for (int ks = 0; ks < 4; ++ks) {
-            if (p < 2) {   // G hi: hi x hi, lo x hi
-              mma_ss(tmem, sdesc(ahi + 32 * ks), sdesc(gp + 32 * ks), ID, (p | ks) ? 1u : 0u);
-              mma_ss(tmem, sdesc(alo + 32 * ks), sdesc(gp + 32 * ks), ID, 1);
-            } else {       // G lo: hi x lo
-              mma_ss(tmem, sdesc(ahi + 32 * ks), sdesc(gp + 32 * ks), ID, 1);
+            if (p < 2) {   // G hi: hi x hi, hi x lo
+              mma_ss(tmem, sdesc(gp + 32 * ks), sdesc(chi + 32 * ks), ID, (p | ks) ? 1u : 0u);
+              mma_ss(tmem, sdesc(gp + 32 * ks), sdesc(clo + 32 * ks), ID, 1);
+            } else {       // G lo: lo x hi
+              mma_ss(tmem, sdesc(gp + 32 * ks), sdesc(chi + 32 * ks), ID, 1);
             }
           }
+          commit(rfree + 8 * sl[p]);   // the slot is refilled once these MMAs finish
         }
         if (!ok) break;
-        for (int p = 0; p < 4; ++p) commit(rfree + 8 * sl[p]);
         commit(d1full);
         ok = wait_bar(b2full, (uint32_t)(n & 1));
         if (!ok) break;
         fence_after();
         // stage 2, per y tile: D2[buf] = A_t U; pieces A hi k0, A hi k1, A lo k0, A lo k1; B = U^T (b2)
-        for (int t = t0; t < t1 && ok; ++t, ++m) {
+        for (int k = 0; k < t1 - t0 && ok; ++k, ++m) {
+          const int t = tile_of(t0, t1, k);
           if (m >= 2) {
             ok = wait_bar(acce + 8 * ab.slot, ab.phase ^ 1u);
             if (!ok) break;
@@ -258,9 +219,9 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
                 mma_ss(d2, sdesc(ap + 32 * ks), sdesc(bhi + 32 * ks), ID, 1);
               }
             }
+            commit(rfree + 8 * sl[p]);   // the slot is refilled once these MMAs finish (the next tile's piece)
           }
           if (!ok) break;
-          for (int p = 0; p < 4; ++p) commit(rfree + 8 * sl[p]);
           commit(accf + 8 * ab.slot);
           ab.next(2);
         }
@@ -274,10 +235,9 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
       }
     }
   } else {
-    // ---- warps 0-7: fold, U transpose, V drain
+    // ---- warps 0-7: fold, U^T conversion, V drain
     unsigned char* a1 = gbase + A1_OFF;
     unsigned char* b2 = gbase + B2_OFF;
-    float* uf = (float*)(gbase + A1_OFF);   // U staging, [128 sr][129]: aliases a1 once stage 1 has finished
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
     const int half = warp >> 2, row = 32 * (warp & 3) + lane;
     Ring ab{0, 0};
@@ -286,7 +246,7 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
     for (int n = 0; n < NI && ok; ++n) {
       const long long it = i0 + n, img = it / H;
       const int grp = (int)(it % H), t0 = grp * a.tp, t1 = min(TY, t0 + a.tp);
-      if (vt >= 1) {   // the previous item's last V tile has left the staging (the stage-1 A region)
+      if (vt >= 1) {   // the previous item's last V tile has left the staging (the stage-1 operand region)
         ok = warp_wait(vsfree, (vt - 1) & 1u);
         if (!ok) break;
       }
@@ -295,54 +255,36 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
       fence_before();
       __syncwarp();
       if (lane == 0) arrive(a1full);
-      // U from tensor memory (lane = sr, columns n of this warp's half) into the fp32 staging
       ok = warp_wait(d1full, (uint32_t)(n & 1));
       if (!ok) break;
       fence_after();
-      {
-        float u0[32], u1[32];
-        const uint32_t ta = tmem + lane_base + 64 * half;
-        tmem_ld32x2(ta, ta + 32, u0, u1);
-        float* dst = uf + row * UF_STRIDE + 64 * half;
-#pragma unroll
-        for (int k = 0; k < 32; ++k) dst[k] = u0[k];
-#pragma unroll
-        for (int k = 0; k < 32; ++k) dst[32 + k] = u1[k];
-      }
-      fence_before();
-      __syncwarp();
-      if (lane == 0) arrive(ustage);
-      ok = warp_wait(ustage, (uint32_t)(n & 1));     // the staging holds all of U
-      if (!ok) break;
       if (n >= 1) {                                  // the previous item's stage 2 no longer reads b2
         ok = warp_wait(b2free, (uint32_t)((n - 1) & 1));
         if (!ok) break;
       }
-      // B2 = U^T as bf16 hi / lo, K = sr: tasks (row nn, K block kb, chunk q)
-#pragma unroll 1
-      for (int t = 0; t < 8; ++t) {
-        const int task = tid + 256 * t, nn = task & 127, kq = task >> 7, kb = kq >> 3, q = kq & 7;
-        float v[8];
+      // B2 = U^T as bf16 hi / lo straight from tensor memory: lane = row n, this warp's half = K block (sr)
+      {
+        float u0[32], u1[32];
+        const uint32_t ta = tmem + lane_base + 64 * half;
+        tmem_ld32x2(ta, ta + 32, u0, u1);
 #pragma unroll
-        for (int e = 0; e < 8; ++e) v[e] = uf[(64 * kb + 8 * q + e) * UF_STRIDE + nn];
-        uint32_t hi[4], lo[4];
+        for (int q = 0; q < 8; ++q) {
+          const float* src = q < 4 ? u0 + 8 * q : u1 + 8 * (q - 4);
+          uint32_t hi[4], lo[4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) split2(v[2 * e], v[2 * e + 1], hi[e], lo[e]);
-        const uint32_t o = swz(nn, q);
-        *(uint4*)(b2 + kb * OPER + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-        *(uint4*)(b2 + (2 + kb) * OPER + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+          for (int e = 0; e < 4; ++e) split2(src[2 * e], src[2 * e + 1], hi[e], lo[e]);
+          const uint32_t o = swz(row, q);
+          *(uint4*)(b2 + half * OPER + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+          *(uint4*)(b2 + (2 + half) * OPER + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        }
       }
       fence_async_smem();
       fence_before();
       __syncwarp();
-      if (lane == 0) {
-        arrive(b2full);
-        arrive(uread);
-      }
-      ok = warp_wait(uread, (uint32_t)(n & 1));      // every read of the staging is done before the next fold
-      if (!ok) break;
+      if (lane == 0) arrive(b2full);
       // V tiles: lane = y of the tile, this warp's half = re (blocks hi 0, lo 2) or im (hi 1, lo 3)
-      for (int t = t0; t < t1 && ok; ++t, ++vt) {
+      for (int k = 0; k < t1 - t0 && ok; ++k, ++vt) {
+        const int t = tile_of(t0, t1, k);
         ok = warp_wait(accf + 8 * ab.slot, ab.phase);
         if (!ok) break;
         fence_after();
@@ -352,7 +294,7 @@ __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __gri
         fence_before();
         __syncwarp();
         if (lane == 0) arrive(acce + 8 * ab.slot);
-        if (vt >= 1 && t > t0) {   // the previous tile's copies have read the staging
+        if (vt >= 1 && k > 0) {   // the previous tile's copies have read the staging
           ok = warp_wait(vsfree, (vt - 1) & 1u);
           if (!ok) break;
         }
