@@ -70,6 +70,55 @@ __device__ __forceinline__ void fail_status() { atomicExch(&g_synth_status, 1); 
 // The k-th y tile of a CTA's group [t0, t1).
 __device__ __forceinline__ int tile_of(int t0, int, int k) { return t0 + k; }
 
+// Converter warps' share of the fold: image `img`, 2048 tasks (row sr, 8-column chunk q16) over 256 threads,
+// partial sums added in order, written as the bf16 hi / lo stage-1 B operand (blocks [hi k0 | hi k1 | lo k0 |
+// lo k1], K = sc).
+__device__ __forceinline__ void fold(const Args& a, long long img, int tid, unsigned char* a1) {
+  const float* src = a.coarse + img * (long long)(M * M);
+  float4 acc[16], x[16];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {   // the first two partial sums' loads in flight together
+    const int task = tid + 256 * t, sr = task >> 4, q16 = task & 15;
+    const float4* p = (const float4*)(src + sr * M + 8 * q16);
+    acc[2 * t] = __ldg(p);
+    acc[2 * t + 1] = __ldg(p + 1);
+    if (a.nparts > 1) {
+      x[2 * t] = __ldg(p + a.part_stride / 4);
+      x[2 * t + 1] = __ldg(p + a.part_stride / 4 + 1);
+    }
+  }
+  for (int part = 1; part < a.nparts; ++part) {
+    if (part > 1) {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int task = tid + 256 * t, sr = task >> 4, q16 = task & 15;
+        const float4* p = (const float4*)(src + part * a.part_stride + sr * M + 8 * q16);
+        x[2 * t] = __ldg(p);
+        x[2 * t + 1] = __ldg(p + 1);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      acc[k].x += x[k].x;
+      acc[k].y += x[k].y;
+      acc[k].z += x[k].z;
+      acc[k].w += x[k].w;
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int task = tid + 256 * t, sr = task >> 4, q16 = task & 15, kb = q16 >> 3, q = q16 & 7;
+    uint32_t hi[4], lo[4];
+    split2(acc[2 * t].x, acc[2 * t].y, hi[0], lo[0]);
+    split2(acc[2 * t].z, acc[2 * t].w, hi[1], lo[1]);
+    split2(acc[2 * t + 1].x, acc[2 * t + 1].y, hi[2], lo[2]);
+    split2(acc[2 * t + 1].z, acc[2 * t + 1].w, hi[3], lo[3]);
+    const uint32_t o = swz(sr, q);
+    *(uint4*)(a1 + kb * OPER + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *(uint4*)(a1 + (2 + kb) * OPER + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  }
+}
+
 __global__ void __launch_bounds__(T, 1) synth_prep_tc_kernel(Args a, const __grid_constant__ CUtensorMap k_map) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
