@@ -269,9 +269,7 @@ OI_API int oi_coarse_to_image_tc(float* coarse, int nparts, int count, int br, i
  * c the coarse intensity (128 x 128, the sum of its nparts partial sums), v the band rows of the image spectrum
  * written as the V operand tiles of the row pass (oi_rows_inv_tc_tiles layout).  ny a multiple of 128 up to 4096,
  * bc <= 64, 2br-1 <= 128.
- *   oi_synth_tc_constants  the tables from which each CTA generates G and A in shared memory (float: the
- *                          row Dirichlet kernel g[ny], then cos and sin of 2 pi j / 128, j < 128): (ny + 256) * 4
- *                          bytes
+ *   oi_synth_tc_constants  the constant image of G and A for (ny, br, bc): (1 + ny/128) * 65536 bytes
  *   oi_synth_tiles_tc      V tiles [count * ny / 128][64 KB] from coarse [nparts][count][128][128]
  *   oi_coarse_to_image_tcs oi_synth_tiles_tc then oi_rows_inv_tc_tiles (cconsts from oi_rows_tc_constants(1, ...)):
  *                          the same result as oi_coarse_to_image_tc

@@ -156,12 +156,12 @@ class Plan:
         return c
 
     def synth_consts(self) -> torch.Tensor:
-        """Tables of the tensor-core synthesis preparation's generated operands (oi_synth_tc_constants: the row
-        Dirichlet kernel of this grid and band, cos / sin of the coarse grid), built once per plan."""
+        """Constant operands of the tensor-core synthesis preparation (oi_synth_tc_constants: the coarse spectrum's
+        column DFT and the row Dirichlet kernels of this grid and band), built once per plan."""
         c = getattr(self, '_synth_consts', None)
         if c is None:
             b = self.band
-            nbytes = (self.ny + 256) * 4
+            nbytes = (1 + self.ny // 128) * 65536
             c = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
             N.call('oi_synth_tc_constants', self.ny, b.br, b.bc, N.ptr(c), nbytes, N.stream_handle(self.device))
             self._synth_consts = c

@@ -348,7 +348,7 @@ def test_synth_tiles_tc_direct(oi, count, nparts, ny, br, bc):
     g = np.random.default_rng(count * ny + br)
     coarse = g.random((nparts, count, 128, 128)).astype(np.float32)
     c = coarse.astype(np.float64).sum(axis=0)
-    consts = torch.empty((ny + 256) * 4, dtype=torch.uint8, device=dev)
+    consts = torch.empty((1 + ny // 128) * 65536, dtype=torch.uint8, device=dev)
     s = N.stream_handle(dev)
     N.call('oi_synth_tc_constants', ny, br, bc, N.ptr(consts), consts.numel(), s)
     cd = torch.from_numpy(coarse).to(dev)
