@@ -517,7 +517,8 @@ class CudaExecutor:
             used = max(0, free0 - torch.cuda.mem_get_info(self.device)[0])
             g = self.graphs[gk] = (graph, used)
             self._bytes[spec.key] = self._bytes.get(spec.key, 0) + used
-            if b >= 8:   # device time per image of this spec, from one replay (the copies are timed apart)
+            if b >= 8:   # device time per image of this spec, from a warm replay (the copies are timed apart)
+                graph.replay()                                     # the first replay uploads the graph
                 a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record(s)
                 graph.replay()
