@@ -188,12 +188,16 @@ __global__ void __launch_bounds__(256, 3) fft_rows_fwd_kernel(const void* __rest
 // SYM: t holds the non-negative columns kx = 0 .. bc-1 of a real mask's row transform and the band is the
 // symmetric bco x br band (m0c = -(bco-1)/2, m0r = -(br-1)/2): column kx lands at ic = kx + (bco-1)/2 and, for
 // kx > 0, its mirror band[-ky][-kx] = conj(band[ky][kx]) at row br-1-ir, column (bco-1)/2 - kx.
+// Blocks of COLS_T threads (G = COLS_T / N1 columns each): at the symmetric band's 30 columns per image a batch
+// of 64 has 1920 columns, which 8-column blocks spread over 148 SMs as 0.54 waves.
+constexpr int COLS_T = 128;
+
 template <int N1, bool SYM>
-__global__ void __launch_bounds__(256, 3) fft_cols_fwd_kernel(const float2* __restrict__ t, long long ncols, int bc,
-                                                           const float2* __restrict__ wn_g, int m0r, int br,
-                                                           float scale, float2* __restrict__ band, int bco,
-                                                           int dbl_from) {
-  constexpr int N = 32 * N1, G = 256 / N1;
+__global__ void __launch_bounds__(COLS_T, 6) fft_cols_fwd_kernel(const float2* __restrict__ t, long long ncols, int bc,
+                                                              const float2* __restrict__ wn_g, int m0r, int br,
+                                                              float scale, float2* __restrict__ band, int bco,
+                                                              int dbl_from) {
+  constexpr int N = 32 * N1, G = COLS_T / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const float2* t2 = wn_g;
   const float2* t1 = wn_g + 32 * N1;
@@ -561,7 +565,7 @@ static int launch_coarse_spec_fft(float* coarse, int nparts, int count, int br, 
 template <int N1>
 static size_t smem_rows_fwd(int nu) { return sizeof(float2) * ((256 / N1) * 32 * (N1 + 1) + (256 / N1) * nu); }
 template <int N1>
-static size_t smem_cols_fwd() { return sizeof(float2) * ((256 / N1) * 32 * (N1 + 1)); }
+static size_t smem_cols_fwd() { return sizeof(float2) * ((COLS_T / N1) * 32 * (N1 + 1)); }
 
 
 template <int N1>
@@ -594,12 +598,12 @@ static int band_fft(const void* field, int kind, int batch, int ny, int nx, int 
 template <int N1, bool SYM = false>
 static int cols_fwd(const float2* t, int batch, int bc, const float2* wn_y, int m0r, int br, float scale,
                     float2* band, cudaStream_t s, int bco = 0, int dbl_from = 0x7fffffff) {
-  constexpr int G = 256 / N1;
+  constexpr int G = COLS_T / N1;
   size_t smem = smem_cols_fwd<N1>();
   int rc = set_smem(fft_cols_fwd_kernel<N1, SYM>, smem, "oi_band_spectrum_fft/cols");
   if (rc) return rc;
   const long long ncols = (long long)batch * bc;
-  (void)launch_pdl(fft_cols_fwd_kernel<N1, SYM>, dim3((unsigned)ceil_div(ncols, G)), dim3(256), smem, s,
+  (void)launch_pdl(fft_cols_fwd_kernel<N1, SYM>, dim3((unsigned)ceil_div(ncols, G)), dim3(COLS_T), smem, s,
                    (const float2*)t, ncols, bc, wn_y, m0r, br, scale, band, SYM ? bco : bc, dbl_from);
   oi::note_launch();
   return check_launch("oi_band_spectrum_fft/cols");
