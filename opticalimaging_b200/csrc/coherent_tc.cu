@@ -21,16 +21,22 @@
 // to slot (CTA - first CTA of that image); the first CTA of an image zero-fills the slots no CTA owns, so
 // the partial sums fold in a fixed order (deterministic).
 //
-// Pipeline (warp 0 lane 0 issues every MMA; all 8 warps read tensor memory, two per lane quarter):
-//   barrier A | warp 0: issue stage 2 of t    | warps 1-7: build the stage-1 operand of t+1 from the staged
-//             |                               |            pupil and band (copied ahead with cp.async)
-//   barrier B | warp 0: issue stage 1 of t+1  | all: copy the pupil and band of t+2 into the stage
-//   all: wait stage 2 of t, accumulate |E|^2 (overlaps stage 1 of t+1); wait stage 1 of t+1, convert its
-//   accumulator to the stage-2 operand -> barrier A of the next task.
+// Pipeline (12 warps, each role waiting on mbarriers only):
+//   warps 0-7   tensor-memory warps, two per lane quarter: convert the stage-1 accumulator of field i, in place,
+//               into its stage-2 A operand (bf16 hi / lo), build 224 of the 512 chunks of a coming field's
+//               stage-1 B operand, and accumulate w |E|^2 of field i-1 from the stage-2 accumulator into registers;
+//   warps 8-10  build the other 288 chunks of the stage-1 B operand of the coming fields (P .* band, read from
+//               global memory where both stay L2-resident) into a ring of B1 slots: 2 for a symmetric band, 1 when
+//               Cc needs its own 64 KB; every warp but the MMA warp builds the first slots' fields at the start;
+//   warp 11     lane 0 issues the MMAs in the order S1(i), S2(i-1), S1(i+1), S2(i), ...
+// Tensor memory holds E^T (256 columns) and two regions of 128 columns, each the stage-1 accumulator H^T of a
+// field and, after its conversion, that field's stage-2 operand.  So the tensor pipe runs S1(i+1) while field
+// i-1's |E|^2 is read out and S2(i) while field i+1 is converted and later fields are built: the conversions and
+// builds leave its critical path.  S1(i+1) reuses the region S2(i-1) read and is issued once S2(i-1) completes.
 //
-// Waits on the MMA-completion barriers are bounded (2 s of %globaltimer) and warp-uniform; on expiry the CTA
-// records a status (oi_device_status), waits a bounded time for its outstanding MMAs, frees tensor memory and
-// exits.
+// Every wait is bounded (2 s of %globaltimer); on expiry a role records a status (oi_device_status) and stops,
+// the roles waiting on it then expire in turn, and the MMA thread waits (bounded) for the MMAs it issued before
+// the CTA frees tensor memory and exits.
 #include "tc_common.cuh"
 
 namespace oi {
@@ -39,7 +45,9 @@ __device__ int g_device_status = 0;
 
 namespace tc {
 
-constexpr int T = 256;              // threads per CTA (8 warps: two per tensor-memory lane quarter)
+constexpr int T = 384;              // threads per CTA: 8 tensor-memory warps, 3 build warps, the MMA warp
+constexpr int NBUILD = 3;           // build warps (8 .. 10)
+constexpr int MMA_WARP = 11;
 constexpr int MC = 128, MR = 128;   // coarse grid
 constexpr int BMAX = 64;            // band rows / columns (padded)
 // Shared memory, from a 1024-byte aligned base.  Every operand is K-major with 64 bf16 (128 bytes) per row,
@@ -48,25 +56,21 @@ constexpr uint32_t ROWS = 128;                                // bytes per opera
 constexpr uint32_t CR3_BYTES = 384 * ROWS;                    // [-Cri; Crr; Cri], one precision
 constexpr uint32_t CC_BYTES = 256 * ROWS;                     // [Ccr; Cci], one precision (m0r != m0c)
 constexpr uint32_t B1_BYTES = 192 * ROWS;                     // [-Ai; Ar; Ai], one precision
-constexpr uint32_t MISC_BYTES = 64;
+constexpr uint32_t MISC_BYTES = 128;
 // tensor memory columns (128 lanes x 512 columns of 32 bits)
 constexpr uint32_t COL_D2 = 0;      // E^T: re [0,128), im [128,256)
-constexpr uint32_t COL_D1 = 256;    // H^T: re [256,320), im [320,384)
-constexpr uint32_t COL_A2H = 384;   // H^T as bf16 pairs, hi: [Hr | Hi] along K (64 columns)
-constexpr uint32_t COL_A2L = 448;   // lo
+constexpr uint32_t COL_R = 256;     // regions 256 + 128 r, r = field index mod 2: H^T re [0,64), im [64,128);
+                                    // converted: [Hr hi | Hr lo | Hi hi | Hi lo], 32 columns of bf16 pairs each
 constexpr uint32_t NCOLS = 512;
 
 struct Layout {
-  uint32_t cr3, cc, cc_lo, b1, stage, stage_arr, misc, bytes;  // cc: Ccr hi; Cci = cc + 128 rows; lo = cc + cc_lo
-  uint32_t consts;                                             // bytes of the constant image (cr3 [+ cc])
-  bool staged;
+  uint32_t cr3, cc, cc_lo, b1, nb1, misc, bytes;  // cc: Ccr hi; Cci = cc + 128 rows; lo = cc + cc_lo
+  uint32_t consts;                                // bytes of the constant image (cr3 [+ cc])
 };
 
-// Shared-memory layout for a band of `plane` elements.  The constant image (CR3 hi, lo, then Cc hi, lo when the
-// column DFT differs) comes first, as oi_tc_constants writes it.  The stage holds the pupil and the band of a
-// coming field (float2, `plane` + 2 elements each: element e at 8 (e + d), d in {0, 1} aligning the bulk copy)
-// and is used when it fits.
-__host__ __device__ inline Layout make_layout(bool sym, int plane) {
+// Shared-memory layout.  The constant image (CR3 hi, lo, then Cc hi, lo when the column DFT differs) comes first,
+// as oi_tc_constants writes it, then the B1 slots (hi, lo each).
+__host__ __device__ inline Layout make_layout(bool sym) {
   Layout l;
   l.cr3 = 0;
   uint32_t off = 2 * CR3_BYTES;
@@ -80,15 +84,15 @@ __host__ __device__ inline Layout make_layout(bool sym, int plane) {
   }
   l.consts = off;
   l.b1 = off;
-  off += 2 * B1_BYTES;
-  l.stage_arr = (uint32_t)(8 * (plane + 2) + 15) & ~15u;
-  l.staged = off + 2 * l.stage_arr + MISC_BYTES + 1024 <= SMEM_LIMIT;
-  l.stage = off;
-  if (l.staged) off += 2 * l.stage_arr;
+  l.nb1 = sym ? 2 : 1;
+  off += l.nb1 * 2 * B1_BYTES;
   l.misc = off;
   l.bytes = off + MISC_BYTES + 1024;
   return l;
 }
+static_assert(2 * CR3_BYTES + 2 * 2 * B1_BYTES + MISC_BYTES + 1024 <= SMEM_LIMIT, "coherent_tc: shared memory");
+static_assert(2 * CR3_BYTES + 2 * CC_BYTES + 2 * B1_BYTES + MISC_BYTES + 1024 <= SMEM_LIMIT,
+              "coherent_tc: shared memory");
 
 // Writes rows of the DFT matrix C[s][i] = exp(-2 pi i (m0+i) s / 128), s < 128, i < 64, into an operand image
 // (same bytes as the shared-memory operands): re at rows [re_row, +128), im at [im_row, +128) and, if
@@ -192,78 +196,64 @@ __device__ __forceinline__ FieldSrc field_src(const Args& a, const TaskPos& p) {
   return s;
 }
 
-// Alignment shift of a float2 array in the stage: element e sits at 8 (e + d).
-__device__ __forceinline__ int stage_shift(const float2* p) { return (int)(((uintptr_t)p >> 3) & 1); }
-
-// Copy of n float2 from p into the stage array at s (16-byte aligned): the 16-byte aligned body by one bulk
-// copy completing on `bar`, the (at most two) unaligned end elements by plain loads.  Returns the bulk bytes.
-__device__ __forceinline__ uint32_t stage_array(uint32_t s, const float2* p, int n, uint32_t bar) {
-  const int d = stage_shift(p);
-  const int nb = (n - d) & ~1;
-  if (nb > 0) bulk_g2s(s + 8 * (2 * d), p + d, 8u * nb, bar);
-  if (d && n > 0) {
-    const float2 v = __ldg(p);
-    asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(s + 8), "f"(v.x), "f"(v.y) : "memory");
-  }
-  if (d + nb < n) {
-    const float2 v = __ldg(p + n - 1);
-    asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(s + 8 * (n - 1 + d)), "f"(v.x), "f"(v.y) : "memory");
-  }
-  return nb > 0 ? 8u * nb : 0u;
-}
-
-// Stage copy of task t's pupil and band (issued by one thread; completes on `bar`).
-// The band is copied only when it differs from the one the stage holds (consecutive fields of one image and
-// channel share it: the SOCS kernels of a clip).
-__device__ __forceinline__ void stage_copy(const Args& a, const FieldSrc& f, uint32_t stage, uint32_t arr, uint32_t bar,
-                                           bool with_band) {
-  const int plane = a.br * a.bc;
-  const uint32_t bytes = 8u * ((plane - stage_shift(f.pupil)) & ~1) +
-                         (with_band ? 8u * ((plane - stage_shift(f.band)) & ~1) : 0u);
-  expect_tx(bar, bytes);
-  stage_array(stage, f.pupil, plane, bar);
-  if (with_band) stage_array(stage + arr, f.band, plane, bar);
-}
-
 // The stage-1 B operand of a field, A = P .* band zero-padded to 64 x 64: rows [0,64) = -Ai, [64,128) = Ar,
-// [128,192) = Ai (K = ic), hi at b1, lo at b1 + B1_BYTES.  pk / hc are generic pointers (stage or global).
-// Threads bt = 0 .. nthreads-1 share the 512 chunks of 8 columns.
-__device__ __forceinline__ void build_field(const float2* pk, const float2* hc, int br, int bc, uint32_t b1, int bt,
-                                            int nthreads) {
-  for (int chunk = bt; chunk < 64 * 8; chunk += nthreads) {
-    const int ir = chunk >> 3, g = chunk & 7;
-    float2 v[8];
+// [128,192) = Ai (K = ic), hi at b1, lo at b1 + B1_BYTES, in 512 chunks of 8 columns.  The calling thread builds
+// chunks c0, c0 + step, ... (COUNT of them), two at a time (all 32 loads of a pair issued before any product).
+template <int COUNT>
+__device__ __forceinline__ void build_chunks(const float2* __restrict__ pk, const float2* __restrict__ hc, int br,
+                                             int bc, uint32_t b1, int c0, int step) {
+  constexpr int count = COUNT;
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int ic = 8 * g + e;
-      v[e] = make_float2(0.f, 0.f);
-      if (ir < br && ic < bc) {
+  for (int k = 0; k < count; k += 2) {
+    float2 p[2][8], h[2][8];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int chunk = c0 + (k + u) * step, ir = chunk >> 3, g = chunk & 7;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int ic = 8 * g + e;
+        const bool in = k + u < count && ir < br && ic < bc;
         const int o = ir * bc + ic;
-        v[e] = cmul(pk[o], hc[o]);
+        p[u][e] = in ? __ldg(pk + o) : make_float2(0.f, 0.f);
+        h[u][e] = in ? __ldg(hc + o) : make_float2(0.f, 0.f);
       }
     }
-    uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      split2(v[2 * e].x, v[2 * e + 1].x, rh[e], rl[e]);
-      split2(v[2 * e].y, v[2 * e + 1].y, ih[e], il[e]);
+    for (int u = 0; u < 2; ++u) {
+      if (k + u >= count) break;
+      const int chunk = c0 + (k + u) * step, ir = chunk >> 3, g = chunk & 7;
+      uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float2 v0 = cmul(p[u][2 * e], h[u][2 * e]), v1 = cmul(p[u][2 * e + 1], h[u][2 * e + 1]);
+        split2(v0.x, v1.x, rh[e], rl[e]);
+        split2(v0.y, v1.y, ih[e], il[e]);
+      }
+      const uint32_t sg = 0x80008000u;
+      const uint32_t o_ng = b1 + swz(ir, g), o_re = b1 + swz(64 + ir, g), o_im = b1 + swz(128 + ir, g);
+      st_shared_v4(o_ng, ih[0] ^ sg, ih[1] ^ sg, ih[2] ^ sg, ih[3] ^ sg);
+      st_shared_v4(o_ng + B1_BYTES, il[0] ^ sg, il[1] ^ sg, il[2] ^ sg, il[3] ^ sg);
+      st_shared_v4(o_re, rh[0], rh[1], rh[2], rh[3]);
+      st_shared_v4(o_re + B1_BYTES, rl[0], rl[1], rl[2], rl[3]);
+      st_shared_v4(o_im, ih[0], ih[1], ih[2], ih[3]);
+      st_shared_v4(o_im + B1_BYTES, il[0], il[1], il[2], il[3]);
     }
-    const uint32_t sg = 0x80008000u;
-    const uint32_t o_ng = b1 + swz(ir, g), o_re = b1 + swz(64 + ir, g), o_im = b1 + swz(128 + ir, g);
-    st_shared_v4(o_ng, ih[0] ^ sg, ih[1] ^ sg, ih[2] ^ sg, ih[3] ^ sg);
-    st_shared_v4(o_ng + B1_BYTES, il[0] ^ sg, il[1] ^ sg, il[2] ^ sg, il[3] ^ sg);
-    st_shared_v4(o_re, rh[0], rh[1], rh[2], rh[3]);
-    st_shared_v4(o_re + B1_BYTES, rl[0], rl[1], rl[2], rl[3]);
-    st_shared_v4(o_im, ih[0], ih[1], ih[2], ih[3]);
-    st_shared_v4(o_im + B1_BYTES, il[0], il[1], il[2], il[3]);
   }
+}
+
+// Chunks of a field's B1 per thread: the build warps take chunks [0, 288) (three each), tensor-memory threads
+// 0 .. 223 one each of [288, 512).
+constexpr int BUILD_CHUNKS = 3 * 32 * NBUILD;
+static_assert(BUILD_CHUNKS + 224 == 512 && 224 <= 256, "coherent_tc: B1 chunks");
+__device__ __forceinline__ void build_share(const FieldSrc& f, int br, int bc, uint32_t b1, int tid) {
+  if (tid >= 256) build_chunks<3>(f.pupil, f.band, br, bc, b1, tid - 256, 32 * NBUILD);
+  else if (tid < 224) build_chunks<1>(f.pupil, f.band, br, bc, b1, BUILD_CHUNKS + tid, 0);
 }
 
 // Stage 1: D1[sc][n] = sum_ic Cc[sc][ic] B1[n][ic], n < 64 re / n >= 64 im of H^T:  Ccr x [Ar; Ai] (B1 rows
-// 64..191) + Cci x [-Ai; Ar] (rows 0..127).  24 MMAs of 128 x 128 x 16.
-__device__ __forceinline__ void issue_stage1(uint32_t tmem, uint32_t cc, uint32_t cc_lo, uint32_t b1) {
+// 64..191) + Cci x [-Ai; Ar] (rows 0..127).  24 MMAs of 128 x 128 x 16 into the region at column d.
+__device__ __forceinline__ void issue_stage1(uint32_t d, uint32_t cc, uint32_t cc_lo, uint32_t b1) {
   constexpr uint32_t ID = idesc(128, false);
-  const uint32_t d = tmem + COL_D1;
 #pragma unroll
   for (int term = 0; term < 2; ++term) {
     const uint32_t x = cc + term * 128 * ROWS;
@@ -279,14 +269,15 @@ __device__ __forceinline__ void issue_stage1(uint32_t tmem, uint32_t cc, uint32_
 }
 
 // Stage 2: D2[sc][n] = sum_k A2[sc][k] CR3[row(n)][k], n < 128 re / n >= 128 im of E^T:  Hr x [Crr; Cri]
-// (CR3 rows 128..383) + Hi x [-Cri; Crr] (rows 0..255).  24 MMAs of 128 x 256 x 16.
-__device__ __forceinline__ void issue_stage2(uint32_t tmem, uint32_t cr3) {
+// (CR3 rows 128..383) + Hi x [-Cri; Crr] (rows 0..255), A2 the converted region at column r.  24 MMAs of
+// 128 x 256 x 16.
+__device__ __forceinline__ void issue_stage2(uint32_t tmem, uint32_t r, uint32_t cr3) {
   constexpr uint32_t ID = idesc(256, false);
   const uint32_t d = tmem + COL_D2;
 #pragma unroll
   for (int ks = 0; ks < 8; ++ks) {
     const uint32_t bm = cr3 + ((ks >> 2) ? 0u : 128 * ROWS) + 32 * (ks & 3);
-    const uint32_t ah = tmem + COL_A2H + 8 * ks, al = tmem + COL_A2L + 8 * ks;
+    const uint32_t ah = tmem + r + 64 * (ks >> 2) + 8 * (ks & 3), al = ah + 32;
     mma_ts(d, ah, sdesc(bm), ID, ks ? 1u : 0u);                              // hi hi
     mma_ts(d, ah, sdesc(bm + CR3_BYTES), ID, 1);                              // hi lo
     mma_ts(d, al, sdesc(bm), ID, 1);                                          // lo hi
@@ -296,229 +287,217 @@ __device__ __forceinline__ void issue_stage2(uint32_t tmem, uint32_t cr3) {
 // w |E|^2 of the finished stage 2 into acc (this warp's lane quarter and column half).
 __device__ __forceinline__ void accumulate(float (&acc)[64], uint32_t taddr, int half, float w) {
 #pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    float re[32], im[32];
-    tmem_ld32x2(taddr + COL_D2 + 64 * half + 32 * p, taddr + COL_D2 + 128 + 64 * half + 32 * p, re, im);
+  for (int p = 0; p < 4; ++p) {
+    float re[16], im[16];
+    tmem_ld16x2(taddr + COL_D2 + 64 * half + 16 * p, taddr + COL_D2 + 128 + 64 * half + 16 * p, re, im);
 #pragma unroll
-    for (int j = 0; j < 32; ++j) acc[32 * p + j] = fmaf(w, fmaf(re[j], re[j], im[j] * im[j]), acc[32 * p + j]);
+    for (int j = 0; j < 16; ++j) acc[16 * p + j] = fmaf(w, fmaf(re[j], re[j], im[j] * im[j]), acc[16 * p + j]);
   }
 }
 
-// The stage-1 accumulator (H^T, FP32) -> the stage-2 A operand (bf16 hi / lo pairs); half 0 converts Hr, 1 Hi.
-__device__ __forceinline__ void convert(uint32_t taddr, int half) {
-  float h[32], h2[32];
-  tmem_ld32x2(taddr + COL_D1 + 64 * half, taddr + COL_D1 + 64 * half + 32, h, h2);
-  uint32_t hi[32], lo[32];
+// The stage-1 accumulator in the region at column r (H^T, FP32) -> the stage-2 A operand in place: half 0
+// converts Hr (columns [0,64) -> hi at [0,32), lo at [32,64)), half 1 Hi (columns [64,128)), 32 columns at a
+// time; every column a warp writes is one it has already read.
+__device__ __forceinline__ void convert(uint32_t taddr, uint32_t r, int half) {
+  const uint32_t c = taddr + r + 64 * half;
+  float x[32];
+  uint32_t hi[16], lo[16], lo2[16];
+  tmem_ld32(c, x);
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    split2(h[2 * j], h[2 * j + 1], hi[j], lo[j]);
-    split2(h2[2 * j], h2[2 * j + 1], hi[16 + j], lo[16 + j]);
-  }
-  tmem_st32(taddr + COL_A2H + 32 * half, hi);
-  tmem_st32(taddr + COL_A2L + 32 * half, lo);
+  for (int j = 0; j < 16; ++j) split2(x[2 * j], x[2 * j + 1], hi[j], lo[j]);
+  tmem_st16(c, hi);        // columns [0,16): read
+  tmem_ld32(c + 32, x);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) split2(x[2 * j], x[2 * j + 1], hi[j], lo2[j]);
+  tmem_st16(c + 16, hi);
+  tmem_st16(c + 32, lo);   // columns [32,64): read by the second load
+  tmem_st16(c + 48, lo2);
   wait_st();
 }
 
 __global__ void __launch_bounds__(T, 1) coherent_tc_kernel(Args a) {
   extern __shared__ unsigned char smem_raw[];
-  const bool sym = a.m0r == a.m0c;
-  const int plane = a.br * a.bc;
-  const Layout L = make_layout(sym, plane);
+  const Layout L = make_layout(a.m0r == a.m0c);
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* gbase = smem_raw + (base - raw);
-  const uint32_t bar1 = base + L.misc, bar2 = bar1 + 8, bar3 = bar1 + 16, bar4 = bar1 + 24;
-  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + L.misc + 32);
-  const float2* st_p = (const float2*)(gbase + L.stage);
-  const float2* st_h = (const float2*)(gbase + L.stage + L.stage_arr);
-  const uint32_t cr3 = base + L.cr3, cc = base + L.cc, b1 = base + L.b1, stage = base + L.stage;
+  const uint32_t misc = base + L.misc;
+  // barriers: cbar (constants landed), bfull[2] (B1 slot built), bfree[2] (S1 reading the slot finished),
+  // s1done[2] (S1 into region r finished), conv[2] (region r converted), s2done (S2 finished: E^T complete and
+  // its region free), d2free (E^T read out), fin (every issued MMA finished, at the end)
+  const uint32_t cbar = misc, bfull = misc + 8, bfree = misc + 24, s1done = misc + 40, conv = misc + 56,
+                 s2done = misc + 72, d2free = misc + 80, fin = misc + 88;
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + L.misc + 96);
+  const uint32_t cr3 = base + L.cr3, cc = base + L.cc, b1 = base + L.b1;
+  const int nb1 = (int)L.nb1;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long long G = gridDim.x;
   const long long t0 = (long long)blockIdx.x * a.tasks / G, t1 = ((long long)blockIdx.x + 1) * a.tasks / G;
+  const int n = (int)(t1 - t0);   // fields of this CTA, >= 1
   const int F = a.nk * a.nch;
 
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(base + L.misc + 32),
-                 "r"(NCOLS)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  TaskPos pt;                                   // position of task t (t0 before the loop)
-  pt.init(a, t0);
-  FieldSrc cur = field_src(a, pt);
-  if (tid == 0) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1 + 8 * i) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  if (warp == 0) tmem_alloc(misc + 96, NCOLS);
+  if (tid == 32 * MMA_WARP) {
+    mbar_init(cbar, 1);
+    for (int r = 0; r < 2; ++r) {
+      mbar_init(bfull + 8 * r, 8 + NBUILD);
+      mbar_init(bfree + 8 * r, 1);
+      mbar_init(s1done + 8 * r, 1);
+      mbar_init(conv + 8 * r, 8);
+    }
+    mbar_init(s2done, 1);
+    mbar_init(d2free, 8);
+    mbar_init(fin, 1);
+    mbar_init_fence();
     // constant operands: one bulk copy per 16 KB
-    expect_tx(bar4, L.consts);
+    expect_tx(cbar, L.consts);
     for (uint32_t o = 0; o < L.consts; o += 16384)
-      bulk_g2s(base + o, a.consts + o, L.consts - o < 16384 ? L.consts - o : 16384, bar4);
-    pdl_wait();   // the band comes from the spectrum pass
-    if (L.staged) stage_copy(a, cur, stage, L.stage_arr, bar3, true);
+      bulk_g2s(base + o, a.consts + o, L.consts - o < 16384 ? L.consts - o : 16384, cbar);
   }
-  __syncthreads();  // barrier inits and the stage's unaligned end elements
-  pdl_trigger();
-  pdl_wait();
-  uint32_t ph3 = 0;
-  bool bad = false;
-  if (L.staged) {
-    bad = !warp_wait(bar3, ph3);
-    ph3 ^= 1;
-  }
-  if (!bad) {
-    const float2* pk = L.staged ? st_p + stage_shift(cur.pupil) : cur.pupil;
-    const float2* hc = L.staged ? st_h + stage_shift(cur.band) : cur.band;
-    build_field(pk, hc, a.br, a.bc, b1, tid, T);
-  }
-  if (tid == 0) bad |= !wait_bar(bar4, 0);  // the constants have landed
-  fence_async_smem();
   fence_before();
-  bool failed = __syncthreads_or(bad);
+  __syncthreads();
   fence_after();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);  // this warp's lane quarter
-  const int half = warp >> 2;                                          // column half this warp reads
-  const int sc = 32 * (warp & 3) + lane;                               // coarse column = accumulator row
-  uint32_t ph1 = 0, ph2 = 0;
-  int pending1 = 0, pending2 = 0, pending3 = 0;
-  if (!failed) {
-    if (tid == 0) {
-      issue_stage1(tmem, cc, L.cc_lo, b1);
-      commit(bar1);
-    }
-    pending1 = 1;
-    FieldSrc nxt = cur;
-    TaskPos p1 = pt;
-    p1.next(a);
-    if (t0 + 1 < t1) nxt = field_src(a, p1);
-    if (L.staged && t0 + 1 < t1) {
-      if (tid == 32) stage_copy(a, nxt, stage, L.stage_arr, bar3, nxt.band != cur.band);
-      pending3 = 1;
-    }
-  }
-
-  float acc[64];
-#pragma unroll
-  for (int j = 0; j < 64; ++j) acc[j] = 0.f;
-  float wprev = 0.f;
-
-  for (long long t = t0; t < t1 && !failed; ++t) {
-    bad = false;
-    TaskPos p1 = pt, p2;
-    p1.next(a);
-    p2 = p1;
-    p2.next(a);
-    // (1) |E|^2 of task t-1 (overlaps stage 1 of t on the tensor pipe)
-    if (t > t0) {
-      if (warp_wait(bar2, ph2)) {
-        fence_after();
-        accumulate(acc, taddr, half, wprev);
-      } else {
-        bad = true;
-      }
-      ph2 ^= 1;
-      pending2 = 0;
-      if (pt.first()) {  // task t-1 was the last of its image in this range
-        const long long qp = pt.q - 1;
-        const long long slot = blockIdx.x - cta_of(qp * F, a.tasks, G);
-        float* out = a.coarse + (slot * a.images + qp) * (long long)(MR * MC) + sc;
-#pragma unroll
-        for (int j = 0; j < 64; ++j) {
-          out[(64 * half + j) * MC] = acc[j];
-          acc[j] = 0.f;
-        }
-      }
-    }
-    // (2) stage-1 accumulator of t -> stage-2 A operand
-    if (warp_wait(bar1, ph1)) {
-      fence_after();
-      convert(taddr, half);
-    } else {
-      bad = true;
-    }
-    ph1 ^= 1;
-    pending1 = 0;
-    wprev = cur.w;
-    if (t + 1 < t1) cur = field_src(a, p1);
-    // zero-fill the partial slots of this image that no CTA owns (done by the image's first CTA)
-    if (pt.first()) {
-      const long long q = pt.q;
-      const long long first = cta_of(q * F, a.tasks, G), last = cta_of(q * F + F - 1, a.tasks, G);
-      for (long long slot = last - first + 1; slot < a.nparts; ++slot) {
-        float* out = a.coarse + (slot * a.images + q) * (long long)(MR * MC);
-        for (int e = tid; e < MR * MC / 4; e += T) ((float4*)out)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-    }
-    if (pending3) {  // the stage holds task t+1
-      bad |= !warp_wait(bar3, ph3);
-      ph3 ^= 1;
-      pending3 = 0;
-    }
-    fence_before();
-    if (__syncthreads_or(bad)) {  // barrier A
-      failed = true;
-      break;
-    }
-    if (warp == 0) {
-      if (lane == 0) {
-        fence_after();
-        issue_stage2(tmem, cr3);
-        commit(bar2);
-      }
+  pdl_trigger();
+  pdl_wait();   // bands, pupils and weights are read, and partial sums written, from here on
+  if (warp != MMA_WARP) {   // every warp but the MMA warp builds the first fields' B1 (one per slot)
+    TaskPos p;
+    p.init(a, t0);
+    for (int f = 0; f < n && f < nb1; ++f) {
+      build_share(field_src(a, p), a.br, a.bc, b1 + f * 2 * B1_BYTES, tid);
+      fence_async_smem();
       __syncwarp();
-    } else if (t + 1 < t1) {
-      const float2* pk = L.staged ? st_p + stage_shift(cur.pupil) : cur.pupil;
-      const float2* hc = L.staged ? st_h + stage_shift(cur.band) : cur.band;
-      build_field(pk, hc, a.br, a.bc, b1, tid - 32, T - 32);
+      if (lane == 0) arrive(bfull + 8 * f);
+      p.next(a);
     }
-    pending2 = 1;
-    fence_async_smem();
-    __syncthreads();  // barrier B: the stage-1 operand of t+1 is built and the stage is free
-    if (t + 1 < t1) {
-      if (tid == 0) {
-        fence_after();
-        issue_stage1(tmem, cc, L.cc_lo, b1);
-        commit(bar1);
-      }
-      pending1 = 1;
-      if (L.staged && t + 2 < t1) {
-        if (tid == 32) {
-          const FieldSrc f2 = field_src(a, p2);
-          stage_copy(a, f2, stage, L.stage_arr, bar3, f2.band != cur.band);   // cur: field t+1, in the stage
+  }
+
+  if (warp == MMA_WARP) {
+    // ---- MMA issue: S1(i) into region i & 1 (its B1 slot built, S2(i-2) done with the region), then S2(i-1)
+    // (region converted, E^T of field i-2 read out)
+    if (lane == 0) {
+      const bool cok = wait_bar(cbar, 0);
+      bool ok = cok, issued = false;
+      Ring bs{0, 0};
+      for (int i = 0; i <= n && ok; ++i) {
+        if (i < n) {
+          ok = wait_bar(bfull + 8 * bs.slot, bs.phase);
+          if (ok && i >= 2) ok = wait_bar(s2done, (uint32_t)((i - 2) & 1));
+          if (!ok) break;
+          fence_after();
+          issue_stage1(tmem + COL_R + 128u * (i & 1), cc, L.cc_lo, b1 + bs.slot * 2 * B1_BYTES);
+          commit(s1done + 8 * (i & 1));
+          commit(bfree + 8 * bs.slot);
+          issued = true;
+          bs.next(nb1);
         }
-        pending3 = 1;
+        if (i >= 1) {
+          const int j = i - 1;
+          ok = wait_bar(conv + 8 * (j & 1), (uint32_t)((j >> 1) & 1));
+          if (ok && j >= 1) ok = wait_bar(d2free, (uint32_t)((j - 1) & 1));
+          if (!ok) break;
+          fence_after();
+          issue_stage2(tmem, COL_R + 128u * (j & 1), cr3);
+          commit(s2done);
+        }
+      }
+      if (!ok) atomicExch(&g_device_status, 1);
+      if (!cok) wait_bar(cbar, 0);   // the constant copies land before shared memory is released
+      if (issued) {                  // every MMA issued has finished before tensor and shared memory are released
+        commit(fin);
+        wait_bar(fin, 0);
       }
     }
-    pt = p1;
-  }
-  if (!failed) {
-    if (warp_wait(bar2, ph2)) {
-      fence_after();
-      accumulate(acc, taddr, half, wprev);
-      pending2 = 0;
-      const long long qp = (t1 - 1) / F;
-      const long long slot = blockIdx.x - cta_of(qp * F, a.tasks, G);
-      float* out = a.coarse + (slot * a.images + qp) * (long long)(MR * MC) + sc;
-#pragma unroll
-      for (int j = 0; j < 64; ++j) out[(64 * half + j) * MC] = acc[j];
-    } else {
-      failed = true;
+  } else if (warp >= 8) {
+    // ---- build warps: their share of B1 of field i >= nb1 into slot i mod nb1 once S1(i - nb1) has read it; the
+    // first CTA of an image zero-fills the partial slots of that image that no CTA owns
+    const int bt = tid - 256;
+    TaskPos p;
+    p.init(a, t0);
+    Ring bs{0, 0};
+    bool ok = true;
+    for (int i = 0; i < n; ++i) {
+      if (i >= nb1) {
+        ok = warp_wait(bfree + 8 * bs.slot, bs.phase ^ 1u);
+        if (!ok) break;
+        build_share(field_src(a, p), a.br, a.bc, b1 + bs.slot * 2 * B1_BYTES, tid);
+        fence_async_smem();
+        __syncwarp();
+        if (lane == 0) arrive(bfull + 8 * bs.slot);
+      }
+      if (p.first()) {
+        const long long q = p.q;
+        const long long first = cta_of(q * F, a.tasks, G), last = cta_of(q * F + F - 1, a.tasks, G);
+        for (long long slot = last - first + 1; slot < a.nparts; ++slot) {
+          float* out = a.coarse + (slot * a.images + q) * (long long)(MR * MC);
+          for (int e = bt; e < MR * MC / 4; e += 32 * NBUILD) ((float4*)out)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+      bs.next(nb1);
+      p.next(a);
     }
-  }
-  if (failed) {
-    if (lane == 0) atomicExch(&g_device_status, 1);
-    // let outstanding MMAs and copies finish (bounded) before tensor memory and shared memory are released
-    if (pending2) wait_bar(bar2, ph2);
-    if (pending1) wait_bar(bar1, ph1);
-    if (pending3) wait_bar(bar3, ph3);
-    if (tid == 0) wait_bar(bar4, 0);
+    if (!ok && lane == 0) atomicExch(&g_device_status, 1);
+  } else {
+    // ---- tensor-memory warps: convert(i), their share of B1 of field i + nb1 (its slot was read by S1(i)), then
+    // w |E|^2 of field i-1; a finished image's partial sum is stored
+    const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);   // this warp's lane quarter
+    const int half = warp >> 2;                                           // column half this warp handles
+    const int sc = 32 * (warp & 3) + lane;                                // coarse column = accumulator row
+    float acc[64];
+#pragma unroll
+    for (int j = 0; j < 64; ++j) acc[j] = 0.f;
+    TaskPos pj, pb;   // field j = i - 1, field i + nb1
+    pj.init(a, t0);
+    pb = pj;
+    for (int f = 0; f < nb1; ++f) pb.next(a);
+    bool ok = true;
+    for (int i = 0; i <= n; ++i) {
+      if (i < n) {
+        ok = warp_wait(s1done + 8 * (i & 1), (uint32_t)((i >> 1) & 1));
+        if (!ok) break;
+        fence_after();
+        convert(taddr, COL_R + 128u * (i & 1), half);
+        fence_before();
+        __syncwarp();
+        if (lane == 0) arrive(conv + 8 * (i & 1));
+        if (i + nb1 < n) {
+          const int slot = i % nb1;
+          build_share(field_src(a, pb), a.br, a.bc, b1 + slot * 2 * B1_BYTES, tid);
+          fence_async_smem();
+          __syncwarp();
+          if (lane == 0) arrive(bfull + 8 * slot);
+          pb.next(a);
+        }
+      }
+      if (i >= 1) {
+        const int j = i - 1;
+        ok = warp_wait(s2done, (uint32_t)(j & 1));
+        if (!ok) break;
+        fence_after();
+        accumulate(acc, taddr, half, __ldg(a.weight + (long long)pj.z * a.nk + pj.k));
+        fence_before();
+        __syncwarp();
+        if (lane == 0) arrive(d2free);
+        const long long q = pj.q;
+        pj.next(a);
+        if (j == n - 1 || pj.first()) {   // field j was the last of image q in this range
+          const long long slot = blockIdx.x - cta_of(q * F, a.tasks, G);
+          float* out = a.coarse + (slot * a.images + q) * (long long)(MR * MC) + sc;
+#pragma unroll
+          for (int jj = 0; jj < 64; ++jj) {
+            out[(64 * half + jj) * MC] = acc[jj];
+            acc[jj] = 0.f;
+          }
+        }
+      }
+    }
+    if (!ok && lane == 0) atomicExch(&g_device_status, 1);
   }
   fence_before();
   __syncthreads();
   if (warp == 0) {
     fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS) : "memory");
+    tmem_dealloc(tmem, NCOLS);
   }
 }
 
@@ -582,7 +561,7 @@ extern "C" int oi_coherent_coarse_tc(const void* band, int batch, int nch, int m
   tc::Args a{(const float2*)band, (long long)nch * br * bc, nch, br, bc, m0r, m0c, (const float2*)pupil,
              pupil_batch_stride, weight, nz, nk, images, images * fields, nparts, coarse,
              (const unsigned char*)consts};
-  const tc::Layout L = tc::make_layout(m0r == m0c, br * bc);
+  const tc::Layout L = tc::make_layout(m0r == m0c);
   int rc = ensure_smem((const void*)tc::coherent_tc_kernel, L.bytes, "oi_coherent_coarse_tc");
   if (rc) return rc;
   (void)launch_pdl(tc::coherent_tc_kernel, dim3((unsigned)ctas), dim3(tc::T), (size_t)L.bytes, (cudaStream_t)stream, a);

@@ -62,27 +62,43 @@ __device__ __forceinline__ void split8(const float (&v)[8], uint32_t (&hi)[4], u
 // ------------------------------------------------------------------------------------------ forward
 // Items are pairs of 128-row blocks (rows 256 P .. 256 P + 255): one W chunk feeds both blocks' MMAs, so each
 // 64-column chunk of mask costs 32 KB of mask plus 16 KB of W over the SM-to-L2 path instead of 32 + 32 (that
-// path, about 30 bytes per cycle per SM, bounds this pass).  Shared memory: a ring of 2 staging slots (the chunk
+// path, about 30 bytes per cycle per SM, bounds this pass).  Shared memory: a ring of staging slots (the chunk
 // of both blocks: per block two 128-byte-swizzled [128][32] float boxes, or one 64-byte-swizzled [128][64]
-// uint8 box) and a ring of 3 W chunks (hi, lo).  Tensor memory: the two blocks' accumulators (columns 0 and
-// 128, 128 each) and two A slots at 256 + 128 s (block h: hi at 64 h, lo at 64 h + 32), the chunk as bf16 hi /
-// lo written by the converters, read by the MMA.  A pair past the last row block (odd count) reads zeros and
-// stores nothing for its second block.
+// uint8 box) and a ring of W chunks (hi, lo); FwdCfg sizes both rings to fill the 224 KB, so that as many mask
+// bytes as fit are in flight from DRAM while a slot is converted.  Tensor memory: the two blocks' accumulators
+// (columns 0 and 128, 128 each) and two A slots at 256 + 128 s (block h: hi at 64 h, lo at 64 h + 32), the
+// chunk as bf16 hi / lo written by the converters, read by the MMA.  A pair past the last row block (odd count)
+// reads zeros and stores nothing for its second block.
 // NB = band columns per real / imaginary part of W: 64 (a band of up to 64 columns, N = 128), or 32 for the
 // Hermitian half of a real mask's symmetric band (columns 0 .. bch-1 only, N = 64, a 16 KB W chunk: half the
 // W bytes per mask byte over the SM-to-L2 path and half the MMA width).
-constexpr int F_NS = 2;                              // staging slots (pairs)
-constexpr int F_NWS = 3;                             // W slots
 constexpr uint32_t F_STG = 128 * 64 * 4;             // one row block's chunk (float)
-constexpr uint32_t F_PSTG = 2 * F_STG;               // one staging slot: both blocks
-constexpr uint32_t F_W = 2 * OPER;                   // one W slot (a chunk's hi and lo at NB = 64)
-constexpr uint32_t F_WOFF = F_NS * F_PSTG;
-constexpr uint32_t F_MISC = F_WOFF + F_NWS * F_W;
-constexpr uint32_t F_SMEM = F_MISC + 384 + 1024;
 constexpr uint32_t F_ACC = 128;                      // accumulator columns per block
 constexpr uint32_t F_COL_A = 2 * F_ACC;
 constexpr uint32_t F_TMEM_COLS = 512;
-static_assert(F_SMEM <= SMEM_LIMIT, "forward row pass: shared memory");
+
+template <int KIND, int NB>
+struct FwdCfg {
+  static constexpr bool U8 = KIND == OI_FIELD_U8;
+  static constexpr uint32_t BLK = U8 ? 128 * 64 : F_STG;   // one block's chunk
+  static constexpr uint32_t PSTG = 2 * BLK;                 // one staging slot: both blocks
+  static constexpr uint32_t WOP = 2 * NB * 128;             // one precision of a W chunk: [2 NB rows][64 bf16]
+  static constexpr uint32_t FW = 2 * WOP;                   // one W chunk (hi, lo) and its slot
+  // float32 chunks: 2 slots of 64 KB beside 3 W slots of 32 KB (NB = 64), 3 beside 2 of 16 KB (NB = 32);
+  // uint8 chunks: 8 slots of 16 KB
+  static constexpr int NS = U8 ? 8 : (NB == 32 ? 3 : 2);
+  static constexpr int NWS = (!U8 && NB == 32) ? 2 : 3;
+  static constexpr uint32_t WOFF = NS * PSTG;
+  static constexpr uint32_t MISC = WOFF + NWS * FW;
+  static constexpr uint32_t SMEM = MISC + 384 + 1024;
+  // mbarriers from MISC: sfull[NS], sfree[NS], wfull[NWS], wdone[NWS], conv[2], adone[2], accf, acce, fin;
+  // the tensor-memory address at MISC + 248, the lo flags at MISC + 256 .. 319
+  static constexpr uint32_t SFULL = 0, SFREE = 8 * NS, WFULL = 16 * NS, WDONE = WFULL + 8 * NWS,
+                            CONV = WDONE + 8 * NWS, ADONE = CONV + 16, ACCF = ADONE + 16, ACCE = ACCF + 8,
+                            FIN = ACCE + 8;
+  static_assert(FIN + 8 <= 248, "forward row pass: barriers");
+  static_assert(SMEM <= SMEM_LIMIT, "forward row pass: shared memory");
+};
 
 struct FwdArgs {
   long long rows;           // batch * ny (a multiple of 128)
@@ -96,22 +112,24 @@ constexpr int F_NT = NT + 32;   // + a warp issuing the W loads
 template <int KIND, int NB>
 __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const __grid_constant__ CUtensorMap mask_map) {
   static_assert(NB == 64 || NB == 32, "forward row pass: NB");
-  constexpr uint32_t WOP = 2 * NB * 128;             // one precision of a W chunk: [2 NB rows][64 bf16]
-  constexpr uint32_t FW = 2 * WOP;                   // one W chunk (hi, lo)
+  using Cfg = FwdCfg<KIND, NB>;
+  constexpr int F_NS = Cfg::NS, F_NWS = Cfg::NWS;
+  constexpr uint32_t WOP = Cfg::WOP, FW = Cfg::FW;
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* gbase = smem_raw + (base - raw);
-  const uint32_t misc = base + F_MISC;
-  // barriers: sfull[2] (staging landed), sfree[2] (staging read), wfull[3] (W landed), wdone[3] (MMAs reading
-  // the W slot finished), conv[2] (A slot written), adone[2] (MMAs reading the A slot finished), accf
-  // (accumulators complete), acce (accumulators drained), fin (every issued MMA finished, at the end)
-  const uint32_t sfull = misc, sfree = misc + 16, wfull = misc + 32, wdone = misc + 56, conv = misc + 80,
-                 adone = misc + 96, accf = misc + 112, acce = misc + 120, fin = misc + 128;
-  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + F_MISC + 192);
+  const uint32_t misc = base + Cfg::MISC;
+  // barriers: sfull (staging landed), sfree (staging read), wfull (W landed), wdone (MMAs reading the W slot
+  // finished), conv[2] (A slot written), adone[2] (MMAs reading the A slot finished), accf (accumulators
+  // complete), acce (accumulators drained), fin (every issued MMA finished, at the end)
+  const uint32_t sfull = misc + Cfg::SFULL, sfree = misc + Cfg::SFREE, wfull = misc + Cfg::WFULL,
+                 wdone = misc + Cfg::WDONE, conv = misc + Cfg::CONV, adone = misc + Cfg::ADONE,
+                 accf = misc + Cfg::ACCF, acce = misc + Cfg::ACCE, fin = misc + Cfg::FIN;
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(gbase + Cfg::MISC + 248);
   // per A slot and converter warp: 1 when the warp's part of the chunk has a non-zero bf16 lo half (a mask value
   // not exact in bf16); when no warp sets it the lo x hi products are exactly zero and are not issued
-  volatile uint32_t* lo_flags = (volatile uint32_t*)(gbase + F_MISC + 256);
+  volatile uint32_t* lo_flags = (volatile uint32_t*)(gbase + Cfg::MISC + 256);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int KC = a.nx / 64;
   const long long R = a.rows / 128;                  // row blocks
@@ -120,9 +138,9 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
   const long long i0 = (long long)blockIdx.x * items / G, i1 = ((long long)blockIdx.x + 1) * items / G;
   const long long nchunks = (i1 - i0) * KC;
   constexpr bool U8 = KIND == OI_FIELD_U8;
-  constexpr uint32_t BLK = U8 ? 128 * 64 : F_STG;    // bytes of one block's chunk
+  constexpr uint32_t BLK = Cfg::BLK;
 
-  if (warp == 0) tmem_alloc(misc + 192, F_TMEM_COLS);
+  if (warp == 0) tmem_alloc(misc + 248, F_TMEM_COLS);
   if (tid == 0) {
     for (int s = 0; s < F_NS; ++s) {
       mbar_init(sfull + 8 * s, 1);
@@ -160,12 +178,12 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
           fail_status();
           break;
         }
-        const uint32_t dst = base + st.slot * F_PSTG;
+        const uint32_t dst = base + st.slot * Cfg::PSTG;
         expect_tx(sfull + 8 * st.slot, 2 * BLK);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {   // rows past the tensor's end read as zeros
-          tma_load_2d(dst + h * F_STG, &mask_map, 64 * c, y + 128 * h, sfull + 8 * st.slot);
-          if (!U8) tma_load_2d(dst + h * F_STG + F_STG / 2, &mask_map, 64 * c + 32, y + 128 * h, sfull + 8 * st.slot);
+          tma_load_2d(dst + h * BLK, &mask_map, 64 * c, y + 128 * h, sfull + 8 * st.slot);
+          if (!U8) tma_load_2d(dst + h * BLK + BLK / 2, &mask_map, 64 * c + 32, y + 128 * h, sfull + 8 * st.slot);
         }
         st.next(F_NS);
         if (++c == KC) {
@@ -186,7 +204,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
           break;
         }
         expect_tx(wfull + 8 * ws.slot, FW);
-        bulk_g2s(base + F_WOFF + ws.slot * F_W, a.w + (long long)c * FW, FW, wfull + 8 * ws.slot);
+        bulk_g2s(base + Cfg::WOFF + ws.slot * FW, a.w + (long long)c * FW, FW, wfull + 8 * ws.slot);
         ws.next(F_NWS);
         if (++c == KC) c = 0;
       }
@@ -209,7 +227,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
         }
         issued = true;
         fence_after();
-        const uint32_t wch = base + F_WOFF + ws.slot * F_W;
+        const uint32_t wch = base + Cfg::WOFF + ws.slot * FW;
         uint32_t lo_any = 0;
         if (!U8) {   // the eight warps' flags of this A slot, as two 16-byte reads
           uint32_t f0, f1, f2, f3, f4, f5, f6, f7;
@@ -291,7 +309,7 @@ __global__ void __launch_bounds__(F_NT, 1) rows_fwd_tc_kernel(FwdArgs a, const _
 #pragma unroll 1
       for (int h = 0; h < 2; ++h) {
         float v[32];
-        const unsigned char* blk = gbase + st.slot * F_PSTG + h * F_STG;
+        const unsigned char* blk = gbase + st.slot * Cfg::PSTG + h * BLK;
         if (U8) {
           const unsigned char* row = blk + r * 64;   // 64-byte swizzle: chunk j at j ^ ((r >> 1) & 3)
 #pragma unroll
@@ -748,16 +766,17 @@ static int rows_fwd_launch(const void* field, int kind, int batch, int ny, int n
                          u8 ? 64 : 32, 128, u8 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B);
   if (rc) return rc;
   if (u8) {
-    rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_U8, NB>, rt::F_SMEM, what);
+    constexpr uint32_t smem = rt::FwdCfg<OI_FIELD_U8, NB>::SMEM;
+    rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_U8, NB>, smem, what);
     if (rc) return rc;
-    (void)launch_pdl(rt::rows_fwd_tc_kernel<OI_FIELD_U8, NB>, dim3((unsigned)ctas), dim3(rt::F_NT), rt::F_SMEM, s, a,
-                     map);
+    (void)launch_pdl(rt::rows_fwd_tc_kernel<OI_FIELD_U8, NB>, dim3((unsigned)ctas), dim3(rt::F_NT), smem, s, a, map);
     oi::note_launch();
   } else {
-    rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32, NB>, rt::F_SMEM, what);
+    constexpr uint32_t smem = rt::FwdCfg<OI_FIELD_REAL_F32, NB>::SMEM;
+    rc = ensure_smem((const void*)rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32, NB>, smem, what);
     if (rc) return rc;
-    (void)launch_pdl(rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32, NB>, dim3((unsigned)ctas), dim3(rt::F_NT), rt::F_SMEM,
-                     s, a, map);
+    (void)launch_pdl(rt::rows_fwd_tc_kernel<OI_FIELD_REAL_F32, NB>, dim3((unsigned)ctas), dim3(rt::F_NT), smem, s, a,
+                     map);
     oi::note_launch();
   }
   return check_launch(what);
