@@ -14,9 +14,10 @@
 // N = 256 rows, K = (re | im) x 64 band columns) = C x V^T, C = [cos | sin] of the x tile (constant image,
 // streamed in 16 KB pieces), V = v as bf16 hi / lo operand tiles (resident while the row-block pair lasts).  The
 // accumulator's lanes are the rows (forward) or the columns (inverse), so every warp store of the result is one
-// coalesced segment.  The forward pass takes its A operand (converted on the fly) from tensor memory; the
-// inverse reads both operands from shared memory (at N = 128 an A operand in tensor memory halves the MMA rate,
-// which only the forward pass's conversion justifies).
+// coalesced segment.  The forward pass takes its A operand (converted on the fly) from tensor memory, so its
+// converters write no shared memory; the inverse reads both operands from shared memory, where its V tiles land
+// by TMA.  (Measured issue rates, M = 128, K = 16: 64 cycles at N = 128 and 128 at N = 256 with either operand
+// source; at N = 64, 48 cycles from shared memory and 56 with A in tensor memory, against 32.)
 //
 // Roles (352 threads): warps 0-7 convert the staged mask chunks into the A operand in tensor memory (forward)
 // and drain finished accumulators to global memory (two warps per tensor-memory lane quarter); warps 8 and 10
