@@ -122,6 +122,24 @@ __device__ __forceinline__ float2 outer_bin(const float2* ys, const float2* t1, 
   for (int n1 = 0; n1 < N1; ++n1) cfma(acc, row[n1], sgn<SIGN>(tw[n1]));
   return acc;
 }
+// Two bins at once (ka, kb), each summed in two interleaved halves: four independent chains.
+template <int SIGN, int N1>
+__device__ __forceinline__ void outer_bin2(const float2* ys, const float2* t1, int ka, int kb, float2& va, float2& vb) {
+  const float2* ra = ys + (ka & 31) * (N1 + 1);
+  const float2* rb = ys + (kb & 31) * (N1 + 1);
+  const float2* ta = t1 + (ka >> 5) * N1;
+  const float2* tb = t1 + (kb >> 5) * N1;
+  float2 a0 = make_float2(0.f, 0.f), a1 = a0, b0 = a0, b1 = a0;
+#pragma unroll 4
+  for (int n1 = 0; n1 < N1; n1 += 2) {
+    cfma(a0, ra[n1], sgn<SIGN>(ta[n1]));
+    cfma(a1, ra[n1 + 1], sgn<SIGN>(ta[n1 + 1]));
+    cfma(b0, rb[n1], sgn<SIGN>(tb[n1]));
+    cfma(b1, rb[n1 + 1], sgn<SIGN>(tb[n1 + 1]));
+  }
+  va = make_float2(a0.x + a1.x, a0.y + a1.y);
+  vb = make_float2(b0.x + b1.x, b0.y + b1.y);
+}
 
 // --------------------------------------------------------------------------------- forward, rows
 // field rows [nrows = batch*ny][N] (real or u8) -> t[b][ic][y], ic over the band m0c .. m0c+bc-1.
@@ -188,9 +206,20 @@ __global__ void __launch_bounds__(256, 3) fft_rows_fwd_kernel(const void* __rest
 // SYM: t holds the non-negative columns kx = 0 .. bc-1 of a real mask's row transform and the band is the
 // symmetric bco x br band (m0c = -(bco-1)/2, m0r = -(br-1)/2): column kx lands at ic = kx + (bco-1)/2 and, for
 // kx > 0, its mirror band[-ky][-kx] = conj(band[ky][kx]) at row br-1-ir, column (bco-1)/2 - kx.
-// Blocks of COLS_T threads (G = COLS_T / N1 columns each): at the symmetric band's 30 columns per image a batch
-// of 64 has 1920 columns, which 8-column blocks spread over 148 SMs as 0.54 waves.
+// Blocks of COLS_T threads (G = COLS_T / N1 columns each, 32 KB of t): the block's columns are contiguous in t
+// and are staged into shared memory by 16-byte asynchronous copies (cp.async, completed per thread: no waits on
+// another thread's progress), from where each thread reads its 32 strided values; the twiddled rows then reuse
+// the same shared memory.  At the symmetric band's 30 columns per image a batch of 64 has 1920 columns: 480
+// blocks, all resident at once.
 constexpr int COLS_T = 128;
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
 
 template <int N1, bool SYM>
 __global__ void __launch_bounds__(COLS_T, 6) fft_cols_fwd_kernel(const float2* __restrict__ t, long long ncols, int bc,
@@ -203,20 +232,29 @@ __global__ void __launch_bounds__(COLS_T, 6) fft_cols_fwd_kernel(const float2* _
   const float2* t1 = wn_g + 32 * N1;
   float2* ys = (float2*)smem_raw;
   const int tid = threadIdx.x, g = tid / N1, n1 = tid % N1;
-  const long long col = (long long)blockIdx.x * G + g;
+  const long long col0 = (long long)blockIdx.x * G, col = col0 + g;
   pdl_trigger();
   pdl_wait();   // t comes from the row pass
+  {
+    const long long cols = ncols - col0 < G ? ncols - col0 : G;
+    const int chunks = (int)(cols * N / 2);   // 16-byte pieces of the block's contiguous columns
+    const float4* src = (const float4*)(t + col0 * N);
+    float4* dst = (float4*)smem_raw;
+    for (int c = tid; c < chunks; c += COLS_T) cp_async16(dst + c, src + c);
+    cp_async_wait_all();
+    __syncthreads();
+  }
   float2 z[32];
   if (col < ncols) {
-    const float2* src = t + col * N;
+    const float2* stg = ys + g * N;
 #pragma unroll
-    for (int n2 = 0; n2 < 32; ++n2) z[n2] = src[n1 + N1 * n2];
+    for (int n2 = 0; n2 < 32; ++n2) z[n2] = stg[n1 + N1 * n2];
   } else {
 #pragma unroll
     for (int n2 = 0; n2 < 32; ++n2) z[n2] = make_float2(0.f, 0.f);
   }
+  __syncthreads();   // the stage is overwritten by the twiddled rows below
   fft32<+1>(z);
-  __syncthreads();
   float2* yg = ys + g * 32 * (N1 + 1);
   twiddle_store<+1, N1>(z, t2, n1, yg);
   __syncthreads();
@@ -229,12 +267,18 @@ __global__ void __launch_bounds__(COLS_T, 6) fft_cols_fwd_kernel(const float2* _
       float2 v = outer_bin<+1, N1>(yg, t1, (m0r + ir) & (N - 1));
       band[(b * br + ir) * (long long)bc + ic] = make_float2(v.x * sc, v.y * sc);
     }
-  } else {
+  } else {   // bins ir and ir + N1 together
     const int h = (bco - 1) / 2;
-    for (int ir = n1; ir < br; ir += N1) {
-      float2 v = outer_bin<+1, N1>(yg, t1, (m0r + ir) & (N - 1));
-      band[(b * br + ir) * (long long)bco + h + ic] = make_float2(v.x * scale, v.y * scale);
-      if (ic > 0) band[(b * br + br - 1 - ir) * (long long)bco + h - ic] = make_float2(v.x * scale, -v.y * scale);
+    for (int ir = n1; ir < br; ir += 2 * N1) {
+      float2 v[2];
+      outer_bin2<+1, N1>(yg, t1, (m0r + ir) & (N - 1), (m0r + ir + N1) & (N - 1), v[0], v[1]);
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int r = ir + u * N1;
+        if (r >= br) break;
+        band[(b * br + r) * (long long)bco + h + ic] = make_float2(v[u].x * scale, v[u].y * scale);
+        if (ic > 0) band[(b * br + br - 1 - r) * (long long)bco + h - ic] = make_float2(v[u].x * scale, -v[u].y * scale);
+      }
     }
   }
 }
@@ -599,6 +643,7 @@ template <int N1, bool SYM = false>
 static int cols_fwd(const float2* t, int batch, int bc, const float2* wn_y, int m0r, int br, float scale,
                     float2* band, cudaStream_t s, int bco = 0, int dbl_from = 0x7fffffff) {
   constexpr int G = COLS_T / N1;
+  if ((uintptr_t)t % 16) return fail(OI_EINVAL, "oi_band_spectrum_fft/cols: scratch must be 16-byte aligned");
   size_t smem = smem_cols_fwd<N1>();
   int rc = set_smem(fft_cols_fwd_kernel<N1, SYM>, smem, "oi_band_spectrum_fft/cols");
   if (rc) return rc;
