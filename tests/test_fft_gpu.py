@@ -102,6 +102,33 @@ def test_large_band_coarse_256_fft_vs_dft_and_oracle(eng):
     assert N.device_status() == 0
 
 
+def test_clip_2048_large_band_vs_oracle(eng):
+    """A 2048 x 2048 clip at 2 nm per pixel (4096 nm period, band 117 > 64: coarse grid 256 x 256, the FP32 FFT
+    form the served 2048-point clips take) against the FP64 oracle with the same SOCS kernels, at the FP32
+    forms' bound of 1e-5 of peak."""
+    from opticalimaging_b200 import imaging, workloads as W, _native as N
+    from opticalimaging_b200.params import Scatter
+    sr, po, nm = W.config3_optics(order=8)
+    model = imaging.socs_model(sr, po, nm, 4096.0, 4096.0, 2048, 2048)
+    assert model.band.br > 64 and model.plan.mr == 256 and model.plan.fft
+    rng = np.random.default_rng(21)
+    masks = np.stack([W.rect_mask(2048, 2048, 4096.0, 4096.0, 30, 40, 600, rng) for _ in range(2)])
+    img = model.image(torch.from_numpy(masks).cuda())[:, 0].cpu().numpy()
+    b = model.band
+    full = torch.zeros((2048, 2048, model.count), dtype=torch.complex64, device=model.device)
+    full[:b.br, :b.bc, :] = model.pupils[0].permute(1, 2, 0)
+    K = torch.roll(full, shifts=(b.m0r, b.m0c), dims=(0, 1)).cpu().numpy().astype(np.complex128)
+    del full
+    sc = Scatter()
+    sc.Period_X = sc.Period_Y = 4096.0
+    for i in range(2):
+        sc.ScatterField = W.thin_field(masks[i])
+        err = rel_err(img[i], O.socs(sc, K, sr, po))
+        print(f'2048 x 2048 clip {i}: max error {err:.2e} of peak')
+        assert err < 1e-5
+    assert N.device_status() == 0
+
+
 @pytest.mark.parametrize('nparts,count,m,br,bc', [(3, 2, 256, 117, 59), (1, 3, 256, 70, 66), (2, 1, 512, 128, 128)])
 def test_coarse_half_spectrum_fft(eng, nparts, count, m, br, bc):
     """oi_coarse_half_spectrum_fft (parts summed in the row pass, columns qc > 0 doubled) against FP64
