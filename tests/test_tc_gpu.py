@@ -134,6 +134,45 @@ def test_tc_ranges_cross_images_deterministic(oi, batch):
     assert N.device_status() == 0
 
 
+@pytest.mark.parametrize('band', [(-29, 59, -29, 59), (-20, 41, -13, 27)])
+@pytest.mark.parametrize('ctas', [1, 3, 7])
+def test_coherent_tc_long_ranges_vs_fp64(oi, band, ctas):
+    """Few CTAs, so each runs tens of fields through its pipeline (two operand slots for the symmetric band, one
+    for the asymmetric band), against the coarse intensity evaluated in FP64 by torch; the partial sums of any
+    cut add up to the same image."""
+    from opticalimaging_b200 import _native as N
+    from opticalimaging_b200.engine import Band, Plan, TC_COARSE
+    dev = torch.device('cuda')
+    b = Band(*band)
+    batch, nk = 3, 9
+    g = torch.Generator().manual_seed(ctas + b.bc)
+    spec = torch.randn((batch, 1, b.br, b.bc), dtype=torch.complex64, generator=g)
+    pup = torch.randn((1, nk, b.br, b.bc), dtype=torch.complex64, generator=g)
+    w = torch.rand((1, nk), generator=g) + 0.5
+    plan = Plan.get(256, 256, b, dev, coarse=TC_COARSE)
+    s = N.stream_handle(dev)
+    specd, pupd, wd = spec.to(dev), pup.to(dev), w.to(dev)
+
+    def run(c, nparts):
+        coarse = torch.full((nparts, batch, 1, 128, 128), float('nan'), device=dev)
+        N.call('oi_coherent_coarse_tc', N.ptr(specd), batch, 1, b.m0r, b.br, b.m0c, b.bc, N.ptr(pupd), 0, N.ptr(wd),
+               1, nk, N.ptr(plan.tc_constants()), c, nparts, N.ptr(coarse), s)
+        return coarse.double().sum(dim=0)[:, 0].cpu()
+
+    got = run(ctas, ctas + 1)            # slots past the cut's own are zero-filled
+    default = run(*N.tc_layout(batch, nk))
+    # FP64: E[sr][sc] = sum_ir sum_ic exp(-2 pi i ((m0r+ir) sr + (m0c+ic) sc) / 128) P[ir][ic] band[ir][ic]
+    s128 = torch.arange(128, dtype=torch.float64)
+    cr = torch.exp(-2j * np.pi * torch.outer(s128, b.m0r + torch.arange(b.br, dtype=torch.float64)) / 128)
+    cc = torch.exp(-2j * np.pi * torch.outer(s128, b.m0c + torch.arange(b.bc, dtype=torch.float64)) / 128)
+    a = spec[:, 0, None].to(torch.complex128) * pup[0, None].to(torch.complex128)   # [batch][nk][br][bc]
+    e = torch.einsum('ri,bkij,cj->bkrc', cr, a, cc)
+    ref = torch.einsum('k,bkrc->brc', w[0].double(), e.abs() ** 2)
+    assert rel_err(got.numpy(), ref.numpy()) < BF16X3_VS_FP64
+    assert rel_err(got.numpy(), default.numpy()) < 1e-6
+    assert N.device_status() == 0
+
+
 @pytest.mark.parametrize('ny,nx,band', [
     (256, 256, (-15, 31, -15, 31)),
     (512, 1024, (-29, 59, -29, 59)),
