@@ -609,7 +609,9 @@ def kernel_rooflines(sk, masks, reps=10):
     s = N.stream_handle(dev)
     t = torch.empty(B * sk.ny * b.bc, dtype=torch.complex64, device=dev)
     band = band_spectrum(masks, N.FIELD_REAL_F32, plan, form='bf16x3')
-    ctas, nparts = N.tc_layout(B, sk.count)   # nparts also sizes the synthesis kernel's partial sums
+    pupils, weights = sk.fields_for(N.FIELD_REAL_F32)   # the fields the image path runs for real masks
+    nf = pupils.shape[1]
+    ctas, nparts = N.tc_layout(B, nf)   # nparts also sizes the synthesis kernel's partial sums
     coarse = torch.empty((nparts, B, 1, 128, 128), device=dev)
     v = torch.zeros(B * b.bc * sk.ny, dtype=torch.complex64, device=dev)
     tiles = torch.empty(B * sk.ny * 512, dtype=torch.uint8, device=dev)
@@ -628,7 +630,7 @@ def kernel_rooflines(sk, masks, reps=10):
         "synth_tc": lambda: N.call('oi_synth_tiles_tc', N.ptr(scoarse), nparts, B, b.br, b.bc,    # noqa: E731
                                    N.ptr(tplan.synth_consts()), sk.ny, N.ptr(stiles), s),
         "coherent_tc": lambda: N.call('oi_coherent_coarse_tc', N.ptr(band), B, 1, b.m0r, b.br, b.m0c, b.bc,
-                                      N.ptr(sk.pupils), 0, N.ptr(sk.weights), 1, sk.count,
+                                      N.ptr(pupils), 0, N.ptr(weights), 1, nf,
                                       N.ptr(tplan.tc_constants()), ctas, nparts, N.ptr(coarse), s),
         "rows_inv_tc": lambda: N.call('oi_rows_inv_tc_tiles', N.ptr(tiles), B, sk.ny, sk.nx,
                                       N.ptr(tplan.rows_consts(1)), N.ptr(out), s),
@@ -649,12 +651,13 @@ def kernel_rooflines(sk, masks, reps=10):
         torch.cuda.synchronize()
         sec = e0.elapsed_time(e1) / 1e3 / reps
         if name == "coherent_tc":
-            flops = 8.0 * B * sk.count * (128 * b.br * b.bc + 128 * 128 * b.br)
+            flops = 8.0 * B * nf * (128 * b.br * b.bc + 128 * 128 * b.br)
             ach = flops / sec / 1e12
             res[name] = {"bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16,
                          "traffic": NCU_TRAFFIC.get(name), "us": sec * 1e6, "peak_source": src,
-                         "algorithmic": "8 (M B^2 + M^2 B) flops per field, M = 128, B = 59, 24 fields per image",
-                         "executed_tflops": 3 * 8.0 * B * sk.count * (128 * 64 * 64 + 128 * 128 * 64) / sec / 1e12}
+                         "algorithmic": f"8 (M B^2 + M^2 B) flops per field, M = {128}, B = {b.br}, {nf} fields per "
+                                        f"image (the {sk.count} SOCS kernels of a real mask as packed real fields)",
+                         "executed_tflops": 3 * 8.0 * B * nf * (128 * 64 * 64 + 128 * 128 * 64) / sec / 1e12}
         elif name == "synth_tc":   # two real GEMMs per image: U = c G (128 x 2bc x 128), v = A U (ny x 2bc x 128)
             flops = 2.0 * B * (128 * 2 * b.bc * 128 + sk.ny * 2 * b.bc * 128)
             ach = flops / sec / 1e12

@@ -401,6 +401,54 @@ def centred(start: int, n: int) -> int:
 
 
 # ------------------------------------------------------------------------------------- resident models
+def pack_real_fields(pupils: torch.Tensor, weights: torch.Tensor, band: Band, tol: float = 1e-14):
+    """The fields of a model, packed two to a transform for real masks.
+
+    A real mask's band spectrum c is Hermitian on a band centred on frequency 0: c(-f) = conj c(f).  So is the
+    product of two Hermitian arrays, and a Hermitian spectrum transforms to a real field.  A weighted field
+    Q = sqrt(w) P splits into the Hermitian parts H1 = (Q + conj Q(-f)) / 2 and H2 = (Q - conj Q(-f)) / 2i,
+    Q = H1 + i H2, so IDFT(Q c) = R1 + i R2 with R1, R2 real and w |IDFT(P c)|^2 = R1^2 + R2^2.  The image
+    is thus a sum of squares of real fields, sum_j (L h_j)^2, L the real linear map from a Hermitian array to a
+    real field, and depends on the 2K arrays h_j (as real vectors [Re | Im]) only through S = sum_j h_j h_j^T.
+    With U an orthonormal basis of the range of the Gram matrix h h^T (FP64 eigenvectors whose eigenvalue
+    exceeds `tol` of the largest), g = U^T h gives the same S from rank(h) arrays, still Hermitian (real
+    combinations).  Two real fields g1, g2 packed as g1 + i g2 give back |IDFT((g1 + i g2) c)|^2 =
+    (L g1)^2 + (L g2)^2.  A plane's K fields so become ceil(rank / 2) fields of weight 1.  SOCS kernels of optics
+    symmetric under f -> -f span K real dimensions -- degenerate eigenpairs, which an eigensolver returns as
+    complex mixtures, included -- so K kernels pack into ceil(K / 2) transforms.  The identity needs nothing of
+    the kernels, only a real single-channel mask, and holds for every form of the coherent sum.
+
+    Returns (pupils [Z, K', br, bc] complex64, weights [Z, K'] float32) with planes padded by zero fields of
+    weight 0, or None when the band is not centred, a weight is negative, or nothing is gained (K' >= K).
+    """
+    br, bc = pupils.shape[-2], pupils.shape[-1]
+    if not (br % 2 == 1 and bc % 2 == 1 and band.m0r == -(br - 1) // 2 and band.m0c == -(bc - 1) // 2):
+        return None
+    if bool((weights < 0).any()):
+        return None
+    q = pupils.to(torch.complex128) * weights.to(torch.float64).sqrt()[..., None, None]
+    m = torch.flip(q, dims=(-2, -1)).conj()                            # conj Q(-f) on the centred band
+    h = torch.stack(((q + m) / 2, (q - m) / 2j), dim=2).flatten(1, 2)  # [Z, 2K, br, bc], Hermitian
+    planes = []
+    for z in range(h.shape[0]):
+        v = torch.cat((h[z].real, h[z].imag), dim=-1).flatten(1).cpu()   # [2K, 2 br bc] real vectors
+        sig, u = torch.linalg.eigh(v @ v.T)
+        keep = sig > tol * max(float(sig.max()), 1e-300)
+        g = (u[:, keep].T @ v).view(-1, br, 2 * bc)
+        planes.append(torch.complex(g[..., :bc], g[..., bc:]))
+    kp = max(1, max((g.shape[0] + 1) // 2 for g in planes))
+    if kp >= pupils.shape[1]:
+        return None
+    out = torch.zeros((len(planes), kp, br, bc), dtype=torch.complex128)
+    w = torch.zeros((len(planes), kp), dtype=torch.float32)
+    for z, g in enumerate(planes):
+        j = g.shape[0]
+        out[z, :(j + 1) // 2] = g[0::2]
+        out[z, :j // 2] += 1j * g[1::2]
+        w[z, :(j + 1) // 2] = 1.0
+    return out.to(pupils.device, torch.complex64).contiguous(), w.to(pupils.device)
+
+
 class CoherentModel:
     """Fields resident on the device for one optics key and grid: pupils [Z, K, br, bc] complex64 with weights
     [Z, K] on `band`, for a ny x nx grid.  image() of a batch of masks is
@@ -426,6 +474,9 @@ class CoherentModel:
             raise ValueError(f'the bf16x3 form covers bands up to 64 x 64 (this one is {band.br} x {band.bc})')
         self.band, self.ny, self.nx, self.kind, self.form = band, ny, nx, kind, form
         self.plan = Plan.get(ny, nx, band, self.device)
+        # the same images from fewer transforms for real single-channel masks (pack_real_fields), or None; SOCS
+        # models only, whose fields and weights stay fixed (an Abbe model's weights follow its source)
+        self.packed = pack_real_fields(self.pupils, self.weights, band) if kind == 'socs' else None
 
     @property
     def planes(self):
@@ -434,6 +485,13 @@ class CoherentModel:
     @property
     def count(self):
         return self.pupils.shape[1]
+
+    def fields_for(self, kind: int, nch: int = 1):
+        """(pupils, weights) the coherent sum of image() uses for masks of this kind: the packed fields for real
+        single-channel masks when packing gains, else the model's own."""
+        if self.packed is not None and kind in (N.FIELD_REAL_F32, N.FIELD_U8) and nch == 1:
+            return self.packed
+        return self.pupils, self.weights
 
     @property
     def nbytes(self):
@@ -477,7 +535,8 @@ class CoherentModel:
         _mark(marks, 'start')
         band = band_spectrum(masks.contiguous(), kind, self.plan, nch=nch, scale=scale, form=form)
         _mark(marks, 'band_spectrum')
-        return coherent_image(band, self.pupils, self.weights, self.plan, out=out, marks=marks, form=form)
+        pupils, weights = self.fields_for(kind, nch)
+        return coherent_image(band, pupils, weights, self.plan, out=out, marks=marks, form=form)
 
 
     def image_host(self, masks: torch.Tensor, out: torch.Tensor, chunk: int = 16, check: bool = False,

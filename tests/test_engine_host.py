@@ -1,6 +1,7 @@
 """Host-side logic of the engine (no GPU): band selection, kernel support, field split, coarse sizes."""
 import math
 
+import numpy as np
 import torch
 
 from opticalimaging_b200 import engine as E
@@ -122,3 +123,83 @@ def test_plan_cache_is_bounded_lru(monkeypatch):
     assert FakePlan.get(8, 8, band, 'cpu') is first
     FakePlan.get(9, 9, band, 'cpu')                 # evicted earlier: built again
     assert made.count((9, 9)) == 2 and made.count((8, 8)) == 1
+
+
+def _coherent_sum_fp64(pupils, weights, band, mask):
+    """sum_k w_k |IDFT(P_k .* c)|^2 on the mask's grid in FP64, c the band of the mask's DFT (numpy)."""
+    ny, nx = mask.shape
+    spec = np.fft.fft2(mask) / (ny * nx)
+    rows = (band.m0r + np.arange(band.br)) % ny
+    cols = (band.m0c + np.arange(band.bc)) % nx
+    c = spec[np.ix_(rows, cols)]
+    out = np.zeros((pupils.shape[0], ny, nx))
+    for z in range(pupils.shape[0]):
+        for k in range(pupils.shape[1]):
+            full = np.zeros((ny, nx), dtype=np.complex128)
+            full[np.ix_(rows, cols)] = pupils[z, k] * c
+            out[z] += weights[z, k] * np.abs(np.fft.ifft2(full) * ny * nx) ** 2
+    return out
+
+
+def test_packed_real_fields_give_the_same_images():
+    """For a real mask, kernels that are Hermitian up to a phase pack two to a transform and generic complex
+    kernels split into two real fields each; the packed set gives the same sum of |IDFT|^2 in FP64."""
+    import torch
+    from opticalimaging_b200.engine import Band, pack_real_fields
+    rng = np.random.default_rng(5)
+    band = Band(-7, 15, -5, 11)
+    herm = []
+    for _ in range(6):                 # Hermitian kernels times a random phase
+        h = rng.normal(size=(15, 11)) + 1j * rng.normal(size=(15, 11))
+        h = (h + np.conj(h[::-1, ::-1])) / 2
+        herm.append(h * np.exp(1j * rng.uniform(0, 2 * np.pi)))
+    generic = [rng.normal(size=(15, 11)) + 1j * rng.normal(size=(15, 11)) for _ in range(3)]
+    P = np.stack(herm + generic)[None]
+    w = rng.uniform(0.2, 2.0, size=(1, 9))
+    packed = pack_real_fields(torch.from_numpy(P), torch.from_numpy(w), band)
+    assert packed is not None
+    Q, wq = packed
+    assert Q.shape == (1, 6, 15, 11)           # J = 6 + 2 * 3 = 12 real fields -> 6 transforms instead of 9
+    assert torch.equal(wq, torch.ones((1, 6)))
+    for seed in range(3):
+        mask = (np.random.default_rng(seed).uniform(size=(40, 36)) > 0.6).astype(np.float64)
+        a = _coherent_sum_fp64(P, w, band, mask)
+        b = _coherent_sum_fp64(Q.numpy().astype(np.complex128), wq.numpy(), band, mask)
+        assert np.max(np.abs(a - b)) / np.max(a) < 1e-6     # the packed set is stored as complex64
+
+
+def test_packing_declines_what_it_cannot_use():
+    """No packing for an off-centre band, a negative weight, or fields that gain nothing (all generic)."""
+    import torch
+    from opticalimaging_b200.engine import Band, pack_real_fields
+    rng = np.random.default_rng(6)
+    P = torch.from_numpy(rng.normal(size=(1, 4, 9, 9)) + 1j * rng.normal(size=(1, 4, 9, 9)))
+    w = torch.ones((1, 4), dtype=torch.float64)
+    assert pack_real_fields(P, w, Band(-3, 9, -4, 9)) is None          # not centred on frequency 0
+    assert pack_real_fields(P, w, Band(-4, 9, -4, 9)) is None          # 8 real fields: 4 transforms again
+    h = (P + torch.flip(P, dims=(-2, -1)).conj()) / 2
+    assert pack_real_fields(h, w, Band(-4, 9, -4, 9)) is not None
+    assert pack_real_fields(h, -w, Band(-4, 9, -4, 9)) is None
+
+
+def test_packing_sees_through_degenerate_mixtures():
+    """Kernels that are unitary mixtures of Hermitian ones ((A + iB) / sqrt 2, (A - iB) / sqrt 2: what an
+    eigensolver may return for a degenerate pair) span two real dimensions: two kernels, one transform."""
+    import torch
+    from opticalimaging_b200.engine import Band, pack_real_fields
+    rng = np.random.default_rng(8)
+    band = Band(-6, 13, -6, 13)
+    herm = []
+    for _ in range(4):
+        a = rng.normal(size=(13, 13)) + 1j * rng.normal(size=(13, 13))
+        herm.append((a + np.conj(a[::-1, ::-1])) / 2)
+    mix = [(herm[0] + 1j * herm[1]) / np.sqrt(2), (herm[0] - 1j * herm[1]) / np.sqrt(2),
+           (herm[2] + 1j * herm[3]) * np.exp(0.7j) / np.sqrt(2), (herm[2] - 1j * herm[3]) * np.exp(-1.1j) / np.sqrt(2)]
+    P = np.stack(mix)[None]
+    w = np.ones((1, 4))
+    Q, wq = pack_real_fields(torch.from_numpy(P), torch.from_numpy(w), band)
+    assert Q.shape == (1, 2, 13, 13)
+    mask = (np.random.default_rng(1).uniform(size=(30, 34)) > 0.5).astype(np.float64)
+    a = _coherent_sum_fp64(P, w, band, mask)
+    b = _coherent_sum_fp64(Q.numpy().astype(np.complex128), wq.numpy(), band, mask)
+    assert np.max(np.abs(a - b)) / np.max(a) < 1e-6
