@@ -590,7 +590,7 @@ def cpu_reference_sample(sk_info, masks_np, budget_s, threads):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the three largest kernels at this
 # workload, measured by ncu on a B200 for the kernels as they are built now; a constant, re-measured whenever
 # those kernels change (the date and the capture command travel with the numbers: NCU_TRAFFIC_SOURCE).
-NCU_TRAFFIC = {"rows_fwd_tc": 278.7e6, "rows_inv_tc": 249.3e6, "coherent_tc": 2.6e6, "synth_tc": 17.4e6}
+NCU_TRAFFIC = {"rows_fwd_tc": 278.7e6, "rows_inv_tc": 249.3e6, "coherent_tc": 2.3e6, "synth_tc": 17.4e6}
 NCU_TRAFFIC_SOURCE = ("ncu --set full --clock-control none -k regex:<kernel> -s 1 -c 1 on bench.py --steps 2 "
                       "--warmup 3 --no-cpu --no-serve --no-configs: dram__bytes_read.sum + dram__bytes_write.sum of "
                       "one 64-clip launch of each kernel, measured 2026-12-04")

@@ -173,6 +173,32 @@ def test_batched_socs_matches_single(oi):
             assert rel_err(one.numpy(), ref) < FP32_VS_FP64
 
 
+@pytest.mark.parametrize('form', ['fft', 'dft', 'bf16x3'])
+def test_packed_real_fields_match_the_kernels(oi, form):
+    """Configuration-3 optics (SOCS-24, centred 59 x 59 band): the model packs the 24 kernels into 12 real-field
+    pairs for real masks; float32 masks (packed fields) and the same masks as complex64 (the model's own 24
+    kernels) give the same images, and both match FP64."""
+    from opticalimaging_b200 import workloads as W, _native as N
+    from opticalimaging_b200.params import Scatter
+    sr, po, nm = W.config3_optics(order=24)
+    T, fg = oi.CalculateTCCMatrix(sr, [2048, 2048], po, 0.0, nm)
+    sk = oi.socs_kernels_from_tcc(T, fg, [256, 256], nm)
+    assert sk.packed is not None and sk.packed[0].shape[1] == 12
+    assert sk.fields_for(N.FIELD_COMPLEX_C64)[0] is sk.pupils
+    masks = W.manhattan_masks(3, 256, 2048.0, seed=4)
+    md = torch.from_numpy(masks).cuda()
+    packed = sk.image(md, form=form).cpu().numpy()
+    own = sk.image(md.to(torch.complex64).unsqueeze(-1), form=form).cpu().numpy()
+    bound = FP32_VS_FP64 if form != 'bf16x3' else 1e-4
+    assert rel_err(packed, own) < bound
+    sc = Scatter()
+    sc.Period_X = sc.Period_Y = 2048
+    sc.ScatterField = W.thin_field(masks[0])
+    ref = O.socs(sc, oi.DecomposeTCC_SOCS(T, fg, [256, 256], nm).cpu().numpy().astype(np.complex128), sr, po)
+    assert rel_err(packed[0], ref) < bound
+    assert N.device_status() == 0
+
+
 @pytest.mark.parametrize('ny,nx', [(17, 23), (64, 64), (33, 40)])
 def test_small_and_odd_grids_single_point(oi, ny, nx):
     """Edge cases: tiny odd grids, a single source point on axis (ideal low-pass), K=1."""
