@@ -512,7 +512,8 @@ def configs_measure(dev, steps=5):
     md = torch.from_numpy(masks).to(dev)
     sc.ScatterField = W.thin_field(masks[0])
     ref = O.abbe(sr, sc, po, nm)[0]
-    c1 = {"fields": model.count, "band": [model.band.br, model.band.bc], "batch": 64}
+    c1 = {"fields": model.count, "band": [model.band.br, model.band.bc], "batch": 64,
+          "packed_fields": None if model.packed is None else model.packed[0].shape[1]}
     for form in ('fft', 'bf16x3'):
         o = torch.empty((64, 1, 256, 256), device=dev)
         ms = time_device(lambda: model.image(md, out=o, form=form), steps)
@@ -526,7 +527,8 @@ def configs_measure(dev, steps=5):
                       for i in range(16)])
     md = torch.from_numpy(masks).to(dev)
     ref = O.abbe(sr, sc, po, nm)                   # clip 0 is the configuration's own (seed 2)
-    c2 = {"fields": model.count, "planes": model.planes, "band": [model.band.br, model.band.bc], "batch": 16}
+    c2 = {"fields": model.count, "planes": model.planes, "band": [model.band.br, model.band.bc], "batch": 16,
+          "packed_fields": None if model.packed is None else model.packed[0].shape[1]}
     for form in ('fft', 'bf16x3'):
         o = torch.empty((16, 5, 512, 512), device=dev)
         ms = time_device(lambda: model.image(md, out=o, form=form), steps)

@@ -431,22 +431,22 @@ def pack_real_fields(pupils: torch.Tensor, weights: torch.Tensor, band: Band, to
     h = torch.stack(((q + m) / 2, (q - m) / 2j), dim=2).flatten(1, 2)  # [Z, 2K, br, bc], Hermitian
     planes = []
     for z in range(h.shape[0]):
-        v = torch.cat((h[z].real, h[z].imag), dim=-1).flatten(1).cpu()   # [2K, 2 br bc] real vectors
-        sig, u = torch.linalg.eigh(v @ v.T)
+        v = torch.cat((h[z].real, h[z].imag), dim=-1).flatten(1)       # [2K, 2 br bc] real vectors
+        sig, u = torch.linalg.eigh((v @ v.T).cpu())                    # the Gram matrix's eigenpairs, on the host
         keep = sig > tol * max(float(sig.max()), 1e-300)
-        g = (u[:, keep].T @ v).view(-1, br, 2 * bc)
+        g = (u[:, keep].T.to(v.device) @ v).view(-1, br, 2 * bc)
         planes.append(torch.complex(g[..., :bc], g[..., bc:]))
     kp = max(1, max((g.shape[0] + 1) // 2 for g in planes))
     if kp >= pupils.shape[1]:
         return None
-    out = torch.zeros((len(planes), kp, br, bc), dtype=torch.complex128)
-    w = torch.zeros((len(planes), kp), dtype=torch.float32)
+    out = torch.zeros((len(planes), kp, br, bc), dtype=torch.complex128, device=pupils.device)
+    w = torch.zeros((len(planes), kp), dtype=torch.float32, device=pupils.device)
     for z, g in enumerate(planes):
         j = g.shape[0]
         out[z, :(j + 1) // 2] = g[0::2]
         out[z, :j // 2] += 1j * g[1::2]
         w[z, :(j + 1) // 2] = 1.0
-    return out.to(pupils.device, torch.complex64).contiguous(), w.to(pupils.device)
+    return out.to(torch.complex64).contiguous(), w
 
 
 class CoherentModel:
@@ -474,9 +474,9 @@ class CoherentModel:
             raise ValueError(f'the bf16x3 form covers bands up to 64 x 64 (this one is {band.br} x {band.bc})')
         self.band, self.ny, self.nx, self.kind, self.form = band, ny, nx, kind, form
         self.plan = Plan.get(ny, nx, band, self.device)
-        # the same images from fewer transforms for real single-channel masks (pack_real_fields), or None; SOCS
-        # models only, whose fields and weights stay fixed (an Abbe model's weights follow its source)
-        self.packed = pack_real_fields(self.pupils, self.weights, band) if kind == 'socs' else None
+        # the same images from fewer transforms for real single-channel masks (pack_real_fields), or None; it is
+        # dropped when the weights change (an Abbe model re-weighted for a new source runs its own fields)
+        self.packed = pack_real_fields(self.pupils, self.weights, band)
 
     @property
     def planes(self):

@@ -79,6 +79,7 @@ def set_source_weights(model: CoherentModel, values: torch.Tensor, index_image: 
     P = getattr(model, 'pol_states', 1)          # fields are [polarisation state][point][component]
     per = w.repeat_interleave(K // (P * v.numel())).repeat(P)
     model.weights.copy_(per.to(torch.float32)[None].expand(Z, K))
+    model.packed = None   # packed for the previous weights
 
 
 def optimize_source_mask(model: CoherentModel, values: torch.Tensor, index_image: float, target: torch.Tensor,
