@@ -53,6 +53,26 @@ def test_set_source_weights_matches_rebuilt_model():
     assert rel_err(m1.image(mask).cpu().numpy(), m2.image(mask).cpu().numpy()) < 1e-6
 
 
+def test_reweighting_drops_the_packed_fields():
+    """A centrosymmetric source's Abbe fields pack two real fields to a transform for real masks; re-weighting
+    the model for another source drops that packed set, and the images follow the new weights."""
+    from opticalimaging_b200.ilt import set_source_weights
+    from opticalimaging_b200 import workloads as W
+    rng = np.random.default_rng(11)
+    v = 0.2 + rng.random((7, 7))
+    v1 = (v + v[::-1, ::-1]) / 2                    # symmetric under s -> -s
+    v2 = 0.2 + rng.random((7, 7))
+    sr1, po, m1 = _small_abbe(v1)
+    sr2, _, m2 = _small_abbe(v2)
+    assert m1.packed is not None and m1.packed[0].shape[1] < m1.count
+    mask = torch.from_numpy(W.rect_mask(40, 48, 400.0, 480.0, 8, 40, 160, rng)).cuda()[None]
+    own = m1.image(mask.to(torch.complex64).unsqueeze(-1)).cpu().numpy()
+    assert rel_err(m1.image(mask).cpu().numpy(), own) < 1e-5
+    set_source_weights(m1, sr2.Calc_SourceSimple().Value, po.IndexImage)
+    assert m1.packed is None
+    assert rel_err(m1.image(mask).cpu().numpy(), m2.image(mask).cpu().numpy()) < 1e-6
+
+
 def test_source_mask_optimisation_lowers_the_loss():
     from opticalimaging_b200.ilt import ResistModel, optimize_source_mask
     from opticalimaging_b200 import workloads as W
