@@ -854,6 +854,7 @@ def run_engine(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16x3" if args.form == 'bf16x3' else "fp32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "batch_per_gpu": BATCH, "kernels": sk.count,
+                       "coherent_fields": int(sk.fields_for(N.FIELD_REAL_F32)[0].shape[1]),
                        "band": [sk.band.br, sk.band.bc], "form": args.form,
                        "coarse": [128, 128] if args.form == 'bf16x3' else [sk.plan.mr, sk.plan.mc],
                        "l2": "inputs larger than L2 (256 MB float32 masks + 256 MB images per step)",
