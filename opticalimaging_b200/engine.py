@@ -458,7 +458,7 @@ class CoherentModel:
     """
 
     def __init__(self, pupils: torch.Tensor, weights: torch.Tensor, band: Band, ny: int, nx: int, kind: str = 'socs',
-                 form: str | None = None):
+                 form: str | None = None, pack: bool = True):
         if pupils.dim() != 4 or pupils.shape[2:] != (band.br, band.bc):
             raise ValueError('pupils must be [Z, K, br, bc] on the band')
         if weights.shape != pupils.shape[:2]:
@@ -475,8 +475,9 @@ class CoherentModel:
         self.band, self.ny, self.nx, self.kind, self.form = band, ny, nx, kind, form
         self.plan = Plan.get(ny, nx, band, self.device)
         # the same images from fewer transforms for real single-channel masks (pack_real_fields), or None; it is
-        # dropped when the weights change (an Abbe model re-weighted for a new source runs its own fields)
-        self.packed = pack_real_fields(self.pupils, self.weights, band)
+        # dropped when the weights change (an Abbe model re-weighted for a new source runs its own fields).  A model
+        # built for one call (pack=False) skips it.
+        self.packed = pack_real_fields(self.pupils, self.weights, band) if pack else None
 
     @property
     def planes(self):

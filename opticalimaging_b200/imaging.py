@@ -266,7 +266,7 @@ def _image_data(intensity, scatter, projector):
 
 
 # ----------------------------------------------------------------------------------------------- Abbe
-def abbe_model(source, projector, numerics, period_y, period_x, ny, nx, focus=None) -> CoherentModel:
+def abbe_model(source, projector, numerics, period_y, period_x, ny, nx, focus=None, pack=True) -> CoherentModel:
     """Abbe pupils of every (focus plane, source point, field component) resident on the device
     (CalculateAerialImage.py:30-75): a CoherentModel whose image() is the Abbe image of a batch of masks."""
     vector = _mode(numerics)
@@ -309,7 +309,7 @@ def abbe_model(source, projector, numerics, period_y, period_x, ny, nx, focus=No
     else:
         pupils = torch.cat([p for p, _ in sets], dim=1)
         weights = torch.cat([w for _, w in sets], dim=1)
-    model = CoherentModel(pupils, weights, band, ny, nx, kind='abbe')
+    model = CoherentModel(pupils, weights, band, ny, nx, kind='abbe', pack=pack)
     model.pol_states = len(sets)
     return model
 
@@ -335,7 +335,7 @@ def abbe_intensity(source, scatter, projector, numerics, h=None):
     if sd.Value.numel() == 0:   # the reference divides 0 by a zero source weight
         _mode(numerics)
         return torch.full((len(zs), ny, nx), float('nan'), device=dev)
-    model = abbe_model(source, projector, numerics, scatter.Period_Y, scatter.Period_X, ny, nx)
+    model = abbe_model(source, projector, numerics, scatter.Period_Y, scatter.Period_X, ny, nx, pack=False)
     if model is None:
         return torch.zeros((len(zs), ny, nx), device=dev)
     return model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=nch)[0]
@@ -547,7 +547,11 @@ def CalculateAerialImage_SOCS(scatter, TCCMatrix_SOCS, source, projector):
     sk = _socs_kernels_of(TCCMatrix_SOCS, dev)
     hfull = _device_field(scatter, dev)
     h = _live_channels(hfull)
-    img = sk.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
+    if h.shape[2] == 1 and not bool(h.imag.any()):
+        # one real-valued channel (a thin mask, the usual ScatterField): the model's real-mask path
+        img = sk.image(h[..., 0].real.unsqueeze(0).contiguous(), kind=N.FIELD_REAL_F32)[0]
+    else:
+        img = sk.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
     pim = _pupil_image(scatter, projector, source, hfull, dev)
     rd = _result_device(scatter)
     img, pim = _to_host(img, rd), _to_host(pim, rd)
@@ -555,7 +559,7 @@ def CalculateAerialImage_SOCS(scatter, TCCMatrix_SOCS, source, projector):
     return img, pim
 
 
-def socs_model(source, projector, numerics, period_y, period_x, ny, nx, focus=None) -> CoherentModel:
+def socs_model(source, projector, numerics, period_y, period_x, ny, nx, focus=None, pack=True) -> CoherentModel:
     """SOCS kernels of every focus plane resident on the device: per plane TCC -> FP64 top-K eigenpairs ->
     kernels placed as the reference places them (CalculateAerialImage.py:112-119).  image() gives the Hopkins
     image of a batch of masks, all planes in one pass."""
@@ -569,7 +573,8 @@ def socs_model(source, projector, numerics, period_y, period_x, ny, nx, focus=No
                          device=sets[0].kernels.device)
     for i, s in enumerate(sets):
         pupils[i, :s.count] = s.kernels
-    return CoherentModel(pupils, torch.ones((len(zs), k), device=pupils.device), sets[0].band, ny, nx, 'socs')
+    return CoherentModel(pupils, torch.ones((len(zs), k), device=pupils.device), sets[0].band, ny, nx, 'socs',
+                         pack=pack)
 
 
 def hopkins_intensity(source, scatter, projector, numerics, h=None):
@@ -578,7 +583,7 @@ def hopkins_intensity(source, scatter, projector, numerics, h=None):
     if h is None:
         h = _field_on_device(scatter, dev)
     ny, nx = h.shape[0], h.shape[1]
-    model = socs_model(source, projector, numerics, scatter.Period_Y, scatter.Period_X, ny, nx)
+    model = socs_model(source, projector, numerics, scatter.Period_Y, scatter.Period_X, ny, nx, pack=False)
     return model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
 
 
