@@ -342,9 +342,11 @@ def test_eig_topk_small_and_edge_cases(oi):
 
 
 def test_dropin_large_host_field_through_pinned_staging(oi):
-    """A 1024 x 1024 x 3 complex64 host ScatterField (24 MiB, pageable) takes the pinned staging to the device;
-    the drop-in image equals the resident kernels' image of the same mask, and comes back as a host tensor."""
-    from opticalimaging_b200 import workloads as W
+    """A 1024 x 1024 x 3 complex64 host ScatterField (24 MiB, pageable) goes through the pinned staging.  As one real
+    channel it takes the real-mask path: the drop-in image is the resident kernels' image of the same mask, bit for
+    bit, and the pupil image comes from the real channel's band pass; with an imaginary part in another channel
+    the live channels take the complex path.  Images and pupil images come back as host tensors."""
+    from opticalimaging_b200 import _native as N, workloads as W
     from opticalimaging_b200.params import Scatter
     sr, po, nm = W.config3_optics(order=8)
     T, fg = oi.CalculateTCCMatrix(sr, [2048.0, 2048.0], po, 0.0, nm)
@@ -358,6 +360,26 @@ def test_dropin_large_host_field_through_pinned_staging(oi):
     assert img.device.type == 'cpu' and img.shape == (1024, 1024)
     sk = oi._SOCS_CACHE[K][1]
     want = sk.image(torch.from_numpy(mask).cuda()[None])[0].cpu().numpy()
-    # two FP32 paths (complex field through the DFT band pass, float mask through the FFT): rounding only (2.1e-6
-    # measured); a staging fault would show as O(1)
-    assert rel_err(img.numpy(), want) < 1e-5
+    # one real channel: the image is the real-mask path's
+    assert np.array_equal(img.numpy(), want)
+    # the pupil image from the real channel's FFT band pass against the complex field's DFT band pass
+    full = sc.ScatterField.cuda()
+    ref = oi._pupil_image(sc, po, sr, full, torch.device('cuda')).cpu().numpy()
+    assert pim.shape == ref.shape and pim.device.type == 'cpu'
+    np.testing.assert_array_equal(np.isnan(pim.numpy()), np.isnan(ref))
+    ok = ~np.isnan(ref)
+    assert rel_err(pim.numpy()[ok], ref[ok]) < 1e-5
+    assert not np.any(pim.numpy()[..., 1:][ok[..., 1:]])      # the zero channels stay exactly zero
+    # a field that is not one real channel (an imaginary part in channel 2): channels 0 and 2 in the complex path
+    f2 = sc.ScatterField.clone()
+    f2[:, :, 2] = 0.25j * f2[:, :, 0]
+    sc.ScatterField = f2
+    img2, pim2 = oi.CalculateAerialImage_SOCS(sc, K, sr, po)
+    h2 = f2.cuda()[:, :, [0, 2]].contiguous()
+    want2 = sk.image(h2[None], kind=N.FIELD_COMPLEX_C64, nch=2)[0].cpu().numpy()
+    assert np.array_equal(img2.numpy(), want2)
+    ref2 = oi._pupil_image(sc, po, sr, f2.cuda(), torch.device('cuda')).cpu().numpy()
+    ok2 = ~np.isnan(ref2)
+    np.testing.assert_array_equal(np.isnan(pim2.numpy()), ~ok2)
+    assert rel_err(pim2.numpy()[ok2], ref2[ok2]) < 1e-6
+    assert rel_err(img2.numpy(), 1.0625 * want) < 1e-5        # |m|^2 (1 + 1/16): the same mask, scaled intensity
