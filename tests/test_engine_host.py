@@ -203,3 +203,54 @@ def test_packing_sees_through_degenerate_mixtures():
     a = _coherent_sum_fp64(P, w, band, mask)
     b = _coherent_sum_fp64(Q.numpy().astype(np.complex128), wq.numpy(), band, mask)
     assert np.max(np.abs(a - b)) / np.max(a) < 1e-6
+
+
+def _field(f):
+    from opticalimaging_b200.params import Scatter
+    sc = Scatter()
+    sc.ScatterField = torch.from_numpy(f)
+    return sc
+
+
+def test_drop_in_field_classifies_channels():
+    """The drop-in's one reduction (run here on a small host field) finds the live channels and whether the field
+    is one real channel: -0 counts as zero, NaN as non-zero, an all-zero field keeps channel 0."""
+    dev = torch.device('cpu')
+    rng = np.random.default_rng(3)
+    m = (rng.random((12, 10)) > 0.5).astype(np.float32)
+    f = np.zeros((12, 10, 3), np.complex64)
+    f[:, :, 0] = m
+    d = I._DropInField(_field(f), dev)
+    assert d.live == [0] and d.real is not None
+    np.testing.assert_array_equal(d.real.numpy(), m)
+    assert d.live_complex().shape == (12, 10, 1)
+
+    g = f.copy()
+    g.imag[:, :, 0] = np.float32(-0.0)                    # negative zero imaginary parts: still one real channel
+    d = I._DropInField(_field(g), dev)
+    assert d.real is not None and d.live == [0]
+
+    g = f.copy()
+    g[3, 4, 2] = 0.5j                                     # a second, complex channel
+    d = I._DropInField(_field(g), dev)
+    assert d.real is None and d.live == [0, 2]
+    np.testing.assert_array_equal(d.live_complex().numpy(), g[:, :, [0, 2]])
+
+    g = f.copy()
+    g[0, 0, 1] = np.nan                                   # NaN is non-zero
+    d = I._DropInField(_field(g), dev)
+    assert d.real is None and d.live == [0, 1]
+
+    g = f.copy()
+    g[5, 5, 0] += 1e-30j                                  # one imaginary part makes channel 0 complex
+    d = I._DropInField(_field(g), dev)
+    assert d.real is None and d.live == [0]
+
+    d = I._DropInField(_field(np.zeros((12, 10, 3), np.complex64)), dev)
+    assert d.live == [0] and d.real is not None and not d.real.any()
+
+    d = I._DropInField(_field(np.zeros((12, 10, 3), np.complex64)[:, :, :2].copy()), dev)
+    assert d.nch == 2 and d.live == [0]
+    import pytest
+    with pytest.raises(ValueError):
+        I._DropInField(_field(np.zeros((12, 10), np.complex64)), dev)
