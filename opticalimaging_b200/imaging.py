@@ -138,6 +138,10 @@ class _DropInField:
             self.real = self._cplx[:, :, 0].real.contiguous()
         self.live = [c for c in range(self.nch) if nz[c][0] or nz[c][1]] or [0]
 
+    def carrier(self) -> torch.Tensor:
+        """What the imaging takes: the real channel (float32 [Ny, Nx]) when there is one, else live_complex()."""
+        return self.real if self.real is not None else self.live_complex()
+
     def live_complex(self) -> torch.Tensor:
         """The live channels as complex64 [Ny, Nx, L] on the device."""
         h = self._cplx if len(self.live) == self.nch else self._cplx[:, :, self.live]
@@ -374,12 +378,21 @@ def _pol_states(source, X, Y, vector, dev):
     return [torch.view_as_real(st.to(torch.complex128)).reshape(-1, 4).contiguous().to(dev) for st in states]
 
 
+def _field_image(model, h):
+    """model.image of one field: h float32 [Ny, Nx] (one real channel, the real-mask band pass) or complex64
+    [Ny, Nx, C]."""
+    if h.dim() == 2:
+        return model.image(h.unsqueeze(0), kind=N.FIELD_REAL_F32)[0]
+    return model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
+
+
 def abbe_intensity(source, scatter, projector, numerics, h=None):
-    """Abbe image [nFocus, Ny, Nx] float32 on the device (CalculateAerialImage.py:18-92)."""
+    """Abbe image [nFocus, Ny, Nx] float32 on the device (CalculateAerialImage.py:18-92).  h: the field on the
+    device, complex64 [Ny, Nx, C] or, for one real channel, float32 [Ny, Nx]."""
     dev = require_cuda()
     if h is None:
         h = _field_on_device(scatter, dev)
-    ny, nx, nch = h.shape
+    ny, nx = h.shape[0], h.shape[1]
     zs = _focus_list(projector)
     sd = source.Calc_SourceSimple()
     if sd.Value.numel() == 0:   # the reference divides 0 by a zero source weight
@@ -388,14 +401,14 @@ def abbe_intensity(source, scatter, projector, numerics, h=None):
     model = abbe_model(source, projector, numerics, scatter.Period_Y, scatter.Period_X, ny, nx, pack=False)
     if model is None:
         return torch.zeros((len(zs), ny, nx), device=dev)
-    return model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=nch)[0]
+    return _field_image(model, h)
 
 
 def CalculateAbbeImage(source, scatter, projector, numerics):
     """Abbe aerial image -> (ImageData, pupilImage) (CalculateAerialImage.py:18-103)."""
     dev = require_cuda()
     fld = _DropInField(scatter, dev)
-    inten = abbe_intensity(source, scatter, projector, numerics, h=fld.live_complex())
+    inten = abbe_intensity(source, scatter, projector, numerics, h=fld.carrier())
     pim = fld.pupil_image(scatter, projector, source, dev)
     rd = _result_device(scatter)
     inten, pim = _to_host(inten, rd), _to_host(pim, rd)
@@ -628,20 +641,21 @@ def socs_model(source, projector, numerics, period_y, period_x, ny, nx, focus=No
 
 
 def hopkins_intensity(source, scatter, projector, numerics, h=None):
-    """Hopkins image [nFocus, Ny, Nx] on the device: per plane TCC -> top-K kernels -> SOCS image."""
+    """Hopkins image [nFocus, Ny, Nx] on the device: per plane TCC -> top-K kernels -> SOCS image.  h as for
+    abbe_intensity."""
     dev = require_cuda()
     if h is None:
         h = _field_on_device(scatter, dev)
     ny, nx = h.shape[0], h.shape[1]
     model = socs_model(source, projector, numerics, scatter.Period_Y, scatter.Period_X, ny, nx, pack=False)
-    return model.image(h.unsqueeze(0), kind=N.FIELD_COMPLEX_C64, nch=h.shape[2])[0]
+    return _field_image(model, h)
 
 
 def CalculateHopkinsImage(source, scatter, projector, numerics):
     """Hopkins aerial image -> (ImageData, pupilImage) (CalculateAerialImage.py:105-130)."""
     dev = require_cuda()
     fld = _DropInField(scatter, dev)
-    inten = hopkins_intensity(source, scatter, projector, numerics, h=fld.live_complex())
+    inten = hopkins_intensity(source, scatter, projector, numerics, h=fld.carrier())
     pim = fld.pupil_image(scatter, projector, source, dev)
     rd = _result_device(scatter)
     inten, pim = _to_host(inten, rd), _to_host(pim, rd)
